@@ -1,0 +1,201 @@
+/*
+ * rla_b200.h -- C ABI of the B200 (sm_100a) sketch / randomized-rangefinder library.
+ *
+ * This is the drop-in boundary for RandLinearAlgebra.jl v0.2.4.  The reference's own
+ * extension mechanism is Julia multiple dispatch: a package adds new `Compressor` /
+ * `CompressorRecipe` and `RangeApproximator` / `RangeApproximatorRecipe` subtypes and
+ * methods for `complete_compressor`, `update_compressor!`, `mul!`, `*` and
+ * `complete_approximator` / `rapproximate!`.  Each entry point below is what such a
+ * method reaches through `ccall`; the citations name the reference method it replaces
+ * (paths relative to the RandLinearAlgebra.jl source tree).
+ *
+ * Conventions
+ *  - Every function returns an int status (RLA_OK = 0).  After a failure,
+ *    rla_ctx_last_error() holds a message; for dimension and argument errors it is the
+ *    same text the reference throws (src/helpers/mul_dim_checks.jl:49-60, constructors).
+ *  - All matrix arguments are DEVICE pointers owned by the caller.  Matrices are
+ *    column-major with an explicit leading dimension (Julia layout).  A `trans_*` flag of
+ *    1 says the logical operand is the transpose of the stored column-major matrix (the
+ *    layout of Julia's `transpose(X)` / `X'` wrapper of a real matrix), so the reference's
+ *    adjoint routes (src/Compressors.jl:363-410) need no copies on the caller's side.
+ *  - Sketch state (random draws and the derived device tables) is owned by the opaque
+ *    rla_sketch and freed by rla_sketch_destroy.
+ *  - Work is issued on the context's stream.  rla_sketch_mul, rla_rangefinder and
+ *    rla_randsvd return after the result is complete (Julia `mul!` semantics).
+ *  - beta == 0 means C is not read (BLAS convention), so C may hold garbage or NaN.
+ *  - Real Float32 (RLA_F32) and Float64 (RLA_F64) element types.
+ */
+#ifndef RLA_B200_H
+#define RLA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------------------- */
+#define RLA_OK 0
+#define RLA_E_DIM 1          /* Julia DimensionMismatch */
+#define RLA_E_ARG 2          /* Julia ArgumentError */
+#define RLA_E_DOMAIN 3       /* Julia DomainError */
+#define RLA_E_OOM 4          /* device allocation failed */
+#define RLA_E_CUDA 5         /* CUDA runtime error */
+#define RLA_E_TIMEOUT 6      /* a bounded device-side wait ran out */
+#define RLA_E_NUMERIC 7      /* Cholesky breakdown not repaired by the shifted fallback */
+#define RLA_E_UNSUPPORTED 8  /* combination not provided by this build */
+
+/* ---- enumerations ---------------------------------------------------------------- */
+#define RLA_F32 0
+#define RLA_F64 1
+
+#define RLA_LEFT 0           /* Left() cardinality (src/Compressors.jl:31) */
+#define RLA_RIGHT 1          /* Right() cardinality (src/Compressors.jl:38) */
+
+#define RLA_SPARSE_SIGN 0    /* src/Compressors/sparse_sign.jl */
+#define RLA_COUNT_SKETCH 1   /* src/Compressors/count_sketch.jl */
+#define RLA_SRHT 2           /* src/Compressors/srht.jl */
+#define RLA_FJLT 3           /* src/Compressors/fjlt.jl */
+#define RLA_GAUSSIAN 4       /* src/Compressors/gaussian.jl */
+
+#define RLA_SIDE_LEFT 0      /* C = alpha*op(S)*A + beta*C */
+#define RLA_SIDE_RIGHT 1     /* C = alpha*A*op(S) + beta*C */
+
+#define RLA_PREC_NATIVE 0    /* GEMMs in the element type on CUDA cores */
+#define RLA_PREC_SPLIT_BF16 1 /* GEMMs as split-BF16 (hi+lo) tcgen05 products, FP32 accumulate */
+
+typedef struct rla_ctx rla_ctx;
+typedef struct rla_sketch rla_sketch;
+
+/* ---- library / context ----------------------------------------------------------- */
+int rla_version(void);
+const char *rla_status_string(int status);
+
+/* Create a context on `device`.  `stream` is a cudaStream_t to borrow, or NULL for a
+ * stream owned by the context. */
+int rla_ctx_create(int device, void *stream, rla_ctx **out);
+int rla_ctx_destroy(rla_ctx *ctx);
+const char *rla_ctx_last_error(const rla_ctx *ctx);
+int rla_ctx_synchronize(rla_ctx *ctx);
+/* Issue the context's work on `stream` from now on (a cudaStream_t; NULL selects the
+ * legacy default stream).  A stream the context created itself is released. */
+int rla_ctx_set_stream(rla_ctx *ctx, void *stream);
+/* Scratch high-water mark (bytes) the context holds for partial sums and transposes. */
+int rla_ctx_scratch_bytes(const rla_ctx *ctx, int64_t *bytes);
+
+/* ---- compressors ----------------------------------------------------------------- */
+typedef struct rla_sketch_params {
+    int kind;                /* RLA_SPARSE_SIGN ... RLA_GAUSSIAN */
+    int card;                /* RLA_LEFT / RLA_RIGHT */
+    int dtype;               /* RLA_F32 / RLA_F64: the compressor's `type` field */
+    int64_t compression_dim; /* s */
+    int64_t long_dim;        /* size(A,1) for Left, size(A,2) for Right */
+    int64_t nnz;             /* SparseSign nonzeros per long index */
+    int64_t block_size;      /* SRHT/FJLT padding block (kept for parity; kernels fuse it away) */
+    double sparsity;         /* FJLT; 0 selects 0.25*log(L)^2/L (fjlt.jl:181) */
+    uint64_t seed;
+} rla_sketch_params;
+
+typedef struct rla_sketch_info {
+    int kind, card, dtype;
+    int64_t n_rows, n_cols;  /* size(S) (src/Compressors.jl:310-316) */
+    int64_t compression_dim, long_dim, nnz, block_size;
+    int64_t padded;          /* SRHT/FJLT padded size N */
+    int64_t k_nnz;           /* FJLT: stored nonzeros of K */
+    double sparsity;         /* FJLT */
+    double scale;            /* SRHT/FJLT `scale`, SparseSign 1/sqrt(nnz), Gaussian 1/sqrt(s) */
+    uint64_t draw_count;     /* number of draws made (1 after create, +1 per update) */
+} rla_sketch_info;
+
+/* complete_compressor(::SparseSign|CountSketch|SRHT|FJLT|Gaussian, A)
+ * (sparse_sign.jl:297-305, count_sketch.jl:149-156, srht.jl:193-201, fjlt.jl:228-240,
+ * gaussian.jl:126-133; constructor checks sparse_sign.jl:71-87, count_sketch.jl:65-80,
+ * srht.jl:67-77, fjlt.jl (FJLT inner constructor), gaussian.jl:54-60).
+ * Draws are made on the device from `seed`. */
+int rla_sketch_create(rla_ctx *ctx, const rla_sketch_params *params, rla_sketch **out);
+
+/* update_compressor!(S) (sparse_sign.jl:307-336, count_sketch.jl:158-163,
+ * srht.jl:205-217, fjlt.jl:242-254, gaussian.jl:136-141): fresh draws in place. */
+int rla_sketch_update(rla_ctx *ctx, rla_sketch *sk);
+int rla_sketch_destroy(rla_sketch *sk);
+int rla_sketch_get_info(const rla_sketch *sk, rla_sketch_info *out);
+
+/* Parity mode: copy the draws to HOST buffers in the layout of the reference's recipe
+ * fields (0-based indices; a caller filling a Julia struct adds 1):
+ *   SparseSign   idx = op.rowval (Left) / op.parent.rowval (Right)  [long_dim*nnz]
+ *                vals = nzval [long_dim*nnz]
+ *   CountSketch  idx = mat.rowval [long_dim], vals = mat.nzval [long_dim]
+ *   SRHT         idx = op [compression_dim], signs = signs [padded] (1 = +1)
+ *   FJLT         kptr = op.colptr, idx = op.rowval, vals = op.nzval, signs [padded]
+ *   Gaussian     vals = op, column-major n_rows x n_cols
+ * Pointers a kind does not use may be NULL. */
+int rla_sketch_get_draws(rla_ctx *ctx, const rla_sketch *sk, int64_t *idx, void *vals,
+                         uint8_t *signs, int64_t *kptr);
+/* Load externally supplied draws (same layouts) and rebuild the derived device tables.
+ * For FJLT `k_nnz` is the number of stored entries of op; otherwise it is ignored. */
+int rla_sketch_set_draws(rla_ctx *ctx, rla_sketch *sk, const int64_t *idx, const void *vals,
+                         const uint8_t *signs, const int64_t *kptr, int64_t k_nnz);
+
+/* mul!(C, S, A, alpha, beta) / mul!(C, A, S, alpha, beta) and the adjoint forms
+ * (src/Compressors.jl:331-384, sparse_sign.jl:339-361, count_sketch.jl:166-213,
+ * srht.jl:220-504, fjlt.jl:257-535, gaussian.jl:145-170).
+ *   side == RLA_SIDE_LEFT :  C = alpha*op(S)*A + beta*C
+ *   side == RLA_SIDE_RIGHT:  C = alpha*A*op(S) + beta*C
+ *   op(S) = S when trans_s == 0, S' when trans_s == 1 (CompressorAdjoint).
+ * A is the logical (a_rows x a_cols) operand, C the logical (c_rows x c_cols) result;
+ * see the trans_* convention above.  Dimension errors carry the reference's messages
+ * (left_mul_dimcheck / right_mul_dimcheck). */
+int rla_sketch_mul(rla_ctx *ctx, const rla_sketch *sk, int side, int trans_s,
+                   int64_t c_rows, int64_t c_cols, void *C, int64_t ldc, int trans_c,
+                   int64_t a_rows, int64_t a_cols, const void *A, int64_t lda, int trans_a,
+                   double alpha, double beta);
+
+/* As rla_sketch_mul, but returns once the work is queued on the context's stream; the
+ * result is valid after rla_ctx_synchronize (or later stream-ordered work).  No
+ * reference counterpart: it lets a caller overlap several applies. */
+int rla_sketch_mul_async(rla_ctx *ctx, const rla_sketch *sk, int side, int trans_s,
+                         int64_t c_rows, int64_t c_cols, void *C, int64_t ldc, int trans_c,
+                         int64_t a_rows, int64_t a_cols, const void *A, int64_t lda, int trans_a,
+                         double alpha, double beta);
+
+/* ---- range approximators --------------------------------------------------------- */
+typedef struct rla_range_params {
+    int64_t power_its;       /* q (randsvd.jl:339, rangefinder.jl) */
+    int orthogonalize;       /* rand_ortho_it (1) or rand_power_it (0) (power_its.jl) */
+    int precision;           /* RLA_PREC_NATIVE or RLA_PREC_SPLIT_BF16 */
+} rla_range_params;
+
+/* rapproximate!(::RangeFinderRecipe, A) (rangefinder.jl:134-143 with
+ * power_its.jl:15-80): Q (m x l, element type of A) spans range(A*Omega) after the
+ * power iterations.  `omega` is a Right-cardinality compressor with long_dim == n.
+ * Orthogonalisation is CholeskyQR2 with an FP64 Gram matrix (shifted CholeskyQR3 on
+ * breakdown); Q's columns follow the R-diagonal-positive sign convention. */
+int rla_rangefinder(rla_ctx *ctx, const rla_sketch *omega, int dtype, int64_t m, int64_t n,
+                    const void *A, int64_t lda, const rla_range_params *params,
+                    void *Q, int64_t ldq);
+
+/* rapproximate!(::RandSVDRecipe, A) (randsvd.jl:174-189): Q as above, B = Q'A, the SVD
+ * of B in FP64, U = Q*W.  U (m x l) and V (n x l) are written in `out_dtype`
+ * (RLA_F64 matches the reference, which promotes the factors to Float64); S (l values,
+ * descending) is always Float64. */
+int rla_randsvd(rla_ctx *ctx, const rla_sketch *omega, int dtype, int64_t m, int64_t n,
+                const void *A, int64_t lda, const rla_range_params *params, int out_dtype,
+                void *U, int64_t ldu, double *S, void *V, int64_t ldv);
+
+/* mul! for completed approximators: RandSVD (randsvd.jl:198-293) with R = U*diag(S)*V'
+ * (U m x k, V n x k, S k values in FP64), and RangeFinder (rangefinder.jl:151-191) with
+ * S = V = NULL and R = U (m x k, n == k).  trans_r selects R' (ApproximatorAdjoint,
+ * src/Approximators.jl:363-384).  Factors are `factor_dtype`, A and C are `dtype`;
+ * A, C, side and trans flags as in rla_sketch_mul.  Device pointers; synchronous. */
+int rla_lowrank_mul(rla_ctx *ctx, int factor_dtype, int dtype, int side, int trans_r,
+                    int64_t m, int64_t n, int64_t k, const void *U, int64_t ldu, const double *S,
+                    const void *V, int64_t ldv,
+                    int64_t c_rows, int64_t c_cols, void *C, int64_t ldc, int trans_c,
+                    int64_t a_rows, int64_t a_cols, const void *A, int64_t lda, int trans_a,
+                    double alpha, double beta);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RLA_B200_H */

@@ -1,0 +1,17 @@
+"""B200-native RandLinearAlgebra.jl sketch / RandSVD path: the host-side mirror of the
+reference's Compressor and RangeApproximator API over librla_b200.so.
+
+The directory name is not a Python identifier; load it with
+``__graft_entry__.load_package()`` (module name ``randlinearalgebra_b200``).
+"""
+from .errors import ArgumentError, DimensionMismatch, DomainError, RLAError
+from .compressors import (Cardinality, Left, Right, Undef, Compressor, CompressorRecipe, CompressorAdjoint,
+                          SparseSign, SparseSignRecipe, CountSketch, CountSketchRecipe, SRHT, SRHTRecipe, FJLT,
+                          FJLTRecipe, Gaussian, GaussianRecipe, complete_compressor, update_compressor_, mul_,
+                          adjoint, transpose, size, seed_)
+from .approximators import (Approximator, RangeApproximator, ApproximatorRecipe, RangeApproximatorRecipe,
+                            ApproximatorAdjoint, RangeFinder, RangeFinderRecipe, RandSVD, RandSVDRecipe,
+                            complete_approximator, rapproximate_, rapproximate)
+from ._lib import RLA_PREC_NATIVE, RLA_PREC_SPLIT_BF16, lib, Context
+
+__version__ = "0.1.0"

@@ -1,0 +1,158 @@
+// rla_ctx.cu -- context, error reporting and workspace management.
+#include <stdarg.h>
+
+#include "rla_internal.cuh"
+
+namespace rla {
+
+int set_error(rla_ctx *ctx, int code, const char *fmt, ...) {
+    if (ctx) {
+        char buf[1024];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof(buf), fmt, ap);
+        va_end(ap);
+        ctx->last_error = buf;
+    }
+    return code;
+}
+
+int check_launch(rla_ctx *ctx, const char *what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return set_error(ctx, RLA_E_CUDA, "%s launch failed: %s", what, cudaGetErrorString(e));
+    return RLA_OK;
+}
+
+int scratch_get(rla_ctx *ctx, size_t bytes, void **out) {
+    bytes = (bytes + 255) & ~size_t(255);
+    if (bytes == 0) bytes = 256;
+    if (ctx->scratch.bytes < bytes) {
+        // Work already queued may still use the old buffer.
+        RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+        if (ctx->scratch.ptr) RLA_CUDA_TRY(ctx, cudaFree(ctx->scratch.ptr));
+        ctx->scratch.ptr = nullptr;
+        ctx->scratch.bytes = 0;
+        RLA_CUDA_TRY(ctx, cudaMalloc(&ctx->scratch.ptr, bytes));
+        ctx->scratch.bytes = bytes;
+        if ((int64_t)bytes > ctx->scratch_high_water) ctx->scratch_high_water = (int64_t)bytes;
+    }
+    *out = ctx->scratch.ptr;
+    return RLA_OK;
+}
+
+int counters_get(rla_ctx *ctx, size_t n, int **out) {
+    size_t bytes = ((n * sizeof(int)) + 255) & ~size_t(255);
+    if (bytes == 0) bytes = 256;
+    if (ctx->counters.bytes < bytes) {
+        RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+        if (ctx->counters.ptr) RLA_CUDA_TRY(ctx, cudaFree(ctx->counters.ptr));
+        ctx->counters.ptr = nullptr;
+        ctx->counters.bytes = 0;
+        RLA_CUDA_TRY(ctx, cudaMalloc(&ctx->counters.ptr, bytes));
+        RLA_CUDA_TRY(ctx, cudaMemsetAsync(ctx->counters.ptr, 0, bytes, ctx->stream));
+        ctx->counters.bytes = bytes;
+    }
+    *out = (int *)ctx->counters.ptr;
+    return RLA_OK;
+}
+
+}  // namespace rla
+
+using namespace rla;
+
+extern "C" {
+
+int rla_version(void) { return 1; }
+
+const char *rla_status_string(int status) {
+    switch (status) {
+        case RLA_OK: return "ok";
+        case RLA_E_DIM: return "DimensionMismatch";
+        case RLA_E_ARG: return "ArgumentError";
+        case RLA_E_DOMAIN: return "DomainError";
+        case RLA_E_OOM: return "out of device memory";
+        case RLA_E_CUDA: return "CUDA error";
+        case RLA_E_TIMEOUT: return "device wait timed out";
+        case RLA_E_NUMERIC: return "numerical breakdown";
+        case RLA_E_UNSUPPORTED: return "unsupported";
+        default: return "unknown status";
+    }
+}
+
+int rla_ctx_create(int device, void *stream, rla_ctx **out) {
+    if (!out) return RLA_E_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) return RLA_E_CUDA;
+    if (device < 0 || device >= ndev) return RLA_E_ARG;
+    rla_ctx *ctx = new rla_ctx();
+    ctx->device = device;
+    if (cudaSetDevice(device) != cudaSuccess) {
+        delete ctx;
+        return RLA_E_CUDA;
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) {
+        delete ctx;
+        return RLA_E_CUDA;
+    }
+    if (prop.major < 10) {
+        delete ctx;
+        return RLA_E_UNSUPPORTED;  // sm_100a kernels only
+    }
+    ctx->sm_count = prop.multiProcessorCount;
+    ctx->smem_optin = (int)prop.sharedMemPerBlockOptin;
+    if (stream) {
+        ctx->stream = (cudaStream_t)stream;
+        ctx->owns_stream = false;
+    } else {
+        if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            delete ctx;
+            return RLA_E_CUDA;
+        }
+        ctx->owns_stream = true;
+    }
+    *out = ctx;
+    return RLA_OK;
+}
+
+int rla_ctx_destroy(rla_ctx *ctx) {
+    if (!ctx) return RLA_OK;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    if (ctx->scratch.ptr) cudaFree(ctx->scratch.ptr);
+    if (ctx->counters.ptr) cudaFree(ctx->counters.ptr);
+    if (ctx->owns_stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return RLA_OK;
+}
+
+const char *rla_ctx_last_error(const rla_ctx *ctx) { return ctx ? ctx->last_error.c_str() : ""; }
+
+int rla_ctx_synchronize(rla_ctx *ctx) {
+    if (!ctx) return RLA_E_ARG;
+    RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return RLA_OK;
+}
+
+int rla_ctx_set_stream(rla_ctx *ctx, void *stream) {
+    if (!ctx) return RLA_E_ARG;
+    if ((cudaStream_t)stream == ctx->stream) return RLA_OK;
+    if (ctx->owns_stream) {
+        RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+        RLA_CUDA_TRY(ctx, cudaStreamDestroy(ctx->stream));
+        ctx->owns_stream = false;
+    }
+    ctx->stream = (cudaStream_t)stream;  // NULL selects the legacy default stream
+    return RLA_OK;
+}
+
+int rla_ctx_scratch_bytes(const rla_ctx *ctx, int64_t *bytes) {
+    if (!ctx || !bytes) return RLA_E_ARG;
+    *bytes = ctx->scratch_high_water;
+    return RLA_OK;
+}
+
+}  // extern "C"

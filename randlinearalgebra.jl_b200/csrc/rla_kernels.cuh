@@ -1,0 +1,55 @@
+// rla_kernels.cuh -- internal launcher declarations shared by the translation units.
+#pragma once
+
+#include "rla_internal.cuh"
+
+namespace rla {
+
+// mul! without the final stream synchronisation (rla_api.cu).
+int sketch_mul_impl(rla_ctx *ctx, const rla_sketch *sk, int side, int trans_s, int64_t c_rows, int64_t c_cols,
+                    void *C, int64_t ldc, int trans_c, int64_t a_rows, int64_t a_cols, const void *A, int64_t lda,
+                    int trans_a, double alpha, double beta);
+
+// SparseSign / CountSketch (rla_sparse.cu).  Vectors of the input X: element (k, v) at
+// X[k*x_es + v*x_vs]; the output likewise.  Compress maps length-L vectors to length s,
+// expand maps length-s vectors to length L.
+template <class T>
+int sparse_compress(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_t x_es, int64_t x_vs, int64_t nv, T *Y,
+                    int64_t y_es, int64_t y_vs, double alpha, double beta);
+template <class T>
+int sparse_expand(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_t x_es, int64_t x_vs, int64_t nv, T *Y,
+                  int64_t y_es, int64_t y_vs, double alpha, double beta);
+
+// SRHT / FJLT (rla_wht.cu)
+template <class T>
+int srht_compress(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_t x_es, int64_t x_vs, int64_t nv, T *Y,
+                  int64_t y_es, int64_t y_vs, double alpha, double beta);
+template <class T>
+int srht_expand(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_t x_es, int64_t x_vs, int64_t nv, T *Y,
+                int64_t y_es, int64_t y_vs, double alpha, double beta);
+template <class T>
+int fjlt_compress(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_t x_es, int64_t x_vs, int64_t nv, T *Y,
+                  int64_t y_es, int64_t y_vs, double alpha, double beta);
+template <class T>
+int fjlt_expand(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_t x_es, int64_t x_vs, int64_t nv, T *Y,
+                int64_t y_es, int64_t y_vs, double alpha, double beta);
+
+// CUDA-core GEMM (rla_gemm.cu): C = alpha*op(A)*op(B) + beta*C, column-major.
+template <class TA, class TB, class TC, class TAcc>
+int gemm(rla_ctx *ctx, int64_t M, int64_t N, int64_t K, const TA *A, int64_t lda, int ta, const TB *B, int64_t ldb,
+         int tb, TC *C, int64_t ldc, double alpha, double beta);
+
+// Small dense FP64 kernels (rla_linalg.cu)
+// In place: G (l x l, ld l) -> upper Cholesky factor R (lower part zeroed).  `shift` is
+// added to the diagonal first.  *breakdown (device int) is set to 1 when a pivot is not
+// positive.
+int cholesky_upper(rla_ctx *ctx, double *G, int64_t l, double shift, int *breakdown);
+// Rinv = R^{-1} for upper-triangular R (l x l, ld l).
+int tri_inv_upper(rla_ctx *ctx, const double *R, int64_t l, double *Rinv);
+// One-sided Jacobi on X (l x l, ld l) with accumulated rotations J (initialised to I):
+// on return the columns of X are orthogonal, sigma[i] = ||X(:, i)||, columns sorted by
+// descending sigma, X(:, i) normalised, J permuted alongside.  `work` holds at least
+// 2*l*l + 2*l doubles.
+int jacobi_svd(rla_ctx *ctx, double *X, double *J, double *sigma, int64_t l, double *work);
+
+}  // namespace rla

@@ -1,0 +1,301 @@
+// rla_range.cu -- rapproximate! for RangeFinder and RandSVD.
+//
+// rand_power_it / rand_ortho_it (power_its.jl:15-80) with the products on the GPU and
+// every `Array(qr!(Y).Q)` replaced by CholeskyQR2:
+//   G = Y'Y (FP64 accumulate), D = diag(G)^-1/2, R = chol(D G D), Q = Y D R^-1, twice;
+// shifted CholeskyQR3 (Fukaya et al., SIAM J. Sci. Comput. 2020) when a Cholesky pivot
+// breaks down.  The column signs of Q are then set to what LAPACK's Householder QR of Y
+// returns: for orthonormal Q, Householder QR yields R = diag(+-1), and those signs follow
+// from an LU elimination of the top l x l block (Ballard et al., "Reconstructing
+// Householder vectors from tall-skinny QR", 2015), so Q matches qr!(Y).Q column by column.
+//
+// RandSVD (randsvd.jl:174-189): Bt = A'Q (n x l, FP64), Bt = Qb Rb (CholeskyQR2 in FP64),
+// one-sided Jacobi on Rb' gives Rb' J = W Sigma, so B = Q'A = W Sigma (Qb J)' and
+// U = Q W, V = Qb J, S = Sigma.
+#include <math.h>
+
+#include "rla_internal.cuh"
+#include "rla_kernels.cuh"
+
+namespace rla {
+
+// dscale[i] = 1/sqrt(G_ii)
+__global__ void diag_rsqrt_kernel(const double *G, int64_t l, double *dscale) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= l) return;
+    const double g = G[i + i * l];
+    dscale[i] = g > 0 ? rsqrt(g) : 1.0;
+}
+
+// G <- D G D
+__global__ void sym_scale_kernel(double *G, int64_t l, const double *dscale) {
+    const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (idx >= l * l) return;
+    G[idx] *= dscale[idx % l] * dscale[idx / l];
+}
+
+static int equilibrate(rla_ctx *ctx, double *G, int64_t l, double *dscale) {
+    diag_rsqrt_kernel<<<ceil_div_i(l, 256), 256, 0, ctx->stream>>>(G, l, dscale);
+    sym_scale_kernel<<<ceil_div_i(l * l, 256), 256, 0, ctx->stream>>>(G, l, dscale);
+    return check_launch(ctx, "equilibrate");
+}
+
+// Rinv <- D * Rinv (row scaling)
+__global__ void row_scale_kernel(double *M, int64_t l, const double *d) {
+    const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (idx >= l * l) return;
+    M[idx] *= d[idx % l];
+}
+
+__global__ void copy_diag_kernel(const double *G, int64_t l, double *out) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < l) out[i] = G[i + i * l];
+}
+
+// Householder column signs of orthonormal Q (m x l, ld ldq) from its top block.
+template <class T>
+__global__ void __launch_bounds__(1024) house_signs_kernel(T *Q, int64_t m, int64_t l, int64_t ldq, double *W) {
+    __shared__ double piv_s;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int64_t idx = tid; idx < l * l; idx += nt) W[idx] = (double)Q[(idx % l) + (idx / l) * ldq];
+    __syncthreads();
+    double *S = W + l * l;
+    for (int64_t k = 0; k < l; ++k) {
+        if (tid == 0) {
+            const double piv = W[k + k * l];
+            const double sk = (k == m - 1) ? (piv >= 0 ? 1.0 : -1.0) : (piv >= 0 ? -1.0 : 1.0);
+            S[k] = sk;
+            W[k + k * l] = piv - sk;
+            piv_s = W[k + k * l];
+        }
+        __syncthreads();
+        for (int64_t i = k + 1 + tid; i < l; i += nt) W[i + k * l] /= piv_s;
+        __syncthreads();
+        const int64_t n = l - k - 1;
+        for (int64_t idx = tid; idx < n * n; idx += nt) {
+            const int64_t i = k + 1 + idx % n, j = k + 1 + idx / n;
+            W[i + j * l] -= W[i + k * l] * W[k + j * l];
+        }
+        __syncthreads();
+    }
+    for (int64_t idx = tid; idx < m * l; idx += nt) {
+        const int64_t r = idx % m, c = idx / m;
+        if (S[c] < 0) Q[r + c * ldq] = -Q[r + c * ldq];
+    }
+}
+
+template <class T>
+__global__ void transpose_to_kernel(const T *X, int64_t rows, int64_t cols, int64_t ldx, T *Y, int64_t ldy) {
+    // Y (cols x rows) = X'
+    const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (idx >= rows * cols) return;
+    const int64_t r = idx % rows, c = idx / rows;
+    Y[c + r * ldy] = X[r + c * ldx];
+}
+
+template <class TI, class TO>
+__global__ void convert_kernel(const TI *X, int64_t rows, int64_t cols, int64_t ldx, TO *Y, int64_t ldy) {
+    const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (idx >= rows * cols) return;
+    const int64_t r = idx % rows, c = idx / rows;
+    Y[r + c * ldy] = (TO)X[r + c * ldx];
+}
+
+struct OrthWork {
+    double *G, *Rinv, *dscale, *diag, *hw;
+    int *flag;
+    void *tmp;  // rows x l of T
+};
+
+// In-place orthonormalisation of Y (rows x l, ld ldy); Q columns get Householder signs.
+template <class T>
+static int orth(rla_ctx *ctx, T *Y, int64_t rows, int64_t l, int64_t ldy, OrthWork &w) {
+    if (l > rows)
+        return set_error(ctx, RLA_E_UNSUPPORTED, "compression dimension %lld exceeds the %lld rows being orthogonalised",
+                         (long long)l, (long long)rows);
+    T *tmp = (T *)w.tmp;
+    int passes = 2;
+    bool shifted_done = false;
+    for (int pass = 0; pass < passes; ++pass) {
+        RLA_TRY((gemm<T, T, double, double>(ctx, l, l, rows, Y, ldy, 1, Y, ldy, 0, w.G, l, 1.0, 0.0)));
+        double shift = 0.0;
+        RLA_TRY(equilibrate(ctx, w.G, l, w.dscale));
+        RLA_TRY(cholesky_upper(ctx, w.G, l, shift, w.flag));
+        int bad = 0;
+        RLA_CUDA_TRY(ctx, cudaMemcpyAsync(&bad, w.flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+        if (bad) {
+            if (shifted_done) return set_error(ctx, RLA_E_NUMERIC, "CholeskyQR breakdown persists after the shift");
+            // Shifted CholeskyQR: on the equilibrated Gram matrix (unit diagonal, so
+            // ||Y D||_F^2 = l) the shift is 11 (rows*l + l(l+1)) u ||Y D||_2^2 <= ... * l.
+            RLA_TRY((gemm<T, T, double, double>(ctx, l, l, rows, Y, ldy, 1, Y, ldy, 0, w.G, l, 1.0, 0.0)));
+            RLA_TRY(equilibrate(ctx, w.G, l, w.dscale));
+            const double u = sizeof(T) == 4 ? 5.96e-8 : 1.11e-16;
+            shift = 11.0 * ((double)rows * l + (double)l * (l + 1)) * u * (double)l;
+            RLA_TRY(cholesky_upper(ctx, w.G, l, shift, w.flag));
+            RLA_CUDA_TRY(ctx, cudaMemcpyAsync(&bad, w.flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+            RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+            if (bad) return set_error(ctx, RLA_E_NUMERIC, "shifted CholeskyQR broke down (rank-deficient block)");
+            shifted_done = true;
+            passes = pass + 3;  // shifted pass followed by two plain passes
+        }
+        RLA_TRY(tri_inv_upper(ctx, w.G, l, w.Rinv));
+        row_scale_kernel<<<ceil_div_i(l * l, 256), 256, 0, ctx->stream>>>(w.Rinv, l, w.dscale);
+        RLA_TRY(check_launch(ctx, "row_scale"));
+        RLA_TRY((gemm<T, double, T, double>(ctx, rows, l, l, Y, ldy, 0, w.Rinv, l, 0, tmp, rows, 1.0, 0.0)));
+        convert_kernel<T, T><<<ceil_div_i(rows * l, 256), 256, 0, ctx->stream>>>(tmp, rows, l, rows, Y, ldy);
+        RLA_TRY(check_launch(ctx, "copy_back"));
+    }
+    house_signs_kernel<T><<<1, 1024, 0, ctx->stream>>>(Y, rows, l, ldy, w.hw);
+    return check_launch(ctx, "house_signs");
+}
+
+template <class T>
+static int alloc_orth(rla_ctx *ctx, OrthWork &w, int64_t rows, int64_t l, std::vector<void *> &owned) {
+    auto get = [&](size_t bytes, void **p) -> int {
+        RLA_CUDA_TRY(ctx, cudaMallocAsync(p, std::max<size_t>(bytes, 16), ctx->stream));
+        owned.push_back(*p);
+        return RLA_OK;
+    };
+    RLA_TRY(get(sizeof(double) * l * l, (void **)&w.G));
+    RLA_TRY(get(sizeof(double) * l * l, (void **)&w.Rinv));
+    RLA_TRY(get(sizeof(double) * l, (void **)&w.dscale));
+    RLA_TRY(get(sizeof(double) * l, (void **)&w.diag));
+    RLA_TRY(get(sizeof(double) * (l * l + l), (void **)&w.hw));
+    RLA_TRY(get(sizeof(int), (void **)&w.flag));
+    RLA_TRY(get(sizeof(T) * rows * l, &w.tmp));
+    return RLA_OK;
+}
+
+struct Owned {
+    rla_ctx *ctx;
+    std::vector<void *> ptrs;
+    ~Owned() {
+        for (void *p : ptrs) cudaFreeAsync(p, ctx->stream);
+    }
+};
+
+// Q (m x l, ld ldq) <- range of A*Omega after the power iterations.
+template <class T>
+static int range_core(rla_ctx *ctx, const rla_sketch *om, int64_t m, int64_t n, const T *A, int64_t lda,
+                      const rla_range_params *pr, T *Q, int64_t ldq, Owned &own) {
+    const int64_t l = om->n_cols;
+    OrthWork wq{}, wz{};
+    RLA_TRY(alloc_orth<T>(ctx, wq, m, l, own.ptrs));
+    T *Z = nullptr;
+    if (pr->power_its > 0) {
+        RLA_TRY(alloc_orth<T>(ctx, wz, n, l, own.ptrs));
+        RLA_CUDA_TRY(ctx, cudaMallocAsync((void **)&Z, sizeof(T) * n * l, ctx->stream));
+        own.ptrs.push_back(Z);
+    }
+    // Y = A * Omega (power_its.jl:21 / :59)
+    RLA_TRY(sketch_mul_impl(ctx, om, RLA_SIDE_RIGHT, 0, m, l, Q, ldq, 0, m, n, A, lda, 0, 1.0, 0.0));
+    if (pr->orthogonalize) {
+        RLA_TRY(orth<T>(ctx, Q, m, l, ldq, wq));
+        for (int64_t it = 0; it < pr->power_its; ++it) {
+            RLA_TRY((gemm<T, T, T, double>(ctx, n, l, m, A, lda, 1, Q, ldq, 0, Z, n, 1.0, 0.0)));
+            RLA_TRY(orth<T>(ctx, Z, n, l, n, wz));
+            RLA_TRY((gemm<T, T, T, double>(ctx, m, l, n, A, lda, 0, Z, n, 0, Q, ldq, 1.0, 0.0)));
+            RLA_TRY(orth<T>(ctx, Q, m, l, ldq, wq));
+        }
+    } else {
+        for (int64_t it = 0; it < pr->power_its; ++it) {
+            RLA_TRY((gemm<T, T, T, double>(ctx, n, l, m, A, lda, 1, Q, ldq, 0, Z, n, 1.0, 0.0)));
+            RLA_TRY((gemm<T, T, T, double>(ctx, m, l, n, A, lda, 0, Z, n, 0, Q, ldq, 1.0, 0.0)));
+        }
+        RLA_TRY(orth<T>(ctx, Q, m, l, ldq, wq));
+    }
+    return RLA_OK;
+}
+
+static int check_range_args(rla_ctx *ctx, const rla_sketch *om, int dtype, int64_t m, int64_t n, const void *A,
+                             int64_t lda, const rla_range_params *pr) {
+    if (!ctx) return RLA_E_ARG;
+    if (!om || !pr || !A) return set_error(ctx, RLA_E_ARG, "NULL argument.");
+    if (pr->power_its < 0) return set_error(ctx, RLA_E_ARG, "Field `power_its` must be non-negative.");
+    if (dtype != om->p.dtype) return set_error(ctx, RLA_E_ARG, "Compressor type and matrix type differ.");
+    if (m <= 0 || n <= 0 || lda < m) return set_error(ctx, RLA_E_ARG, "Bad matrix dimensions.");
+    if (pr->precision != RLA_PREC_NATIVE)
+        return set_error(ctx, RLA_E_UNSUPPORTED, "precision mode %d is not available in this build", pr->precision);
+    return RLA_OK;
+}
+
+template <class T, class TO>
+static int randsvd_t(rla_ctx *ctx, const rla_sketch *om, int64_t m, int64_t n, const T *A, int64_t lda,
+                     const rla_range_params *pr, TO *U, int64_t ldu, double *S, TO *V, int64_t ldv) {
+    const int64_t l = om->n_cols;
+    Owned own{ctx, {}};
+    T *Q;
+    RLA_CUDA_TRY(ctx, cudaMallocAsync((void **)&Q, sizeof(T) * m * l, ctx->stream));
+    own.ptrs.push_back(Q);
+    RLA_TRY(range_core<T>(ctx, om, m, n, A, lda, pr, Q, m, own));
+    // Bt = A'Q (n x l) in FP64 (randsvd.jl:183-185 forms QA in Float64)
+    double *Bt, *X, *J, *sig, *jw;
+    RLA_CUDA_TRY(ctx, cudaMallocAsync((void **)&Bt, sizeof(double) * n * l, ctx->stream));
+    own.ptrs.push_back(Bt);
+    RLA_TRY((gemm<T, T, double, double>(ctx, n, l, m, A, lda, 1, Q, m, 0, Bt, n, 1.0, 0.0)));
+    double *Qb;
+    RLA_CUDA_TRY(ctx, cudaMallocAsync((void **)&Qb, sizeof(double) * n * l, ctx->stream));
+    own.ptrs.push_back(Qb);
+    RLA_CUDA_TRY(ctx, cudaMemcpyAsync(Qb, Bt, sizeof(double) * n * l, cudaMemcpyDeviceToDevice, ctx->stream));
+    OrthWork wb{};
+    RLA_TRY(alloc_orth<double>(ctx, wb, n, l, own.ptrs));
+    RLA_TRY(orth<double>(ctx, Qb, n, l, n, wb));
+    RLA_CUDA_TRY(ctx, cudaMallocAsync((void **)&X, sizeof(double) * l * l, ctx->stream));
+    own.ptrs.push_back(X);
+    RLA_CUDA_TRY(ctx, cudaMallocAsync((void **)&J, sizeof(double) * l * l, ctx->stream));
+    own.ptrs.push_back(J);
+    RLA_CUDA_TRY(ctx, cudaMallocAsync((void **)&sig, sizeof(double) * l, ctx->stream));
+    own.ptrs.push_back(sig);
+    RLA_CUDA_TRY(ctx, cudaMallocAsync((void **)&jw, sizeof(double) * (2 * l * l + 2 * l), ctx->stream));
+    own.ptrs.push_back(jw);
+    // X = Rb' = Bt' Qb (l x l)
+    RLA_TRY((gemm<double, double, double, double>(ctx, l, l, n, Bt, n, 1, Qb, n, 0, X, l, 1.0, 0.0)));
+    RLA_TRY(jacobi_svd(ctx, X, J, sig, l, jw));
+    // U = Q W, V = Qb J
+    RLA_TRY((gemm<T, double, TO, double>(ctx, m, l, l, Q, m, 0, X, l, 0, U, ldu, 1.0, 0.0)));
+    RLA_TRY((gemm<double, double, TO, double>(ctx, n, l, l, Qb, n, 0, J, l, 0, V, ldv, 1.0, 0.0)));
+    RLA_CUDA_TRY(ctx, cudaMemcpyAsync(S, sig, sizeof(double) * l, cudaMemcpyDeviceToDevice, ctx->stream));
+    RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return RLA_OK;
+}
+
+}  // namespace rla
+
+using namespace rla;
+
+extern "C" {
+
+int rla_rangefinder(rla_ctx *ctx, const rla_sketch *om, int dtype, int64_t m, int64_t n, const void *A, int64_t lda,
+                    const rla_range_params *pr, void *Q, int64_t ldq) {
+    RLA_TRY(check_range_args(ctx, om, dtype, m, n, A, lda, pr));
+    if (!Q || ldq < m) return set_error(ctx, RLA_E_ARG, "Bad Q buffer.");
+    RLA_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    Owned own{ctx, {}};
+    int rc = dtype == RLA_F32
+                 ? range_core<float>(ctx, om, m, n, (const float *)A, lda, pr, (float *)Q, ldq, own)
+                 : range_core<double>(ctx, om, m, n, (const double *)A, lda, pr, (double *)Q, ldq, own);
+    RLA_TRY(rc);
+    RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return RLA_OK;
+}
+
+int rla_randsvd(rla_ctx *ctx, const rla_sketch *om, int dtype, int64_t m, int64_t n, const void *A, int64_t lda,
+                const rla_range_params *pr, int out_dtype, void *U, int64_t ldu, double *S, void *V, int64_t ldv) {
+    RLA_TRY(check_range_args(ctx, om, dtype, m, n, A, lda, pr));
+    const int64_t l = om->n_cols;
+    if (!U || !S || !V || ldu < m || ldv < n) return set_error(ctx, RLA_E_ARG, "Bad U/S/V buffers.");
+    if (l > n) return set_error(ctx, RLA_E_UNSUPPORTED, "compression dimension %lld exceeds n = %lld", (long long)l, (long long)n);
+    if (out_dtype != RLA_F32 && out_dtype != RLA_F64) return set_error(ctx, RLA_E_ARG, "out_dtype must be RLA_F32 or RLA_F64.");
+    RLA_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    if (dtype == RLA_F32) {
+        if (out_dtype == RLA_F64)
+            return randsvd_t<float, double>(ctx, om, m, n, (const float *)A, lda, pr, (double *)U, ldu, S, (double *)V, ldv);
+        return randsvd_t<float, float>(ctx, om, m, n, (const float *)A, lda, pr, (float *)U, ldu, S, (float *)V, ldv);
+    }
+    if (out_dtype == RLA_F64)
+        return randsvd_t<double, double>(ctx, om, m, n, (const double *)A, lda, pr, (double *)U, ldu, S, (double *)V, ldv);
+    return randsvd_t<double, float>(ctx, om, m, n, (const double *)A, lda, pr, (float *)U, ldu, S, (float *)V, ldv);
+}
+
+}  // extern "C"

@@ -1,0 +1,637 @@
+// rla_sketch.cu -- complete_compressor / update_compressor! : device draws and tables.
+//
+// The random draws are made on the device from a counter-based generator (Philox4x32-10)
+// keyed by the sketch seed and the draw count, so a sketch is reproducible from
+// (seed, number of updates).  The reference draws the same distributions on the host:
+//   SparseSign  nnz distinct rows per long index, values +-T(1/sqrt(nnz))   sparse_sign.jl:155-172, :248-252
+//   CountSketch one uniform bucket and one +-1 per long index               count_sketch.jl:124-127, :160-161
+//   SRHT        N sign bits, s rows of 0:N-1 without replacement, unordered  srht.jl:150-151
+//   FJLT        K = sprandn(.., q): Bernoulli(q) pattern, N(0,1) values     fjlt.jl:183, :217
+//   Gaussian    T(1/sqrt(s)) * randn(T, ..)                                  gaussian.jl:106-107, :121-122
+#include <math.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "rla_internal.cuh"
+
+namespace rla {
+
+// Per-thread word source over one Philox stream position.
+struct WordStream {
+    Rng rng;
+    uint32_t stream;
+    uint64_t base;   // index of the first block
+    uint64_t block = 0;
+    int used = 4;
+    P4 cur{};
+    __device__ uint32_t operator()() {
+        if (used == 4) {
+            cur = rng.at(stream, base + block++);
+            used = 0;
+        }
+        uint32_t w = used == 0 ? cur.x : used == 1 ? cur.y : used == 2 ? cur.z : cur.w;
+        ++used;
+        return w;
+    }
+};
+
+// SparseSign / CountSketch: per long index j, nnz distinct buckets (Floyd's algorithm,
+// then sorted ascending like StatsBase.sample!(...; ordered=true)) and nnz sign bits.
+__global__ void draw_sparse_kernel(Rng rng, uint32_t stream, int64_t L, int nnz, int64_t s,
+                                   int32_t *bucket, uint8_t *negative) {
+    int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= L) return;
+    WordStream ws{rng, stream, (uint64_t)j << 24};
+    int32_t *out = bucket + j * nnz;
+    int cnt = 0;
+    for (int64_t t = s - nnz; t < s; ++t) {
+        uint32_t r = uniform_below((uint32_t)(t + 1), ws);
+        bool found = false;
+        for (int q = 0; q < cnt; ++q) found |= (out[q] == (int32_t)r);
+        out[cnt++] = found ? (int32_t)t : (int32_t)r;
+    }
+    for (int a = 1; a < cnt; ++a) {  // insertion sort (nnz is small)
+        int32_t v = out[a];
+        int b = a - 1;
+        while (b >= 0 && out[b] > v) {
+            out[b + 1] = out[b];
+            --b;
+        }
+        out[b + 1] = v;
+    }
+    for (int e = 0; e < nnz; ++e) negative[j * nnz + e] = (uint8_t)(ws() & 1u);
+}
+
+// Packed metadata for the contiguous-vector compress kernel.  The kernel maps tile
+// element j = 128*tile + 4*lane + t to (lane, sub-round t); for every sub-round (tile, t,
+// e) this marks the lanes whose bucket repeats inside the sub-round, so the kernel can
+// take a conflict-free fast path whenever no mark is set.
+__global__ void build_meta_kernel(const int32_t *bucket, const uint8_t *negative, int64_t L,
+                                  int nnz, uint32_t *meta) {
+    int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    int64_t ntile = (L + 127) / 128;
+    int64_t total = ntile * 4 * nnz;
+    if (warp >= total) return;  // warp-uniform
+    int e = (int)(warp % nnz);
+    int t = (int)((warp / nnz) % 4);
+    int64_t tile = warp / (4 * nnz);
+    int64_t j = tile * 128 + 4 * lane + t;
+    bool valid = j < L;
+    uint32_t b = valid ? (uint32_t)bucket[j * nnz + e] : 0u;
+    unsigned key = valid ? b : (0x80000000u | (unsigned)lane);
+    unsigned grp = __match_any_sync(FULL, key);
+    if (valid) {
+        uint32_t dup = __popc(grp) > 1 ? 1u : 0u;
+        meta[j * nnz + e] = b | (dup << 30) | ((uint32_t)negative[j * nnz + e] << 31);
+    }
+}
+
+__global__ void draw_signbits_kernel(Rng rng, int64_t nwords, uint32_t *bits) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i * 4 >= nwords) return;
+    P4 r = rng.at(STREAM_SRHT_SIGNS, (uint64_t)i);
+    uint32_t v[4] = {r.x, r.y, r.z, r.w};
+    for (int k = 0; k < 4; ++k)
+        if (i * 4 + k < nwords) bits[i * 4 + k] = v[k];
+}
+
+// s distinct rows of 0:N-1 in random order: Floyd's algorithm over a bitmap, followed by
+// a Fisher-Yates shuffle (Floyd's insertion order is not uniform).  Single thread; the
+// bitmap lives in shared memory when it fits.
+__global__ void draw_rows_kernel(Rng rng, int64_t N, int64_t s, uint32_t *gbitmap,
+                                 int use_smem, int32_t *rows) {
+    extern __shared__ uint32_t sbitmap[];
+    uint32_t *bm = use_smem ? sbitmap : gbitmap;
+    int64_t nw = (N + 31) / 32;
+    for (int64_t i = threadIdx.x; i < nw; i += blockDim.x) bm[i] = 0;
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    WordStream ws{rng, STREAM_SRHT_ROWS, 0};
+    int64_t cnt = 0;
+    for (int64_t t = N - s; t < N; ++t) {
+        uint32_t r = uniform_below((uint32_t)(t + 1), ws);
+        uint32_t bit = 1u << (r & 31);
+        uint32_t pick = (bm[r >> 5] & bit) ? (uint32_t)t : r;
+        bm[pick >> 5] |= 1u << (pick & 31);
+        rows[cnt++] = (int32_t)pick;
+    }
+    for (int64_t i = s - 1; i > 0; --i) {
+        uint32_t k = uniform_below((uint32_t)(i + 1), ws);
+        int32_t tmp = rows[i];
+        rows[i] = rows[k];
+        rows[k] = tmp;
+    }
+}
+
+__device__ inline double normal_pair(WordStream &ws, double *second) {
+    double u1 = u01_open_d(ws(), ws());
+    double u2 = u01_open_d(ws(), ws());
+    double r = sqrt(-2.0 * log(u1));
+    double sn, cs;
+    sincospi(2.0 * u2, &sn, &cs);
+    *second = r * sn;
+    return r * cs;
+}
+
+// FJLT: rows of Kc (s x N) with a Bernoulli(q) pattern drawn by geometric gaps.
+// Pass 0 counts, pass 1 fills; both passes replay the same word stream.
+template <class T>
+__global__ void draw_fjlt_rows_kernel(Rng rng, int64_t s, int64_t N, double q, int pass,
+                                      int32_t *counts, const int32_t *ptr, int32_t *col, T *val) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= s) return;
+    WordStream ws{rng, STREAM_FJLT_K, (uint64_t)i << 28};
+    double lq = log1p(-q);
+    int64_t pos = -1;
+    int32_t c = 0;
+    int32_t base = pass ? ptr[i] : 0;
+    while (true) {
+        double u = u01_open_d(ws(), ws());
+        double g = (q >= 1.0) ? 0.0 : floor(log(u) / lq);
+        if (!(g < (double)N)) break;
+        pos += (int64_t)g + 1;
+        if (pos >= N) break;
+        double z2;
+        double z = normal_pair(ws, &z2);
+        if (pass) {
+            col[base + c] = (int32_t)pos;
+            val[base + c] = (T)z;
+        }
+        ++c;
+    }
+    if (!pass) counts[i] = c;
+}
+
+template <class T>
+__global__ void draw_gaussian_kernel(Rng rng, int64_t n, T scale, T *out) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (2 * i >= n) return;
+    WordStream ws{rng, STREAM_GAUSS, (uint64_t)i};
+    double z2;
+    double z1 = normal_pair(ws, &z2);
+    out[2 * i] = scale * (T)z1;
+    if (2 * i + 1 < n) out[2 * i + 1] = scale * (T)z2;
+}
+
+template <class T>
+static int fjlt_build(rla_ctx *ctx, rla_sketch *sk, const Rng &rng) {
+    int64_t s = sk->s, N = sk->N;
+    int32_t *counts = nullptr;
+    RLA_CUDA_TRY(ctx, cudaMallocAsync(&counts, sizeof(int32_t) * (s + 1), ctx->stream));
+    draw_fjlt_rows_kernel<T><<<ceil_div_i(s, 128), 128, 0, ctx->stream>>>(rng, s, N, sk->sparsity, 0,
+                                                                         counts, nullptr, nullptr, nullptr);
+    RLA_TRY(check_launch(ctx, "draw_fjlt_rows(count)"));
+    std::vector<int32_t> hc(s);
+    RLA_CUDA_TRY(ctx, cudaMemcpyAsync(hc.data(), counts, sizeof(int32_t) * s, cudaMemcpyDeviceToHost, ctx->stream));
+    RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    std::vector<int32_t> hp(s + 1, 0);
+    for (int64_t i = 0; i < s; ++i) hp[i + 1] = hp[i] + hc[i];
+    int64_t nnz = hp[s];
+    if (sk->k_ptr) cudaFreeAsync(sk->k_ptr, ctx->stream);
+    if (sk->k_col) cudaFreeAsync(sk->k_col, ctx->stream);
+    if (sk->k_val) cudaFreeAsync(sk->k_val, ctx->stream);
+    RLA_CUDA_TRY(ctx, cudaMallocAsync(&sk->k_ptr, sizeof(int32_t) * (s + 1), ctx->stream));
+    RLA_CUDA_TRY(ctx, cudaMallocAsync(&sk->k_col, sizeof(int32_t) * std::max<int64_t>(nnz, 1), ctx->stream));
+    RLA_CUDA_TRY(ctx, cudaMallocAsync(&sk->k_val, sizeof(T) * std::max<int64_t>(nnz, 1), ctx->stream));
+    RLA_CUDA_TRY(ctx, cudaMemcpyAsync(sk->k_ptr, hp.data(), sizeof(int32_t) * (s + 1), cudaMemcpyHostToDevice, ctx->stream));
+    draw_fjlt_rows_kernel<T><<<ceil_div_i(s, 128), 128, 0, ctx->stream>>>(rng, s, N, sk->sparsity, 1, nullptr,
+                                                                         sk->k_ptr, sk->k_col, (T *)sk->k_val);
+    RLA_TRY(check_launch(ctx, "draw_fjlt_rows(fill)"));
+    RLA_CUDA_TRY(ctx, cudaFreeAsync(counts, ctx->stream));
+    sk->k_nnz = nnz;
+    return RLA_OK;
+}
+
+// Transpose Kc (CSR s x N) into CSR of Kc' (N x s) on the host; entries of each row of
+// the transpose are in ascending column order.
+template <class T>
+static int fjlt_transpose(rla_ctx *ctx, rla_sketch *sk) {
+    int64_t s = sk->s, N = sk->N, nnz = sk->k_nnz;
+    std::vector<int32_t> p(s + 1), c(std::max<int64_t>(nnz, 1));
+    std::vector<T> v(std::max<int64_t>(nnz, 1));
+    RLA_CUDA_TRY(ctx, cudaMemcpyAsync(p.data(), sk->k_ptr, sizeof(int32_t) * (s + 1), cudaMemcpyDeviceToHost, ctx->stream));
+    if (nnz) {
+        RLA_CUDA_TRY(ctx, cudaMemcpyAsync(c.data(), sk->k_col, sizeof(int32_t) * nnz, cudaMemcpyDeviceToHost, ctx->stream));
+        RLA_CUDA_TRY(ctx, cudaMemcpyAsync(v.data(), sk->k_val, sizeof(T) * nnz, cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    std::vector<int32_t> tp(N + 1, 0), tr(std::max<int64_t>(nnz, 1));
+    std::vector<T> tv(std::max<int64_t>(nnz, 1));
+    for (int64_t k = 0; k < nnz; ++k) tp[c[k] + 1]++;
+    for (int64_t r = 0; r < N; ++r) tp[r + 1] += tp[r];
+    std::vector<int32_t> fill(tp.begin(), tp.end() - 1);
+    for (int64_t i = 0; i < s; ++i)
+        for (int32_t k = p[i]; k < p[i + 1]; ++k) {
+            int32_t d = fill[c[k]]++;
+            tr[d] = (int32_t)i;
+            tv[d] = v[k];
+        }
+    if (sk->kt_ptr) cudaFreeAsync(sk->kt_ptr, ctx->stream);
+    if (sk->kt_row) cudaFreeAsync(sk->kt_row, ctx->stream);
+    if (sk->kt_val) cudaFreeAsync(sk->kt_val, ctx->stream);
+    RLA_CUDA_TRY(ctx, cudaMallocAsync(&sk->kt_ptr, sizeof(int32_t) * (N + 1), ctx->stream));
+    RLA_CUDA_TRY(ctx, cudaMallocAsync(&sk->kt_row, sizeof(int32_t) * std::max<int64_t>(nnz, 1), ctx->stream));
+    RLA_CUDA_TRY(ctx, cudaMallocAsync(&sk->kt_val, sizeof(T) * std::max<int64_t>(nnz, 1), ctx->stream));
+    RLA_CUDA_TRY(ctx, cudaMemcpyAsync(sk->kt_ptr, tp.data(), sizeof(int32_t) * (N + 1), cudaMemcpyHostToDevice, ctx->stream));
+    if (nnz) {
+        RLA_CUDA_TRY(ctx, cudaMemcpyAsync(sk->kt_row, tr.data(), sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, ctx->stream));
+        RLA_CUDA_TRY(ctx, cudaMemcpyAsync(sk->kt_val, tv.data(), sizeof(T) * nnz, cudaMemcpyHostToDevice, ctx->stream));
+    }
+    RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return RLA_OK;
+}
+
+// SRHT expand tables: samples grouped by their low log2(chunk) bits.
+static int srht_tables(rla_ctx *ctx, rla_sketch *sk) {
+    int64_t s = sk->s;
+    sk->chunk = std::min<int64_t>(sk->N, 4096);
+    int64_t ch = sk->chunk;
+    std::vector<int32_t> rows(s);
+    RLA_CUDA_TRY(ctx, cudaMemcpyAsync(rows.data(), sk->rows, sizeof(int32_t) * s, cudaMemcpyDeviceToHost, ctx->stream));
+    RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    std::vector<int32_t> ptr(ch + 1, 0), list(s);
+    for (int64_t k = 0; k < s; ++k) ptr[(rows[k] & (ch - 1)) + 1]++;
+    for (int64_t r = 0; r < ch; ++r) ptr[r + 1] += ptr[r];
+    std::vector<int32_t> fill(ptr.begin(), ptr.end() - 1);
+    for (int64_t k = 0; k < s; ++k) list[fill[rows[k] & (ch - 1)]++] = (int32_t)k;
+    if (!sk->p2_ptr) RLA_CUDA_TRY(ctx, cudaMalloc(&sk->p2_ptr, sizeof(int32_t) * (4096 + 1)));
+    if (!sk->p2_list) RLA_CUDA_TRY(ctx, cudaMalloc(&sk->p2_list, sizeof(int32_t) * s));
+    RLA_CUDA_TRY(ctx, cudaMemcpyAsync(sk->p2_ptr, ptr.data(), sizeof(int32_t) * (ch + 1), cudaMemcpyHostToDevice, ctx->stream));
+    RLA_CUDA_TRY(ctx, cudaMemcpyAsync(sk->p2_list, list.data(), sizeof(int32_t) * s, cudaMemcpyHostToDevice, ctx->stream));
+    RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return RLA_OK;
+}
+
+static int build_meta(rla_ctx *ctx, rla_sketch *sk) {
+    int64_t ntile = ceil_div(sk->L, 128);
+    int64_t warps = ntile * 4 * sk->nnz;
+    int64_t threads = warps * 32;
+    build_meta_kernel<<<ceil_div_i(threads, 256), 256, 0, ctx->stream>>>(sk->bucket, sk->negative, sk->L,
+                                                                        (int)sk->nnz, sk->meta);
+    return check_launch(ctx, "build_meta");
+}
+
+static Rng make_rng(const rla_sketch *sk) {
+    Rng r;
+    r.k0 = (uint32_t)sk->p.seed;
+    r.k1 = (uint32_t)(sk->p.seed >> 32);
+    r.epoch = (uint32_t)sk->draw_count;
+    return r;
+}
+
+static int draw(rla_ctx *ctx, rla_sketch *sk) {
+    Rng rng = make_rng(sk);
+    const int kind = sk->p.kind;
+    if (kind == RLA_SPARSE_SIGN || kind == RLA_COUNT_SKETCH) {
+        draw_sparse_kernel<<<ceil_div_i(sk->L, 128), 128, 0, ctx->stream>>>(
+            rng, kind == RLA_SPARSE_SIGN ? STREAM_SPARSE : STREAM_COUNT, sk->L, (int)sk->nnz, sk->s,
+            sk->bucket, sk->negative);
+        RLA_TRY(check_launch(ctx, "draw_sparse"));
+        RLA_TRY(build_meta(ctx, sk));
+    } else if (kind == RLA_SRHT || kind == RLA_FJLT) {
+        int64_t nwords = ceil_div(sk->N, 32);
+        Rng r2 = rng;
+        draw_signbits_kernel<<<ceil_div_i(ceil_div(nwords, 4), 256), 256, 0, ctx->stream>>>(r2, nwords, sk->signbits);
+        RLA_TRY(check_launch(ctx, "draw_signbits"));
+        if (kind == RLA_SRHT) {
+            size_t bm_bytes = sizeof(uint32_t) * nwords;
+            int use_smem = bm_bytes <= 160 * 1024;
+            uint32_t *gbm = nullptr;
+            if (!use_smem) {
+                void *p;
+                RLA_TRY(scratch_get(ctx, bm_bytes, &p));
+                gbm = (uint32_t *)p;
+            } else {
+                RLA_CUDA_TRY(ctx, cudaFuncSetAttribute(draw_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                       (int)bm_bytes));
+            }
+            draw_rows_kernel<<<1, 256, use_smem ? bm_bytes : 0, ctx->stream>>>(rng, sk->N, sk->s, gbm, use_smem, sk->rows);
+            RLA_TRY(check_launch(ctx, "draw_rows"));
+            RLA_TRY(srht_tables(ctx, sk));
+        } else {
+            if (sk->p.dtype == RLA_F32) {
+                RLA_TRY(fjlt_build<float>(ctx, sk, rng));
+                RLA_TRY(fjlt_transpose<float>(ctx, sk));
+            } else {
+                RLA_TRY(fjlt_build<double>(ctx, sk, rng));
+                RLA_TRY(fjlt_transpose<double>(ctx, sk));
+            }
+        }
+    } else if (kind == RLA_GAUSSIAN) {
+        int64_t n = sk->n_rows * sk->n_cols;
+        if (sk->p.dtype == RLA_F32)
+            draw_gaussian_kernel<float><<<ceil_div_i(ceil_div(n, 2), 256), 256, 0, ctx->stream>>>(
+                rng, n, (float)sk->scale, (float *)sk->dense);
+        else
+            draw_gaussian_kernel<double><<<ceil_div_i(ceil_div(n, 2), 256), 256, 0, ctx->stream>>>(
+                rng, n, (double)sk->scale, (double *)sk->dense);
+        RLA_TRY(check_launch(ctx, "draw_gaussian"));
+    }
+    RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return RLA_OK;
+}
+
+static void free_sketch_buffers(rla_sketch *sk) {
+    void *ptrs[] = {sk->bucket, sk->negative, sk->meta, sk->rows, sk->signbits, sk->p2_ptr, sk->p2_list,
+                    sk->k_ptr, sk->k_col, sk->k_val, sk->kt_ptr, sk->kt_row, sk->kt_val, sk->dense};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+}
+
+}  // namespace rla
+
+using namespace rla;
+
+extern "C" {
+
+int rla_sketch_create(rla_ctx *ctx, const rla_sketch_params *pp, rla_sketch **out) {
+    if (!ctx || !pp || !out) return RLA_E_ARG;
+    *out = nullptr;
+    const rla_sketch_params &p = *pp;
+    if (p.kind < RLA_SPARSE_SIGN || p.kind > RLA_GAUSSIAN) return set_error(ctx, RLA_E_ARG, "Unknown compressor kind %d.", p.kind);
+    if (p.card != RLA_LEFT && p.card != RLA_RIGHT)
+        return set_error(ctx, RLA_E_ARG, "`cardinality` must be specified as `Left()` or `Right()`.");
+    if (p.dtype != RLA_F32 && p.dtype != RLA_F64) return set_error(ctx, RLA_E_ARG, "Element type must be Float32 or Float64.");
+    // Constructor checks, with the reference's messages.
+    if (p.compression_dim <= 0) {
+        if (p.kind == RLA_COUNT_SKETCH || p.kind == RLA_GAUSSIAN)
+            return set_error(ctx, RLA_E_ARG, "Field 'compression_dim' must be positive.");
+        return set_error(ctx, RLA_E_ARG, "Field `compression_dim` must be positive.");
+    }
+    if (p.kind == RLA_SPARSE_SIGN) {
+        if (p.nnz > p.compression_dim)
+            return set_error(ctx, RLA_E_ARG,
+                             "Number of non-zero indices, %lld, must be less than or equal to compression dimension, %lld.",
+                             (long long)p.nnz, (long long)p.compression_dim);
+        if (p.nnz <= 0) return set_error(ctx, RLA_E_ARG, "Field `nnz` must be positive.");
+    }
+    if ((p.kind == RLA_SRHT || p.kind == RLA_FJLT) && p.block_size <= 0)
+        return set_error(ctx, RLA_E_ARG, "Field `block_size` must be positive.");
+    if (p.long_dim <= 0) return set_error(ctx, RLA_E_ARG, "The sketched dimension must be positive.");
+    if (p.compression_dim >= (int64_t(1) << 30) || p.long_dim >= (int64_t(1) << 31))
+        return set_error(ctx, RLA_E_UNSUPPORTED, "Dimensions beyond 2^30 (compression) / 2^31 (sketched) are not supported.");
+    if (p.kind == RLA_FJLT && (p.sparsity < 0.0 || p.sparsity > 1.0))
+        return set_error(ctx, RLA_E_ARG, "Field `sparsity` must be in [0, 1].");
+
+    RLA_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    rla_sketch *sk = new rla_sketch();
+    sk->p = p;
+    sk->device = ctx->device;
+    sk->s = p.compression_dim;
+    sk->L = p.long_dim;
+    sk->n_rows = p.card == RLA_LEFT ? sk->s : sk->L;
+    sk->n_cols = p.card == RLA_LEFT ? sk->L : sk->s;
+    const size_t es = dtype_size(p.dtype);
+    int rc = RLA_OK;
+    auto alloc = [&](void **ptr, size_t bytes) {
+        if (rc != RLA_OK) return;
+        cudaError_t e = cudaMalloc(ptr, std::max<size_t>(bytes, 16));
+        if (e != cudaSuccess) rc = set_error(ctx, RLA_E_OOM, "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+    };
+    switch (p.kind) {
+        case RLA_SPARSE_SIGN:
+        case RLA_COUNT_SKETCH: {
+            sk->nnz = p.kind == RLA_SPARSE_SIGN ? p.nnz : 1;
+            sk->scale = p.kind == RLA_SPARSE_SIGN
+                            ? (p.dtype == RLA_F32 ? (double)(float)(1.0 / sqrt((double)sk->nnz)) : 1.0 / sqrt((double)sk->nnz))
+                            : 1.0;
+            size_t ne = (size_t)(sk->L * sk->nnz);
+            alloc((void **)&sk->bucket, ne * 4);
+            alloc((void **)&sk->negative, ne);
+            alloc((void **)&sk->meta, ne * 4);
+            break;
+        }
+        case RLA_SRHT:
+        case RLA_FJLT: {
+            sk->N = next_pow2(sk->L);
+            if (p.kind == RLA_SRHT) {
+                if (sk->s > sk->N) {
+                    delete sk;
+                    return set_error(ctx, RLA_E_ARG, "Cannot draw %lld rows without replacement from %lld.",
+                                     (long long)p.compression_dim, (long long)next_pow2(p.long_dim));
+                }
+                double sc = sqrt((double)sk->s) / sqrt((double)sk->N);
+                sk->scale = p.dtype == RLA_F32 ? (double)(float)sc : sc;
+                alloc((void **)&sk->rows, (size_t)sk->s * 4);
+            } else {
+                sk->sparsity = p.sparsity == 0.0 ? 0.25 * log((double)sk->L) * log((double)sk->L) / (double)sk->L
+                                                 : p.sparsity;
+                if (sk->sparsity > 1.0) sk->sparsity = 1.0;
+                double sc = 1.0 / (sqrt((double)sk->N) * sqrt(sk->sparsity) * sqrt((double)sk->s));
+                sk->scale = p.dtype == RLA_F32 ? (double)(float)sc : sc;
+            }
+            alloc((void **)&sk->signbits, (size_t)ceil_div(sk->N, 32) * 4);
+            break;
+        }
+        case RLA_GAUSSIAN: {
+            double sc = 1.0 / sqrt((double)sk->s);
+            sk->scale = p.dtype == RLA_F32 ? (double)(float)sc : sc;
+            alloc(&sk->dense, (size_t)(sk->n_rows * sk->n_cols) * es);
+            break;
+        }
+    }
+    if (rc == RLA_OK) rc = draw(ctx, sk);
+    if (rc != RLA_OK) {
+        free_sketch_buffers(sk);
+        delete sk;
+        return rc;
+    }
+    sk->draw_count = 1;
+    *out = sk;
+    return RLA_OK;
+}
+
+int rla_sketch_update(rla_ctx *ctx, rla_sketch *sk) {
+    if (!ctx || !sk) return RLA_E_ARG;
+    RLA_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    int rc = draw(ctx, sk);
+    if (rc == RLA_OK) sk->draw_count++;
+    return rc;
+}
+
+int rla_sketch_destroy(rla_sketch *sk) {
+    if (!sk) return RLA_OK;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(sk->device);
+    cudaDeviceSynchronize();
+    free_sketch_buffers(sk);
+    cudaSetDevice(cur);
+    delete sk;
+    return RLA_OK;
+}
+
+int rla_sketch_get_info(const rla_sketch *sk, rla_sketch_info *o) {
+    if (!sk || !o) return RLA_E_ARG;
+    o->kind = sk->p.kind;
+    o->card = sk->p.card;
+    o->dtype = sk->p.dtype;
+    o->n_rows = sk->n_rows;
+    o->n_cols = sk->n_cols;
+    o->compression_dim = sk->s;
+    o->long_dim = sk->L;
+    o->nnz = sk->nnz;
+    o->block_size = sk->p.block_size;
+    o->padded = sk->N;
+    o->k_nnz = sk->k_nnz;
+    o->sparsity = sk->sparsity;
+    o->scale = sk->scale;
+    o->draw_count = sk->draw_count;
+    return RLA_OK;
+}
+
+int rla_sketch_get_draws(rla_ctx *ctx, const rla_sketch *sk, int64_t *idx, void *vals, uint8_t *signs, int64_t *kptr) {
+    if (!ctx || !sk) return RLA_E_ARG;
+    RLA_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    const int kind = sk->p.kind;
+    const size_t es = dtype_size(sk->p.dtype);
+    if (kind == RLA_SPARSE_SIGN || kind == RLA_COUNT_SKETCH) {
+        size_t ne = (size_t)(sk->L * sk->nnz);
+        std::vector<int32_t> b(ne);
+        std::vector<uint8_t> ng(ne);
+        RLA_CUDA_TRY(ctx, cudaMemcpy(b.data(), sk->bucket, ne * 4, cudaMemcpyDeviceToHost));
+        RLA_CUDA_TRY(ctx, cudaMemcpy(ng.data(), sk->negative, ne, cudaMemcpyDeviceToHost));
+        if (idx)
+            for (size_t i = 0; i < ne; ++i) idx[i] = b[i];
+        if (vals) {
+            for (size_t i = 0; i < ne; ++i) {
+                double v = ng[i] ? -sk->scale : sk->scale;
+                if (es == 4) ((float *)vals)[i] = (float)v;
+                else ((double *)vals)[i] = v;
+            }
+        }
+    } else if (kind == RLA_SRHT || kind == RLA_FJLT) {
+        if (signs) {
+            int64_t nw = ceil_div(sk->N, 32);
+            std::vector<uint32_t> w(nw);
+            RLA_CUDA_TRY(ctx, cudaMemcpy(w.data(), sk->signbits, nw * 4, cudaMemcpyDeviceToHost));
+            for (int64_t r = 0; r < sk->N; ++r) signs[r] = (uint8_t)((w[r >> 5] >> (r & 31)) & 1u);
+        }
+        if (kind == RLA_SRHT) {
+            if (idx) {
+                std::vector<int32_t> r(sk->s);
+                RLA_CUDA_TRY(ctx, cudaMemcpy(r.data(), sk->rows, sk->s * 4, cudaMemcpyDeviceToHost));
+                for (int64_t i = 0; i < sk->s; ++i) idx[i] = r[i];
+            }
+        } else {
+            // Left: op = Kc (s x N) as CSC == CSR of Kc' ; Right: op = Kc' (N x s) as CSC == CSR of Kc
+            bool left = sk->p.card == RLA_LEFT;
+            int64_t ncol = left ? sk->N : sk->s;
+            const int32_t *dptr = left ? sk->kt_ptr : sk->k_ptr;
+            const int32_t *didx = left ? sk->kt_row : sk->k_col;
+            const void *dval = left ? sk->kt_val : sk->k_val;
+            std::vector<int32_t> hp(ncol + 1), hi(std::max<int64_t>(sk->k_nnz, 1));
+            RLA_CUDA_TRY(ctx, cudaMemcpy(hp.data(), dptr, (ncol + 1) * 4, cudaMemcpyDeviceToHost));
+            if (sk->k_nnz) RLA_CUDA_TRY(ctx, cudaMemcpy(hi.data(), didx, sk->k_nnz * 4, cudaMemcpyDeviceToHost));
+            if (kptr)
+                for (int64_t i = 0; i <= ncol; ++i) kptr[i] = hp[i];
+            if (idx)
+                for (int64_t i = 0; i < sk->k_nnz; ++i) idx[i] = hi[i];
+            if (vals && sk->k_nnz) RLA_CUDA_TRY(ctx, cudaMemcpy(vals, dval, sk->k_nnz * es, cudaMemcpyDeviceToHost));
+        }
+    } else if (kind == RLA_GAUSSIAN) {
+        if (vals) RLA_CUDA_TRY(ctx, cudaMemcpy(vals, sk->dense, sk->n_rows * sk->n_cols * es, cudaMemcpyDeviceToHost));
+    }
+    return RLA_OK;
+}
+
+int rla_sketch_set_draws(rla_ctx *ctx, rla_sketch *sk, const int64_t *idx, const void *vals, const uint8_t *signs,
+                         const int64_t *kptr, int64_t k_nnz) {
+    if (!ctx || !sk) return RLA_E_ARG;
+    RLA_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    const int kind = sk->p.kind;
+    const size_t es = dtype_size(sk->p.dtype);
+    auto val_at = [&](size_t i) -> double { return es == 4 ? (double)((const float *)vals)[i] : ((const double *)vals)[i]; };
+    if (kind == RLA_SPARSE_SIGN || kind == RLA_COUNT_SKETCH) {
+        if (!idx || !vals) return set_error(ctx, RLA_E_ARG, "Sparse draws need indices and values.");
+        size_t ne = (size_t)(sk->L * sk->nnz);
+        std::vector<int32_t> b(ne);
+        std::vector<uint8_t> ng(ne);
+        for (size_t i = 0; i < ne; ++i) {
+            if (idx[i] < 0 || idx[i] >= sk->s)
+                return set_error(ctx, RLA_E_ARG, "Row index %lld out of range 0:%lld.", (long long)idx[i], (long long)sk->s - 1);
+            b[i] = (int32_t)idx[i];
+            double v = val_at(i);
+            if (v == sk->scale) ng[i] = 0;
+            else if (v == -sk->scale) ng[i] = 1;
+            else
+                return set_error(ctx, RLA_E_ARG, "Nonzero values must be +-%.17g (the compressor's scale).", sk->scale);
+        }
+        RLA_CUDA_TRY(ctx, cudaMemcpy(sk->bucket, b.data(), ne * 4, cudaMemcpyHostToDevice));
+        RLA_CUDA_TRY(ctx, cudaMemcpy(sk->negative, ng.data(), ne, cudaMemcpyHostToDevice));
+        RLA_TRY(build_meta(ctx, sk));
+    } else if (kind == RLA_SRHT || kind == RLA_FJLT) {
+        if (!signs) return set_error(ctx, RLA_E_ARG, "SRHT/FJLT draws need signs.");
+        int64_t nw = ceil_div(sk->N, 32);
+        std::vector<uint32_t> w(nw, 0);
+        for (int64_t r = 0; r < sk->N; ++r) w[r >> 5] |= (signs[r] ? 1u : 0u) << (r & 31);
+        RLA_CUDA_TRY(ctx, cudaMemcpy(sk->signbits, w.data(), nw * 4, cudaMemcpyHostToDevice));
+        if (kind == RLA_SRHT) {
+            if (!idx) return set_error(ctx, RLA_E_ARG, "SRHT draws need the sampled rows.");
+            std::vector<int32_t> r(sk->s);
+            for (int64_t i = 0; i < sk->s; ++i) {
+                if (idx[i] < 0 || idx[i] >= sk->N)
+                    return set_error(ctx, RLA_E_ARG, "Sampled row %lld out of range 0:%lld.", (long long)idx[i], (long long)sk->N - 1);
+                r[i] = (int32_t)idx[i];
+            }
+            RLA_CUDA_TRY(ctx, cudaMemcpy(sk->rows, r.data(), sk->s * 4, cudaMemcpyHostToDevice));
+            RLA_TRY(srht_tables(ctx, sk));
+        } else {
+            if (!idx || !vals || !kptr) return set_error(ctx, RLA_E_ARG, "FJLT draws need op.colptr, op.rowval and op.nzval.");
+            bool left = sk->p.card == RLA_LEFT;
+            // Given CSC of op: Left op = Kc (s x N) -> CSC == CSR of Kc' (N rows of s);
+            // Right op = Kc' (N x s) -> CSC == CSR of Kc (s rows of N).  Build CSR of Kc.
+            int64_t ncol = left ? sk->N : sk->s;
+            int64_t nrow = left ? sk->s : sk->N;
+            if (kptr[0] != 0 || kptr[ncol] != k_nnz) return set_error(ctx, RLA_E_ARG, "Inconsistent op.colptr.");
+            for (int64_t c = 0; c < ncol; ++c)
+                if (kptr[c + 1] < kptr[c]) return set_error(ctx, RLA_E_ARG, "op.colptr must be nondecreasing.");
+            for (int64_t k = 0; k < k_nnz; ++k)
+                if (idx[k] < 0 || idx[k] >= nrow) return set_error(ctx, RLA_E_ARG, "op.rowval out of range.");
+            std::vector<int32_t> cp(sk->s + 1, 0), cc(std::max<int64_t>(k_nnz, 1));
+            std::vector<char> cv(std::max<int64_t>(k_nnz, 1) * es);
+            if (!left) {
+                for (int64_t c = 0; c <= sk->s; ++c) cp[c] = (int32_t)kptr[c];
+                for (int64_t k = 0; k < k_nnz; ++k) cc[k] = (int32_t)idx[k];
+                memcpy(cv.data(), vals, k_nnz * es);
+            } else {
+                for (int64_t k = 0; k < k_nnz; ++k) cp[idx[k] + 1]++;
+                for (int64_t i = 0; i < sk->s; ++i) cp[i + 1] += cp[i];
+                std::vector<int32_t> fill(cp.begin(), cp.end() - 1);
+                for (int64_t c = 0; c < ncol; ++c)
+                    for (int64_t k = kptr[c]; k < kptr[c + 1]; ++k) {
+                        int32_t d = fill[idx[k]]++;
+                        cc[d] = (int32_t)c;
+                        memcpy(cv.data() + d * es, (const char *)vals + k * es, es);
+                    }
+            }
+            if (sk->k_ptr) cudaFree(sk->k_ptr);
+            if (sk->k_col) cudaFree(sk->k_col);
+            if (sk->k_val) cudaFree(sk->k_val);
+            sk->k_ptr = sk->k_col = nullptr;
+            sk->k_val = nullptr;
+            RLA_CUDA_TRY(ctx, cudaMalloc(&sk->k_ptr, (sk->s + 1) * 4));
+            RLA_CUDA_TRY(ctx, cudaMalloc(&sk->k_col, std::max<int64_t>(k_nnz, 1) * 4));
+            RLA_CUDA_TRY(ctx, cudaMalloc(&sk->k_val, std::max<int64_t>(k_nnz, 1) * es));
+            RLA_CUDA_TRY(ctx, cudaMemcpy(sk->k_ptr, cp.data(), (sk->s + 1) * 4, cudaMemcpyHostToDevice));
+            if (k_nnz) {
+                RLA_CUDA_TRY(ctx, cudaMemcpy(sk->k_col, cc.data(), k_nnz * 4, cudaMemcpyHostToDevice));
+                RLA_CUDA_TRY(ctx, cudaMemcpy(sk->k_val, cv.data(), k_nnz * es, cudaMemcpyHostToDevice));
+            }
+            sk->k_nnz = k_nnz;
+            if (sk->p.dtype == RLA_F32) RLA_TRY(fjlt_transpose<float>(ctx, sk));
+            else RLA_TRY(fjlt_transpose<double>(ctx, sk));
+        }
+    } else if (kind == RLA_GAUSSIAN) {
+        if (!vals) return set_error(ctx, RLA_E_ARG, "Gaussian draws need values.");
+        RLA_CUDA_TRY(ctx, cudaMemcpy(sk->dense, vals, sk->n_rows * sk->n_cols * es, cudaMemcpyHostToDevice));
+    }
+    RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return RLA_OK;
+}
+
+}  // extern "C"

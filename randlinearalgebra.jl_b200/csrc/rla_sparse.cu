@@ -1,0 +1,440 @@
+// rla_sparse.cu -- SparseSign / CountSketch application kernels.
+//
+// A SparseSign (nnz per long index) or CountSketch (nnz = 1) operator is stored by its
+// compress side P (s x L): long index j carries nnz (bucket, sign) entries with a common
+// magnitude `scale`.  The reference applies it through SparseArrays' CSC kernels
+// (sparse_sign.jl:339-361, count_sketch.jl:166-213); here:
+//
+//  * compress, contiguous vectors (S*A with Left S on column-major A, the sketch hot
+//    path): each warp owns private shared-memory bins for one output vector and streams
+//    128-element tiles of its input vector with 16-byte loads.  Lanes whose buckets
+//    collide inside a sub-round are combined in lane order with shuffles (the collisions
+//    are flagged ahead of time in the packed metadata), so no atomics are used and the
+//    result is bit-for-bit reproducible.  Input tiles are split over all warps of the
+//    GPU (stream-K); a vector shared by several warps is finished by the last warp to
+//    arrive, which adds the partial bins in warp order.
+//  * compress, strided vectors (A*S with Right S: rows of column-major A): lane = vector,
+//    the bucket is warp-uniform, bins are [bucket][lane] (conflict-free).
+//  * expand (S'*A, A*S' ...): a gather, one thread per output element.
+#include "rla_internal.cuh"
+
+namespace rla {
+
+struct Split {  // contiguous split of `total` units over W workers
+    int64_t total;
+    int W;
+    __host__ __device__ int64_t start(int g) const { return (int64_t)((__int128)g * total / W); }
+    __device__ int owner(int64_t u) const {
+        int g = (int)((__int128)u * W / total);
+        if (g >= W) g = W - 1;
+        while (g + 1 < W && start(g + 1) <= u) ++g;
+        while (g > 0 && start(g) > u) --g;
+        return g;
+    }
+};
+
+template <class T>
+struct CompressContigParams {
+    const T *X;
+    int64_t x_ld;  // vector stride; element (j, v) at X[j + v*x_ld]
+    int64_t L, nv;
+    const uint32_t *meta;
+    int nnz;
+    int64_t bin_lo;
+    int bin_cnt;
+    T *Y;
+    int64_t y_es, y_vs;  // element (i, v) of the output at Y[i*y_es + v*y_vs]
+    T alpha, beta;
+    int beta_zero;
+    T *partials;
+    int *counters;
+    int64_t tpv;  // 128-element tiles per vector
+    Split split;
+};
+
+template <class T>
+__device__ __forceinline__ void bin_add(T *bins, T x, uint32_t w, bool valid, int64_t bin_lo, int bin_cnt, int lane) {
+    int b = (int)(w & 0x3fffffffu) - (int)bin_lo;
+    bool inwin = valid && (unsigned)b < (unsigned)bin_cnt;
+    if (w >> 31) x = -x;
+    bool dup = inwin && ((w >> 30) & 1u);
+    if (__any_sync(FULL, dup)) {
+        unsigned key = inwin ? (unsigned)b : (0x80000000u | (unsigned)lane);
+        unsigned grp = __match_any_sync(FULL, key);
+        int cnt = __popc(grp);
+        int maxc = (int)__reduce_max_sync(FULL, (unsigned)cnt);
+        T sum = T(0);
+        for (int q = 0; q < maxc; ++q) {
+            int src = q < cnt ? (int)__fns(grp, 0, q + 1) : lane;
+            T y = __shfl_sync(FULL, x, src);
+            if (q < cnt) sum += y;
+        }
+        if (inwin && (grp & ((1u << lane) - 1u)) == 0u) bins[b] += sum;
+    } else if (inwin) {
+        bins[b] += x;
+    }
+    __syncwarp();
+}
+
+template <class T, bool VEC>
+__device__ __forceinline__ void load4(const T *xv, int64_t j0, int64_t L, bool tile_ok, T (&v)[4]) {
+    if (VEC && tile_ok && j0 + 3 < L) {
+        if constexpr (sizeof(T) == 4) {
+            float4 q = __ldg(reinterpret_cast<const float4 *>(xv + j0));
+            v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+        } else {
+            double2 a = __ldg(reinterpret_cast<const double2 *>(xv + j0));
+            double2 b = __ldg(reinterpret_cast<const double2 *>(xv + j0 + 2));
+            v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+        }
+    } else {
+#pragma unroll
+        for (int t = 0; t < 4; ++t) v[t] = (tile_ok && j0 + t < L) ? __ldg(xv + j0 + t) : T(0);
+    }
+}
+
+template <class T>
+__device__ void flush_vector(const CompressContigParams<T> &p, T *bins, int g, int64_t v, bool first_of_warp,
+                             bool exclusive, int lane) {
+    __syncwarp();
+    if (exclusive) {
+        for (int i = lane; i < p.bin_cnt; i += 32) {
+            T *yp = p.Y + (p.bin_lo + i) * p.y_es + v * p.y_vs;
+            T r = p.alpha * bins[i];
+            if (!p.beta_zero) r += p.beta * *yp;
+            *yp = r;
+            bins[i] = T(0);
+        }
+        __syncwarp();
+        return;
+    }
+    int slot = 2 * g + (first_of_warp ? 0 : 1);
+    T *part = p.partials + (int64_t)slot * p.bin_cnt;
+    for (int i = lane; i < p.bin_cnt; i += 32) {
+        part[i] = bins[i];
+        bins[i] = T(0);
+    }
+    __threadfence();
+    __syncwarp();
+    const int64_t ua = v * p.tpv, ub = v * p.tpv + p.tpv - 1;
+    const int gf = p.split.owner(ua), gl = p.split.owner(ub);
+    int ncontrib = 0;
+    for (int gg = gf; gg <= gl; ++gg) ncontrib += p.split.start(gg + 1) > p.split.start(gg);
+    int old = 0;
+    if (lane == 0) old = atomicAdd(&p.counters[v], 1);
+    old = __shfl_sync(FULL, old, 0);
+    if (old == ncontrib - 1) {
+        __threadfence();
+        for (int i = lane; i < p.bin_cnt; i += 32) {
+            T acc = T(0);
+            for (int gg = gf; gg <= gl; ++gg) {
+                int64_t sg = p.split.start(gg);
+                if (p.split.start(gg + 1) <= sg) continue;
+                int sl = 2 * gg + ((sg / p.tpv) == v ? 0 : 1);
+                acc += __ldcg(p.partials + (int64_t)sl * p.bin_cnt + i);
+            }
+            T *yp = p.Y + (p.bin_lo + i) * p.y_es + v * p.y_vs;
+            T r = p.alpha * acc;
+            if (!p.beta_zero) r += p.beta * *yp;
+            *yp = r;
+        }
+        if (lane == 0) p.counters[v] = 0;
+    }
+    __syncwarp();
+}
+
+// U = tiles in flight per warp (nnz == 1 path prefetches their metadata too).
+template <class T, bool VEC, bool NNZ1, int U>
+__global__ void __launch_bounds__(384) compress_contig_kernel(CompressContigParams<T> p) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int warps = blockDim.x >> 5;
+    const int g = blockIdx.x * warps + wib;
+    T *bins = reinterpret_cast<T *>(smem_raw) + (int64_t)wib * p.bin_cnt;
+    for (int i = lane; i < p.bin_cnt; i += 32) bins[i] = T(0);
+    __syncwarp();
+    if (g >= p.split.W) return;
+    const int64_t u0 = p.split.start(g), u1 = p.split.start(g + 1);
+    if (u0 >= u1) return;
+    int64_t v = u0 / p.tpv;
+    int64_t u = u0;
+    while (u < u1) {
+        const int64_t vbeg = v * p.tpv;
+        const int64_t vend = min(u1, vbeg + p.tpv);
+        const T *xv = p.X + v * p.x_ld;
+        for (int64_t k = u - vbeg; k < vend - vbeg; k += U) {
+            T val[U][4];
+            uint32_t mw[U][4];
+#pragma unroll
+            for (int b = 0; b < U; ++b) {
+                const int64_t kk = k + b;
+                const bool tile_ok = kk < vend - vbeg;
+                const int64_t j0 = kk * 128 + lane * 4;
+                load4<T, VEC>(xv, j0, p.L, tile_ok, val[b]);
+                if constexpr (NNZ1) {
+                    if (tile_ok && j0 + 3 < p.L) {
+                        uint4 q = __ldg(reinterpret_cast<const uint4 *>(p.meta + j0));
+                        mw[b][0] = q.x; mw[b][1] = q.y; mw[b][2] = q.z; mw[b][3] = q.w;
+                    } else {
+#pragma unroll
+                        for (int t = 0; t < 4; ++t) mw[b][t] = (tile_ok && j0 + t < p.L) ? __ldg(p.meta + j0 + t) : 0u;
+                    }
+                }
+            }
+#pragma unroll
+            for (int b = 0; b < U; ++b) {
+                const int64_t kk = k + b;
+                const bool tile_ok = kk < vend - vbeg;
+                const int64_t j0 = kk * 128 + lane * 4;
+#pragma unroll
+                for (int t = 0; t < 4; ++t) {
+                    const bool valid = tile_ok && (j0 + t < p.L);
+                    if constexpr (NNZ1) {
+                        bin_add(bins, val[b][t], mw[b][t], valid, p.bin_lo, p.bin_cnt, lane);
+                    } else {
+                        for (int e = 0; e < p.nnz; ++e) {
+                            uint32_t w = valid ? __ldg(p.meta + (j0 + t) * p.nnz + e) : 0u;
+                            bin_add(bins, val[b][t], w, valid, p.bin_lo, p.bin_cnt, lane);
+                        }
+                    }
+                }
+            }
+        }
+        const bool first = (v == u0 / p.tpv);
+        const bool exclusive = (u0 <= vbeg) && (vbeg + p.tpv <= u1);
+        flush_vector(p, bins, g, v, first, exclusive, lane);
+        u = vend;
+        ++v;
+    }
+}
+
+// ---- strided-vector compress: element (k, v) at X[v + k*x_ld]; lane = vector ----------
+template <class T>
+struct CompressStridedParams {
+    const T *X;
+    int64_t x_ld;
+    int64_t L, nv;
+    const int32_t *bucket;
+    const uint8_t *negative;
+    int nnz;
+    int64_t bin_lo;
+    int bin_cnt;
+    T *Y;
+    int64_t y_es, y_vs;
+    T alpha, beta;
+    int beta_zero;
+    T *partials;  // [group][split][bin_cnt][32] when P > 1
+    int64_t klen;
+    int P;
+    int64_t ngroups;
+};
+
+template <class T>
+__global__ void __launch_bounds__(256) compress_strided_kernel(CompressStridedParams<T> p) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int warps = blockDim.x >> 5;
+    const int64_t unit = (int64_t)blockIdx.x * warps + wib;
+    T *bins = reinterpret_cast<T *>(smem_raw) + (int64_t)wib * p.bin_cnt * 32;
+    for (int i = lane; i < p.bin_cnt * 32; i += 32) bins[i] = T(0);
+    __syncwarp();
+    if (unit >= p.ngroups * p.P) return;
+    const int64_t grp = unit / p.P;
+    const int split = (int)(unit % p.P);
+    const int64_t v = grp * 32 + lane;
+    const bool vok = v < p.nv;
+    const int64_t k0 = split * p.klen, k1 = min(p.L, k0 + p.klen);
+    constexpr int UK = 8;
+    for (int64_t k = k0; k < k1; k += UK) {
+        T xs[UK];
+#pragma unroll
+        for (int b = 0; b < UK; ++b) xs[b] = (vok && k + b < k1) ? __ldg(p.X + v + (k + b) * p.x_ld) : T(0);
+#pragma unroll
+        for (int b = 0; b < UK; ++b) {
+            if (k + b >= k1) break;
+            for (int e = 0; e < p.nnz; ++e) {
+                const int64_t idx = (k + b) * p.nnz + e;
+                int bb = __ldg(p.bucket + idx) - (int)p.bin_lo;
+                if ((unsigned)bb < (unsigned)p.bin_cnt) {
+                    T x = __ldg(p.negative + idx) ? -xs[b] : xs[b];
+                    bins[bb * 32 + lane] += x;
+                }
+            }
+        }
+    }
+    __syncwarp();
+    if (p.P == 1) {
+        if (vok)
+            for (int i = 0; i < p.bin_cnt; ++i) {
+                T *yp = p.Y + (p.bin_lo + i) * p.y_es + v * p.y_vs;
+                T r = p.alpha * bins[i * 32 + lane];
+                if (!p.beta_zero) r += p.beta * *yp;
+                *yp = r;
+            }
+    } else {
+        T *part = p.partials + unit * (int64_t)p.bin_cnt * 32;
+        for (int i = 0; i < p.bin_cnt; ++i) part[i * 32 + lane] = bins[i * 32 + lane];
+    }
+}
+
+template <class T>
+__global__ void compress_strided_reduce_kernel(CompressStridedParams<T> p) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t per = (int64_t)p.bin_cnt * 32;
+    if (t >= p.ngroups * per) return;
+    const int64_t grp = t / per;
+    const int64_t rem = t % per;
+    const int i = (int)(rem / 32), lane = (int)(rem % 32);
+    const int64_t v = grp * 32 + lane;
+    if (v >= p.nv) return;
+    T acc = T(0);
+    for (int sp = 0; sp < p.P; ++sp) acc += p.partials[(grp * p.P + sp) * per + rem];
+    T *yp = p.Y + (p.bin_lo + i) * p.y_es + v * p.y_vs;
+    T r = p.alpha * acc;
+    if (!p.beta_zero) r += p.beta * *yp;
+    *yp = r;
+}
+
+// ---- expand: Y(j, v) = alpha * sum_e sign(j,e) * X(bucket(j,e), v) + beta * Y(j, v) ------
+template <class T>
+__global__ void expand_kernel(const T *X, int64_t x_es, int64_t x_vs, int64_t L, int64_t nv,
+                              const int32_t *bucket, const uint8_t *negative, int nnz, T *Y, int64_t y_es,
+                              int64_t y_vs, int out_contig, T alpha, T beta, int beta_zero) {
+    // fast thread index runs along the contiguous output dimension
+    int64_t a = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t b = blockIdx.y * (int64_t)blockDim.y + threadIdx.y;
+    int64_t j = out_contig ? a : b;
+    int64_t v = out_contig ? b : a;
+    for (; (out_contig ? v : j) < (out_contig ? nv : L); ) {
+        if (j < L && v < nv) {
+            T acc = T(0);
+            for (int e = 0; e < nnz; ++e) {
+                const int64_t idx = j * nnz + e;
+                T x = X[(int64_t)bucket[idx] * x_es + v * x_vs];
+                acc += negative[idx] ? -x : x;
+            }
+            T *yp = Y + j * y_es + v * y_vs;
+            T r = alpha * acc;
+            if (!beta_zero) r += beta * *yp;
+            *yp = r;
+        }
+        if (out_contig) v += (int64_t)gridDim.y * blockDim.y;
+        else j += (int64_t)gridDim.y * blockDim.y;
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// host-side launchers
+// ------------------------------------------------------------------------------------
+template <class T>
+int sparse_compress(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_t x_es, int64_t x_vs, int64_t nv,
+                    T *Y, int64_t y_es, int64_t y_vs, double alpha, double beta) {
+    const int64_t L = sk->L, s = sk->s;
+    const size_t es = sizeof(T);
+    const int cap = ctx->smem_optin - 1024;
+    const bool beta_zero = beta == 0.0;
+    const T a = (T)(alpha * sk->scale);
+    if (nv == 0) return RLA_OK;
+    if (x_es == 1) {
+        // contiguous vectors
+        int warps = (int)std::min<int64_t>(12, cap / (int64_t)(s * es));
+        int bin_cnt = (int)s;
+        if (warps < 1) {
+            warps = 4;
+            bin_cnt = (int)(cap / (4 * es));
+        }
+        const int64_t tpv = ceil_div(L, 128);
+        const int64_t total = tpv * nv;
+        const int blocks_per_sm = std::max(1, cap / (int)(warps * bin_cnt * es + 1));
+        int64_t W = (int64_t)ctx->sm_count * blocks_per_sm * warps;
+        W = std::min<int64_t>(W, nv * 32);
+        W = std::min<int64_t>(W, ceil_div(total, 4));
+        W = std::max<int64_t>(W, 1);
+        const int blocks = ceil_div_i(W, warps);
+        const size_t smem = (size_t)warps * bin_cnt * es;
+        void *part = nullptr;
+        int *cnt = nullptr;
+        RLA_TRY(scratch_get(ctx, (size_t)(2 * W) * bin_cnt * es, &part));
+        RLA_TRY(counters_get(ctx, (size_t)nv, &cnt));
+        const bool vec = (x_vs % (16 / es) == 0) && ((uintptr_t)X % 16 == 0);
+        CompressContigParams<T> p{X, x_vs, L, nv, sk->meta, (int)sk->nnz, 0, bin_cnt, Y, y_es, y_vs, a, (T)beta,
+                                  beta_zero, (T *)part, cnt, tpv, Split{total, (int)W}};
+        for (int64_t lo = 0; lo < s; lo += bin_cnt) {
+            p.bin_lo = lo;
+            p.bin_cnt = (int)std::min<int64_t>(bin_cnt, s - lo);
+            auto launch = [&](auto kern) {
+                cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                kern<<<blocks, warps * 32, smem, ctx->stream>>>(p);
+            };
+            if (sk->nnz == 1) {
+                if (vec) launch(compress_contig_kernel<T, true, true, 4>);
+                else launch(compress_contig_kernel<T, false, true, 4>);
+            } else {
+                if (vec) launch(compress_contig_kernel<T, true, false, 2>);
+                else launch(compress_contig_kernel<T, false, false, 2>);
+            }
+            RLA_TRY(check_launch(ctx, "compress_contig"));
+        }
+        return RLA_OK;
+    }
+    // strided vectors (x_vs == 1): lane = vector
+    int warps = 8;
+    int bin_cnt = (int)std::min<int64_t>(s, cap / (int64_t)(warps * 32 * es));
+    if (bin_cnt < 1) return set_error(ctx, RLA_E_UNSUPPORTED, "shared memory too small");
+    if (bin_cnt < s && bin_cnt < 64) {
+        warps = 2;
+        bin_cnt = (int)std::min<int64_t>(s, cap / (int64_t)(warps * 32 * es));
+    }
+    const int64_t ngroups = ceil_div(nv, 32);
+    const int64_t want = (int64_t)ctx->sm_count * 2 * warps;
+    int P = (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(want, ngroups), ceil_div(L, 256)));
+    const int64_t klen = ceil_div(L, P);
+    P = (int)ceil_div(L, klen);
+    const size_t smem = (size_t)warps * bin_cnt * 32 * es;
+    void *part = nullptr;
+    if (P > 1) RLA_TRY(scratch_get(ctx, (size_t)ngroups * P * bin_cnt * 32 * es, &part));
+    CompressStridedParams<T> p{X, x_es, L, nv, sk->bucket, sk->negative, (int)sk->nnz, 0, bin_cnt, Y, y_es, y_vs,
+                               a, (T)beta, beta_zero, (T *)part, klen, P, ngroups};
+    for (int64_t lo = 0; lo < s; lo += bin_cnt) {
+        p.bin_lo = lo;
+        p.bin_cnt = (int)std::min<int64_t>(bin_cnt, s - lo);
+        const int64_t units = ngroups * P;
+        cudaFuncSetAttribute(compress_strided_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        compress_strided_kernel<T><<<ceil_div_i(units, warps), warps * 32, smem, ctx->stream>>>(p);
+        RLA_TRY(check_launch(ctx, "compress_strided"));
+        if (P > 1) {
+            const int64_t n = ngroups * (int64_t)p.bin_cnt * 32;
+            compress_strided_reduce_kernel<T><<<ceil_div_i(n, 256), 256, 0, ctx->stream>>>(p);
+            RLA_TRY(check_launch(ctx, "compress_strided_reduce"));
+        }
+    }
+    return RLA_OK;
+}
+
+template <class T>
+int sparse_expand(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_t x_es, int64_t x_vs, int64_t nv, T *Y,
+                  int64_t y_es, int64_t y_vs, double alpha, double beta) {
+    if (nv == 0) return RLA_OK;
+    const int64_t L = sk->L;
+    const int out_contig = y_es == 1;
+    const int64_t fast = out_contig ? L : nv, slow = out_contig ? nv : L;
+    dim3 block(128, 2);
+    dim3 grid(ceil_div_i(fast, 128), (unsigned)std::min<int64_t>(ceil_div(slow, 2), 65535));
+    expand_kernel<T><<<grid, block, 0, ctx->stream>>>(X, x_es, x_vs, L, nv, sk->bucket, sk->negative, (int)sk->nnz, Y,
+                                                      y_es, y_vs, out_contig, (T)(alpha * sk->scale), (T)beta,
+                                                      beta == 0.0);
+    return check_launch(ctx, "sparse_expand");
+}
+
+template int sparse_compress<float>(rla_ctx *, const rla_sketch *, const float *, int64_t, int64_t, int64_t, float *,
+                                    int64_t, int64_t, double, double);
+template int sparse_compress<double>(rla_ctx *, const rla_sketch *, const double *, int64_t, int64_t, int64_t,
+                                     double *, int64_t, int64_t, double, double);
+template int sparse_expand<float>(rla_ctx *, const rla_sketch *, const float *, int64_t, int64_t, int64_t, float *,
+                                  int64_t, int64_t, double, double);
+template int sparse_expand<double>(rla_ctx *, const rla_sketch *, const double *, int64_t, int64_t, int64_t, double *,
+                                   int64_t, int64_t, double, double);
+
+}  // namespace rla
