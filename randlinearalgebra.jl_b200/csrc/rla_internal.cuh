@@ -170,6 +170,30 @@ struct Vec4<double> {
 
 inline size_t dtype_size(int dtype) { return dtype == RLA_F64 ? 8 : 4; }
 
+// Contiguous split of `total` work units over W workers (stream-K style): worker g owns
+// [start(g), start(g+1)); the first `rem` workers take base+1 units, the rest base.
+struct Split {
+    int64_t total = 0, base = 0, rem = 0;
+    int W = 1;
+    static Split make(int64_t total, int W) {
+        Split s;
+        s.total = total;
+        s.W = W;
+        s.base = total / W;
+        s.rem = total % W;
+        return s;
+    }
+    __host__ __device__ int64_t start(int g) const { return (int64_t)g * base + (g < rem ? g : rem); }
+    __host__ __device__ int owner(int64_t u) const {
+        const int64_t cut = rem * (base + 1);
+        if (u < cut) return (int)(u / (base + 1));
+        return (int)(rem + (u - cut) / base);  // base >= 1 whenever u >= cut
+    }
+    // Partial-sum slot of worker g for a segment [vbeg, vbeg+len) it shares: a worker's
+    // first segment uses slot 2g, its last (when it started in an earlier segment) 2g+1.
+    __host__ __device__ int slot(int g, int64_t vbeg) const { return 2 * g + (start(g) < vbeg ? 1 : 0); }
+};
+
 }  // namespace rla
 
 // ------------------------------------------------------------------------------------
@@ -193,6 +217,7 @@ struct rla_sketch {
     // SRHT
     int32_t *rows = nullptr;       // [s] sampled padded rows (op)
     uint32_t *signbits = nullptr;  // [ceil(N/32)] bit r = 1 means +1
+    uint4 *sign_tl = nullptr;      // fused compress kernel: per (chunk, thread) 128 sign bits in register order
     int32_t *p2_ptr = nullptr;     // expand tables: per low-bit position, samples sorted
     int32_t *p2_list = nullptr;
     int64_t chunk = 0;             // WHT chunk length used by the expand tables

@@ -21,6 +21,8 @@ int sparse_expand(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_t x_es, 
                   int64_t y_es, int64_t y_vs, double alpha, double beta);
 
 // SRHT / FJLT (rla_wht.cu)
+// Builds sk->sign_tl (per-thread sign masks of the fused compress kernel) from sk->signbits.
+int build_srht_sign_table(rla_ctx *ctx, rla_sketch *sk);
 template <class T>
 int srht_compress(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_t x_es, int64_t x_vs, int64_t nv, T *Y,
                   int64_t y_es, int64_t y_vs, double alpha, double beta);
@@ -44,6 +46,10 @@ int gemm(rla_ctx *ctx, int64_t M, int64_t N, int64_t K, const TA *A, int64_t lda
 // added to the diagonal first.  *breakdown (device int) is set to 1 when a pivot is not
 // positive.
 int cholesky_upper(rla_ctx *ctx, double *G, int64_t l, double shift, int *breakdown);
+// Explicit Q (in place, m x l, ld ldy) of LAPACK-style Householder QR (dgeqr2 + dorg2r);
+// tau holds l doubles of workspace.
+template <class T>
+int householder_q(rla_ctx *ctx, T *Y, int64_t m, int64_t l, int64_t ldy, double *tau);
 // Rinv = R^{-1} for upper-triangular R (l x l, ld l).
 int tri_inv_upper(rla_ctx *ctx, const double *R, int64_t l, double *Rinv);
 // One-sided Jacobi on X (l x l, ld l) with accumulated rotations J (initialised to I):

@@ -176,6 +176,93 @@ __global__ void __launch_bounds__(1024) jacobi_kernel(double *X, double *J, doub
     for (int64_t c = tid; c < l; c += nt) sigma[c] = sg[perm[c]];
 }
 
+// ---- Householder QR with LAPACK's conventions (dgeqr2 + dlarfg + dorg2r) --------------
+// Used when CholeskyQR breaks down (numerically rank-deficient blocks, e.g. a compression
+// dimension above rank(A)); the explicit Q it forms has LAPACK's column signs.
+__device__ inline double block_sum(double v, double *red) {
+    v = warp_sum(v);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    __syncthreads();
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    double t = threadIdx.x < nw ? red[threadIdx.x] : 0.0;
+    if (warp == 0) t = warp_sum(t);
+    if (threadIdx.x == 0) red[0] = t;
+    __syncthreads();
+    return red[0];
+}
+
+// dlarfg on column k of Y: v stored below the diagonal, beta on the diagonal.
+template <class T>
+__global__ void __launch_bounds__(1024) house_reflector_kernel(T *Y, int64_t m, int64_t ldy, int64_t k, double *tau) {
+    __shared__ double red[32];
+    T *col = Y + k * ldy;
+    double ss = 0.0;
+    for (int64_t i = k + 1 + threadIdx.x; i < m; i += blockDim.x) {
+        const double x = (double)col[i];
+        ss += x * x;
+    }
+    ss = block_sum(ss, red);
+    const double alpha = (double)col[k];
+    if (ss == 0.0) {
+        if (threadIdx.x == 0) tau[k] = 0.0;
+        return;
+    }
+    const double beta = -copysign(sqrt(alpha * alpha + ss), alpha);
+    const double sc = 1.0 / (alpha - beta);
+    for (int64_t i = k + 1 + threadIdx.x; i < m; i += blockDim.x) col[i] = (T)((double)col[i] * sc);
+    if (threadIdx.x == 0) {
+        tau[k] = (beta - alpha) / beta;
+        col[k] = (T)beta;
+    }
+}
+
+// Apply H = I - tau v v' (v_k = 1, v below the diagonal of column k of V) to columns
+// j0.. of X from the left, rows k..m-1.  One block per column.
+template <class T>
+__global__ void __launch_bounds__(1024) house_apply_kernel(const T *V, T *X, int64_t m, int64_t ld, int64_t k,
+                                                           int64_t j0, const double *tau) {
+    __shared__ double red[32];
+    const double t = tau[k];
+    if (t == 0.0) return;
+    const int64_t j = j0 + blockIdx.x;
+    const T *v = V + k * ld;
+    T *x = X + j * ld;
+    double w = 0.0;
+    for (int64_t i = k + threadIdx.x; i < m; i += blockDim.x) w += (i == k ? 1.0 : (double)v[i]) * (double)x[i];
+    w = block_sum(w, red) * t;
+    for (int64_t i = k + threadIdx.x; i < m; i += blockDim.x) x[i] = (T)((double)x[i] - w * (i == k ? 1.0 : (double)v[i]));
+}
+
+// dorg2r step for column i (after H(i) was applied to the columns to its right).
+template <class T>
+__global__ void house_form_col_kernel(T *Y, int64_t m, int64_t ld, int64_t i, const double *tau) {
+    const double t = tau[i];
+    T *col = Y + i * ld;
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < m; r += (int64_t)gridDim.x * blockDim.x) {
+        if (r < i) col[r] = T(0);
+        else if (r == i) col[r] = (T)(1.0 - t);
+        else col[r] = (T)(-t * (double)col[r]);
+    }
+}
+
+template <class T>
+int householder_q(rla_ctx *ctx, T *Y, int64_t m, int64_t l, int64_t ldy, double *tau) {
+    for (int64_t k = 0; k < l; ++k) {
+        house_reflector_kernel<T><<<1, 1024, 0, ctx->stream>>>(Y, m, ldy, k, tau);
+        if (k + 1 < l) house_apply_kernel<T><<<(unsigned)(l - k - 1), 1024, 0, ctx->stream>>>(Y, Y, m, ldy, k, k + 1, tau);
+    }
+    RLA_TRY(check_launch(ctx, "householder_qr"));
+    for (int64_t i = l - 1; i >= 0; --i) {
+        if (i + 1 < l) house_apply_kernel<T><<<(unsigned)(l - i - 1), 1024, 0, ctx->stream>>>(Y, Y, m, ldy, i, i + 1, tau);
+        house_form_col_kernel<T><<<ceil_div_i(m, 256) < 1024 ? ceil_div_i(m, 256) : 1024, 256, 0, ctx->stream>>>(Y, m, ldy, i, tau);
+    }
+    return check_launch(ctx, "householder_org2r");
+}
+
+template int householder_q<float>(rla_ctx *, float *, int64_t, int64_t, int64_t, double *);
+template int householder_q<double>(rla_ctx *, double *, int64_t, int64_t, int64_t, double *);
+
 int cholesky_upper(rla_ctx *ctx, double *G, int64_t l, double shift, int *breakdown) {
     chol_upper_kernel<<<1, 1024, 0, ctx->stream>>>(G, l, shift, breakdown);
     return check_launch(ctx, "chol_upper");

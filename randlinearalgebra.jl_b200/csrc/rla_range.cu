@@ -124,8 +124,12 @@ static int orth(rla_ctx *ctx, T *Y, int64_t rows, int64_t l, int64_t ldy, OrthWo
         int bad = 0;
         RLA_CUDA_TRY(ctx, cudaMemcpyAsync(&bad, w.flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
         RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+        if (bad && shifted_done) {
+            // numerically rank-deficient block: Householder QR gives an orthonormal basis
+            // (and LAPACK's Q) whatever the rank
+            return householder_q<T>(ctx, Y, rows, l, ldy, w.diag);
+        }
         if (bad) {
-            if (shifted_done) return set_error(ctx, RLA_E_NUMERIC, "CholeskyQR breakdown persists after the shift");
             // Shifted CholeskyQR: on the equilibrated Gram matrix (unit diagonal, so
             // ||Y D||_F^2 = l) the shift is 11 (rows*l + l(l+1)) u ||Y D||_2^2 <= ... * l.
             RLA_TRY((gemm<T, T, double, double>(ctx, l, l, rows, Y, ldy, 1, Y, ldy, 0, w.G, l, 1.0, 0.0)));
@@ -135,7 +139,7 @@ static int orth(rla_ctx *ctx, T *Y, int64_t rows, int64_t l, int64_t ldy, OrthWo
             RLA_TRY(cholesky_upper(ctx, w.G, l, shift, w.flag));
             RLA_CUDA_TRY(ctx, cudaMemcpyAsync(&bad, w.flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
             RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-            if (bad) return set_error(ctx, RLA_E_NUMERIC, "shifted CholeskyQR broke down (rank-deficient block)");
+            if (bad) return householder_q<T>(ctx, Y, rows, l, ldy, w.diag);
             shifted_done = true;
             passes = pass + 3;  // shifted pass followed by two plain passes
         }

@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "rla_internal.cuh"
+#include "rla_kernels.cuh"
 
 namespace rla {
 
@@ -83,8 +84,9 @@ __global__ void build_meta_kernel(const int32_t *bucket, const uint8_t *negative
     unsigned key = valid ? b : (0x80000000u | (unsigned)lane);
     unsigned grp = __match_any_sync(FULL, key);
     if (valid) {
+        // tile-blocked layout: for each (tile, e) the 128 words of the tile are contiguous
         uint32_t dup = __popc(grp) > 1 ? 1u : 0u;
-        meta[j * nnz + e] = b | (dup << 30) | ((uint32_t)negative[j * nnz + e] << 31);
+        meta[(tile * nnz + e) * 128 + 4 * lane + t] = b | (dup << 30) | ((uint32_t)negative[j * nnz + e] << 31);
     }
 }
 
@@ -310,6 +312,7 @@ static int draw(rla_ctx *ctx, rla_sketch *sk) {
             draw_rows_kernel<<<1, 256, use_smem ? bm_bytes : 0, ctx->stream>>>(rng, sk->N, sk->s, gbm, use_smem, sk->rows);
             RLA_TRY(check_launch(ctx, "draw_rows"));
             RLA_TRY(srht_tables(ctx, sk));
+            RLA_TRY(build_srht_sign_table(ctx, sk));
         } else {
             if (sk->p.dtype == RLA_F32) {
                 RLA_TRY(fjlt_build<float>(ctx, sk, rng));
@@ -334,7 +337,7 @@ static int draw(rla_ctx *ctx, rla_sketch *sk) {
 }
 
 static void free_sketch_buffers(rla_sketch *sk) {
-    void *ptrs[] = {sk->bucket, sk->negative, sk->meta, sk->rows, sk->signbits, sk->p2_ptr, sk->p2_list,
+    void *ptrs[] = {sk->bucket, sk->negative, sk->meta, sk->rows, sk->signbits, sk->sign_tl, sk->p2_ptr, sk->p2_list,
                     sk->k_ptr, sk->k_col, sk->k_val, sk->kt_ptr, sk->kt_row, sk->kt_val, sk->dense};
     for (void *p : ptrs)
         if (p) cudaFree(p);
@@ -400,7 +403,7 @@ int rla_sketch_create(rla_ctx *ctx, const rla_sketch_params *pp, rla_sketch **ou
             size_t ne = (size_t)(sk->L * sk->nnz);
             alloc((void **)&sk->bucket, ne * 4);
             alloc((void **)&sk->negative, ne);
-            alloc((void **)&sk->meta, ne * 4);
+            alloc((void **)&sk->meta, (size_t)ceil_div(sk->L, 128) * 128 * sk->nnz * 4);
             break;
         }
         case RLA_SRHT:
@@ -580,6 +583,7 @@ int rla_sketch_set_draws(rla_ctx *ctx, rla_sketch *sk, const int64_t *idx, const
             }
             RLA_CUDA_TRY(ctx, cudaMemcpy(sk->rows, r.data(), sk->s * 4, cudaMemcpyHostToDevice));
             RLA_TRY(srht_tables(ctx, sk));
+            RLA_TRY(build_srht_sign_table(ctx, sk));
         } else {
             if (!idx || !vals || !kptr) return set_error(ctx, RLA_E_ARG, "FJLT draws need op.colptr, op.rowval and op.nzval.");
             bool left = sk->p.card == RLA_LEFT;

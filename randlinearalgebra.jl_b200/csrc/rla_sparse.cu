@@ -20,19 +20,6 @@
 
 namespace rla {
 
-struct Split {  // contiguous split of `total` units over W workers
-    int64_t total;
-    int W;
-    __host__ __device__ int64_t start(int g) const { return (int64_t)((__int128)g * total / W); }
-    __device__ int owner(int64_t u) const {
-        int g = (int)((__int128)u * W / total);
-        if (g >= W) g = W - 1;
-        while (g + 1 < W && start(g + 1) <= u) ++g;
-        while (g > 0 && start(g) > u) --g;
-        return g;
-    }
-};
-
 template <class T>
 struct CompressContigParams {
     const T *X;
@@ -52,27 +39,42 @@ struct CompressContigParams {
     Split split;
 };
 
+// Sub-round with colliding buckets: lanes sharing a bucket are summed in lane order and
+// the lowest lane adds the sum (rare for s >> 32, hence kept out of line).
 template <class T>
-__device__ __forceinline__ void bin_add(T *bins, T x, uint32_t w, bool valid, int64_t bin_lo, int bin_cnt, int lane) {
-    int b = (int)(w & 0x3fffffffu) - (int)bin_lo;
-    bool inwin = valid && (unsigned)b < (unsigned)bin_cnt;
-    if (w >> 31) x = -x;
-    bool dup = inwin && ((w >> 30) & 1u);
-    if (__any_sync(FULL, dup)) {
-        unsigned key = inwin ? (unsigned)b : (0x80000000u | (unsigned)lane);
-        unsigned grp = __match_any_sync(FULL, key);
-        int cnt = __popc(grp);
-        int maxc = (int)__reduce_max_sync(FULL, (unsigned)cnt);
-        T sum = T(0);
-        for (int q = 0; q < maxc; ++q) {
-            int src = q < cnt ? (int)__fns(grp, 0, q + 1) : lane;
-            T y = __shfl_sync(FULL, x, src);
-            if (q < cnt) sum += y;
-        }
-        if (inwin && (grp & ((1u << lane) - 1u)) == 0u) bins[b] += sum;
-    } else if (inwin) {
-        bins[b] += x;
+__device__ __noinline__ void bin_add_collide(T *bins, T x, int b, bool inwin, int lane) {
+    const unsigned key = inwin ? (unsigned)b : (0x80000000u | (unsigned)lane);
+    const unsigned grp = __match_any_sync(FULL, key);
+    const int cnt = __popc(grp);
+    const int maxc = (int)__reduce_max_sync(FULL, (unsigned)cnt);
+    T sum = T(0);
+    for (int q = 0; q < maxc; ++q) {
+        const int src = q < cnt ? (int)__fns(grp, 0, q + 1) : lane;
+        const T y = __shfl_sync(FULL, x, src);
+        if (q < cnt) sum += y;
     }
+    if (inwin && (grp & ((1u << lane) - 1u)) == 0u) bins[b] += sum;
+}
+
+// One sub-round: lane adds +-x to bin (w & 0x3fffffff) - bin_lo.  The sign is bit 31 of w
+// (applied as an XOR on the sign bit), bit 30 flags a bucket shared with another lane of
+// the same sub-round.
+template <class T, bool WIN>
+__device__ __forceinline__ void bin_add(T *bins, T x, uint32_t w, bool valid, int64_t bin_lo, int bin_cnt, int lane) {
+    int b = (int)(w & 0x3fffffffu);
+    bool inwin = valid;
+    if constexpr (WIN) {
+        b -= (int)bin_lo;
+        inwin = valid && (unsigned)b < (unsigned)bin_cnt;
+    }
+    if constexpr (sizeof(T) == 4) {
+        x = __uint_as_float(__float_as_uint(x) ^ (w & 0x80000000u));
+    } else {
+        x = __longlong_as_double(__double_as_longlong(x) ^ ((long long)(w & 0x80000000u) << 32));
+    }
+    const bool dup = inwin && ((w >> 30) & 1u);
+    if (__any_sync(FULL, dup)) bin_add_collide(bins, x, b, inwin, lane);
+    else if (inwin) bins[b] += x;
     __syncwarp();
 }
 
@@ -94,8 +96,7 @@ __device__ __forceinline__ void load4(const T *xv, int64_t j0, int64_t L, bool t
 }
 
 template <class T>
-__device__ void flush_vector(const CompressContigParams<T> &p, T *bins, int g, int64_t v, bool first_of_warp,
-                             bool exclusive, int lane) {
+__device__ void flush_vector(const CompressContigParams<T> &p, T *bins, int g, int64_t v, bool exclusive, int lane) {
     __syncwarp();
     if (exclusive) {
         for (int i = lane; i < p.bin_cnt; i += 32) {
@@ -108,31 +109,24 @@ __device__ void flush_vector(const CompressContigParams<T> &p, T *bins, int g, i
         __syncwarp();
         return;
     }
-    int slot = 2 * g + (first_of_warp ? 0 : 1);
-    T *part = p.partials + (int64_t)slot * p.bin_cnt;
+    const int64_t vbeg = v * p.tpv;
+    T *part = p.partials + (int64_t)p.split.slot(g, vbeg) * p.bin_cnt;
     for (int i = lane; i < p.bin_cnt; i += 32) {
         part[i] = bins[i];
         bins[i] = T(0);
     }
     __threadfence();
     __syncwarp();
-    const int64_t ua = v * p.tpv, ub = v * p.tpv + p.tpv - 1;
-    const int gf = p.split.owner(ua), gl = p.split.owner(ub);
-    int ncontrib = 0;
-    for (int gg = gf; gg <= gl; ++gg) ncontrib += p.split.start(gg + 1) > p.split.start(gg);
+    const int gf = p.split.owner(vbeg), gl = p.split.owner(vbeg + p.tpv - 1);
     int old = 0;
     if (lane == 0) old = atomicAdd(&p.counters[v], 1);
     old = __shfl_sync(FULL, old, 0);
-    if (old == ncontrib - 1) {
+    if (old == gl - gf) {
         __threadfence();
+        const T *p0 = p.partials + (int64_t)p.split.slot(gf, vbeg) * p.bin_cnt;
         for (int i = lane; i < p.bin_cnt; i += 32) {
-            T acc = T(0);
-            for (int gg = gf; gg <= gl; ++gg) {
-                int64_t sg = p.split.start(gg);
-                if (p.split.start(gg + 1) <= sg) continue;
-                int sl = 2 * gg + ((sg / p.tpv) == v ? 0 : 1);
-                acc += __ldcg(p.partials + (int64_t)sl * p.bin_cnt + i);
-            }
+            T acc = __ldcg(p0 + i);
+            for (int gg = gf + 1; gg <= gl; ++gg) acc += __ldcg(p.partials + (int64_t)(2 * gg) * p.bin_cnt + i);
             T *yp = p.Y + (p.bin_lo + i) * p.y_es + v * p.y_vs;
             T r = p.alpha * acc;
             if (!p.beta_zero) r += p.beta * *yp;
@@ -143,9 +137,51 @@ __device__ void flush_vector(const CompressContigParams<T> &p, T *bins, int g, i
     __syncwarp();
 }
 
-// U = tiles in flight per warp (nnz == 1 path prefetches their metadata too).
-template <class T, bool VEC, bool NNZ1, int U>
+// One 128-element tile of vector xv: lane holds elements 4*lane .. 4*lane+3; metadata
+// for entry e of the tile's elements is the contiguous block meta[(tile*nnz + e)*128 ...].
+template <class T, bool VEC, bool WIN, bool CHECK>
+__device__ __forceinline__ void do_tile(const CompressContigParams<T> &p, T *bins, const T *xv, int64_t kk,
+                                        int lane) {
+    const int64_t j0 = kk * 128 + lane * 4;
+    T val[4];
+    load4<T, VEC>(xv, j0, p.L, true, val);
+    for (int e = 0; e < p.nnz; ++e) {
+        const uint32_t *mp = p.meta + (kk * p.nnz + e) * 128 + lane * 4;
+        uint32_t mw[4];
+        if (!CHECK || j0 + 3 < p.L) {
+            const uint4 q = __ldg(reinterpret_cast<const uint4 *>(mp));
+            mw[0] = q.x; mw[1] = q.y; mw[2] = q.z; mw[3] = q.w;
+        } else {
+#pragma unroll
+            for (int t = 0; t < 4; ++t) mw[t] = (j0 + t < p.L) ? __ldg(mp + t) : 0u;
+        }
+#pragma unroll
+        for (int t = 0; t < 4; ++t) bin_add<T, WIN>(bins, val[t], mw[t], !CHECK || (j0 + t < p.L), p.bin_lo, p.bin_cnt, lane);
+    }
+}
+
+// U full tiles in flight per warp (CountSketch path: data and metadata prefetched).
+template <class T, bool VEC, bool WIN, int U>
+__device__ __forceinline__ void do_tiles_nnz1(const CompressContigParams<T> &p, T *bins, const T *xv, int64_t kk,
+                                              int lane) {
+    T val[U][4];
+    uint32_t mw[U][4];
+#pragma unroll
+    for (int b = 0; b < U; ++b) {
+        const int64_t j0 = (kk + b) * 128 + lane * 4;
+        load4<T, VEC>(xv, j0, p.L, true, val[b]);
+        const uint4 q = __ldg(reinterpret_cast<const uint4 *>(p.meta + j0));
+        mw[b][0] = q.x; mw[b][1] = q.y; mw[b][2] = q.z; mw[b][3] = q.w;
+    }
+#pragma unroll
+    for (int b = 0; b < U; ++b)
+#pragma unroll
+        for (int t = 0; t < 4; ++t) bin_add<T, WIN>(bins, val[b][t], mw[b][t], true, p.bin_lo, p.bin_cnt, lane);
+}
+
+template <class T, bool VEC, bool WIN, bool NNZ1>
 __global__ void __launch_bounds__(384) compress_contig_kernel(CompressContigParams<T> p) {
+    constexpr int U = 4;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
@@ -157,54 +193,23 @@ __global__ void __launch_bounds__(384) compress_contig_kernel(CompressContigPara
     if (g >= p.split.W) return;
     const int64_t u0 = p.split.start(g), u1 = p.split.start(g + 1);
     if (u0 >= u1) return;
+    const int64_t full_tiles = p.L / 128;  // tiles with all 128 elements inside the vector
     int64_t v = u0 / p.tpv;
     int64_t u = u0;
     while (u < u1) {
         const int64_t vbeg = v * p.tpv;
-        const int64_t vend = min(u1, vbeg + p.tpv);
+        const int64_t kend = min(u1, vbeg + p.tpv) - vbeg;
         const T *xv = p.X + v * p.x_ld;
-        for (int64_t k = u - vbeg; k < vend - vbeg; k += U) {
-            T val[U][4];
-            uint32_t mw[U][4];
-#pragma unroll
-            for (int b = 0; b < U; ++b) {
-                const int64_t kk = k + b;
-                const bool tile_ok = kk < vend - vbeg;
-                const int64_t j0 = kk * 128 + lane * 4;
-                load4<T, VEC>(xv, j0, p.L, tile_ok, val[b]);
-                if constexpr (NNZ1) {
-                    if (tile_ok && j0 + 3 < p.L) {
-                        uint4 q = __ldg(reinterpret_cast<const uint4 *>(p.meta + j0));
-                        mw[b][0] = q.x; mw[b][1] = q.y; mw[b][2] = q.z; mw[b][3] = q.w;
-                    } else {
-#pragma unroll
-                        for (int t = 0; t < 4; ++t) mw[b][t] = (tile_ok && j0 + t < p.L) ? __ldg(p.meta + j0 + t) : 0u;
-                    }
-                }
-            }
-#pragma unroll
-            for (int b = 0; b < U; ++b) {
-                const int64_t kk = k + b;
-                const bool tile_ok = kk < vend - vbeg;
-                const int64_t j0 = kk * 128 + lane * 4;
-#pragma unroll
-                for (int t = 0; t < 4; ++t) {
-                    const bool valid = tile_ok && (j0 + t < p.L);
-                    if constexpr (NNZ1) {
-                        bin_add(bins, val[b][t], mw[b][t], valid, p.bin_lo, p.bin_cnt, lane);
-                    } else {
-                        for (int e = 0; e < p.nnz; ++e) {
-                            uint32_t w = valid ? __ldg(p.meta + (j0 + t) * p.nnz + e) : 0u;
-                            bin_add(bins, val[b][t], w, valid, p.bin_lo, p.bin_cnt, lane);
-                        }
-                    }
-                }
-            }
+        int64_t k = u - vbeg;
+        const int64_t kfull = min(kend, full_tiles);
+        if constexpr (NNZ1) {
+            for (; k + U <= kfull; k += U) do_tiles_nnz1<T, VEC, WIN, U>(p, bins, xv, k, lane);
         }
-        const bool first = (v == u0 / p.tpv);
+        for (; k < kfull; ++k) do_tile<T, VEC, WIN, false>(p, bins, xv, k, lane);
+        for (; k < kend; ++k) do_tile<T, VEC, WIN, true>(p, bins, xv, k, lane);
         const bool exclusive = (u0 <= vbeg) && (vbeg + p.tpv <= u1);
-        flush_vector(p, bins, g, v, first, exclusive, lane);
-        u = vend;
+        flush_vector(p, bins, g, v, exclusive, lane);
+        u = vbeg + kend;
         ++v;
     }
 }
@@ -349,7 +354,7 @@ int sparse_compress(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_t x_es
         const int64_t total = tpv * nv;
         const int blocks_per_sm = std::max(1, cap / (int)(warps * bin_cnt * es + 1));
         int64_t W = (int64_t)ctx->sm_count * blocks_per_sm * warps;
-        W = std::min<int64_t>(W, nv * 32);
+        W = std::min<int64_t>(W, nv * 8);
         W = std::min<int64_t>(W, ceil_div(total, 4));
         W = std::max<int64_t>(W, 1);
         const int blocks = ceil_div_i(W, warps);
@@ -360,7 +365,7 @@ int sparse_compress(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_t x_es
         RLA_TRY(counters_get(ctx, (size_t)nv, &cnt));
         const bool vec = (x_vs % (16 / es) == 0) && ((uintptr_t)X % 16 == 0);
         CompressContigParams<T> p{X, x_vs, L, nv, sk->meta, (int)sk->nnz, 0, bin_cnt, Y, y_es, y_vs, a, (T)beta,
-                                  beta_zero, (T *)part, cnt, tpv, Split{total, (int)W}};
+                                  beta_zero, (T *)part, cnt, tpv, Split::make(total, (int)W)};
         for (int64_t lo = 0; lo < s; lo += bin_cnt) {
             p.bin_lo = lo;
             p.bin_cnt = (int)std::min<int64_t>(bin_cnt, s - lo);
@@ -368,13 +373,17 @@ int sparse_compress(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_t x_es
                 cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
                 kern<<<blocks, warps * 32, smem, ctx->stream>>>(p);
             };
-            if (sk->nnz == 1) {
-                if (vec) launch(compress_contig_kernel<T, true, true, 4>);
-                else launch(compress_contig_kernel<T, false, true, 4>);
+            const bool win = p.bin_cnt < s;
+            const bool n1 = sk->nnz == 1;
+#define RLA_CC(V, W, N) launch(compress_contig_kernel<T, V, W, N>)
+            if (vec) {
+                if (win) { if (n1) RLA_CC(true, true, true); else RLA_CC(true, true, false); }
+                else { if (n1) RLA_CC(true, false, true); else RLA_CC(true, false, false); }
             } else {
-                if (vec) launch(compress_contig_kernel<T, true, false, 2>);
-                else launch(compress_contig_kernel<T, false, false, 2>);
+                if (win) { if (n1) RLA_CC(false, true, true); else RLA_CC(false, true, false); }
+                else { if (n1) RLA_CC(false, false, true); else RLA_CC(false, false, false); }
             }
+#undef RLA_CC
             RLA_TRY(check_launch(ctx, "compress_contig"));
         }
         return RLA_OK;

@@ -20,19 +20,6 @@
 
 namespace rla {
 
-struct SplitB {
-    int64_t total;
-    int W;
-    __host__ __device__ int64_t start(int g) const { return (int64_t)((__int128)g * total / W); }
-    __device__ int owner(int64_t u) const {
-        int g = (int)((__int128)u * W / total);
-        if (g >= W) g = W - 1;
-        while (g + 1 < W && start(g + 1) <= u) ++g;
-        while (g > 0 && start(g) > u) --g;
-        return g;
-    }
-};
-
 template <class T>
 struct WhtCfg;
 template <>
@@ -44,27 +31,65 @@ struct WhtCfg<double> {
     static constexpr int TB = 6, VB = 1;
 };
 
-template <int TB, class T>
-__device__ __forceinline__ void wht_regs(T (&r)[1 << TB]) {
-#pragma unroll
-    for (int h = 0; h < TB; ++h) {
-#pragma unroll
-        for (int q = 0; q < (1 << TB); ++q) {
-            if (!(q & (1 << h))) {
-                T a = r[q], b = r[q | (1 << h)];
-                r[q] = a + b;
-                r[q | (1 << h)] = a - b;
-            }
-        }
+// Register storage of one thread's 2^TB chunk elements.  FP32 values live in float2
+// pairs so that the butterflies over every register-index bit but the lowest use the
+// packed sm_100 FP32x2 instructions (a+b as fadd2, a-b as ffma2(b, -1, a), both exact
+// to one rounding like the scalar forms).
+template <class T, int TB>
+struct Regs;
+
+template <int TB>
+struct Regs<float, TB> {
+    float2 d[(1 << TB) / 2];
+    __device__ __forceinline__ float get(int q) const { return (q & 1) ? d[q >> 1].y : d[q >> 1].x; }
+    __device__ __forceinline__ void set(int q, float v) {
+        if (q & 1) d[q >> 1].y = v;
+        else d[q >> 1].x = v;
     }
-}
+    __device__ __forceinline__ void wht() {
+#pragma unroll
+        for (int p = 0; p < (1 << TB) / 2; ++p) {
+            const float a = d[p].x, b = d[p].y;
+            d[p].x = a + b;
+            d[p].y = a - b;
+        }
+        const float2 m1 = make_float2(-1.f, -1.f);
+#pragma unroll
+        for (int h = 0; h < TB - 1; ++h)
+#pragma unroll
+            for (int p = 0; p < (1 << TB) / 2; ++p)
+                if (!(p & (1 << h))) {
+                    const float2 a = d[p], b = d[p | (1 << h)];
+                    d[p] = __fadd2_rn(a, b);
+                    d[p | (1 << h)] = __ffma2_rn(b, m1, a);
+                }
+    }
+};
+
+template <int TB>
+struct Regs<double, TB> {
+    double d[1 << TB];
+    __device__ __forceinline__ double get(int q) const { return d[q]; }
+    __device__ __forceinline__ void set(int q, double v) { d[q] = v; }
+    __device__ __forceinline__ void wht() {
+#pragma unroll
+        for (int h = 0; h < TB; ++h)
+#pragma unroll
+            for (int q = 0; q < (1 << TB); ++q)
+                if (!(q & (1 << h))) {
+                    const double a = d[q], b = d[q | (1 << h)];
+                    d[q] = a + b;
+                    d[q | (1 << h)] = a - b;
+                }
+    }
+};
 
 template <class T>
 struct SrhtParams {
     const T *X;
     int64_t x_ld;  // element (j, v) at X[j + v*x_ld]
     int64_t L, N;
-    const uint32_t *signbits;
+    const uint4 *sign_tl;  // per (chunk, thread): sign bits in pass-A register order
     const int32_t *rows;
     int64_t s_lo;
     int s_cnt;
@@ -75,7 +100,7 @@ struct SrhtParams {
     T *partials;
     int *counters;
     int64_t cpv;  // chunks per column
-    SplitB split;
+    Split split;
 };
 
 // Position of chunk element e in the swizzled shared buffer: the low 3 bits of the
@@ -87,97 +112,132 @@ __device__ __forceinline__ int swz(int e) {
     return (f << VB) | (e & ((1 << VB) - 1));
 }
 
+template <class T>
+__device__ __forceinline__ T flip(T x, uint32_t keep) {
+    if constexpr (sizeof(T) == 4) {
+        return __uint_as_float(__float_as_uint(x) ^ ((~keep & 1u) << 31));
+    } else {
+        return keep & 1u ? x : -x;
+    }
+}
+
+// Pass-A loads of chunk c of column xv: thread t holds elements (t << VB) + (k << (VB+TB)) + i.
+template <class T, bool VEC, int TB, int VB>
+__device__ __forceinline__ void load_chunk(const T *__restrict__ xv, int64_t cbase, int64_t L, int t,
+                                           Regs<T, TB> &r) {
+    constexpr int VW = 1 << VB, KV = 1 << (TB - VB);
+#pragma unroll
+    for (int k = 0; k < KV; ++k) {
+        const int64_t e0 = cbase + ((int64_t)t << VB) + ((int64_t)k << (VB + TB));
+        if (VEC && e0 + VW <= L) {
+            if constexpr (sizeof(T) == 4) {
+                const float4 q = __ldg(reinterpret_cast<const float4 *>(xv + e0));
+                r.d[2 * k] = make_float2(q.x, q.y);
+                r.d[2 * k + 1] = make_float2(q.z, q.w);
+            } else {
+                const double2 q = __ldg(reinterpret_cast<const double2 *>(xv + e0));
+                r.d[2 * k] = q.x;
+                r.d[2 * k + 1] = q.y;
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < VW; ++i) r.set(k * VW + i, (e0 + i < L) ? __ldg(xv + e0 + i) : T(0));
+        }
+    }
+}
+
 template <class T, bool VEC>
-__global__ void __launch_bounds__(1 << WhtCfg<T>::TB) srht_fused_kernel(SrhtParams<T> p) {
+__global__ void __launch_bounds__(1 << WhtCfg<T>::TB, 2) srht_fused_kernel(SrhtParams<T> p) {
     constexpr int TB = WhtCfg<T>::TB, VB = WhtCfg<T>::VB;
     constexpr int CH = 2 * TB, NT = 1 << TB, VW = 1 << VB, KV = 1 << (TB - VB);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *Z = reinterpret_cast<T *>(smem_raw);
     T *acc = Z + (1 << CH);
+    uint32_t *srow = reinterpret_cast<uint32_t *>(acc + p.s_cnt);  // (r1 << CH) | swz(r2)
     __shared__ int last_flag;
     const int t = threadIdx.x;
     const int g = blockIdx.x;
-    for (int i = t; i < p.s_cnt; i += NT) acc[i] = T(0);
+    for (int i = t; i < p.s_cnt; i += NT) {
+        acc[i] = T(0);
+        const uint32_t row = (uint32_t)__ldg(p.rows + p.s_lo + i);
+        srow[i] = ((row >> CH) << CH) | (uint32_t)swz<TB, VB>((int)(row & ((1u << CH) - 1)));
+    }
     __syncthreads();
     const int64_t u0 = p.split.start(g), u1 = p.split.start(g + 1);
     if (u0 >= u1) return;
     const int t_lo = t & (VW - 1), t_hi = t >> VB;
-    int64_t v = u0 / p.cpv;
-    int64_t u = u0;
-    while (u < u1) {
-        const int64_t vbeg = v * p.cpv;
-        const int64_t vend = min(u1, vbeg + p.cpv);
-        const T *xv = p.X + v * p.x_ld;
-        for (int64_t c = u - vbeg; c < vend - vbeg; ++c) {
-            T r[1 << TB];
-            const int64_t cbase = c << CH;
-            // ---- pass A: coalesced 16-byte loads, sign flip ----
+    // The swizzle only permutes the low 3 bits of a vector index, so every address this
+    // thread touches is one of 8 per-thread bases plus a compile-time offset.
+    int offA[8], offB[8];
 #pragma unroll
-            for (int k = 0; k < KV; ++k) {
-                const int64_t e0 = cbase + ((int64_t)t << VB) + ((int64_t)k << (VB + TB));
-                T vals[VW];
-                if (VEC && e0 + VW <= p.L) {
-                    if constexpr (sizeof(T) == 4) {
-                        float4 q = __ldg(reinterpret_cast<const float4 *>(xv + e0));
-                        vals[0] = q.x; vals[1] = q.y; vals[2] = q.z; vals[3] = q.w;
-                    } else {
-                        double2 q = __ldg(reinterpret_cast<const double2 *>(xv + e0));
-                        vals[0] = q.x; vals[1] = q.y;
-                    }
-                } else {
+    for (int j = 0; j < 8; ++j) {
+        offA[j] = (t ^ j) << VB;
+        offB[j] = ((j ^ (t_hi & 7)) << VB) + (t_hi << (TB + VB)) + t_lo;
+    }
+    Regs<T, TB> r;
+    uint4 sg;
+    int64_t v = u0 / p.cpv, c = u0 - v * p.cpv;
+    load_chunk<T, VEC, TB, VB>(p.X + v * p.x_ld, c << CH, p.L, t, r);
+    sg = __ldg(p.sign_tl + c * NT + t);
+    for (int64_t u = u0; u < u1; ++u) {
+        // ---- pass A: sign flip, butterflies over the register bits, swizzled store ----
 #pragma unroll
-                    for (int i = 0; i < VW; ++i) vals[i] = (e0 + i < p.L) ? __ldg(xv + e0 + i) : T(0);
-                }
-                const uint32_t bits = __ldg(p.signbits + (e0 >> 5)) >> (e0 & 31);
-#pragma unroll
-                for (int i = 0; i < VW; ++i) r[k * VW + i] = ((bits >> i) & 1u) ? vals[i] : -vals[i];
-            }
-            wht_regs<TB>(r);
-#pragma unroll
-            for (int k = 0; k < KV; ++k) {
-                const int f = (t ^ (k & 7)) + (k << TB);
-                if constexpr (sizeof(T) == 4) {
-                    *reinterpret_cast<float4 *>(Z + (f << VB)) = make_float4(r[k * 4], r[k * 4 + 1], r[k * 4 + 2], r[k * 4 + 3]);
-                } else {
-                    *reinterpret_cast<double2 *>(Z + (f << VB)) = make_double2(r[k * 2], r[k * 2 + 1]);
-                }
-            }
-            __syncthreads();
-            // ---- pass B: remaining TB bits ----
-#pragma unroll
-            for (int q = 0; q < (1 << TB); ++q) {
-                const int e = t_lo + (q << VB) + (t_hi << (VB + TB));
-                r[q] = Z[swz<TB, VB>(e)];
-            }
-            wht_regs<TB>(r);
-#pragma unroll
-            for (int q = 0; q < (1 << TB); ++q) {
-                const int e = t_lo + (q << VB) + (t_hi << (VB + TB));
-                Z[swz<TB, VB>(e)] = r[q];
-            }
-            __syncthreads();
-            // ---- sampled rows: acc[i] += (-1)^popc(r1 & c) * Z_c[r2] ----
-            for (int i = t; i < p.s_cnt; i += NT) {
-                const int32_t row = __ldg(p.rows + p.s_lo + i);
-                const T z = Z[swz<TB, VB>(row & ((1 << CH) - 1))];
-                const int par = __popcll((unsigned long long)(row >> CH) & (unsigned long long)c) & 1;
-                acc[i] += par ? -z : z;
-            }
-            __syncthreads();
+        for (int q = 0; q < (1 << TB); ++q) {
+            const uint32_t w = q < 32 ? sg.x : q < 64 ? sg.y : q < 96 ? sg.z : sg.w;
+            r.set(q, flip<T>(r.get(q), w >> (q & 31)));
         }
+        r.wht();
+#pragma unroll
+        for (int k = 0; k < KV; ++k) {
+            T *dst = Z + offA[k & 7] + (k << (TB + VB));
+            if constexpr (sizeof(T) == 4) {
+                *reinterpret_cast<float4 *>(dst) =
+                    make_float4(r.d[2 * k].x, r.d[2 * k].y, r.d[2 * k + 1].x, r.d[2 * k + 1].y);
+            } else {
+                *reinterpret_cast<double2 *>(dst) = make_double2(r.d[2 * k], r.d[2 * k + 1]);
+            }
+        }
+        __syncthreads();
+        // ---- pass B: the remaining TB bits ----
+#pragma unroll
+        for (int q = 0; q < (1 << TB); ++q) r.set(q, Z[offB[q & 7] + ((q & ~7) << VB)]);
+        r.wht();
+#pragma unroll
+        for (int q = 0; q < (1 << TB); ++q) Z[offB[q & 7] + ((q & ~7) << VB)] = r.get(q);
+        __syncthreads();
+        // ---- prefetch the next chunk while the sampled rows are accumulated ----
+        const int64_t vcur = v, ccur = c;
+        if (u + 1 < u1) {
+            if (++c == p.cpv) {
+                c = 0;
+                ++v;
+            }
+            load_chunk<T, VEC, TB, VB>(p.X + v * p.x_ld, c << CH, p.L, t, r);
+            sg = __ldg(p.sign_tl + c * NT + t);
+        }
+        const uint32_t cc = (uint32_t)ccur;
+#pragma unroll 4
+        for (int i = t; i < p.s_cnt; i += NT) {
+            const uint32_t pk = srow[i];
+            const T z = Z[pk & ((1u << CH) - 1)];
+            acc[i] += (__popc((pk >> CH) & cc) & 1) ? -z : z;
+        }
+        __syncthreads();
+        const bool col_done = (u + 1 == u1) || (ccur + 1 == p.cpv);
+        if (!col_done) continue;
         // ---- column finished in this CTA's range ----
-        const bool first = (v == u0 / p.cpv);
+        const int64_t vbeg = vcur * p.cpv;
         const bool exclusive = (u0 <= vbeg) && (vbeg + p.cpv <= u1);
         if (exclusive) {
             for (int i = t; i < p.s_cnt; i += NT) {
-                T *yp = p.Y + (p.s_lo + i) * p.y_es + v * p.y_vs;
+                T *yp = p.Y + (p.s_lo + i) * p.y_es + vcur * p.y_vs;
                 T res = p.alpha * acc[i];
                 if (!p.beta_zero) res += p.beta * *yp;
                 *yp = res;
                 acc[i] = T(0);
             }
         } else {
-            T *part = p.partials + (int64_t)(2 * g + (first ? 0 : 1)) * p.s_cnt;
+            T *part = p.partials + (int64_t)p.split.slot(g, vbeg) * p.s_cnt;
             for (int i = t; i < p.s_cnt; i += NT) {
                 part[i] = acc[i];
                 acc[i] = T(0);
@@ -185,35 +245,57 @@ __global__ void __launch_bounds__(1 << WhtCfg<T>::TB) srht_fused_kernel(SrhtPara
             __threadfence();
             __syncthreads();
             const int gf = p.split.owner(vbeg), gl = p.split.owner(vbeg + p.cpv - 1);
-            if (t == 0) {
-                int ncontrib = 0;
-                for (int gg = gf; gg <= gl; ++gg) ncontrib += p.split.start(gg + 1) > p.split.start(gg);
-                int old = atomicAdd(&p.counters[v], 1);
-                last_flag = (old == ncontrib - 1);
-            }
+            if (t == 0) last_flag = (atomicAdd(&p.counters[vcur], 1) == gl - gf);
             __syncthreads();
             if (last_flag) {
                 __threadfence();
                 for (int i = t; i < p.s_cnt; i += NT) {
-                    T a = T(0);
-                    for (int gg = gf; gg <= gl; ++gg) {
-                        const int64_t sg = p.split.start(gg);
-                        if (p.split.start(gg + 1) <= sg) continue;
-                        const int sl = 2 * gg + ((sg / p.cpv) == v ? 0 : 1);
-                        a += __ldcg(p.partials + (int64_t)sl * p.s_cnt + i);
-                    }
-                    T *yp = p.Y + (p.s_lo + i) * p.y_es + v * p.y_vs;
+                    T a = __ldcg(p.partials + (int64_t)p.split.slot(gf, vbeg) * p.s_cnt + i);
+                    for (int gg = gf + 1; gg <= gl; ++gg) a += __ldcg(p.partials + (int64_t)(2 * gg) * p.s_cnt + i);
+                    T *yp = p.Y + (p.s_lo + i) * p.y_es + vcur * p.y_vs;
                     T res = p.alpha * a;
                     if (!p.beta_zero) res += p.beta * *yp;
                     *yp = res;
                 }
-                if (t == 0) p.counters[v] = 0;
+                if (t == 0) p.counters[vcur] = 0;
             }
         }
         __syncthreads();
-        u = vend;
-        ++v;
     }
+}
+
+// Per (chunk, thread) sign masks in pass-A register order (bit q = element
+// (t << VB) + ((q >> VB) << (VB+TB)) + (q & (VW-1)) of the chunk), so a thread reads its
+// 2^TB signs with one 16-byte load.
+template <class T>
+__global__ void sign_table_kernel(const uint32_t *signbits, int64_t nchunks, uint4 *out) {
+    constexpr int TB = WhtCfg<T>::TB, VB = WhtCfg<T>::VB, CH = 2 * TB, NT = 1 << TB, VW = 1 << VB;
+    const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (idx >= nchunks * NT) return;
+    const int64_t c = idx / NT;
+    const int t = (int)(idx % NT);
+    uint32_t w[4] = {0u, 0u, 0u, 0u};
+    for (int q = 0; q < (1 << TB); ++q) {
+        const int k = q / VW, i = q % VW;
+        const int64_t e = (c << CH) + ((int64_t)t << VB) + ((int64_t)k << (VB + TB)) + i;
+        const uint32_t b = (signbits[e >> 5] >> (e & 31)) & 1u;
+        w[q >> 5] |= b << (q & 31);
+    }
+    out[idx] = make_uint4(w[0], w[1], w[2], w[3]);
+}
+
+int build_srht_sign_table(rla_ctx *ctx, rla_sketch *sk) {
+    const int CH = sk->p.dtype == RLA_F32 ? 2 * WhtCfg<float>::TB : 2 * WhtCfg<double>::TB;
+    const int NT = sk->p.dtype == RLA_F32 ? (1 << WhtCfg<float>::TB) : (1 << WhtCfg<double>::TB);
+    if (sk->N < ((int64_t)1 << CH)) return RLA_OK;
+    const int64_t nchunks = sk->N >> CH;
+    if (!sk->sign_tl) RLA_CUDA_TRY(ctx, cudaMalloc(&sk->sign_tl, sizeof(uint4) * nchunks * NT));
+    const int64_t n = nchunks * NT;
+    if (sk->p.dtype == RLA_F32)
+        sign_table_kernel<float><<<ceil_div_i(n, 256), 256, 0, ctx->stream>>>(sk->signbits, nchunks, sk->sign_tl);
+    else
+        sign_table_kernel<double><<<ceil_div_i(n, 256), 256, 0, ctx->stream>>>(sk->signbits, nchunks, sk->sign_tl);
+    return check_launch(ctx, "sign_table");
 }
 
 // Small padded sizes (N <= 2^(2*TB)): one CTA per column, the whole padded column in
@@ -434,10 +516,10 @@ int srht_compress(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_t x_es, 
     char *scratch = nullptr;
     const int64_t cpv = N >> CH;
     const int cap = ctx->smem_optin - 2048;
-    int s_win = (int)std::min<int64_t>(s, (cap / 2 - (int64_t)(es << CH)) / (int64_t)es);
-    if (s_win < 256) s_win = (int)std::min<int64_t>(s, (cap - (int64_t)(es << CH)) / (int64_t)es);
+    int s_win = (int)std::min<int64_t>(s, (cap / 2 - (int64_t)(es << CH)) / (int64_t)(es + 4));
+    if (s_win < 256) s_win = (int)std::min<int64_t>(s, (cap - (int64_t)(es << CH)) / (int64_t)(es + 4));
     const int64_t total = cpv * nv;
-    const int blocks_per_sm = std::max(1, cap / (int)((es << CH) + s_win * es + 64));
+    const int blocks_per_sm = std::max(1, cap / (int)((es << CH) + s_win * (es + 4) + 64));
     int64_t W = std::min<int64_t>((int64_t)ctx->sm_count * std::min(blocks_per_sm, 2), std::max<int64_t>(total, 1));
     const size_t need_t = x_es != 1 ? (size_t)L * nv * es : 0;
     const size_t need_p = N >= ((int64_t)1 << CH) ? (size_t)(2 * W) * s_win * es : 0;
@@ -463,9 +545,9 @@ int srht_compress(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_t x_es, 
     int *cnt = nullptr;
     RLA_TRY(counters_get(ctx, (size_t)nv, &cnt));
     const bool vec = (ldx % (int64_t)(1 << VB) == 0) && ((uintptr_t)Xc % 16 == 0);
-    SrhtParams<T> p{Xc, ldx, L, N, sk->signbits, sk->rows, 0, s_win, Y, y_es, y_vs, a, (T)beta, beta_zero,
-                    (T *)(scratch + off_partials), cnt, cpv, SplitB{total, (int)W}};
-    const size_t smem = (es << CH) + (size_t)s_win * es;
+    SrhtParams<T> p{Xc, ldx, L, N, sk->sign_tl, sk->rows, 0, s_win, Y, y_es, y_vs, a, (T)beta, beta_zero,
+                    (T *)(scratch + off_partials), cnt, cpv, Split::make(total, (int)W)};
+    const size_t smem = (es << CH) + (size_t)s_win * (es + 4);
     for (int64_t lo = 0; lo < s; lo += s_win) {
         p.s_lo = lo;
         p.s_cnt = (int)std::min<int64_t>(s_win, s - lo);

@@ -91,10 +91,29 @@ def test_randsvd_matches_oracle(rla, orc, dev, ortho):
     rec = rla.rapproximate(rla.RandSVD(compressor=comp, power_its=2, orthogonalize=ortho), to_dev(A, dev), seed=9)
     ref = orc.randsvd(A, oracle_recipe(orc, rec.compressor), q=2, orthogonalize=ortho)
     S = rec.S.cpu().numpy()
-    assert rel_err(S, ref.S) < 1e-12
+    # Without orthogonalisation Y = (AA')^2 A Omega has cond(Y) ~ (s1/s20)^5 ~ 5e9 here, which
+    # amplifies rounding in both the Householder oracle and CholeskyQR2 alike.
+    tol = 1e-12 if ortho else 1e-8
+    assert rel_err(S, ref.S) < tol
     U, V = rec.U.cpu().numpy(), rec.V.cpu().numpy()
     sgn = np.sign(np.sum(U * ref.U, axis=0))
-    assert rel_err(U * sgn, ref.U) < 1e-9 and rel_err(V * sgn, ref.V) < 1e-9
+    assert rel_err(U * sgn, ref.U) < 1e3 * tol and rel_err(V * sgn, ref.V) < 1e3 * tol
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_rank_deficient_sketch(rla, dev, dtype):
+    """Compression dimension above rank(A): CholeskyQR breaks down and the Householder path
+    takes over; the factorization is still exact and orthonormal."""
+    rng = np.random.default_rng(22)
+    U0 = qr_Q(rng.standard_normal((300, 8)))
+    V0 = qr_Q(rng.standard_normal((120, 8)))
+    M = ((U0 * (2.0 ** -np.arange(8))) @ V0.T).astype(dtype)
+    comp = rla.Gaussian(cardinality=rla.Right(), compression_dim=10, type=dtype)
+    rec = rla.rapproximate(rla.RandSVD(compressor=comp), to_dev(M, dev), seed=23)
+    U, S, V = rec.U.cpu().numpy(), rec.S.cpu().numpy(), rec.V.cpu().numpy()
+    tol = 1e-10 if dtype == np.float64 else 1e-5
+    assert rel_err((U * S) @ V.T, M) < tol
+    assert np.allclose(U.T @ U, np.eye(10), atol=tol) and np.allclose(V.T @ V, np.eye(10), atol=tol)
 
 
 def test_randsvd_float32_vs_fp64_oracle(rla, orc, dev):
