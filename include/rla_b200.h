@@ -195,6 +195,27 @@ int rla_lowrank_mul(rla_ctx *ctx, int factor_dtype, int dtype, int side, int tra
                     int64_t a_rows, int64_t a_cols, const void *A, int64_t lda, int trans_a,
                     double alpha, double beta);
 
+/* ---- allocation-free SRHT apply -------------------------------------------------- */
+/* No counterpart in the reference.  C = alpha*S*A + beta*C for a Left-cardinality SRHT
+ * recipe S (s x m), column-major A (m x n) and C (s x n), on the context's stream, without
+ * allocating device memory: for callers that cannot call cudaMalloc -- code that owns a
+ * fixed device-memory budget and hands every byte out itself, code whose device memory
+ * belongs to another runtime's pool, code on paths that must not touch the allocator.
+ * The kernel's partial sums live in library-owned fixed device arrays of
+ * RLA_NOALLOC_SCRATCH_BYTES bytes plus RLA_NOALLOC_MAX_COLS counters, held by every GPU
+ * that loads the library until the process exits.  n above RLA_NOALLOC_MAX_COLS, or a
+ * compression dimension whose partial sums cannot fit, is rejected with RLA_E_ARG.
+ * The first call on a device looks up the arrays' device addresses; make that first call
+ * before any stream capture.  All calls share the arrays, which keep the last call's
+ * contents: calls whose GPU work overlaps (other streams or threads without ordering)
+ * race.  Returns once the work is queued; synchronize the stream before reading C. */
+#define RLA_NOALLOC_SCRATCH_BYTES (8u << 20)
+#define RLA_NOALLOC_MAX_COLS 65536
+int rla_srht_mul_noalloc(rla_ctx *ctx, const rla_sketch *sk,
+                         int64_t c_rows, int64_t c_cols, void *C, int64_t ldc,
+                         int64_t a_rows, int64_t a_cols, const void *A, int64_t lda,
+                         double alpha, double beta);
+
 #ifdef __cplusplus
 }
 #endif

@@ -69,6 +69,8 @@ SIGNATURES = {
     "rla_lowrank_mul": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, i64, i64, i64,
                                        vp, i64, vp, vp, i64, i64, i64, vp, i64, ctypes.c_int, i64, i64, vp, i64,
                                        ctypes.c_int, ctypes.c_double, ctypes.c_double]),
+    "rla_srht_mul_noalloc": (ctypes.c_int, [vp, vp, i64, i64, vp, i64, i64, i64, vp, i64, ctypes.c_double,
+                                            ctypes.c_double]),
 }
 
 _lib = None

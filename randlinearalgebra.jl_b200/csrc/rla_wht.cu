@@ -16,6 +16,8 @@
 // shared accumulator.  Columns are split over the persistent grid (stream-K); a column
 // shared by several CTAs is finished by the last CTA to arrive, which adds the partial
 // accumulators in CTA order, so results are reproducible bit for bit.
+#include <mutex>
+
 #include "rla_internal.cuh"
 
 namespace rla {
@@ -632,6 +634,90 @@ int fjlt_expand(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_t x_es, in
     return check_launch(ctx, "fjlt_expand_out");
 }
 
+// ------------------------------------------------------------------------------------
+// Allocation-free SRHT left apply.
+//
+// Some callers cannot call cudaMalloc: code that owns a fixed device-memory budget and
+// hands every byte out itself (a serving process that partitions HBM up front), code whose
+// device memory is managed by another runtime's pool allocator, and code on a path that
+// must not touch the CUDA allocator at all (latency-critical request handling).  For them
+// the partial-sum scratch of the stream-K SRHT kernel lives in fixed device arrays that the
+// library defines; every GPU that loads the library holds them until the process exits.
+// All calls share these arrays, so calls whose work overlaps on the GPU (different streams
+// or host threads without ordering between them) race and give wrong results.
+// ------------------------------------------------------------------------------------
+static __device__ __align__(256) unsigned char g_noalloc_partials[RLA_NOALLOC_SCRATCH_BYTES];
+static __device__ __align__(256) int g_noalloc_counters[RLA_NOALLOC_MAX_COLS];
+
+struct NoallocDevice {
+    bool ready = false;
+    void *partials = nullptr;  // device address of g_noalloc_partials on this device
+    int *counters = nullptr;   // device address of g_noalloc_counters on this device
+};
+
+static int noalloc_setup(rla_ctx *ctx, NoallocDevice **out) {
+    static std::mutex mu;
+    static NoallocDevice dev[64];
+    if (ctx->device < 0 || ctx->device >= 64) return set_error(ctx, RLA_E_ARG, "device index out of range");
+    std::lock_guard<std::mutex> lock(mu);
+    NoallocDevice &d = dev[ctx->device];
+    if (!d.ready) {
+        // In host code the array names are host-side stand-ins; the device addresses come
+        // from the runtime, per device, with that device current.
+        RLA_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+        RLA_CUDA_TRY(ctx, cudaGetSymbolAddress(&d.partials, g_noalloc_partials));
+        RLA_CUDA_TRY(ctx, cudaGetSymbolAddress((void **)&d.counters, g_noalloc_counters));
+        d.ready = true;
+    }
+    *out = &d;
+    return RLA_OK;
+}
+
+template <class T>
+static int srht_noalloc_t(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_t ldx, int64_t nv, T *Y,
+                          int64_t ldy, double alpha, double beta, const NoallocDevice &nd) {
+    constexpr int TB = WhtCfg<T>::TB, VB = WhtCfg<T>::VB, CH = 2 * TB;
+    const size_t es = sizeof(T);
+    const int64_t L = sk->L, N = sk->N, s = sk->s;
+    const T a = (T)(alpha * sk->scale);
+    const bool beta_zero = beta == 0.0;
+    if (N < ((int64_t)1 << CH)) {
+        const size_t smem = (size_t)N * es;
+        cudaFuncSetAttribute(srht_small_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        const int grid = (int)std::min<int64_t>(nv, (int64_t)ctx->sm_count * 8);
+        srht_small_kernel<T><<<grid, 256, smem, ctx->stream>>>(X, ldx, L, N, nv, sk->signbits, sk->rows, s, Y, 1, ldy,
+                                                               a, (T)beta, beta_zero);
+        return check_launch(ctx, "srht_small(noalloc)");
+    }
+    const int cap = ctx->smem_optin - 2048;
+    int s_win = (int)std::min<int64_t>(s, (cap / 2 - (int64_t)(es << CH)) / (int64_t)(es + 4));
+    if (s_win < 256) s_win = (int)std::min<int64_t>(s, (cap - (int64_t)(es << CH)) / (int64_t)(es + 4));
+    const int64_t cpv = N >> CH, total = cpv * nv;
+    int64_t W = std::min<int64_t>((int64_t)ctx->sm_count * 2, total);
+    W = std::min<int64_t>(W, (int64_t)(RLA_NOALLOC_SCRATCH_BYTES / (2 * (size_t)s_win * es)));
+    if (W < 1)
+        return set_error(ctx, RLA_E_ARG, "compression dimension window %d does not fit the %u-byte allocation-free scratch",
+                         s_win, (unsigned)RLA_NOALLOC_SCRATCH_BYTES);
+    RLA_CUDA_TRY(ctx, cudaMemsetAsync(nd.counters, 0, sizeof(int) * (size_t)nv, ctx->stream));
+    const bool vec = (ldx % (int64_t)(1 << VB) == 0) && ((uintptr_t)X % 16 == 0);
+    SrhtParams<T> p{X, ldx, L, N, sk->sign_tl, sk->rows, 0, s_win, Y, 1, ldy, a, (T)beta, beta_zero,
+                    (T *)nd.partials, nd.counters, cpv, Split::make(total, (int)W)};
+    const size_t smem = (es << CH) + (size_t)s_win * (es + 4);
+    for (int64_t lo = 0; lo < s; lo += s_win) {
+        p.s_lo = lo;
+        p.s_cnt = (int)std::min<int64_t>(s_win, s - lo);
+        if (vec) {
+            cudaFuncSetAttribute(srht_fused_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            srht_fused_kernel<T, true><<<(int)W, 1 << TB, smem, ctx->stream>>>(p);
+        } else {
+            cudaFuncSetAttribute(srht_fused_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            srht_fused_kernel<T, false><<<(int)W, 1 << TB, smem, ctx->stream>>>(p);
+        }
+        RLA_TRY(check_launch(ctx, "srht_fused(noalloc)"));
+    }
+    return RLA_OK;
+}
+
 #define RLA_INST(T)                                                                                                  \
     template int srht_compress<T>(rla_ctx *, const rla_sketch *, const T *, int64_t, int64_t, int64_t, T *, int64_t,  \
                                   int64_t, double, double);                                                          \
@@ -645,3 +731,32 @@ RLA_INST(float)
 RLA_INST(double)
 
 }  // namespace rla
+
+using namespace rla;
+
+extern "C" int rla_srht_mul_noalloc(rla_ctx *ctx, const rla_sketch *sk, int64_t c_rows, int64_t c_cols, void *C,
+                                    int64_t ldc, int64_t a_rows, int64_t a_cols, const void *A, int64_t lda,
+                                    double alpha, double beta) {
+    if (!ctx) return RLA_E_ARG;
+    if (!sk || sk->p.kind != RLA_SRHT || sk->p.card != RLA_LEFT)
+        return set_error(ctx, RLA_E_ARG, "rla_srht_mul_noalloc needs a Left-cardinality SRHT recipe.");
+    if (sk->device != ctx->device) return set_error(ctx, RLA_E_ARG, "Compressor lives on another device.");
+    // left_mul_dimcheck (src/helpers/mul_dim_checks.jl:41-64)
+    if (a_rows != sk->n_cols)
+        return set_error(ctx, RLA_E_DIM, "Matrix A has %lld rows while S has %lld columns.", (long long)a_rows, (long long)sk->n_cols);
+    if (a_cols != c_cols)
+        return set_error(ctx, RLA_E_DIM, "Matrix A has %lld columns while C has %lld columns.", (long long)a_cols, (long long)c_cols);
+    if (c_rows != sk->n_rows)
+        return set_error(ctx, RLA_E_DIM, "Matrix C has %lld rows while S has %lld rows.", (long long)c_rows, (long long)sk->n_rows);
+    if (a_cols > RLA_NOALLOC_MAX_COLS)
+        return set_error(ctx, RLA_E_ARG, "%lld columns exceed the allocation-free limit of %d columns per call.",
+                         (long long)a_cols, RLA_NOALLOC_MAX_COLS);
+    if (a_cols == 0) return RLA_OK;
+    if (!A || !C || lda < std::max<int64_t>(1, a_rows) || ldc < std::max<int64_t>(1, c_rows))
+        return set_error(ctx, RLA_E_ARG, "NULL pointer or leading dimension smaller than the row count.");
+    NoallocDevice *nd = nullptr;
+    RLA_TRY(noalloc_setup(ctx, &nd));
+    if (sk->p.dtype == RLA_F32)
+        return srht_noalloc_t<float>(ctx, sk, (const float *)A, lda, a_cols, (float *)C, ldc, alpha, beta, *nd);
+    return srht_noalloc_t<double>(ctx, sk, (const double *)A, lda, a_cols, (double *)C, ldc, alpha, beta, *nd);
+}
