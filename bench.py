@@ -30,11 +30,18 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 M, NCOL, S = 2**20, 512, 4096
-BYTES_PER_APPLY = 4 * (M * NCOL + S * NCOL)      # algorithmic bytes of one apply
+
+
+def bytes_per_apply(ncol: int = NCOL) -> int:
+    """Algorithmic bytes of one apply: read A once, write C once."""
+    return 4 * (M * ncol + S * ncol)
+
+
+BYTES_PER_APPLY = bytes_per_apply()
 WORKLOAD = "srht+countsketch left apply, fp32, A 2^20x512 -> 4096x512"
 METRIC = "sketch apply throughput (SRHT + CountSketch, HBM GB/s of algorithmic bytes)"
 # DRAM bytes per launch from ncu (profiles/); None until a capture of this build exists.
-TRAFFIC_PER_LAUNCH = {"srht_fused_kernel": None, "compress_contig_kernel": None}
+TRAFFIC_PER_LAUNCH = {"srht_fused_kernel": None, "cs_compress_kernel": None}
 
 
 def peaks():
@@ -221,7 +228,9 @@ def b200_arm(args):
     dev = torch.device("cuda", local if world > 1 else 0)
     g = torch.Generator(device=dev)
     g.manual_seed(2 + rank)
-    A = torch.randn(NCOL, M, device=dev, generator=g, dtype=torch.float32).t()  # column-major 2^20 x 512
+    NCOL = args.cols
+    BYTES_PER_APPLY = bytes_per_apply(NCOL)
+    A = torch.randn(NCOL, M, device=dev, generator=g, dtype=torch.float32).t()  # column-major 2^20 x NCOL
     srht = rla.complete_compressor(rla.SRHT(compression_dim=S, type=np.float32), A, seed=1000 + rank)
     cs = rla.complete_compressor(rla.CountSketch(compression_dim=S, type=np.float32), A, seed=2000 + rank)
     C1 = torch.zeros(NCOL, S, device=dev).t()
@@ -297,7 +306,7 @@ def b200_arm(args):
         return
 
     peak, peak_kind = peaks()
-    dom_name, dom_ms = ("srht_fused_kernel", srht_ms) if srht_ms >= cs_ms else ("compress_contig_kernel", cs_ms)
+    dom_name, dom_ms = ("srht_fused_kernel", srht_ms) if srht_ms >= cs_ms else ("cs_compress_kernel", cs_ms)
     achieved = BYTES_PER_APPLY / (dom_ms / 1e3) / 1e9
     traffic = TRAFFIC_PER_LAUNCH.get(dom_name)
     roofline = {"bound": "hbm", "kernel": dom_name, "achieved": round(achieved, 2), "peak": peak,
@@ -320,7 +329,8 @@ def b200_arm(args):
     line = {"metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": K,
             "warmup": args.warmup, "ms_per_step": round(ms / K, 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic N(0,1) generated on device (torch.randn, seed 2+rank)",
-            "config": {"workload": WORKLOAD, "m": M, "n": NCOL, "s": S, "parallelism": f"replicas x{world}",
+            "config": {"workload": WORKLOAD if NCOL == 512 else WORKLOAD.replace("512", str(NCOL)), "m": M, "n": NCOL,
+                       "s": S, "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (2.15 GB per A), no flush needed"},
             "roofline": roofline, "kernels": kernels, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
             "gpu_launches": 2 * K}
@@ -337,6 +347,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cols", type=int, default=NCOL,
+                    help="columns of A (default 512, the benchmark workload; smaller values make small "
+                         "cases of the same kernels for profiler captures)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -213,7 +213,11 @@ struct rla_sketch {
     // SparseSign / CountSketch
     int32_t *bucket = nullptr;     // [L*nnz] compress-side bucket per (j, e), sorted within j
     uint8_t *negative = nullptr;   // [L*nnz] 1 when the value is -scale
-    uint32_t *meta = nullptr;      // [L*nnz] packed (bucket | dup << 30 | neg << 31)
+    uint32_t *meta = nullptr;      // tile-blocked (bucket | deferred << 30 | neg << 31)
+    uint32_t *tile_flags = nullptr;  // per 128-element tile: 0, SLOW, or (first extra round << 8) | rounds
+    uint32_t *extra = nullptr;     // deferred items: 32 words (one per lane) per extra round
+    int64_t extra_rounds_cap = 0;
+    int batch_mode = 0;            // 1: CountSketch schedule over 512-element batches (see rla_sketch.cu)
     // SRHT
     int32_t *rows = nullptr;       // [s] sampled padded rows (op)
     uint32_t *signbits = nullptr;  // [ceil(N/32)] bit r = 1 means +1

@@ -64,30 +64,198 @@ __global__ void draw_sparse_kernel(Rng rng, uint32_t stream, int64_t L, int nnz,
     for (int e = 0; e < nnz; ++e) negative[j * nnz + e] = (uint8_t)(ws() & 1u);
 }
 
-// Packed metadata for the contiguous-vector compress kernel.  The kernel maps tile
-// element j = 128*tile + 4*lane + t to (lane, sub-round t); for every sub-round (tile, t,
-// e) this marks the lanes whose bucket repeats inside the sub-round, so the kernel can
-// take a conflict-free fast path whenever no mark is set.
-__global__ void build_meta_kernel(const int32_t *bucket, const uint8_t *negative, int64_t L,
-                                  int nnz, uint32_t *meta) {
-    int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    int lane = threadIdx.x & 31;
-    int64_t ntile = (L + 127) / 128;
-    int64_t total = ntile * 4 * nnz;
-    if (warp >= total) return;  // warp-uniform
-    int e = (int)(warp % nnz);
-    int t = (int)((warp / nnz) % 4);
-    int64_t tile = warp / (4 * nnz);
-    int64_t j = tile * 128 + 4 * lane + t;
-    bool valid = j < L;
-    uint32_t b = valid ? (uint32_t)bucket[j * nnz + e] : 0u;
-    unsigned key = valid ? b : (0x80000000u | (unsigned)lane);
-    unsigned grp = __match_any_sync(FULL, key);
-    if (valid) {
-        // tile-blocked layout: for each (tile, e) the 128 words of the tile are contiguous
-        uint32_t dup = __popc(grp) > 1 ? 1u : 0u;
-        meta[(tile * nnz + e) * 128 + 4 * lane + t] = b | (dup << 30) | ((uint32_t)negative[j * nnz + e] << 31);
+// Metadata of the contiguous-vector compress kernel.  The kernel maps element
+// j = 128*tile + 4*lane + t of a tile to lane `lane`, and runs one sub-round per (t, e)
+// with every lane adding one value to its bucket.  Here, per tile (one warp per tile):
+//  * in every sub-round, lanes whose bucket repeats an earlier lane's are marked deferred
+//    (bit 30 of their main word), so the main sub-rounds touch distinct bins;
+//  * deferred items are packed greedily, in (sub-round, lane) order, into extra rounds in
+//    which each lane holds at most one item and all buckets differ;
+//  * tiles with more than MAX_DEFER deferred items or MAX_XROUNDS extra rounds are marked
+//    SLOW and resolved at run time instead (only for tiny compression dimensions).
+// Pass 0 writes the main words and counts extra rounds; pass 1 (after an exclusive scan of
+// the counts) writes the extra words and the tile flags.  Both passes schedule identically.
+constexpr int SCHED_WARPS = 8, MAX_DEFER = 64, MAX_XROUNDS = 16;
+constexpr uint32_t TILE_SLOW = 0x80000000u;
+
+template <int PASS>
+__global__ void __launch_bounds__(SCHED_WARPS * 32) sparse_sched_kernel(const int32_t *bucket, const uint8_t *negative,
+                                                                         int64_t L, int nnz, uint32_t *meta,
+                                                                         int32_t *nrounds, const int64_t *round_base,
+                                                                         uint32_t *tile_flags, uint32_t *extra) {
+    __shared__ uint32_t list[SCHED_WARPS][MAX_DEFER];
+    __shared__ uint32_t rlanes[SCHED_WARPS][MAX_XROUNDS];
+    __shared__ uint32_t rbkt[SCHED_WARPS][MAX_XROUNDS][32];
+    __shared__ uint8_t place[SCHED_WARPS][MAX_DEFER];
+    __shared__ int nround_s[SCHED_WARPS];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t tile = (int64_t)blockIdx.x * SCHED_WARPS + w;
+    const int64_t ntile = (L + 127) / 128;
+    if (tile >= ntile) return;  // warp-uniform
+    const unsigned lt = (1u << lane) - 1u;
+    int cnt = 0;
+    for (int e = 0; e < nnz; ++e)
+        for (int t = 0; t < 4; ++t) {
+            const int64_t j = tile * 128 + 4 * lane + t;
+            const bool valid = j < L;
+            const uint32_t b = valid ? (uint32_t)bucket[j * nnz + e] : 0u;
+            const uint32_t neg = valid ? (uint32_t)negative[j * nnz + e] : 0u;
+            const unsigned grp = __match_any_sync(FULL, valid ? b : (0x80000000u | (unsigned)lane));
+            const bool defer = valid && (grp & lt) != 0u;
+            if (PASS == 0 && valid) meta[(tile * nnz + e) * 128 + 4 * lane + t] = b | ((uint32_t)defer << 30) | (neg << 31);
+            const unsigned bal = __ballot_sync(FULL, defer);
+            if (defer) {
+                const int pos = cnt + __popc(bal & lt);
+                if (pos < MAX_DEFER) list[w][pos] = b | ((uint32_t)t << 22) | ((uint32_t)lane << 24) | (neg << 31);
+            }
+            cnt += __popc(bal);
+        }
+    __syncwarp();
+    int R = 0;
+    bool slow = cnt > MAX_DEFER;
+    if (!slow && lane == 0) {
+        for (int k = 0; k < cnt && !slow; ++k) {
+            const uint32_t it = list[w][k];
+            const uint32_t bk = it & 0x3fffffu, ln = (it >> 24) & 31u;
+            int r = 0;
+            for (; r < R; ++r) {
+                if (rlanes[w][r] & (1u << ln)) continue;
+                bool clash = false;
+                for (int q = 0; q < 32 && !clash; ++q)
+                    if ((rlanes[w][r] >> q) & 1u) clash = rbkt[w][r][q] == bk;
+                if (!clash) break;
+            }
+            if (r == R) {
+                if (R == MAX_XROUNDS) {
+                    slow = true;
+                    break;
+                }
+                rlanes[w][R++] = 0u;
+            }
+            rlanes[w][r] |= 1u << ln;
+            rbkt[w][r][ln] = bk;
+            place[w][k] = (uint8_t)r;
+        }
+        nround_s[w] = slow ? -1 : R;
     }
+    __syncwarp();
+    if (!slow) R = nround_s[w];
+    if (R < 0) {
+        slow = true;
+        R = 0;
+    }
+    if (PASS == 0) {
+        if (lane == 0) nrounds[tile] = slow ? 0 : R;
+        return;
+    }
+    if (slow) {
+        if (lane == 0) tile_flags[tile] = TILE_SLOW;
+        return;
+    }
+    const int64_t base = round_base[tile];
+    for (int r = 0; r < R; ++r) extra[(base + r) * 32 + lane] = 0u;
+    __syncwarp();
+    if (lane == 0) {
+        for (int k = 0; k < cnt; ++k) {
+            const uint32_t it = list[w][k];
+            const uint32_t ln = (it >> 24) & 31u;
+            extra[(base + place[w][k]) * 32 + ln] = (it & 0x3fffffu) | (it & (3u << 22)) | (1u << 30) | (it & 0x80000000u);
+        }
+        tile_flags[tile] = R == 0 ? 0u : (uint32_t)((base << 8) | (uint32_t)R);
+    }
+}
+
+// CountSketch (nnz = 1, s <= 2^16): 512-element batches (4 tiles, 16 sub-rounds of 32
+// lanes).  An element is deferred when its bucket already occurred earlier in the batch,
+// in (sub-round, lane) order, so all non-deferred elements of a batch hit distinct bins and
+// the apply kernel issues a whole batch's read-modify-writes at once.  Deferred elements
+// are written by the apply kernel to a per-warp list (their list position is in bits
+// 22..27 of their word) and added in up to CS_XROUNDS extra rounds of 32 entries, any lane
+// taking any entry; the list is ordered here so that each round's buckets are distinct.
+// xbucket[batch*64 + k] holds entry k's bucket (0xffffffff when empty); flags[batch] is the
+// number of extra rounds, or TILE_SLOW when the batch needs run-time resolution.
+constexpr int CS_SCHED_WARPS = 4, CS_BATCH = 512, CS_XROUNDS = 2;
+
+__global__ void __launch_bounds__(CS_SCHED_WARPS * 32) cs_sched_kernel(const int32_t *bucket, const uint8_t *negative,
+                                                                        int64_t L, int64_t s, uint32_t *meta,
+                                                                        uint32_t *flags, uint32_t *xbucket) {
+    extern __shared__ uint32_t bm_all[];
+    __shared__ uint32_t list[CS_SCHED_WARPS][MAX_DEFER];
+    __shared__ uint32_t slot[CS_SCHED_WARPS][CS_XROUNDS * 32];
+    __shared__ int pos_of[CS_SCHED_WARPS][MAX_DEFER];
+    __shared__ int ok_s[CS_SCHED_WARPS];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t batch = (int64_t)blockIdx.x * CS_SCHED_WARPS + w;
+    const int64_t nb = (L + CS_BATCH - 1) / CS_BATCH;
+    if (batch >= nb) return;  // warp-uniform
+    const int nw = (int)((s + 31) / 32);
+    uint32_t *bm = bm_all + (int64_t)w * nw;
+    for (int i = lane; i < nw; i += 32) bm[i] = 0u;
+    __syncwarp();
+    const unsigned lt = (1u << lane) - 1u;
+    int cnt = 0;
+    uint32_t myword[16];
+    int mylist[16];
+    for (int r = 0; r < 16; ++r) {
+        const int64_t j = batch * CS_BATCH + (r >> 2) * 128 + 4 * lane + (r & 3);
+        const bool valid = j < L;
+        const uint32_t b = valid ? (uint32_t)bucket[j] : 0u;
+        const uint32_t neg = valid ? (uint32_t)negative[j] : 0u;
+        const unsigned grp = __match_any_sync(FULL, valid ? b : (0x80000000u | (unsigned)lane));
+        const bool leader = valid && (grp & lt) == 0u;
+        const bool seen = leader && ((bm[b >> 5] >> (b & 31)) & 1u);
+        const bool defer = valid && (!leader || seen);
+        __syncwarp();
+        if (leader && !seen) atomicOr(&bm[b >> 5], 1u << (b & 31));
+        __syncwarp();
+        const unsigned bal = __ballot_sync(FULL, defer);
+        mylist[r] = -1;
+        if (defer) {
+            const int pos = cnt + __popc(bal & lt);
+            if (pos < MAX_DEFER) list[w][pos] = b;
+            mylist[r] = pos;
+        }
+        cnt += __popc(bal);
+        myword[r] = valid ? (b | ((uint32_t)defer << 30) | (neg << 31)) : 0u;
+    }
+    __syncwarp();
+    // order the deferred entries into rounds of 32 with distinct buckets (lane 0, greedy)
+    if (lane == 0) {
+        int ok = cnt <= MAX_DEFER;
+        int fill[CS_XROUNDS] = {0};
+        for (int k = 0; k < cnt && ok; ++k) {
+            const uint32_t bk = list[w][k];
+            int r = 0;
+            for (; r < CS_XROUNDS; ++r) {
+                if (fill[r] == 32) continue;
+                bool clash = false;
+                for (int q = 0; q < fill[r] && !clash; ++q) clash = slot[w][r * 32 + q] == bk;
+                if (!clash) break;
+            }
+            if (r == CS_XROUNDS) {
+                ok = 0;
+                break;
+            }
+            slot[w][r * 32 + fill[r]] = bk;
+            pos_of[w][k] = r * 32 + fill[r];
+            ++fill[r];
+        }
+        for (int r = 0; r < CS_XROUNDS; ++r)
+            for (int q = fill[r]; q < 32; ++q) slot[w][r * 32 + q] = 0xffffffffu;
+        ok_s[w] = ok ? (fill[1] > 0 ? 2 : (fill[0] > 0 ? 1 : 0)) : -1;
+    }
+    __syncwarp();
+    const int R = ok_s[w];
+    for (int r = 0; r < 16; ++r) {
+        const int64_t j = batch * CS_BATCH + (r >> 2) * 128 + 4 * lane + (r & 3);
+        if (j >= L) continue;
+        uint32_t word = myword[r];
+        if (R >= 0 && mylist[r] >= 0) word |= (uint32_t)pos_of[w][mylist[r]] << 22;
+        meta[j] = word;
+    }
+    for (int k = lane; k < CS_XROUNDS * 32; k += 32)
+        xbucket[batch * 64 + k] = (R > 0) ? slot[w][k] : 0xffffffffu;
+    if (lane == 0) flags[batch] = R < 0 ? TILE_SLOW : (uint32_t)R;
 }
 
 __global__ void draw_signbits_kernel(Rng rng, int64_t nwords, uint32_t *bits) {
@@ -267,12 +435,55 @@ static int srht_tables(rla_ctx *ctx, rla_sketch *sk) {
 }
 
 static int build_meta(rla_ctx *ctx, rla_sketch *sk) {
-    int64_t ntile = ceil_div(sk->L, 128);
-    int64_t warps = ntile * 4 * sk->nnz;
-    int64_t threads = warps * 32;
-    build_meta_kernel<<<ceil_div_i(threads, 256), 256, 0, ctx->stream>>>(sk->bucket, sk->negative, sk->L,
-                                                                        (int)sk->nnz, sk->meta);
-    return check_launch(ctx, "build_meta");
+    if (sk->s > (1 << 22)) return RLA_OK;  // compression dimension beyond the packed form: strided/expand paths only
+    sk->batch_mode = (sk->nnz == 1 && sk->s <= 65536) ? 1 : 0;
+    if (sk->batch_mode) {
+        const int64_t nb = ceil_div(sk->L, CS_BATCH);
+        const size_t bm_bytes = (size_t)CS_SCHED_WARPS * ceil_div(sk->s, 32) * 4;
+        if (!sk->tile_flags) RLA_CUDA_TRY(ctx, cudaMalloc(&sk->tile_flags, sizeof(uint32_t) * nb));
+        if (!sk->extra) {
+            RLA_CUDA_TRY(ctx, cudaMalloc(&sk->extra, sizeof(uint32_t) * 64 * nb));
+            sk->extra_rounds_cap = 2 * nb;
+        }
+        if (bm_bytes > 48 * 1024)
+            RLA_CUDA_TRY(ctx, cudaFuncSetAttribute(cs_sched_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bm_bytes));
+        cs_sched_kernel<<<ceil_div_i(nb, CS_SCHED_WARPS), CS_SCHED_WARPS * 32, bm_bytes, ctx->stream>>>(
+            sk->bucket, sk->negative, sk->L, sk->s, sk->meta, sk->tile_flags, sk->extra);
+        return check_launch(ctx, "cs_sched");
+    }
+    const int64_t ntile = ceil_div(sk->L, 128);
+    const int blocks = ceil_div_i(ntile, SCHED_WARPS);
+    int32_t *nr = nullptr;
+    int64_t *base = nullptr;
+    RLA_CUDA_TRY(ctx, cudaMallocAsync((void **)&nr, sizeof(int32_t) * ntile, ctx->stream));
+    RLA_CUDA_TRY(ctx, cudaMallocAsync((void **)&base, sizeof(int64_t) * ntile, ctx->stream));
+    sparse_sched_kernel<0><<<blocks, SCHED_WARPS * 32, 0, ctx->stream>>>(sk->bucket, sk->negative, sk->L, (int)sk->nnz,
+                                                                         sk->meta, nr, nullptr, nullptr, nullptr);
+    RLA_TRY(check_launch(ctx, "sparse_sched(0)"));
+    std::vector<int32_t> hn(ntile);
+    std::vector<int64_t> hb(ntile);
+    RLA_CUDA_TRY(ctx, cudaMemcpyAsync(hn.data(), nr, sizeof(int32_t) * ntile, cudaMemcpyDeviceToHost, ctx->stream));
+    RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    int64_t tot = 0;
+    for (int64_t i = 0; i < ntile; ++i) {
+        hb[i] = tot;
+        tot += hn[i];
+    }
+    if (tot >= (int64_t(1) << 24)) return set_error(ctx, RLA_E_UNSUPPORTED, "too many deferred rounds");
+    if (tot > sk->extra_rounds_cap) {
+        if (sk->extra) RLA_CUDA_TRY(ctx, cudaFree(sk->extra));
+        sk->extra = nullptr;
+        sk->extra_rounds_cap = std::max<int64_t>(tot, 1) + tot / 4;
+        RLA_CUDA_TRY(ctx, cudaMalloc(&sk->extra, sizeof(uint32_t) * 32 * sk->extra_rounds_cap));
+    }
+    if (!sk->tile_flags) RLA_CUDA_TRY(ctx, cudaMalloc(&sk->tile_flags, sizeof(uint32_t) * std::max<int64_t>(ntile, 1)));
+    RLA_CUDA_TRY(ctx, cudaMemcpyAsync(base, hb.data(), sizeof(int64_t) * ntile, cudaMemcpyHostToDevice, ctx->stream));
+    sparse_sched_kernel<1><<<blocks, SCHED_WARPS * 32, 0, ctx->stream>>>(sk->bucket, sk->negative, sk->L, (int)sk->nnz,
+                                                                         sk->meta, nr, base, sk->tile_flags, sk->extra);
+    RLA_TRY(check_launch(ctx, "sparse_sched(1)"));
+    RLA_CUDA_TRY(ctx, cudaFreeAsync(nr, ctx->stream));
+    RLA_CUDA_TRY(ctx, cudaFreeAsync(base, ctx->stream));
+    return RLA_OK;
 }
 
 static Rng make_rng(const rla_sketch *sk) {
@@ -337,7 +548,7 @@ static int draw(rla_ctx *ctx, rla_sketch *sk) {
 }
 
 static void free_sketch_buffers(rla_sketch *sk) {
-    void *ptrs[] = {sk->bucket, sk->negative, sk->meta, sk->rows, sk->signbits, sk->sign_tl, sk->p2_ptr, sk->p2_list,
+    void *ptrs[] = {sk->bucket, sk->negative, sk->meta, sk->rows, sk->signbits, sk->sign_tl, sk->tile_flags, sk->extra, sk->p2_ptr, sk->p2_list,
                     sk->k_ptr, sk->k_col, sk->k_val, sk->kt_ptr, sk->kt_row, sk->kt_val, sk->dense};
     for (void *p : ptrs)
         if (p) cudaFree(p);

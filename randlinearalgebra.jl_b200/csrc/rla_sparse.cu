@@ -26,6 +26,8 @@ struct CompressContigParams {
     int64_t x_ld;  // vector stride; element (j, v) at X[j + v*x_ld]
     int64_t L, nv;
     const uint32_t *meta;
+    const uint32_t *tile_flags;
+    const uint32_t *extra;
     int nnz;
     int64_t bin_lo;
     int bin_cnt;
@@ -56,25 +58,41 @@ __device__ __noinline__ void bin_add_collide(T *bins, T x, int b, bool inwin, in
     if (inwin && (grp & ((1u << lane) - 1u)) == 0u) bins[b] += sum;
 }
 
-// One sub-round: lane adds +-x to bin (w & 0x3fffffff) - bin_lo.  The sign is bit 31 of w
-// (applied as an XOR on the sign bit), bit 30 flags a bucket shared with another lane of
-// the same sub-round.
+constexpr uint32_t TILE_SLOW = 0x80000000u;
+constexpr uint32_t BUCKET_MASK = 0x3fffffu;  // bits 0..21
+constexpr uint32_t BIT_DEFER = 1u << 30;     // main word: processed in an extra round
+constexpr uint32_t BIT_VALID = 1u << 30;     // extra word: slot holds an item
+
+template <class T>
+__device__ __forceinline__ T apply_sign(T x, uint32_t w) {
+    if constexpr (sizeof(T) == 4) return __uint_as_float(__float_as_uint(x) ^ (w & 0x80000000u));
+    else return __longlong_as_double(__double_as_longlong(x) ^ ((long long)(w & 0x80000000u) << 32));
+}
+
+// Predicated read-modify-write of one bin; within a sub-round the active lanes' bins are
+// distinct by construction (collisions were deferred when the sketch was drawn).
 template <class T, bool WIN>
-__device__ __forceinline__ void bin_add(T *bins, T x, uint32_t w, bool valid, int64_t bin_lo, int bin_cnt, int lane) {
-    int b = (int)(w & 0x3fffffffu);
+__device__ __forceinline__ void rmw(T *bins, T x, uint32_t w, bool on, int64_t bin_lo, int bin_cnt) {
+    int b = (int)(w & BUCKET_MASK);
+    if constexpr (WIN) {
+        b -= (int)bin_lo;
+        on = on && (unsigned)b < (unsigned)bin_cnt;
+    }
+    x = apply_sign(x, w);
+    if (on) bins[b] += x;
+}
+
+// Run-time resolution for SLOW tiles: lanes sharing a bucket are summed in lane order.
+template <class T, bool WIN>
+__device__ __noinline__ void rmw_resolve(T *bins, T x, uint32_t w, bool valid, int64_t bin_lo, int bin_cnt, int lane) {
+    int b = (int)(w & BUCKET_MASK);
     bool inwin = valid;
     if constexpr (WIN) {
         b -= (int)bin_lo;
         inwin = valid && (unsigned)b < (unsigned)bin_cnt;
     }
-    if constexpr (sizeof(T) == 4) {
-        x = __uint_as_float(__float_as_uint(x) ^ (w & 0x80000000u));
-    } else {
-        x = __longlong_as_double(__double_as_longlong(x) ^ ((long long)(w & 0x80000000u) << 32));
-    }
-    const bool dup = inwin && ((w >> 30) & 1u);
-    if (__any_sync(FULL, dup)) bin_add_collide(bins, x, b, inwin, lane);
-    else if (inwin) bins[b] += x;
+    x = apply_sign(x, w);
+    bin_add_collide(bins, x, b, inwin, lane);
     __syncwarp();
 }
 
@@ -137,14 +155,28 @@ __device__ void flush_vector(const CompressContigParams<T> &p, T *bins, int g, i
     __syncwarp();
 }
 
-// One 128-element tile of vector xv: lane holds elements 4*lane .. 4*lane+3; metadata
-// for entry e of the tile's elements is the contiguous block meta[(tile*nnz + e)*128 ...].
-template <class T, bool VEC, bool WIN, bool CHECK>
-__device__ __forceinline__ void do_tile(const CompressContigParams<T> &p, T *bins, const T *xv, int64_t kk,
-                                        int lane) {
-    const int64_t j0 = kk * 128 + lane * 4;
-    T val[4];
-    load4<T, VEC>(xv, j0, p.L, true, val);
+template <class T>
+__device__ __forceinline__ T pick4(const T (&v)[4], uint32_t t) {
+    const T lo = (t & 1u) ? v[1] : v[0];
+    const T hi = (t & 1u) ? v[3] : v[2];
+    return (t & 2u) ? hi : lo;
+}
+
+// One 128-element tile kk of vector xv whose values are already in registers: lane holds
+// elements 4*lane .. 4*lane+3; metadata of nonzero slot e is meta[(kk*nnz + e)*128 ...].
+template <class T, bool WIN, bool CHECK>
+__device__ __forceinline__ void tile_rounds(const CompressContigParams<T> &p, T *bins, const T (&val)[4], int64_t kk,
+                                            int64_t j0, uint32_t flag, int lane) {
+    if (flag & TILE_SLOW) {
+        for (int e = 0; e < p.nnz; ++e)
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                const bool valid = !CHECK || (j0 + t < p.L);
+                const uint32_t w = valid ? __ldg(p.meta + (kk * p.nnz + e) * 128 + lane * 4 + t) : 0u;
+                rmw_resolve<T, WIN>(bins, val[t], w, valid, p.bin_lo, p.bin_cnt, lane);
+            }
+        return;
+    }
     for (int e = 0; e < p.nnz; ++e) {
         const uint32_t *mp = p.meta + (kk * p.nnz + e) * 128 + lane * 4;
         uint32_t mw[4];
@@ -156,28 +188,69 @@ __device__ __forceinline__ void do_tile(const CompressContigParams<T> &p, T *bin
             for (int t = 0; t < 4; ++t) mw[t] = (j0 + t < p.L) ? __ldg(mp + t) : 0u;
         }
 #pragma unroll
-        for (int t = 0; t < 4; ++t) bin_add<T, WIN>(bins, val[t], mw[t], !CHECK || (j0 + t < p.L), p.bin_lo, p.bin_cnt, lane);
+        for (int t = 0; t < 4; ++t) {
+            const bool valid = !CHECK || (j0 + t < p.L);
+            rmw<T, WIN>(bins, val[t], mw[t], valid && !(mw[t] & BIT_DEFER), p.bin_lo, p.bin_cnt);
+            __syncwarp();
+        }
+    }
+    if (flag) {  // extra rounds for the deferred items (warp-uniform)
+        const int R = (int)(flag & 0xffu);
+        const uint32_t *xp = p.extra + (int64_t)(flag >> 8) * 32 + lane;
+        for (int r = 0; r < R; ++r) {
+            const uint32_t w = __ldg(xp + r * 32);
+            rmw<T, WIN>(bins, pick4(val, (w >> 22) & 3u), w, (w & BIT_VALID) != 0u, p.bin_lo, p.bin_cnt);
+            __syncwarp();
+        }
     }
 }
 
-// U full tiles in flight per warp (CountSketch path: data and metadata prefetched).
-template <class T, bool VEC, bool WIN, int U>
-__device__ __forceinline__ void do_tiles_nnz1(const CompressContigParams<T> &p, T *bins, const T *xv, int64_t kk,
-                                              int lane) {
+// U full CountSketch tiles held in registers.
+template <class T, int U>
+struct Batch {
     T val[U][4];
-    uint32_t mw[U][4];
+    uint32_t mw[U][4], fl[U];
+    template <bool VEC>
+    __device__ __forceinline__ void load_(const CompressContigParams<T> &p, const T *xv, int64_t k, int lane) {
 #pragma unroll
-    for (int b = 0; b < U; ++b) {
-        const int64_t j0 = (kk + b) * 128 + lane * 4;
-        load4<T, VEC>(xv, j0, p.L, true, val[b]);
-        const uint4 q = __ldg(reinterpret_cast<const uint4 *>(p.meta + j0));
-        mw[b][0] = q.x; mw[b][1] = q.y; mw[b][2] = q.z; mw[b][3] = q.w;
+        for (int b = 0; b < U; ++b) {
+            const int64_t j0 = (k + b) * 128 + lane * 4;
+            load4<T, VEC>(xv, j0, p.L, true, val[b]);
+            const uint4 q = __ldg(reinterpret_cast<const uint4 *>(p.meta + j0));
+            mw[b][0] = q.x; mw[b][1] = q.y; mw[b][2] = q.z; mw[b][3] = q.w;
+            fl[b] = __ldg(p.tile_flags + k + b);
+        }
     }
+    __device__ __forceinline__ void load(const CompressContigParams<T> &p, const T *xv, int64_t k, int lane) {
+        // vector loads when the column start is 16-byte aligned
+        if ((reinterpret_cast<uintptr_t>(xv) & 15u) == 0) load_<true>(p, xv, k, lane);
+        else load_<false>(p, xv, k, lane);
+    }
+    template <bool WIN>
+    __device__ __forceinline__ void run(const CompressContigParams<T> &p, T *bins, int64_t k, int lane) {
 #pragma unroll
-    for (int b = 0; b < U; ++b)
+        for (int b = 0; b < U; ++b) {
+            if (fl[b] & TILE_SLOW) {
+                tile_rounds<T, WIN, false>(p, bins, val[b], k + b, (k + b) * 128 + lane * 4, fl[b], lane);
+                continue;
+            }
 #pragma unroll
-        for (int t = 0; t < 4; ++t) bin_add<T, WIN>(bins, val[b][t], mw[b][t], true, p.bin_lo, p.bin_cnt, lane);
-}
+            for (int t = 0; t < 4; ++t) {
+                rmw<T, WIN>(bins, val[b][t], mw[b][t], !(mw[b][t] & BIT_DEFER), p.bin_lo, p.bin_cnt);
+                __syncwarp();
+            }
+            if (fl[b]) {
+                const int R = (int)(fl[b] & 0xffu);
+                const uint32_t *xp = p.extra + (int64_t)(fl[b] >> 8) * 32 + lane;
+                for (int r = 0; r < R; ++r) {
+                    const uint32_t w = __ldg(xp + r * 32);
+                    rmw<T, WIN>(bins, pick4(val[b], (w >> 22) & 3u), w, (w & BIT_VALID) != 0u, p.bin_lo, p.bin_cnt);
+                    __syncwarp();
+                }
+            }
+        }
+    }
+};
 
 template <class T, bool VEC, bool WIN, bool NNZ1>
 __global__ void __launch_bounds__(384) compress_contig_kernel(CompressContigParams<T> p) {
@@ -203,10 +276,163 @@ __global__ void __launch_bounds__(384) compress_contig_kernel(CompressContigPara
         int64_t k = u - vbeg;
         const int64_t kfull = min(kend, full_tiles);
         if constexpr (NNZ1) {
-            for (; k + U <= kfull; k += U) do_tiles_nnz1<T, VEC, WIN, U>(p, bins, xv, k, lane);
+            // CountSketch: batches of U tiles (data, metadata, flags); the next batch's loads
+            // are issued before the current batch is processed (register double buffer).
+            Batch<T, U> ba, bb;
+            if (k + U <= kfull) ba.load(p, xv, k, lane);
+            while (k + U <= kfull) {
+                if (k + 2 * U <= kfull) bb.load(p, xv, k + U, lane);
+                ba.template run<WIN>(p, bins, k, lane);
+                k += U;
+                if (k + U > kfull) break;
+                if (k + 2 * U <= kfull) ba.load(p, xv, k + U, lane);
+                bb.template run<WIN>(p, bins, k, lane);
+                k += U;
+            }
         }
-        for (; k < kfull; ++k) do_tile<T, VEC, WIN, false>(p, bins, xv, k, lane);
-        for (; k < kend; ++k) do_tile<T, VEC, WIN, true>(p, bins, xv, k, lane);
+        for (; k < kend; ++k) {
+            const int64_t j0 = k * 128 + lane * 4;
+            T val[4];
+            const uint32_t fl = __ldg(p.tile_flags + k);
+            if (k < kfull) {
+                load4<T, VEC>(xv, j0, p.L, true, val);
+                tile_rounds<T, WIN, false>(p, bins, val, k, j0, fl, lane);
+            } else {
+                load4<T, VEC>(xv, j0, p.L, true, val);
+                tile_rounds<T, WIN, true>(p, bins, val, k, j0, fl, lane);
+            }
+        }
+        const bool exclusive = (u0 <= vbeg) && (vbeg + p.tpv <= u1);
+        flush_vector(p, bins, g, v, exclusive, lane);
+        u = vbeg + kend;
+        ++v;
+    }
+}
+
+// ---- CountSketch, 512-element batches ------------------------------------------------
+// Lane holds elements 4*lane + (i & 3) of tile (i >> 2) of the batch in val[i].  All
+// non-deferred elements of a batch have distinct buckets, so the batch's 16 reads of
+// the bins are issued before its 16 writes.  Deferred elements are written, sign applied,
+// to the warp's list at the position their metadata carries (bits 22..27); then up to two
+// extra rounds add list entry r*32 + lane to bucket xbucket[batch*64 + r*32 + lane].
+template <class T, bool CHECK>
+struct CsBatch {
+    T val[16];
+    uint32_t mw[16];
+    uint32_t fl, xb0, xb1;
+    template <bool VEC>
+    __device__ __forceinline__ void load(const CompressContigParams<T> &p, const T *xv, int64_t bt, int lane) {
+#pragma unroll
+        for (int tb = 0; tb < 4; ++tb) {
+            const int64_t j0 = bt * 512 + tb * 128 + lane * 4;
+            T v4[4];
+            load4<T, VEC>(xv, j0, p.L, true, v4);
+#pragma unroll
+            for (int t = 0; t < 4; ++t) val[tb * 4 + t] = v4[t];
+            if (!CHECK || j0 + 3 < p.L) {
+                const uint4 q = __ldg(reinterpret_cast<const uint4 *>(p.meta + j0));
+                mw[tb * 4] = q.x; mw[tb * 4 + 1] = q.y; mw[tb * 4 + 2] = q.z; mw[tb * 4 + 3] = q.w;
+            } else {
+#pragma unroll
+                for (int t = 0; t < 4; ++t) mw[tb * 4 + t] = (j0 + t < p.L) ? __ldg(p.meta + j0 + t) : 0u;
+            }
+        }
+        fl = __ldg(p.tile_flags + bt);
+        xb0 = __ldg(p.extra + bt * 64 + lane);
+        xb1 = __ldg(p.extra + bt * 64 + 32 + lane);
+    }
+    template <bool WIN>
+    __device__ __forceinline__ void run(const CompressContigParams<T> &p, T *bins, T *list, int64_t bt, int lane) {
+        if (fl & TILE_SLOW) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                const bool valid = !CHECK || (bt * 512 + (i >> 2) * 128 + lane * 4 + (i & 3) < p.L);
+                rmw_resolve<T, WIN>(bins, val[i], mw[i], valid, p.bin_lo, p.bin_cnt, lane);
+            }
+            return;
+        }
+        int bi[16];
+        bool on[16];
+        T old[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            const bool valid = !CHECK || (bt * 512 + (i >> 2) * 128 + lane * 4 + (i & 3) < p.L);
+            const bool defer = (mw[i] & BIT_DEFER) != 0u;
+            bi[i] = (int)(mw[i] & BUCKET_MASK);
+            on[i] = valid && !defer;
+            if constexpr (WIN) {
+                bi[i] -= (int)p.bin_lo;
+                on[i] = on[i] && (unsigned)bi[i] < (unsigned)p.bin_cnt;
+            }
+            old[i] = on[i] ? bins[bi[i]] : T(0);
+            if (valid && defer) list[(mw[i] >> 22) & 63u] = apply_sign(val[i], mw[i]);
+        }
+#pragma unroll
+        for (int i = 0; i < 16; ++i)
+            if (on[i]) bins[bi[i]] = old[i] + apply_sign(val[i], mw[i]);
+        __syncwarp();
+        const uint32_t R = fl;
+        if (R > 0u) {
+            int b = (int)xb0;
+            bool ok = xb0 != 0xffffffffu;
+            if constexpr (WIN) {
+                b -= (int)p.bin_lo;
+                ok = ok && (unsigned)b < (unsigned)p.bin_cnt;
+            }
+            if (ok) bins[b] += list[lane];
+            __syncwarp();
+            if (R > 1u) {
+                b = (int)xb1;
+                ok = xb1 != 0xffffffffu;
+                if constexpr (WIN) {
+                    b -= (int)p.bin_lo;
+                    ok = ok && (unsigned)b < (unsigned)p.bin_cnt;
+                }
+                if (ok) bins[b] += list[32 + lane];
+                __syncwarp();
+            }
+        }
+    }
+};
+
+template <class T, bool VEC, bool WIN>
+__global__ void __launch_bounds__(384) cs_compress_kernel(CompressContigParams<T> p) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int warps = blockDim.x >> 5;
+    const int g = blockIdx.x * warps + wib;
+    T *bins = reinterpret_cast<T *>(smem_raw) + (int64_t)wib * p.bin_cnt;
+    T *list = reinterpret_cast<T *>(smem_raw) + (int64_t)warps * p.bin_cnt + wib * 64;
+    for (int i = lane; i < p.bin_cnt; i += 32) bins[i] = T(0);
+    __syncwarp();
+    if (g >= p.split.W) return;
+    const int64_t u0 = p.split.start(g), u1 = p.split.start(g + 1);
+    if (u0 >= u1) return;
+    const int64_t full = p.L / 512;  // batches with all 512 elements inside the vector
+    int64_t v = u0 / p.tpv;
+    int64_t u = u0;
+    while (u < u1) {
+        const int64_t vbeg = v * p.tpv;
+        const int64_t kend = min(u1, vbeg + p.tpv) - vbeg;
+        const T *xv = p.X + v * p.x_ld;
+        int64_t k = u - vbeg;
+        const int64_t kfull = min(kend, full);
+        CsBatch<T, false> ba, bb;
+        if (k < kfull) ba.template load<VEC>(p, xv, k, lane);
+        while (k < kfull) {
+            if (k + 1 < kfull) bb.template load<VEC>(p, xv, k + 1, lane);
+            ba.template run<WIN>(p, bins, list, k, lane);
+            if (++k >= kfull) break;
+            if (k + 1 < kfull) ba.template load<VEC>(p, xv, k + 1, lane);
+            bb.template run<WIN>(p, bins, list, k, lane);
+            ++k;
+        }
+        for (; k < kend; ++k) {
+            CsBatch<T, true> bc;
+            bc.template load<false>(p, xv, k, lane);
+            bc.template run<WIN>(p, bins, list, k, lane);
+        }
         const bool exclusive = (u0 <= vbeg) && (vbeg + p.tpv <= u1);
         flush_vector(p, bins, g, v, exclusive, lane);
         u = vbeg + kend;
@@ -344,27 +570,30 @@ int sparse_compress(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_t x_es
     if (nv == 0) return RLA_OK;
     if (x_es == 1) {
         // contiguous vectors
-        int warps = (int)std::min<int64_t>(12, cap / (int64_t)(s * es));
+        if (!sk->tile_flags)
+            return set_error(ctx, RLA_E_UNSUPPORTED, "compression dimension above 2^22 on the contiguous-vector path");
+        int warps = (int)std::min<int64_t>(12, cap / (int64_t)((s + 64) * es));
         int bin_cnt = (int)s;
         if (warps < 1) {
             warps = 4;
-            bin_cnt = (int)(cap / (4 * es));
+            bin_cnt = (int)(cap / (4 * es)) - 64;
         }
-        const int64_t tpv = ceil_div(L, 128);
+        const bool bm = sk->batch_mode != 0;          // CountSketch: 512-element batches
+        const int64_t tpv = bm ? ceil_div(L, 512) : ceil_div(L, 128);
         const int64_t total = tpv * nv;
-        const int blocks_per_sm = std::max(1, cap / (int)(warps * bin_cnt * es + 1));
+        const int blocks_per_sm = std::max(1, cap / (int)(warps * (bin_cnt + 64) * es + 1));
         int64_t W = (int64_t)ctx->sm_count * blocks_per_sm * warps;
         W = std::min<int64_t>(W, nv * 8);
-        W = std::min<int64_t>(W, ceil_div(total, 4));
+        W = std::min<int64_t>(W, bm ? total : ceil_div(total, 4));
         W = std::max<int64_t>(W, 1);
         const int blocks = ceil_div_i(W, warps);
-        const size_t smem = (size_t)warps * bin_cnt * es;
+        const size_t smem = (size_t)warps * (bin_cnt + 64) * es;
         void *part = nullptr;
         int *cnt = nullptr;
         RLA_TRY(scratch_get(ctx, (size_t)(2 * W) * bin_cnt * es, &part));
         RLA_TRY(counters_get(ctx, (size_t)nv, &cnt));
         const bool vec = (x_vs % (16 / es) == 0) && ((uintptr_t)X % 16 == 0);
-        CompressContigParams<T> p{X, x_vs, L, nv, sk->meta, (int)sk->nnz, 0, bin_cnt, Y, y_es, y_vs, a, (T)beta,
+        CompressContigParams<T> p{X, x_vs, L, nv, sk->meta, sk->tile_flags, sk->extra, (int)sk->nnz, 0, bin_cnt, Y, y_es, y_vs, a, (T)beta,
                                   beta_zero, (T *)part, cnt, tpv, Split::make(total, (int)W)};
         for (int64_t lo = 0; lo < s; lo += bin_cnt) {
             p.bin_lo = lo;
@@ -375,6 +604,12 @@ int sparse_compress(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_t x_es
             };
             const bool win = p.bin_cnt < s;
             const bool n1 = sk->nnz == 1;
+            if (bm) {
+                if (vec) { if (win) launch(cs_compress_kernel<T, true, true>); else launch(cs_compress_kernel<T, true, false>); }
+                else { if (win) launch(cs_compress_kernel<T, false, true>); else launch(cs_compress_kernel<T, false, false>); }
+                RLA_TRY(check_launch(ctx, "cs_compress"));
+                continue;
+            }
 #define RLA_CC(V, W, N) launch(compress_contig_kernel<T, V, W, N>)
             if (vec) {
                 if (win) { if (n1) RLA_CC(true, true, true); else RLA_CC(true, true, false); }
