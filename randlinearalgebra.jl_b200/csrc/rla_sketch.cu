@@ -168,17 +168,21 @@ __global__ void __launch_bounds__(SCHED_WARPS * 32) sparse_sched_kernel(const in
 // CountSketch (nnz = 1, s <= 2^16): 512-element batches (4 tiles, 16 sub-rounds of 32
 // lanes).  An element is deferred when its bucket already occurred earlier in the batch,
 // in (sub-round, lane) order, so all non-deferred elements of a batch hit distinct bins and
-// the apply kernel issues a whole batch's read-modify-writes at once.  Deferred elements
-// are written by the apply kernel to a per-warp list (their list position is in bits
-// 22..27 of their word) and added in up to CS_XROUNDS extra rounds of 32 entries, any lane
-// taking any entry; the list is ordered here so that each round's buckets are distinct.
-// xbucket[batch*64 + k] holds entry k's bucket (0xffffffff when empty); flags[batch] is the
-// number of extra rounds, or TILE_SLOW when the batch needs run-time resolution.
+// the apply kernel issues a whole batch's read-modify-writes at once.  The apply kernel's
+// shared memory holds, per warp, s bins, a 64-entry list and 32 dummy slots; each element's
+// word is the byte offset (element size es) of the slot it is added to -- its bin, or for a
+// deferred element its list entry -- with the sign in bit 31.  Up to CS_XROUNDS extra
+// rounds then add list entry r*32 + lane to the bin at byte offset xbucket[batch*64 +
+// r*32 + lane] and clear the entry; the list is ordered here so that each round's buckets
+// are distinct, and empty entries point at the lane's dummy slot.  flags[batch] is the
+// number of extra rounds, or TILE_SLOW when the batch needs run-time resolution (its words
+// then all point at bins).
 constexpr int CS_SCHED_WARPS = 4, CS_BATCH = 512, CS_XROUNDS = 2;
 
 __global__ void __launch_bounds__(CS_SCHED_WARPS * 32) cs_sched_kernel(const int32_t *bucket, const uint8_t *negative,
-                                                                        int64_t L, int64_t s, uint32_t *meta,
-                                                                        uint32_t *flags, uint32_t *xbucket) {
+                                                                        int64_t L, int64_t s, uint32_t es,
+                                                                        uint32_t *meta, uint32_t *flags,
+                                                                        uint32_t *xbucket) {
     extern __shared__ uint32_t bm_all[];
     __shared__ uint32_t list[CS_SCHED_WARPS][MAX_DEFER];
     __shared__ uint32_t slot[CS_SCHED_WARPS][CS_XROUNDS * 32];
@@ -216,7 +220,7 @@ __global__ void __launch_bounds__(CS_SCHED_WARPS * 32) cs_sched_kernel(const int
             mylist[r] = pos;
         }
         cnt += __popc(bal);
-        myword[r] = valid ? (b | ((uint32_t)defer << 30) | (neg << 31)) : 0u;
+        myword[r] = (b * es) | (neg << 31);
     }
     __syncwarp();
     // order the deferred entries into rounds of 32 with distinct buckets (lane 0, greedy)
@@ -250,11 +254,13 @@ __global__ void __launch_bounds__(CS_SCHED_WARPS * 32) cs_sched_kernel(const int
         const int64_t j = batch * CS_BATCH + (r >> 2) * 128 + 4 * lane + (r & 3);
         if (j >= L) continue;
         uint32_t word = myword[r];
-        if (R >= 0 && mylist[r] >= 0) word |= (uint32_t)pos_of[w][mylist[r]] << 22;
+        if (R >= 0 && mylist[r] >= 0)
+            word = ((uint32_t)(s + pos_of[w][mylist[r]]) * es) | (word & 0x80000000u);
         meta[j] = word;
     }
+    const uint32_t dummy = (uint32_t)(s + 64 + lane) * es;
     for (int k = lane; k < CS_XROUNDS * 32; k += 32)
-        xbucket[batch * 64 + k] = (R > 0) ? slot[w][k] : 0xffffffffu;
+        xbucket[batch * 64 + k] = (R > 0 && slot[w][k] != 0xffffffffu) ? slot[w][k] * es : dummy;
     if (lane == 0) flags[batch] = R < 0 ? TILE_SLOW : (uint32_t)R;
 }
 
@@ -448,7 +454,8 @@ static int build_meta(rla_ctx *ctx, rla_sketch *sk) {
         if (bm_bytes > 48 * 1024)
             RLA_CUDA_TRY(ctx, cudaFuncSetAttribute(cs_sched_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bm_bytes));
         cs_sched_kernel<<<ceil_div_i(nb, CS_SCHED_WARPS), CS_SCHED_WARPS * 32, bm_bytes, ctx->stream>>>(
-            sk->bucket, sk->negative, sk->L, sk->s, sk->meta, sk->tile_flags, sk->extra);
+            sk->bucket, sk->negative, sk->L, sk->s, (uint32_t)dtype_size(sk->p.dtype), sk->meta, sk->tile_flags,
+            sk->extra);
         return check_launch(ctx, "cs_sched");
     }
     const int64_t ntile = ceil_div(sk->L, 128);

@@ -113,15 +113,57 @@ __device__ __forceinline__ void load4(const T *xv, int64_t j0, int64_t L, bool t
     }
 }
 
+// 16-byte vector of T
+template <class T>
+struct V16 {
+    using type = float4;
+};
+template <>
+struct V16<double> {
+    using type = double2;
+};
+
+// Finish this warp's share of output vector v: write it (alpha/beta epilogue) when the warp
+// covered the whole vector, else store the partial bins and let the last warp to arrive add
+// all partials in warp order.  Moves 16 bytes per access when the bin count allows it.
 template <class T>
 __device__ void flush_vector(const CompressContigParams<T> &p, T *bins, int g, int64_t v, bool exclusive, int lane) {
+    constexpr int N = 16 / (int)sizeof(T);
+    using V = typename V16<T>::type;
     __syncwarp();
+    const int nvec = (p.bin_cnt % N == 0) ? p.bin_cnt / N : 0;
+    T *y0 = p.Y + p.bin_lo * p.y_es + v * p.y_vs;
+    const bool yvec = p.y_es == 1 && (reinterpret_cast<uintptr_t>(y0) & 15u) == 0;
+    auto out = [&](int64_t i, T acc) {
+        T *yp = y0 + i * p.y_es;
+        T r = p.alpha * acc;
+        if (!p.beta_zero) r += p.beta * *yp;
+        *yp = r;
+    };
+    auto out_vec = [&](int q, V acc) {
+        const T *a = reinterpret_cast<const T *>(&acc);
+        if (yvec) {
+            V y;
+            T *ya = reinterpret_cast<T *>(&y);
+            if (!p.beta_zero) y = *reinterpret_cast<const V *>(y0 + (int64_t)q * N);
+#pragma unroll
+            for (int e = 0; e < N; ++e) ya[e] = p.beta_zero ? p.alpha * a[e] : p.alpha * a[e] + p.beta * ya[e];
+            *reinterpret_cast<V *>(y0 + (int64_t)q * N) = y;
+        } else {
+#pragma unroll
+            for (int e = 0; e < N; ++e) out((int64_t)q * N + e, a[e]);
+        }
+    };
+    V *bv = reinterpret_cast<V *>(bins);
+    const V zero{};
     if (exclusive) {
-        for (int i = lane; i < p.bin_cnt; i += 32) {
-            T *yp = p.Y + (p.bin_lo + i) * p.y_es + v * p.y_vs;
-            T r = p.alpha * bins[i];
-            if (!p.beta_zero) r += p.beta * *yp;
-            *yp = r;
+        for (int q = lane; q < nvec; q += 32) {
+            const V b = bv[q];
+            bv[q] = zero;
+            out_vec(q, b);
+        }
+        for (int i = nvec * N + lane; i < p.bin_cnt; i += 32) {
+            out(i, bins[i]);
             bins[i] = T(0);
         }
         __syncwarp();
@@ -129,7 +171,11 @@ __device__ void flush_vector(const CompressContigParams<T> &p, T *bins, int g, i
     }
     const int64_t vbeg = v * p.tpv;
     T *part = p.partials + (int64_t)p.split.slot(g, vbeg) * p.bin_cnt;
-    for (int i = lane; i < p.bin_cnt; i += 32) {
+    for (int q = lane; q < nvec; q += 32) {
+        reinterpret_cast<V *>(part)[q] = bv[q];
+        bv[q] = zero;
+    }
+    for (int i = nvec * N + lane; i < p.bin_cnt; i += 32) {
         part[i] = bins[i];
         bins[i] = T(0);
     }
@@ -142,13 +188,22 @@ __device__ void flush_vector(const CompressContigParams<T> &p, T *bins, int g, i
     if (old == gl - gf) {
         __threadfence();
         const T *p0 = p.partials + (int64_t)p.split.slot(gf, vbeg) * p.bin_cnt;
-        for (int i = lane; i < p.bin_cnt; i += 32) {
+        for (int q = lane; q < nvec; q += 32) {
+            V acc = __ldcg(reinterpret_cast<const V *>(p0) + q);
+            T *a = reinterpret_cast<T *>(&acc);
+#pragma unroll 4
+            for (int gg = gf + 1; gg <= gl; ++gg) {
+                const V x = __ldcg(reinterpret_cast<const V *>(p.partials + (int64_t)(2 * gg) * p.bin_cnt) + q);
+                const T *xe = reinterpret_cast<const T *>(&x);
+#pragma unroll
+                for (int e = 0; e < N; ++e) a[e] += xe[e];
+            }
+            out_vec(q, acc);
+        }
+        for (int i = nvec * N + lane; i < p.bin_cnt; i += 32) {
             T acc = __ldcg(p0 + i);
             for (int gg = gf + 1; gg <= gl; ++gg) acc += __ldcg(p.partials + (int64_t)(2 * gg) * p.bin_cnt + i);
-            T *yp = p.Y + (p.bin_lo + i) * p.y_es + v * p.y_vs;
-            T r = p.alpha * acc;
-            if (!p.beta_zero) r += p.beta * *yp;
-            *yp = r;
+            out(i, acc);
         }
         if (lane == 0) p.counters[v] = 0;
     }
@@ -310,18 +365,82 @@ __global__ void __launch_bounds__(384) compress_contig_kernel(CompressContigPara
 }
 
 // ---- CountSketch, 512-element batches ------------------------------------------------
-// Lane holds elements 4*lane + (i & 3) of tile (i >> 2) of the batch in val[i].  All
-// non-deferred elements of a batch have distinct buckets, so the batch's 16 reads of
-// the bins are issued before its 16 writes.  Deferred elements are written, sign applied,
-// to the warp's list at the position their metadata carries (bits 22..27); then up to two
-// extra rounds add list entry r*32 + lane to bucket xbucket[batch*64 + r*32 + lane].
+// One warp per CTA.  Shared memory: [bins (bin_cnt) | list (64) | dummy (32)] elements.
+// Lane holds elements 4*lane + (i & 3) of tile (i >> 2) of the batch in val[i], and their
+// words (byte offset of the target slot, sign in bit 31; see cs_sched_kernel) in mw[i].
+// All targets of a batch's main words are distinct, so its 16 reads are issued before its
+// 16 writes, with no predicates: a deferred element lands in its (cleared) list entry.  Up
+// to two extra rounds then move list entry r*32 + lane into the bin at xb[r] and clear it.
+// With WIN (bins cover [bin_lo, bin_lo + bin_cnt) of s) offsets are remapped at run time
+// and targets outside the window go to the lane's dummy slot.
+constexpr uint32_t CS_OFF_MASK = 0x00ffffffu;
+
+template <class T>
+__device__ __forceinline__ T &slot_at(unsigned char *base, uint32_t off) {
+    return *reinterpret_cast<T *>(base + off);
+}
+
+template <class T, bool WIN>
+__device__ __forceinline__ uint32_t cs_target(const CompressContigParams<T> &p, uint32_t off, uint32_t s_bytes,
+                                              uint32_t dummy) {
+    off &= CS_OFF_MASK;
+    if constexpr (WIN) {
+        const uint32_t lo = (uint32_t)p.bin_lo * sizeof(T), win = (uint32_t)p.bin_cnt * sizeof(T);
+        if (off >= s_bytes) return off - s_bytes + win;  // list entry or dummy slot
+        const uint32_t b = off - lo;                        // wraps when below the window
+        return b < win ? b : dummy;
+    }
+    return off;
+}
+
+// Run-time resolution for a batch the scheduler could not place: lanes sharing a target
+// slot are summed in lane order and the lowest lane adds the sum.
+template <class T>
+__device__ __noinline__ void cs_resolve(unsigned char *sm, T x, uint32_t o, int lane) {
+    const unsigned grp = __match_any_sync(FULL, o);
+    const int cnt = __popc(grp);
+    const int maxc = (int)__reduce_max_sync(FULL, (unsigned)cnt);
+    T sum = T(0);
+    for (int q = 0; q < maxc; ++q) {
+        const int src = q < cnt ? (int)__fns(grp, 0, q + 1) : lane;
+        const T y = __shfl_sync(FULL, x, src);
+        if (q < cnt) sum += y;
+    }
+    if ((grp & ((1u << lane) - 1u)) == 0u) slot_at<T>(sm, o) += sum;
+    __syncwarp();
+}
+
 template <class T, bool CHECK>
 struct CsBatch {
     T val[16];
     uint32_t mw[16];
     uint32_t fl, xb0, xb1;
     template <bool VEC>
-    __device__ __forceinline__ void load(const CompressContigParams<T> &p, const T *xv, int64_t bt, int lane) {
+    __device__ __forceinline__ void load(const CompressContigParams<T> &p, const T *xv, int64_t bt, int lane,
+                                         uint32_t pad) {
+        if constexpr (VEC && !CHECK) {
+            // whole batch inside the vector: 16-byte loads at immediate offsets from one base
+            const T *xb = xv + bt * 512 + lane * 4;
+            const uint4 *mb = reinterpret_cast<const uint4 *>(p.meta + bt * 512 + lane * 4);
+#pragma unroll
+            for (int tb = 0; tb < 4; ++tb) {
+                if constexpr (sizeof(T) == 4) {
+                    const float4 q = __ldg(reinterpret_cast<const float4 *>(xb + tb * 128));
+                    val[tb * 4] = q.x; val[tb * 4 + 1] = q.y; val[tb * 4 + 2] = q.z; val[tb * 4 + 3] = q.w;
+                } else {
+                    const double2 a = __ldg(reinterpret_cast<const double2 *>(xb + tb * 128));
+                    const double2 b = __ldg(reinterpret_cast<const double2 *>(xb + tb * 128 + 2));
+                    val[tb * 4] = a.x; val[tb * 4 + 1] = a.y; val[tb * 4 + 2] = b.x; val[tb * 4 + 3] = b.y;
+                }
+                const uint4 m = __ldg(mb + tb * 32);
+                mw[tb * 4] = m.x; mw[tb * 4 + 1] = m.y; mw[tb * 4 + 2] = m.z; mw[tb * 4 + 3] = m.w;
+            }
+            const uint32_t *xp = p.extra + bt * 64 + lane;
+            fl = __ldg(p.tile_flags + bt);
+            xb0 = __ldg(xp);
+            xb1 = __ldg(xp + 32);
+            return;
+        }
 #pragma unroll
         for (int tb = 0; tb < 4; ++tb) {
             const int64_t j0 = bt * 512 + tb * 128 + lane * 4;
@@ -334,7 +453,7 @@ struct CsBatch {
                 mw[tb * 4] = q.x; mw[tb * 4 + 1] = q.y; mw[tb * 4 + 2] = q.z; mw[tb * 4 + 3] = q.w;
             } else {
 #pragma unroll
-                for (int t = 0; t < 4; ++t) mw[tb * 4 + t] = (j0 + t < p.L) ? __ldg(p.meta + j0 + t) : 0u;
+                for (int t = 0; t < 4; ++t) mw[tb * 4 + t] = (j0 + t < p.L) ? __ldg(p.meta + j0 + t) : pad;
             }
         }
         fl = __ldg(p.tile_flags + bt);
@@ -342,53 +461,35 @@ struct CsBatch {
         xb1 = __ldg(p.extra + bt * 64 + 32 + lane);
     }
     template <bool WIN>
-    __device__ __forceinline__ void run(const CompressContigParams<T> &p, T *bins, T *list, int64_t bt, int lane) {
+    __device__ __forceinline__ void run(const CompressContigParams<T> &p, unsigned char *sm, uint32_t s_bytes,
+                                        uint32_t list_off, uint32_t dummy, int lane) {
         if (fl & TILE_SLOW) {
 #pragma unroll
-            for (int i = 0; i < 16; ++i) {
-                const bool valid = !CHECK || (bt * 512 + (i >> 2) * 128 + lane * 4 + (i & 3) < p.L);
-                rmw_resolve<T, WIN>(bins, val[i], mw[i], valid, p.bin_lo, p.bin_cnt, lane);
-            }
+            for (int i = 0; i < 16; ++i)
+                cs_resolve<T>(sm, apply_sign(val[i], mw[i]), cs_target<T, WIN>(p, mw[i], s_bytes, dummy), lane);
             return;
         }
-        int bi[16];
-        bool on[16];
+        uint32_t o[16];
         T old[16];
 #pragma unroll
         for (int i = 0; i < 16; ++i) {
-            const bool valid = !CHECK || (bt * 512 + (i >> 2) * 128 + lane * 4 + (i & 3) < p.L);
-            const bool defer = (mw[i] & BIT_DEFER) != 0u;
-            bi[i] = (int)(mw[i] & BUCKET_MASK);
-            on[i] = valid && !defer;
-            if constexpr (WIN) {
-                bi[i] -= (int)p.bin_lo;
-                on[i] = on[i] && (unsigned)bi[i] < (unsigned)p.bin_cnt;
-            }
-            old[i] = on[i] ? bins[bi[i]] : T(0);
-            if (valid && defer) list[(mw[i] >> 22) & 63u] = apply_sign(val[i], mw[i]);
+            o[i] = cs_target<T, WIN>(p, mw[i], s_bytes, dummy);
+            old[i] = slot_at<T>(sm, o[i]);
         }
 #pragma unroll
-        for (int i = 0; i < 16; ++i)
-            if (on[i]) bins[bi[i]] = old[i] + apply_sign(val[i], mw[i]);
+        for (int i = 0; i < 16; ++i) slot_at<T>(sm, o[i]) = old[i] + apply_sign(val[i], mw[i]);
         __syncwarp();
-        const uint32_t R = fl;
-        if (R > 0u) {
-            int b = (int)xb0;
-            bool ok = xb0 != 0xffffffffu;
-            if constexpr (WIN) {
-                b -= (int)p.bin_lo;
-                ok = ok && (unsigned)b < (unsigned)p.bin_cnt;
-            }
-            if (ok) bins[b] += list[lane];
+        if (fl > 0u) {
+            const uint32_t t0 = cs_target<T, WIN>(p, xb0, s_bytes, dummy);
+            T &e0 = slot_at<T>(sm, list_off + lane * sizeof(T));
+            slot_at<T>(sm, t0) += e0;
+            e0 = T(0);
             __syncwarp();
-            if (R > 1u) {
-                b = (int)xb1;
-                ok = xb1 != 0xffffffffu;
-                if constexpr (WIN) {
-                    b -= (int)p.bin_lo;
-                    ok = ok && (unsigned)b < (unsigned)p.bin_cnt;
-                }
-                if (ok) bins[b] += list[32 + lane];
+            if (fl > 1u) {
+                const uint32_t t1 = cs_target<T, WIN>(p, xb1, s_bytes, dummy);
+                T &e1 = slot_at<T>(sm, list_off + (32 + lane) * sizeof(T));
+                slot_at<T>(sm, t1) += e1;
+                e1 = T(0);
                 __syncwarp();
             }
         }
@@ -396,19 +497,21 @@ struct CsBatch {
 };
 
 template <class T, bool VEC, bool WIN>
-__global__ void __launch_bounds__(384) cs_compress_kernel(CompressContigParams<T> p) {
+__global__ void __launch_bounds__(32) cs_compress_kernel(CompressContigParams<T> p, int64_t s) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int lane = threadIdx.x & 31;
-    const int wib = threadIdx.x >> 5;
-    const int warps = blockDim.x >> 5;
-    const int g = blockIdx.x * warps + wib;
-    T *bins = reinterpret_cast<T *>(smem_raw) + (int64_t)wib * p.bin_cnt;
-    T *list = reinterpret_cast<T *>(smem_raw) + (int64_t)warps * p.bin_cnt + wib * 64;
-    for (int i = lane; i < p.bin_cnt; i += 32) bins[i] = T(0);
+    const int lane = threadIdx.x;
+    const int g = blockIdx.x;
+    T *bins = reinterpret_cast<T *>(smem_raw);
+    for (int i = lane; i < p.bin_cnt + 96; i += 32) bins[i] = T(0);
     __syncwarp();
     if (g >= p.split.W) return;
     const int64_t u0 = p.split.start(g), u1 = p.split.start(g + 1);
     if (u0 >= u1) return;
+    const uint32_t s_bytes = (uint32_t)(s * (int64_t)sizeof(T));
+    const uint32_t list_off = (uint32_t)p.bin_cnt * sizeof(T);
+    const uint32_t dummy = list_off + (64 + lane) * sizeof(T);
+    // a padding element's word: the lane's dummy slot, in the unwindowed encoding
+    const uint32_t pad = (uint32_t)((s + 64 + lane) * (int64_t)sizeof(T));
     const int64_t full = p.L / 512;  // batches with all 512 elements inside the vector
     int64_t v = u0 / p.tpv;
     int64_t u = u0;
@@ -419,19 +522,19 @@ __global__ void __launch_bounds__(384) cs_compress_kernel(CompressContigParams<T
         int64_t k = u - vbeg;
         const int64_t kfull = min(kend, full);
         CsBatch<T, false> ba, bb;
-        if (k < kfull) ba.template load<VEC>(p, xv, k, lane);
+        if (k < kfull) ba.template load<VEC>(p, xv, k, lane, pad);
         while (k < kfull) {
-            if (k + 1 < kfull) bb.template load<VEC>(p, xv, k + 1, lane);
-            ba.template run<WIN>(p, bins, list, k, lane);
+            if (k + 1 < kfull) bb.template load<VEC>(p, xv, k + 1, lane, pad);
+            ba.template run<WIN>(p, smem_raw, s_bytes, list_off, dummy, lane);
             if (++k >= kfull) break;
-            if (k + 1 < kfull) ba.template load<VEC>(p, xv, k + 1, lane);
-            bb.template run<WIN>(p, bins, list, k, lane);
+            if (k + 1 < kfull) ba.template load<VEC>(p, xv, k + 1, lane, pad);
+            bb.template run<WIN>(p, smem_raw, s_bytes, list_off, dummy, lane);
             ++k;
         }
         for (; k < kend; ++k) {
             CsBatch<T, true> bc;
-            bc.template load<false>(p, xv, k, lane);
-            bc.template run<WIN>(p, bins, list, k, lane);
+            bc.template load<false>(p, xv, k, lane, pad);
+            bc.template run<WIN>(p, smem_raw, s_bytes, list_off, dummy, lane);
         }
         const bool exclusive = (u0 <= vbeg) && (vbeg + p.tpv <= u1);
         flush_vector(p, bins, g, v, exclusive, lane);
@@ -581,10 +684,38 @@ int sparse_compress(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_t x_es
         const bool bm = sk->batch_mode != 0;          // CountSketch: 512-element batches
         const int64_t tpv = bm ? ceil_div(L, 512) : ceil_div(L, 128);
         const int64_t total = tpv * nv;
+        const bool vec = (x_vs % (16 / es) == 0) && ((uintptr_t)X % 16 == 0);
+        if (bm) {
+            // one warp per CTA: bins + 64 list entries + 32 dummy slots
+            int bins_cs = (int)s;
+            if ((int64_t)(s + 96) * (int64_t)es > cap) bins_cs = (int)(cap / (4 * es)) - 96;
+            const size_t smem = (size_t)(bins_cs + 96) * es;
+            const bool win = bins_cs < s;
+            auto kern = win ? (vec ? cs_compress_kernel<T, true, true> : cs_compress_kernel<T, false, true>)
+                            : (vec ? cs_compress_kernel<T, true, false> : cs_compress_kernel<T, false, false>);
+            RLA_CUDA_TRY(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            int per_sm = 1;
+            RLA_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32, smem));
+            int64_t W = (int64_t)ctx->sm_count * std::max(per_sm, 1);
+            W = std::max<int64_t>(1, std::min<int64_t>(W, ceil_div(total, 32)));
+            void *part = nullptr;
+            int *cnt = nullptr;
+            RLA_TRY(scratch_get(ctx, (size_t)(2 * W) * bins_cs * es, &part));
+            RLA_TRY(counters_get(ctx, (size_t)nv, &cnt));
+            CompressContigParams<T> p{X, x_vs, L, nv, sk->meta, sk->tile_flags, sk->extra, (int)sk->nnz, 0, bins_cs, Y, y_es,
+                                      y_vs, a, (T)beta, beta_zero, (T *)part, cnt, tpv, Split::make(total, (int)W)};
+            for (int64_t lo = 0; lo < s; lo += bins_cs) {
+                p.bin_lo = lo;
+                p.bin_cnt = (int)std::min<int64_t>(bins_cs, s - lo);
+                kern<<<(int)W, 32, smem, ctx->stream>>>(p, s);
+                RLA_TRY(check_launch(ctx, "cs_compress"));
+            }
+            return RLA_OK;
+        }
         const int blocks_per_sm = std::max(1, cap / (int)(warps * (bin_cnt + 64) * es + 1));
         int64_t W = (int64_t)ctx->sm_count * blocks_per_sm * warps;
         W = std::min<int64_t>(W, nv * 8);
-        W = std::min<int64_t>(W, bm ? total : ceil_div(total, 4));
+        W = std::min<int64_t>(W, ceil_div(total, 4));
         W = std::max<int64_t>(W, 1);
         const int blocks = ceil_div_i(W, warps);
         const size_t smem = (size_t)warps * (bin_cnt + 64) * es;
@@ -592,7 +723,6 @@ int sparse_compress(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_t x_es
         int *cnt = nullptr;
         RLA_TRY(scratch_get(ctx, (size_t)(2 * W) * bin_cnt * es, &part));
         RLA_TRY(counters_get(ctx, (size_t)nv, &cnt));
-        const bool vec = (x_vs % (16 / es) == 0) && ((uintptr_t)X % 16 == 0);
         CompressContigParams<T> p{X, x_vs, L, nv, sk->meta, sk->tile_flags, sk->extra, (int)sk->nnz, 0, bin_cnt, Y, y_es, y_vs, a, (T)beta,
                                   beta_zero, (T *)part, cnt, tpv, Split::make(total, (int)W)};
         for (int64_t lo = 0; lo < s; lo += bin_cnt) {
@@ -604,12 +734,6 @@ int sparse_compress(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_t x_es
             };
             const bool win = p.bin_cnt < s;
             const bool n1 = sk->nnz == 1;
-            if (bm) {
-                if (vec) { if (win) launch(cs_compress_kernel<T, true, true>); else launch(cs_compress_kernel<T, true, false>); }
-                else { if (win) launch(cs_compress_kernel<T, false, true>); else launch(cs_compress_kernel<T, false, false>); }
-                RLA_TRY(check_launch(ctx, "cs_compress"));
-                continue;
-            }
 #define RLA_CC(V, W, N) launch(compress_contig_kernel<T, V, W, N>)
             if (vec) {
                 if (win) { if (n1) RLA_CC(true, true, true); else RLA_CC(true, true, false); }

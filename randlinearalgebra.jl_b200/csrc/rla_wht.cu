@@ -148,25 +148,28 @@ __device__ __forceinline__ void load_chunk(const T *__restrict__ xv, int64_t cba
     }
 }
 
-template <class T, bool VEC>
+// SPT = sampled rows per thread: thread t owns samples t + k*NT (k < SPT) of the window,
+// keeping their packed (r1, swizzled r2) and their accumulators in registers.
+template <class T, bool VEC, int SPT>
 __global__ void __launch_bounds__(1 << WhtCfg<T>::TB, 2) srht_fused_kernel(SrhtParams<T> p) {
     constexpr int TB = WhtCfg<T>::TB, VB = WhtCfg<T>::VB;
     constexpr int CH = 2 * TB, NT = 1 << TB, VW = 1 << VB, KV = 1 << (TB - VB);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *Z = reinterpret_cast<T *>(smem_raw);
-    T *acc = Z + (1 << CH);
-    uint32_t *srow = reinterpret_cast<uint32_t *>(acc + p.s_cnt);  // (r1 << CH) | swz(r2)
     __shared__ int last_flag;
     const int t = threadIdx.x;
     const int g = blockIdx.x;
-    for (int i = t; i < p.s_cnt; i += NT) {
-        acc[i] = T(0);
-        const uint32_t row = (uint32_t)__ldg(p.rows + p.s_lo + i);
-        srow[i] = ((row >> CH) << CH) | (uint32_t)swz<TB, VB>((int)(row & ((1u << CH) - 1)));
-    }
-    __syncthreads();
     const int64_t u0 = p.split.start(g), u1 = p.split.start(g + 1);
     if (u0 >= u1) return;
+    T acc[SPT];
+    uint32_t sr[SPT];
+#pragma unroll
+    for (int k = 0; k < SPT; ++k) {
+        const int i = t + k * NT;
+        acc[k] = T(0);
+        const uint32_t row = i < p.s_cnt ? (uint32_t)__ldg(p.rows + p.s_lo + i) : 0u;
+        sr[k] = ((row >> CH) << CH) | (uint32_t)swz<TB, VB>((int)(row & ((1u << CH) - 1)));
+    }
     const int t_lo = t & (VW - 1), t_hi = t >> VB;
     // The swizzle only permutes the low 3 bits of a vector index, so every address this
     // thread touches is one of 8 per-thread bases plus a compile-time offset.
@@ -218,11 +221,10 @@ __global__ void __launch_bounds__(1 << WhtCfg<T>::TB, 2) srht_fused_kernel(SrhtP
             sg = __ldg(p.sign_tl + c * NT + t);
         }
         const uint32_t cc = (uint32_t)ccur;
-#pragma unroll 4
-        for (int i = t; i < p.s_cnt; i += NT) {
-            const uint32_t pk = srow[i];
-            const T z = Z[pk & ((1u << CH) - 1)];
-            acc[i] += (__popc((pk >> CH) & cc) & 1) ? -z : z;
+#pragma unroll
+        for (int k = 0; k < SPT; ++k) {
+            const T z = Z[sr[k] & ((1u << CH) - 1)];
+            acc[k] += (__popc((sr[k] >> CH) & cc) & 1) ? -z : z;
         }
         __syncthreads();
         const bool col_done = (u + 1 == u1) || (ccur + 1 == p.cpv);
@@ -231,18 +233,24 @@ __global__ void __launch_bounds__(1 << WhtCfg<T>::TB, 2) srht_fused_kernel(SrhtP
         const int64_t vbeg = vcur * p.cpv;
         const bool exclusive = (u0 <= vbeg) && (vbeg + p.cpv <= u1);
         if (exclusive) {
-            for (int i = t; i < p.s_cnt; i += NT) {
-                T *yp = p.Y + (p.s_lo + i) * p.y_es + vcur * p.y_vs;
-                T res = p.alpha * acc[i];
-                if (!p.beta_zero) res += p.beta * *yp;
-                *yp = res;
-                acc[i] = T(0);
+#pragma unroll
+            for (int k = 0; k < SPT; ++k) {
+                const int i = t + k * NT;
+                if (i < p.s_cnt) {
+                    T *yp = p.Y + (p.s_lo + i) * p.y_es + vcur * p.y_vs;
+                    T res = p.alpha * acc[k];
+                    if (!p.beta_zero) res += p.beta * *yp;
+                    *yp = res;
+                }
+                acc[k] = T(0);
             }
         } else {
             T *part = p.partials + (int64_t)p.split.slot(g, vbeg) * p.s_cnt;
-            for (int i = t; i < p.s_cnt; i += NT) {
-                part[i] = acc[i];
-                acc[i] = T(0);
+#pragma unroll
+            for (int k = 0; k < SPT; ++k) {
+                const int i = t + k * NT;
+                if (i < p.s_cnt) part[i] = acc[k];
+                acc[k] = T(0);
             }
             __threadfence();
             __syncthreads();
@@ -253,6 +261,7 @@ __global__ void __launch_bounds__(1 << WhtCfg<T>::TB, 2) srht_fused_kernel(SrhtP
                 __threadfence();
                 for (int i = t; i < p.s_cnt; i += NT) {
                     T a = __ldcg(p.partials + (int64_t)p.split.slot(gf, vbeg) * p.s_cnt + i);
+#pragma unroll 4
                     for (int gg = gf + 1; gg <= gl; ++gg) a += __ldcg(p.partials + (int64_t)(2 * gg) * p.s_cnt + i);
                     T *yp = p.Y + (p.s_lo + i) * p.y_es + vcur * p.y_vs;
                     T res = p.alpha * a;
@@ -264,6 +273,29 @@ __global__ void __launch_bounds__(1 << WhtCfg<T>::TB, 2) srht_fused_kernel(SrhtP
         }
         __syncthreads();
     }
+}
+
+// Launch the fused kernel with the smallest samples-per-thread that holds s_cnt samples.
+template <class T, bool VEC>
+static void launch_srht_fused(const SrhtParams<T> &p, int grid, size_t smem, cudaStream_t st) {
+    constexpr int NT = 1 << WhtCfg<T>::TB;
+    auto go = [&](auto kern) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        kern<<<grid, NT, smem, st>>>(p);
+    };
+    const int spt = (p.s_cnt + NT - 1) / NT;
+    if (spt <= 1) go(srht_fused_kernel<T, VEC, 1>);
+    else if (spt <= 2) go(srht_fused_kernel<T, VEC, 2>);
+    else if (spt <= 4) go(srht_fused_kernel<T, VEC, 4>);
+    else if (spt <= 8) go(srht_fused_kernel<T, VEC, 8>);
+    else if (spt <= 16) go(srht_fused_kernel<T, VEC, 16>);
+    else if constexpr (sizeof(T) == 4) go(srht_fused_kernel<T, VEC, 32>);
+}
+
+// Largest samples window of one fused launch: 32 (FP32) or 16 (FP64) samples per thread.
+template <class T>
+constexpr int srht_window() {
+    return (1 << WhtCfg<T>::TB) * (sizeof(T) == 4 ? 32 : 16);
 }
 
 // Per (chunk, thread) sign masks in pass-A register order (bit q = element
@@ -518,10 +550,9 @@ int srht_compress(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_t x_es, 
     char *scratch = nullptr;
     const int64_t cpv = N >> CH;
     const int cap = ctx->smem_optin - 2048;
-    int s_win = (int)std::min<int64_t>(s, (cap / 2 - (int64_t)(es << CH)) / (int64_t)(es + 4));
-    if (s_win < 256) s_win = (int)std::min<int64_t>(s, (cap - (int64_t)(es << CH)) / (int64_t)(es + 4));
+    const int s_win = (int)std::min<int64_t>(s, srht_window<T>());
     const int64_t total = cpv * nv;
-    const int blocks_per_sm = std::max(1, cap / (int)((es << CH) + s_win * (es + 4) + 64));
+    const int blocks_per_sm = std::max(1, cap / (int)((es << CH) + 64));
     int64_t W = std::min<int64_t>((int64_t)ctx->sm_count * std::min(blocks_per_sm, 2), std::max<int64_t>(total, 1));
     const size_t need_t = x_es != 1 ? (size_t)L * nv * es : 0;
     const size_t need_p = N >= ((int64_t)1 << CH) ? (size_t)(2 * W) * s_win * es : 0;
@@ -549,17 +580,12 @@ int srht_compress(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_t x_es, 
     const bool vec = (ldx % (int64_t)(1 << VB) == 0) && ((uintptr_t)Xc % 16 == 0);
     SrhtParams<T> p{Xc, ldx, L, N, sk->sign_tl, sk->rows, 0, s_win, Y, y_es, y_vs, a, (T)beta, beta_zero,
                     (T *)(scratch + off_partials), cnt, cpv, Split::make(total, (int)W)};
-    const size_t smem = (es << CH) + (size_t)s_win * (es + 4);
+    const size_t smem = es << CH;
     for (int64_t lo = 0; lo < s; lo += s_win) {
         p.s_lo = lo;
         p.s_cnt = (int)std::min<int64_t>(s_win, s - lo);
-        if (vec) {
-            cudaFuncSetAttribute(srht_fused_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            srht_fused_kernel<T, true><<<(int)W, 1 << TB, smem, ctx->stream>>>(p);
-        } else {
-            cudaFuncSetAttribute(srht_fused_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            srht_fused_kernel<T, false><<<(int)W, 1 << TB, smem, ctx->stream>>>(p);
-        }
+        if (vec) launch_srht_fused<T, true>(p, (int)W, smem, ctx->stream);
+        else launch_srht_fused<T, false>(p, (int)W, smem, ctx->stream);
         RLA_TRY(check_launch(ctx, "srht_fused"));
     }
     return RLA_OK;
@@ -689,9 +715,7 @@ static int srht_noalloc_t(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_
                                                                a, (T)beta, beta_zero);
         return check_launch(ctx, "srht_small(noalloc)");
     }
-    const int cap = ctx->smem_optin - 2048;
-    int s_win = (int)std::min<int64_t>(s, (cap / 2 - (int64_t)(es << CH)) / (int64_t)(es + 4));
-    if (s_win < 256) s_win = (int)std::min<int64_t>(s, (cap - (int64_t)(es << CH)) / (int64_t)(es + 4));
+    const int s_win = (int)std::min<int64_t>(s, srht_window<T>());
     const int64_t cpv = N >> CH, total = cpv * nv;
     int64_t W = std::min<int64_t>((int64_t)ctx->sm_count * 2, total);
     W = std::min<int64_t>(W, (int64_t)(RLA_NOALLOC_SCRATCH_BYTES / (2 * (size_t)s_win * es)));
@@ -702,17 +726,12 @@ static int srht_noalloc_t(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_
     const bool vec = (ldx % (int64_t)(1 << VB) == 0) && ((uintptr_t)X % 16 == 0);
     SrhtParams<T> p{X, ldx, L, N, sk->sign_tl, sk->rows, 0, s_win, Y, 1, ldy, a, (T)beta, beta_zero,
                     (T *)nd.partials, nd.counters, cpv, Split::make(total, (int)W)};
-    const size_t smem = (es << CH) + (size_t)s_win * (es + 4);
+    const size_t smem = es << CH;
     for (int64_t lo = 0; lo < s; lo += s_win) {
         p.s_lo = lo;
         p.s_cnt = (int)std::min<int64_t>(s_win, s - lo);
-        if (vec) {
-            cudaFuncSetAttribute(srht_fused_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            srht_fused_kernel<T, true><<<(int)W, 1 << TB, smem, ctx->stream>>>(p);
-        } else {
-            cudaFuncSetAttribute(srht_fused_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            srht_fused_kernel<T, false><<<(int)W, 1 << TB, smem, ctx->stream>>>(p);
-        }
+        if (vec) launch_srht_fused<T, true>(p, (int)W, smem, ctx->stream);
+        else launch_srht_fused<T, false>(p, (int)W, smem, ctx->stream);
         RLA_TRY(check_launch(ctx, "srht_fused(noalloc)"));
     }
     return RLA_OK;

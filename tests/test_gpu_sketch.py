@@ -86,6 +86,15 @@ def test_left_compress_fused_path(rla, orc, dev, kind, dtype):
         assert err < TOL[dtype], (kind, L, s, k, err)
 
 
+@pytest.mark.parametrize("dtype,L,s,k", [(np.float64, 70001, 40000, 3), (np.float32, 100003, 60000, 2)])
+def test_count_sketch_windowed_bins(rla, orc, dev, dtype, L, s, k):
+    """Compression dimensions whose bins exceed one CTA's shared memory (several bin windows)."""
+    rng = np.random.default_rng(13)
+    S = make(rla, "count_sketch", "left", s, L, dtype, seed=s)
+    err = run_orient(rla, orc, S, "SA", k, dtype, dev, rng, alpha=0.5, beta=2.0)
+    assert err < TOL[dtype], (L, s, k, err)
+
+
 @pytest.mark.parametrize("kind", ["sparse_sign", "count_sketch", "srht", "gaussian"])
 def test_row_major_operand(rla, orc, dev, kind):
     """A given as Julia's transpose(X) view (row-major storage)."""
