@@ -41,7 +41,9 @@ BYTES_PER_APPLY = bytes_per_apply()
 WORKLOAD = "srht+countsketch left apply, fp32, A 2^20x512 -> 4096x512"
 METRIC = "sketch apply throughput (SRHT + CountSketch, HBM GB/s of algorithmic bytes)"
 # DRAM bytes per launch from ncu (profiles/); None until a capture of this build exists.
-TRAFFIC_PER_LAUNCH = {"srht_fused_kernel": None, "cs_compress_kernel": None}
+# DRAM bytes (read + write) per full-size launch: ncu capture of the 2^20x128 case
+# (profiles/*_2p20x128_f32.md) scaled by 512/128 columns; the work splits evenly by column.
+TRAFFIC_PER_LAUNCH = {"srht_fused_kernel": 2195034112, "cs_compress_kernel": 2250834944}
 
 
 def peaks():
