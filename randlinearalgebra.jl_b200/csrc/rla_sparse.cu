@@ -7,10 +7,10 @@
 //
 //  * compress, contiguous vectors (S*A with Left S on column-major A, the sketch hot
 //    path): each warp owns private shared-memory bins for one output vector and streams
-//    128-element tiles of its input vector with 16-byte loads.  Lanes whose buckets
-//    collide inside a sub-round are combined in lane order with shuffles (the collisions
-//    are flagged ahead of time in the packed metadata), so no atomics are used and the
-//    result is bit-for-bit reproducible.  Input tiles are split over all warps of the
+//    its input vector with 16-byte loads.  Buckets that would collide inside a warp access
+//    were scheduled away when the sketch was drawn (CountSketch: moved to a per-warp list
+//    folded in by extra rounds; SparseSign: extra rounds), so no atomics are used and the
+//    result is bit-for-bit reproducible.  Input batches are split over all warps of the
 //    GPU (stream-K); a vector shared by several warps is finished by the last warp to
 //    arrive, which adds the partial bins in warp order.
 //  * compress, strided vectors (A*S with Right S: rows of column-major A): lane = vector,
