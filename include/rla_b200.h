@@ -195,6 +195,19 @@ int rla_lowrank_mul(rla_ctx *ctx, int factor_dtype, int dtype, int side, int tra
                     int64_t a_rows, int64_t a_cols, const void *A, int64_t lda, int trans_a,
                     double alpha, double beta);
 
+/* ---- split-BF16 tensor-core GEMM ------------------------------------------------ */
+/* No counterpart in the reference (its products go to BLAS gemm): the product kernel used
+ * by RLA_PREC_SPLIT_BF16, exposed for callers and tests.  C = alpha*op(A)*B + beta*C with
+ * FP32 column-major A (op(A) = A, m x k, when trans_a = 0; A', A stored k x m, when
+ * trans_a = 1), B (k x n) and C (m x n).  Each operand is split into hi = bf16(x) and
+ * lo = bf16(x - hi); the 5th-generation tensor cores form hi*hi + hi*lo + lo*hi with FP32
+ * accumulation (about 2^-16 relative error per product).  Device pointers; allocates the
+ * split copies on the context's stream; synchronous.  RLA_E_TIMEOUT when a bounded
+ * pipeline wait on the device ran out. */
+int rla_gemm_bf16x3(rla_ctx *ctx, int trans_a, int64_t m, int64_t n, int64_t k,
+                    const float *A, int64_t lda, const float *B, int64_t ldb,
+                    float *C, int64_t ldc, double alpha, double beta);
+
 /* ---- allocation-free SRHT apply -------------------------------------------------- */
 /* No counterpart in the reference.  C = alpha*S*A + beta*C for a Left-cardinality SRHT
  * recipe S (s x m), column-major A (m x n) and C (s x n), on the context's stream, without

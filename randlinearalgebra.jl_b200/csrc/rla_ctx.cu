@@ -124,6 +124,7 @@ int rla_ctx_destroy(rla_ctx *ctx) {
     cudaStreamSynchronize(ctx->stream);
     if (ctx->scratch.ptr) cudaFree(ctx->scratch.ptr);
     if (ctx->counters.ptr) cudaFree(ctx->counters.ptr);
+    if (ctx->tc_status) cudaFree(ctx->tc_status);
     if (ctx->owns_stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return RLA_OK;

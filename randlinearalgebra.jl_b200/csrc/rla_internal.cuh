@@ -7,6 +7,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <string>
 #include <vector>
 
@@ -40,6 +41,7 @@ struct rla_ctx {
     rla::Scratch scratch;    // grow-only workspace (partials, transposes, WHT buffers)
     rla::Scratch counters;   // zero-initialised ints for last-arriver fix-ups (self-resetting)
     int64_t scratch_high_water = 0;
+    int *tc_status = nullptr;  // non-zero after a tensor-core kernel's bounded wait ran out
 };
 
 namespace rla {
