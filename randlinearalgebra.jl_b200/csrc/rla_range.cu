@@ -16,6 +16,7 @@
 
 #include "rla_internal.cuh"
 #include "rla_kernels.cuh"
+#include "rla_tc.cuh"
 
 namespace rla {
 
@@ -101,6 +102,102 @@ __global__ void convert_kernel(const TI *X, int64_t rows, int64_t cols, int64_t 
     Y[r + c * ldy] = (TO)X[r + c * ldx];
 }
 
+// ---- tall-skinny Gram matrix G = Y'Y (l x l, FP64 accumulation) ------------------------
+// Upper-triangle 64x64 tiles of G times row chunks of Y: each CTA accumulates one tile over
+// one chunk in FP64 registers (4x4 per thread) and writes it to part[chunk][tile]; the
+// reduction adds the chunks in order (deterministic) and mirrors the lower triangle.
+constexpr int GRAM_T = 64, GRAM_KR = 32;
+
+template <class T>
+__global__ void __launch_bounds__(256) gram_tile_kernel(const T *__restrict__ Y, int64_t rows, int64_t l, int64_t ldy,
+                                                        int64_t rows_per_chunk, int ntiles, double *__restrict__ part) {
+    __shared__ __align__(16) double As[GRAM_KR][GRAM_T];
+    __shared__ __align__(16) double Bs[GRAM_KR][GRAM_T];
+    // tile index -> (ti, tj) with ti <= tj, row-major over the upper triangle
+    const int nt = (int)((l + GRAM_T - 1) / GRAM_T);
+    int t = blockIdx.x, ti = 0;
+    while (t >= nt - ti) {
+        t -= nt - ti;
+        ++ti;
+    }
+    const int tj = ti + t;
+    const int64_t chunk = blockIdx.y;
+    const int64_t r0 = chunk * rows_per_chunk, r1 = min(rows, r0 + rows_per_chunk);
+    const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
+    const int64_t ci = (int64_t)ti * GRAM_T, cj = (int64_t)tj * GRAM_T;
+    double acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+    for (int64_t k0 = r0; k0 < r1; k0 += GRAM_KR) {
+#pragma unroll
+        for (int e = 0; e < (GRAM_KR * GRAM_T) / 256; ++e) {
+            const int idx = tid + 256 * e;
+            const int r = idx % GRAM_KR, c = idx / GRAM_KR;
+            const int64_t gr = k0 + r;
+            const bool rin = gr < r1;
+            As[r][c] = (rin && ci + c < l) ? (double)Y[gr + (ci + c) * ldy] : 0.0;
+            Bs[r][c] = (rin && cj + c < l) ? (double)Y[gr + (cj + c) * ldy] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int kk = 0; kk < GRAM_KR; ++kk) {
+            const double2 a01 = *reinterpret_cast<const double2 *>(&As[kk][ty * 4]);
+            const double2 a23 = *reinterpret_cast<const double2 *>(&As[kk][ty * 4 + 2]);
+            const double2 b01 = *reinterpret_cast<const double2 *>(&Bs[kk][tx * 4]);
+            const double2 b23 = *reinterpret_cast<const double2 *>(&Bs[kk][tx * 4 + 2]);
+            const double a[4] = {a01.x, a01.y, a23.x, a23.y}, b[4] = {b01.x, b01.y, b23.x, b23.y};
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+        }
+        __syncthreads();
+    }
+    double *out = part + (chunk * ntiles + blockIdx.x) * (GRAM_T * GRAM_T);
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) out[(ty * 4 + i) * GRAM_T + tx * 4 + j] = acc[i][j];
+}
+
+__global__ void gram_reduce_kernel(const double *__restrict__ part, int64_t nchunks, int ntiles, int64_t l, double *G) {
+    const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (idx >= l * l) return;
+    const int64_t i = idx % l, j = idx / l;
+    if (i > j) return;
+    const int nt = (int)((l + GRAM_T - 1) / GRAM_T);
+    const int ti = (int)(i / GRAM_T), tj = (int)(j / GRAM_T);
+    const int tile = ti * nt - ti * (ti - 1) / 2 + (tj - ti);
+    const int64_t off = (int64_t)tile * GRAM_T * GRAM_T + (i % GRAM_T) * GRAM_T + (j % GRAM_T);
+    double acc = 0.0;
+    for (int64_t c = 0; c < nchunks; ++c) acc += part[c * ntiles * GRAM_T * GRAM_T + off];
+    G[i + j * l] = acc;
+    G[j + i * l] = acc;
+}
+
+template <class T>
+static int gram_fp64(rla_ctx *ctx, const T *Y, int64_t rows, int64_t l, int64_t ldy, double *G) {
+    const int nt = (int)ceil_div(l, GRAM_T);
+    const int ntiles = nt * (nt + 1) / 2;
+    int64_t nchunks = std::max<int64_t>(1, ceil_div(2 * (int64_t)ctx->sm_count * 2, ntiles));
+    int64_t rpc = ceil_div(ceil_div(rows, nchunks), GRAM_KR) * GRAM_KR;
+    rpc = std::max<int64_t>(rpc, 256);
+    nchunks = std::max<int64_t>(1, ceil_div(rows, rpc));
+    if (nchunks > 65535) {
+        nchunks = 65535;
+        rpc = ceil_div(ceil_div(rows, nchunks), GRAM_KR) * GRAM_KR;
+        nchunks = ceil_div(rows, rpc);
+    }
+    void *ws = nullptr;
+    RLA_TRY(scratch_get(ctx, sizeof(double) * (size_t)nchunks * ntiles * GRAM_T * GRAM_T, &ws));
+    gram_tile_kernel<T><<<dim3(ntiles, (unsigned)nchunks), 256, 0, ctx->stream>>>(Y, rows, l, ldy, rpc, ntiles, (double *)ws);
+    RLA_TRY(check_launch(ctx, "gram_tile"));
+    gram_reduce_kernel<<<ceil_div_i(l * l, 256), 256, 0, ctx->stream>>>((const double *)ws, nchunks, ntiles, l, G);
+    return check_launch(ctx, "gram_reduce");
+}
+
 struct OrthWork {
     double *G, *Rinv, *dscale, *diag, *hw;
     int *flag;
@@ -117,7 +214,7 @@ static int orth(rla_ctx *ctx, T *Y, int64_t rows, int64_t l, int64_t ldy, OrthWo
     int passes = 2;
     bool shifted_done = false;
     for (int pass = 0; pass < passes; ++pass) {
-        RLA_TRY((gemm<T, T, double, double>(ctx, l, l, rows, Y, ldy, 1, Y, ldy, 0, w.G, l, 1.0, 0.0)));
+        RLA_TRY(gram_fp64<T>(ctx, Y, rows, l, ldy, w.G));
         double shift = 0.0;
         RLA_TRY(equilibrate(ctx, w.G, l, w.dscale));
         RLA_TRY(cholesky_upper(ctx, w.G, l, shift, w.flag));
@@ -132,7 +229,7 @@ static int orth(rla_ctx *ctx, T *Y, int64_t rows, int64_t l, int64_t ldy, OrthWo
         if (bad) {
             // Shifted CholeskyQR: on the equilibrated Gram matrix (unit diagonal, so
             // ||Y D||_F^2 = l) the shift is 11 (rows*l + l(l+1)) u ||Y D||_2^2 <= ... * l.
-            RLA_TRY((gemm<T, T, double, double>(ctx, l, l, rows, Y, ldy, 1, Y, ldy, 0, w.G, l, 1.0, 0.0)));
+            RLA_TRY(gram_fp64<T>(ctx, Y, rows, l, ldy, w.G));
             RLA_TRY(equilibrate(ctx, w.G, l, w.dscale));
             const double u = sizeof(T) == 4 ? 5.96e-8 : 1.11e-16;
             shift = 11.0 * ((double)rows * l + (double)l * (l + 1)) * u * (double)l;
@@ -179,11 +276,57 @@ struct Owned {
     }
 };
 
-// Q (m x l, ld ldq) <- range of A*Omega after the power iterations.
+// Operands of the split-BF16 tensor-core path (RLA_PREC_SPLIT_BF16, FP32 data): A split
+// once into hi/lo BF16 copies; one hi/lo buffer pair reused for the thin factor of each
+// product (Omega, Q or Z).
+struct TcOps {
+    bf16 *a_hi = nullptr, *a_lo = nullptr;
+    int64_t lda = 0;
+    bf16 *x_hi = nullptr, *x_lo = nullptr;
+};
+
+static int tc_ops_make(rla_ctx *ctx, const float *A, int64_t m, int64_t n, int64_t lda, int64_t l, TcOps &ops,
+                       Owned &own) {
+    ops.lda = ceil_div(m, 8) * 8;
+    const size_t na = (size_t)ops.lda * n, nx = (size_t)ceil_div(std::max(m, n), 8) * 8 * l;
+    bf16 *buf = nullptr;
+    RLA_CUDA_TRY(ctx, cudaMallocAsync((void **)&buf, sizeof(bf16) * 2 * (na + nx), ctx->stream));
+    own.ptrs.push_back(buf);
+    ops.a_hi = buf;
+    ops.a_lo = buf + na;
+    ops.x_hi = buf + 2 * na;
+    ops.x_lo = buf + 2 * na + nx;
+    return split_bf16(ctx, A, m, n, lda, ops.a_hi, ops.a_lo, ops.lda);
+}
+
+// out (rows_out x l) = op(A) * X with X (k x l, ld ldx) FP32; op(A) = A' when at.
+template <class TO>
+static int tc_apply(rla_ctx *ctx, const TcOps &ops, int at, int64_t m, int64_t n, const float *X, int64_t ldx,
+                    int64_t l, TO *out, int64_t ldo) {
+    const int64_t k = at ? m : n, rows_out = at ? n : m;
+    const int64_t ldxs = ceil_div(k, 8) * 8;
+    RLA_TRY(split_bf16(ctx, X, k, l, ldx, ops.x_hi, ops.x_lo, ldxs));
+    return tc_gemm_bf16x3<TO>(ctx, rows_out, l, k, ops.a_hi, ops.a_lo, ops.lda, at, ops.x_hi, ops.x_lo, ldxs, out, ldo,
+                              1.0, 0.0, 0);
+}
+
+// Q (m x l, ld ldq) <- range of A*Omega after the power iterations.  With `tc` (FP32 data
+// only) the products with A run on the tensor cores in split BF16.
 template <class T>
 static int range_core(rla_ctx *ctx, const rla_sketch *om, int64_t m, int64_t n, const T *A, int64_t lda,
-                      const rla_range_params *pr, T *Q, int64_t ldq, Owned &own) {
+                      const rla_range_params *pr, T *Q, int64_t ldq, Owned &own, const TcOps *tc = nullptr) {
     const int64_t l = om->n_cols;
+    // Z = A'Q, Q = A Z
+    auto at_q = [&](const T *Qp, T *Zp) -> int {
+        if constexpr (std::is_same<T, float>::value)
+            if (tc) return tc_apply<float>(ctx, *tc, 1, m, n, Qp, ldq, l, Zp, n);
+        return gemm<T, T, T, double>(ctx, n, l, m, A, lda, 1, Qp, ldq, 0, Zp, n, 1.0, 0.0);
+    };
+    auto a_z = [&](const T *Zp, T *Qp) -> int {
+        if constexpr (std::is_same<T, float>::value)
+            if (tc) return tc_apply<float>(ctx, *tc, 0, m, n, Zp, n, l, Qp, ldq);
+        return gemm<T, T, T, double>(ctx, m, l, n, A, lda, 0, Zp, n, 0, Qp, ldq, 1.0, 0.0);
+    };
     OrthWork wq{}, wz{};
     RLA_TRY(alloc_orth<T>(ctx, wq, m, l, own.ptrs));
     T *Z = nullptr;
@@ -192,20 +335,27 @@ static int range_core(rla_ctx *ctx, const rla_sketch *om, int64_t m, int64_t n, 
         RLA_CUDA_TRY(ctx, cudaMallocAsync((void **)&Z, sizeof(T) * n * l, ctx->stream));
         own.ptrs.push_back(Z);
     }
-    // Y = A * Omega (power_its.jl:21 / :59)
-    RLA_TRY(sketch_mul_impl(ctx, om, RLA_SIDE_RIGHT, 0, m, l, Q, ldq, 0, m, n, A, lda, 0, 1.0, 0.0));
+    // Y = A * Omega (power_its.jl:21 / :59); a dense Gaussian Omega is a GEMM
+    bool done = false;
+    if constexpr (std::is_same<T, float>::value) {
+        if (tc && om->p.kind == RLA_GAUSSIAN) {
+            RLA_TRY(tc_apply<float>(ctx, *tc, 0, m, n, (const float *)om->dense, om->n_rows, l, Q, ldq));
+            done = true;
+        }
+    }
+    if (!done) RLA_TRY(sketch_mul_impl(ctx, om, RLA_SIDE_RIGHT, 0, m, l, Q, ldq, 0, m, n, A, lda, 0, 1.0, 0.0));
     if (pr->orthogonalize) {
         RLA_TRY(orth<T>(ctx, Q, m, l, ldq, wq));
         for (int64_t it = 0; it < pr->power_its; ++it) {
-            RLA_TRY((gemm<T, T, T, double>(ctx, n, l, m, A, lda, 1, Q, ldq, 0, Z, n, 1.0, 0.0)));
+            RLA_TRY(at_q(Q, Z));
             RLA_TRY(orth<T>(ctx, Z, n, l, n, wz));
-            RLA_TRY((gemm<T, T, T, double>(ctx, m, l, n, A, lda, 0, Z, n, 0, Q, ldq, 1.0, 0.0)));
+            RLA_TRY(a_z(Z, Q));
             RLA_TRY(orth<T>(ctx, Q, m, l, ldq, wq));
         }
     } else {
         for (int64_t it = 0; it < pr->power_its; ++it) {
-            RLA_TRY((gemm<T, T, T, double>(ctx, n, l, m, A, lda, 1, Q, ldq, 0, Z, n, 1.0, 0.0)));
-            RLA_TRY((gemm<T, T, T, double>(ctx, m, l, n, A, lda, 0, Z, n, 0, Q, ldq, 1.0, 0.0)));
+            RLA_TRY(at_q(Q, Z));
+            RLA_TRY(a_z(Z, Q));
         }
         RLA_TRY(orth<T>(ctx, Q, m, l, ldq, wq));
     }
@@ -219,8 +369,10 @@ static int check_range_args(rla_ctx *ctx, const rla_sketch *om, int dtype, int64
     if (pr->power_its < 0) return set_error(ctx, RLA_E_ARG, "Field `power_its` must be non-negative.");
     if (dtype != om->p.dtype) return set_error(ctx, RLA_E_ARG, "Compressor type and matrix type differ.");
     if (m <= 0 || n <= 0 || lda < m) return set_error(ctx, RLA_E_ARG, "Bad matrix dimensions.");
-    if (pr->precision != RLA_PREC_NATIVE)
-        return set_error(ctx, RLA_E_UNSUPPORTED, "precision mode %d is not available in this build", pr->precision);
+    if (pr->precision != RLA_PREC_NATIVE && pr->precision != RLA_PREC_SPLIT_BF16)
+        return set_error(ctx, RLA_E_ARG, "Unknown precision mode %d.", pr->precision);
+    if (pr->precision == RLA_PREC_SPLIT_BF16 && dtype != RLA_F32)
+        return set_error(ctx, RLA_E_ARG, "Split-BF16 products take Float32 data.");
     return RLA_OK;
 }
 
@@ -232,12 +384,23 @@ static int randsvd_t(rla_ctx *ctx, const rla_sketch *om, int64_t m, int64_t n, c
     T *Q;
     RLA_CUDA_TRY(ctx, cudaMallocAsync((void **)&Q, sizeof(T) * m * l, ctx->stream));
     own.ptrs.push_back(Q);
-    RLA_TRY(range_core<T>(ctx, om, m, n, A, lda, pr, Q, m, own));
+    TcOps tc;
+    const bool use_tc = pr->precision == RLA_PREC_SPLIT_BF16;
+    if constexpr (std::is_same<T, float>::value)
+        if (use_tc) RLA_TRY(tc_ops_make(ctx, A, m, n, lda, l, tc, own));
+    RLA_TRY(range_core<T>(ctx, om, m, n, A, lda, pr, Q, m, own, use_tc ? &tc : nullptr));
     // Bt = A'Q (n x l) in FP64 (randsvd.jl:183-185 forms QA in Float64)
     double *Bt, *X, *J, *sig, *jw;
     RLA_CUDA_TRY(ctx, cudaMallocAsync((void **)&Bt, sizeof(double) * n * l, ctx->stream));
     own.ptrs.push_back(Bt);
-    RLA_TRY((gemm<T, T, double, double>(ctx, n, l, m, A, lda, 1, Q, m, 0, Bt, n, 1.0, 0.0)));
+    bool bt_done = false;
+    if constexpr (std::is_same<T, float>::value) {
+        if (use_tc) {
+            RLA_TRY(tc_apply<double>(ctx, tc, 1, m, n, Q, m, l, Bt, n));
+            bt_done = true;
+        }
+    }
+    if (!bt_done) RLA_TRY((gemm<T, T, double, double>(ctx, n, l, m, A, lda, 1, Q, m, 0, Bt, n, 1.0, 0.0)));
     double *Qb;
     RLA_CUDA_TRY(ctx, cudaMallocAsync((void **)&Qb, sizeof(double) * n * l, ctx->stream));
     own.ptrs.push_back(Qb);
@@ -261,7 +424,7 @@ static int randsvd_t(rla_ctx *ctx, const rla_sketch *om, int64_t m, int64_t n, c
     RLA_TRY((gemm<double, double, TO, double>(ctx, n, l, l, Qb, n, 0, J, l, 0, V, ldv, 1.0, 0.0)));
     RLA_CUDA_TRY(ctx, cudaMemcpyAsync(S, sig, sizeof(double) * l, cudaMemcpyDeviceToDevice, ctx->stream));
     RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-    return RLA_OK;
+    return use_tc ? tc_status_check(ctx) : RLA_OK;
 }
 
 }  // namespace rla
@@ -276,9 +439,17 @@ int rla_rangefinder(rla_ctx *ctx, const rla_sketch *om, int dtype, int64_t m, in
     if (!Q || ldq < m) return set_error(ctx, RLA_E_ARG, "Bad Q buffer.");
     RLA_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
     Owned own{ctx, {}};
-    int rc = dtype == RLA_F32
-                 ? range_core<float>(ctx, om, m, n, (const float *)A, lda, pr, (float *)Q, ldq, own)
-                 : range_core<double>(ctx, om, m, n, (const double *)A, lda, pr, (double *)Q, ldq, own);
+    int rc;
+    if (dtype == RLA_F32) {
+        TcOps tc;
+        const bool use_tc = pr->precision == RLA_PREC_SPLIT_BF16;
+        if (use_tc) RLA_TRY(tc_ops_make(ctx, (const float *)A, m, n, lda, om->n_cols, tc, own));
+        rc = range_core<float>(ctx, om, m, n, (const float *)A, lda, pr, (float *)Q, ldq, own, use_tc ? &tc : nullptr);
+        RLA_TRY(rc);
+        RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+        return use_tc ? tc_status_check(ctx) : RLA_OK;
+    }
+    rc = range_core<double>(ctx, om, m, n, (const double *)A, lda, pr, (double *)Q, ldq, own);
     RLA_TRY(rc);
     RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     return RLA_OK;

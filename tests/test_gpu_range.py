@@ -189,3 +189,59 @@ def test_doc_example_rank20(rla, dev):
     trunc = (Ut[:, :22] * St[:22]) @ Vt[:22]
     err = np.linalg.norm((U * S) @ V.T - trunc)
     assert err < 1e-9, err
+
+
+def _low_rank_plus_noise(rng, m, n, r, noise=1e-6):
+    Uo = qr_Q(rng.standard_normal((m, r)))
+    Vo = qr_Q(rng.standard_normal((n, r)))
+    sig = np.arange(1, r + 1, dtype=float) ** -1.5
+    return ((Uo * sig) @ Vo.T + noise * rng.standard_normal((m, n))).astype(np.float32)
+
+
+@pytest.mark.parametrize("m,n,k,q", [(2000, 500, 40, 2), (8192, 2048, 272, 2), (3001, 777, 33, 1)])
+def test_randsvd_split_bf16_vs_fp64_oracle(rla, orc, dev, m, n, k, q):
+    """RLA_PREC_SPLIT_BF16 (products with A on the tensor cores as hi*hi + hi*lo + lo*hi BF16
+    with FP32 accumulation; Gram, Cholesky, triangular inverse and the SVD of B in FP64):
+    singular values and the projection error ||A - UU'A|| / ||A|| within 1e-4 of the FP64
+    oracle run of the same algorithm on the same Gaussian draws."""
+    rng = np.random.default_rng(m + k)
+    A = _low_rank_plus_noise(rng, m, n, min(n, 512))
+    comp = rla.Gaussian(cardinality=rla.Right(), compression_dim=k, type=np.float32)
+    rec = rla.rapproximate(rla.RandSVD(compressor=comp, power_its=q, orthogonalize=True,
+                                       precision=rla.RLA_PREC_SPLIT_BF16), to_dev(A, dev), seed=10)
+    A64 = A.astype(np.float64)
+    ref = orc.randsvd(A64, oracle_recipe(orc, rec.compressor), q=q, orthogonalize=True)
+    assert rel_err(rec.S.cpu().numpy(), ref.S) < 1e-4
+    U = rec.U.cpu().numpy().astype(np.float64)
+    nA = np.linalg.norm(A64)
+    e_gpu = np.linalg.norm(A64 - U @ (U.T @ A64)) / nA
+    e_ref = np.linalg.norm(A64 - ref.U @ (ref.U.T @ A64)) / nA
+    assert abs(e_gpu - e_ref) < 1e-4, (e_gpu, e_ref)
+    assert np.allclose(U.T @ U, np.eye(k), atol=1e-5)
+
+
+@pytest.mark.parametrize("q,ortho", [(1, True), (0, False)])
+def test_rangefinder_split_bf16(rla, orc, dev, q, ortho):
+    """Power iterations without re-orthogonalisation are left out: Y = (AA')^q A Omega has
+    cond(Y) ~ (s1/sk)^(2q+1) (1.6e6 for q = 1 here), which turns the 2^-16 product error
+    into subspace error above 1e-4 -- the reason the split path is run orthogonalised."""
+    rng = np.random.default_rng(77)
+    m, n, k = 1500, 640, 24
+    A = _low_rank_plus_noise(rng, m, n, 300)
+    comp = rla.Gaussian(cardinality=rla.Right(), compression_dim=k, type=np.float32)
+    R = rla.rapproximate(rla.RangeFinder(compressor=comp, power_its=q, orthogonalize=ortho,
+                                         precision=rla.RLA_PREC_SPLIT_BF16), to_dev(A, dev), seed=3)
+    A64 = A.astype(np.float64)
+    Qref = orc.rangefinder(A64, oracle_recipe(orc, R.compressor), q=q, orthogonalize=ortho)
+    Q = R.range.cpu().numpy().astype(np.float64)
+    nA = np.linalg.norm(A64)
+    e_gpu = np.linalg.norm(A64 - Q @ (Q.T @ A64)) / nA
+    e_ref = np.linalg.norm(A64 - Qref @ (Qref.T @ A64)) / nA
+    assert abs(e_gpu - e_ref) < 1e-4, (e_gpu, e_ref)
+
+
+def test_split_bf16_rejects_float64(rla, dev):
+    comp = rla.Gaussian(cardinality=rla.Right(), compression_dim=4)
+    A = np.random.default_rng(1).standard_normal((20, 10))
+    with pytest.raises(rla.ArgumentError, match="Split-BF16 products take Float32 data."):
+        rla.rapproximate(rla.RandSVD(compressor=comp, precision=rla.RLA_PREC_SPLIT_BF16), to_dev(A, dev), seed=1)
