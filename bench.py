@@ -13,6 +13,13 @@ N > 1 runs one replica per GPU under torchrun (weak scaling: each rank sketches 
 2^20 x 512 block; no data-path collective), timed on the device as the max over ranks.
 `--impl reference` times the CPU restatement of the reference (oracle/) on the host cores
 on a bounded sample of the same workload.
+
+`--workload randsvd` measures the mixed-precision RandSVD instead: A = U diag(s) V' +
+1e-6 N(0,1), 65536 x 8192 Float32, s_i = i^-1.5 for i <= 512 (U, V orthonormal from QR of
+Gaussians, seed 3), Gaussian sketch, k = 256, p = 16 (l = 272), q = 2, orthogonalised; the
+products with A on the tensor cores in split BF16, Gram/Cholesky/triangular inverse and the
+SVD of B in FP64.  One step = one rapproximate!.  The metric is GFLOP/s of 2*m*n*l*(2q+2);
+the line also carries the error against the FP64 run of the same algorithm on the same draws.
 """
 from __future__ import annotations
 
@@ -342,6 +349,195 @@ def b200_arm(args):
         dist.destroy_process_group()
 
 
+# --------------------------------------------------------------------------------------
+# RandSVD workload (mixed precision)
+# --------------------------------------------------------------------------------------
+RS_M, RS_N, RS_K, RS_P, RS_Q, RS_R = 65536, 8192, 256, 16, 2, 512
+RS_METRIC = "RandSVD throughput (GFLOP/s of 2*m*n*l*(2q+2), split-BF16 tensor-core products)"
+RS_WORKLOAD = "randsvd 65536x8192 fp32, k=256 p=16 q=2 orthogonalize, gaussian sketch"
+
+
+def rs_flops(m=RS_M, n=RS_N, l=RS_K + RS_P, q=RS_Q):
+    return 2.0 * m * n * l * (2 * q + 2)
+
+
+def rs_problem(torch, dev, m, n, r, seed):
+    """Column-major m x n Float32: U diag(i^-1.5) V' + 1e-6 N(0,1)."""
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    U = torch.linalg.qr(torch.randn(m, r, device=dev, generator=g))[0]
+    V = torch.linalg.qr(torch.randn(n, r, device=dev, generator=g))[0]
+    sig = torch.arange(1, r + 1, device=dev, dtype=torch.float32) ** -1.5
+    At = (V * sig) @ U.t()  # n x m row-major storage = A column-major
+    At.add_(torch.randn(n, m, device=dev, generator=g), alpha=1e-6)
+    del U, V
+    return At.t()
+
+
+def rs_cpu_sample(threads_note: str, budget_s: float = 20.0):
+    """FP64 RandSVD of the oracle (numpy/LAPACK, all BLAS threads) on a scaled-down instance
+    of the same problem family; returns (GFLOP/s, description, seconds)."""
+    import numpy as np
+
+    from __graft_entry__ import load_oracle
+    orc = load_oracle()
+    rng = np.random.default_rng(3)
+    m, n, l = 8192, 2048, RS_K + RS_P
+    U = np.linalg.qr(rng.standard_normal((m, RS_R)))[0]
+    V = np.linalg.qr(rng.standard_normal((n, RS_R)))[0]
+    A = np.asfortranarray((U * np.arange(1, RS_R + 1) ** -1.5) @ V.T + 1e-6 * rng.standard_normal((m, n)))
+    R = orc.draw_gaussian(rng, "right", l, n)
+    t0 = time.perf_counter()
+    reps = 0
+    while True:
+        orc.randsvd(A, R, q=RS_Q, orthogonalize=True)
+        reps += 1
+        if time.perf_counter() - t0 > budget_s / 2 or reps >= 5:
+            break
+    dt = (time.perf_counter() - t0) / reps
+    fl = rs_flops(m, n, l, RS_Q)
+    return fl / dt / 1e9, (f"FP64 RandSVD of the oracle (numpy/LAPACK) on an {m}x{n} instance of the same family, "
+                           f"l={l}, q={RS_Q}, orthogonalized, {reps} run(s); {threads_note}"), dt
+
+
+def randsvd_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    rs_cpu_sample(f"{threads} host threads", budget_s=4.0)
+    vals, tot = [], 0.0
+    for _ in range(max(1, min(args.steps, 3))):
+        g, desc, dt = rs_cpu_sample(f"{threads} host threads")
+        vals.append(g)
+        tot += dt
+    v = statistics.median(vals)
+    line = {"impl": "reference", "metric": RS_METRIC, "value": round(v, 3), "unit": "GFLOP/s", "n_gpus": args.gpus,
+            "steps": len(vals), "warmup": 1, "ms_per_step": round(1000 * tot / len(vals), 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic low-rank + noise, seed 3", "config": {"workload": RS_WORKLOAD},
+            "cpu_baseline": {"value": round(v, 3), "unit": "GFLOP/s", "cores": threads, "kind": "port",
+                             "sample": desc},
+            "e2e": {"value": round(v, 3), "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def randsvd_arm(args):
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    world, rank, local = dist_setup(args.gpus)
+    from __graft_entry__ import load_package
+    rla = load_package()
+    from randlinearalgebra_b200 import _lib as L
+    dev = torch.device("cuda", local if world > 1 else 0)
+    m, n, l, q = RS_M, RS_N, RS_K + RS_P, RS_Q
+    A = rs_problem(torch, dev, m, n, RS_R, 3 + rank)
+    comp = rla.Gaussian(cardinality=rla.Right(), compression_dim=l, type=np.float32)
+    rec = rla.complete_approximator(rla.RandSVD(compressor=comp, power_its=q, orthogonalize=True,
+                                                precision=rla.RLA_PREC_SPLIT_BF16, factor_type=np.float32),
+                                    A, seed=3000 + rank)
+    ctx = L.Context.get(dev.index)
+    lib = L.lib()
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(args.warmup):
+        rla.rapproximate_(rec, A)
+    lib.rla_ctx_set_timing(ctx.handle, 1)
+    ms_tc, n_tc = ctypes.c_double(), ctypes.c_int64()
+    L.check(lib.rla_ctx_kernel_time(ctx.handle, 0, ctypes.byref(ms_tc), ctypes.byref(n_tc)), ctx.handle)
+    K = args.steps
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    props = torch.cuda.get_device_properties(dev)
+    clocks = ClockSampler(f"GPU-{props.uuid}" if getattr(props, "uuid", None) else dev.index)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    t0.record(stream)
+    for _ in range(K):
+        rla.rapproximate_(rec, A)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    barrier(world)
+    ms = allreduce_max(t0.elapsed_time(t1), world)
+    L.check(lib.rla_ctx_kernel_time(ctx.handle, 0, ctypes.byref(ms_tc), ctypes.byref(n_tc)), ctx.handle)
+    lib.rla_ctx_set_timing(ctx.handle, 0)
+    fl = rs_flops(m, n, l, q)
+    value = world * fl * K / (ms / 1e3) / 1e9
+
+    # ---- error against the FP64 run of the same algorithm on the same draws --------------
+    U32, S32 = rec.U.double(), rec.S.double()
+    A64 = A.t().double().t()  # column-major FP64 copy
+    comp64 = rla.Gaussian(cardinality=rla.Right(), compression_dim=l, type=np.float64)
+    rec64 = rla.complete_approximator(rla.RandSVD(compressor=comp64, power_its=q, orthogonalize=True), A64, seed=1)
+    rec64.compressor.load_draws(vals=rec.compressor.draws()["op"].astype(np.float64))
+    rla.rapproximate_(rec64, A64)
+    nA = torch.linalg.norm(A64)
+
+    def proj_err(U):
+        return float(torch.linalg.norm(A64 - U @ (U.t() @ A64)) / nA)
+
+    e32, e64 = proj_err(U32), proj_err(rec64.U)
+    s_err = float(torch.linalg.norm(S32 - rec64.S) / torch.linalg.norm(rec64.S))
+    del A64, rec64
+    torch.cuda.empty_cache()
+
+    # ---- end to end: host A (pinned) in, factors out, through the public API --------------
+    A_h = torch.empty(n, m, dtype=torch.float32, pin_memory=True).t()
+    A_h.copy_(A)
+    e2e_steps = 2
+    rla.rapproximate_(rec, A_h)
+    torch.cuda.synchronize()
+    barrier(world)
+    w0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        rla.rapproximate_(rec, A_h)
+        Uh, Sh, Vh = rec.U.cpu(), rec.S.cpu(), rec.V.cpu()
+    e2e_s = allreduce_max((time.perf_counter() - w0) / e2e_steps, world)
+    e2e = {"value": round(world * fl / e2e_s / 1e9, 3), "unit": "GFLOP/s", "h2d_bytes_per_step": 4 * m * n,
+           "d2h_bytes_per_step": 4 * (m + n) * l + 8 * l, "ms_per_step": round(e2e_s * 1e3, 3)}
+    del A_h
+    if rank != 0:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            pk = json.load(f)
+        peak_bf16, peak_kind = float(pk["bf16_tflops"]), "measured"
+    except Exception:
+        peak_bf16, peak_kind = 1590.0, "fallback"
+    tc_avg_ms = ms_tc.value / max(n_tc.value, 1)
+    tc_flops = 2.0 * m * n * l  # each of the 2q+2 products with A
+    achieved = tc_flops / (tc_avg_ms / 1e3) / 1e12
+    roofline = {"bound": "tensor", "kernel": "tc_gemm_kernel", "achieved": round(achieved, 2),
+                "peak": round(peak_bf16 / 3, 2), "peak_source": f"{peak_kind} bf16 dense / 3 (three BF16 products per split product)",
+                "unit": "TFLOP/s", "frac": round(achieved / (peak_bf16 / 3), 4), "traffic": None,
+                "launches_timed": n_tc.value, "avg_launch_ms": round(tc_avg_ms, 4),
+                "tensor_flops_per_launch": 3 * tc_flops}
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        g, desc, _ = rs_cpu_sample(f"{os.cpu_count()} host threads")
+        cpu = {"value": round(g, 3), "unit": "GFLOP/s", "cores": os.cpu_count(), "kind": "port", "sample": desc}
+    line = {"metric": RS_METRIC, "value": round(value, 2), "unit": "GFLOP/s", "n_gpus": world, "steps": K,
+            "warmup": args.warmup, "ms_per_step": round(ms / K, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 data, bf16x3 products, f64 small factorizations",
+            "data": "synthetic U diag(i^-1.5) V' + 1e-6 N(0,1) generated on device (seed 3+rank)",
+            "config": {"workload": RS_WORKLOAD, "m": m, "n": n, "k": RS_K, "p": RS_P, "q": q,
+                       "parallelism": f"replicas x{world}", "l2": "A is 2.15 GB (larger than L2), no flush needed"},
+            "roofline": roofline,
+            "error": {"proj_err_split": e32, "proj_err_fp64": e64, "proj_err_diff": abs(e32 - e64),
+                      "sigma_rel_err": s_err, "tolerance": 1e-4},
+            "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches_tensor_core": n_tc.value}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -352,10 +548,17 @@ def main():
     ap.add_argument("--cols", type=int, default=NCOL,
                     help="columns of A (default 512, the benchmark workload; smaller values make small "
                          "cases of the same kernels for profiler captures)")
+    ap.add_argument("--workload", choices=["sketch", "randsvd"], default="sketch",
+                    help="sketch: SRHT + CountSketch apply (default); randsvd: mixed-precision RandSVD")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == "reference":
+    if args.workload == "randsvd":
+        if args.impl == "reference":
+            randsvd_reference_arm(args)
+        else:
+            randsvd_arm(args)
+    elif args.impl == "reference":
         reference_arm(args)
     else:
         b200_arm(args)

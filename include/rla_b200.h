@@ -195,6 +195,14 @@ int rla_lowrank_mul(rla_ctx *ctx, int factor_dtype, int dtype, int side, int tra
                     int64_t a_rows, int64_t a_cols, const void *A, int64_t lda, int trans_a,
                     double alpha, double beta);
 
+/* ---- kernel timing (tracing aid, no reference counterpart) ------------------------- */
+/* While enabled, the context records CUDA events around each launch of a timed kernel
+ * class on its stream (class 0: the tensor-core GEMM kernel).  rla_ctx_kernel_time
+ * synchronises the stream, returns the summed device time (ms) and launch count of the
+ * class since the last call, and clears the record. */
+int rla_ctx_set_timing(rla_ctx *ctx, int enable);
+int rla_ctx_kernel_time(rla_ctx *ctx, int kernel_class, double *ms_total, int64_t *launches);
+
 /* ---- split-BF16 tensor-core GEMM ------------------------------------------------ */
 /* No counterpart in the reference (its products go to BLAS gemm): the product kernel used
  * by RLA_PREC_SPLIT_BF16, exposed for callers and tests.  C = alpha*op(A)*B + beta*C with

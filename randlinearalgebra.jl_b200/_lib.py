@@ -71,6 +71,8 @@ SIGNATURES = {
                                        ctypes.c_int, ctypes.c_double, ctypes.c_double]),
     "rla_srht_mul_noalloc": (ctypes.c_int, [vp, vp, i64, i64, vp, i64, i64, i64, vp, i64, ctypes.c_double,
                                             ctypes.c_double]),
+    "rla_ctx_set_timing": (ctypes.c_int, [vp, ctypes.c_int]),
+    "rla_ctx_kernel_time": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(i64)]),
     "rla_gemm_bf16x3": (ctypes.c_int, [vp, ctypes.c_int, i64, i64, i64, vp, i64, vp, i64, vp, i64,
                                        ctypes.c_double, ctypes.c_double]),
 }

@@ -102,6 +102,18 @@ int rla_ctx_create(int device, void *stream, rla_ctx **out) {
         delete ctx;
         return RLA_E_UNSUPPORTED;  // sm_100a kernels only
     }
+    {
+        cudaMemPoolProps pp = {};
+        pp.allocType = cudaMemAllocationTypePinned;
+        pp.location.type = cudaMemLocationTypeDevice;
+        pp.location.id = device;
+        if (cudaMemPoolCreate(&ctx->pool, &pp) != cudaSuccess) {
+            delete ctx;
+            return RLA_E_CUDA;
+        }
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
     ctx->sm_count = prop.multiProcessorCount;
     ctx->smem_optin = (int)prop.sharedMemPerBlockOptin;
     if (stream) {
@@ -125,7 +137,13 @@ int rla_ctx_destroy(rla_ctx *ctx) {
     if (ctx->scratch.ptr) cudaFree(ctx->scratch.ptr);
     if (ctx->counters.ptr) cudaFree(ctx->counters.ptr);
     if (ctx->tc_status) cudaFree(ctx->tc_status);
+    for (auto &v : ctx->timed)
+        for (auto &e : v) {
+            cudaEventDestroy(e.first);
+            cudaEventDestroy(e.second);
+        }
     if (ctx->owns_stream) cudaStreamDestroy(ctx->stream);
+    if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
     delete ctx;
     return RLA_OK;
 }
@@ -147,6 +165,31 @@ int rla_ctx_set_stream(rla_ctx *ctx, void *stream) {
         ctx->owns_stream = false;
     }
     ctx->stream = (cudaStream_t)stream;  // NULL selects the legacy default stream
+    return RLA_OK;
+}
+
+int rla_ctx_set_timing(rla_ctx *ctx, int enable) {
+    if (!ctx) return RLA_E_ARG;
+    ctx->timing = enable != 0;
+    return RLA_OK;
+}
+
+int rla_ctx_kernel_time(rla_ctx *ctx, int kernel_class, double *ms_total, int64_t *launches) {
+    if (!ctx || !ms_total || !launches) return RLA_E_ARG;
+    if (kernel_class != 0) return set_error(ctx, RLA_E_ARG, "unknown kernel class %d", kernel_class);
+    RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    double tot = 0.0;
+    auto &v = ctx->timed[kernel_class];
+    for (auto &e : v) {
+        float ms = 0.f;
+        RLA_CUDA_TRY(ctx, cudaEventElapsedTime(&ms, e.first, e.second));
+        tot += ms;
+        cudaEventDestroy(e.first);
+        cudaEventDestroy(e.second);
+    }
+    *ms_total = tot;
+    *launches = (int64_t)v.size();
+    v.clear();
     return RLA_OK;
 }
 

@@ -8,6 +8,7 @@
 
 #include <algorithm>
 #include <type_traits>
+#include <utility>
 #include <string>
 #include <vector>
 
@@ -41,7 +42,10 @@ struct rla_ctx {
     rla::Scratch scratch;    // grow-only workspace (partials, transposes, WHT buffers)
     rla::Scratch counters;   // zero-initialised ints for last-arriver fix-ups (self-resetting)
     int64_t scratch_high_water = 0;
+    cudaMemPool_t pool = nullptr;  // context-owned stream-ordered pool, keeps freed memory mapped
     int *tc_status = nullptr;  // non-zero after a tensor-core kernel's bounded wait ran out
+    bool timing = false;       // record CUDA events around timed kernel classes
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> timed[1];  // class 0: tensor-core GEMM
 };
 
 namespace rla {
@@ -70,6 +74,12 @@ int scratch_get(rla_ctx *ctx, size_t bytes, void **out);
 // Zero-initialised int32 counters (at least n); kernels leave them at zero on exit.
 int counters_get(rla_ctx *ctx, size_t n, int **out);
 int check_launch(rla_ctx *ctx, const char *what);
+// Stream-ordered allocation from the context's pool (memory stays mapped between calls, so
+// repeated calls of the same size do not remap device memory).
+template <class P>
+inline cudaError_t pool_malloc_s(rla_ctx *ctx, P **p, size_t bytes, cudaStream_t s) {
+    return cudaMallocFromPoolAsync(reinterpret_cast<void **>(p), bytes, ctx->pool, s);
+}
 
 inline int ceil_div_i(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }

@@ -11,30 +11,49 @@
 
 namespace rla {
 
+__device__ inline double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+    return v;
+}
+
+// Upper Cholesky factor, left-looking by rows of R: step j forms r_jj from column j of R
+// and then row j, r_ji = (g_ji - R(0:j, j)' R(0:j, i)) / r_jj, one warp per column i with
+// the dot product split over the lanes.  Column j of R is staged in shared memory.
 __global__ void __launch_bounds__(1024) chol_upper_kernel(double *G, int64_t l, double shift, int *breakdown) {
-    __shared__ double rkk;
+    extern __shared__ double colj[];
+    __shared__ double rjj_s;
     __shared__ int bad;
     const int tid = threadIdx.x, nt = blockDim.x;
+    const int lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
     if (tid == 0) bad = 0;
     for (int64_t i = tid; i < l; i += nt) G[i + i * l] += shift;
     __syncthreads();
-    for (int64_t k = 0; k < l; ++k) {
-        if (tid == 0) {
-            double d = G[k + k * l];
-            if (!(d > 0.0) || !isfinite(d)) {
-                bad = 1;
-                d = 1.0;
+    for (int64_t j = 0; j < l; ++j) {
+        for (int64_t k = tid; k < j; k += nt) colj[k] = G[k + j * l];
+        __syncthreads();
+        if (warp == 0) {
+            double d = 0.0;
+            for (int64_t k = lane; k < j; k += 32) d += colj[k] * colj[k];
+            d = warp_sum(d);
+            if (lane == 0) {
+                double v = G[j + j * l] - d;
+                if (!(v > 0.0) || !isfinite(v)) {
+                    bad = 1;
+                    v = 1.0;
+                }
+                rjj_s = sqrt(v);
+                G[j + j * l] = rjj_s;
             }
-            rkk = sqrt(d);
-            G[k + k * l] = rkk;
         }
         __syncthreads();
-        for (int64_t j = k + 1 + tid; j < l; j += nt) G[k + j * l] /= rkk;
-        __syncthreads();
-        const int64_t n = l - k - 1;
-        for (int64_t idx = tid; idx < n * n; idx += nt) {
-            const int64_t a = k + 1 + idx % n, b = k + 1 + idx / n;
-            if (a <= b) G[a + b * l] -= G[k + a * l] * G[k + b * l];
+        const double rjj = rjj_s;
+        for (int64_t i = j + 1 + warp; i < l; i += nwarps) {
+            const double *ci = G + i * l;
+            double d = 0.0;
+            for (int64_t k = lane; k < j; k += 32) d += colj[k] * ci[k];
+            d = warp_sum(d);
+            if (lane == 0) G[j + i * l] = (G[j + i * l] - d) / rjj;
         }
         __syncthreads();
     }
@@ -45,24 +64,29 @@ __global__ void __launch_bounds__(1024) chol_upper_kernel(double *G, int64_t l, 
     if (tid == 0) *breakdown = bad;
 }
 
-__global__ void tri_inv_upper_kernel(const double *R, int64_t l, double *Ri) {
-    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+// Rinv = R^-1 for upper-triangular R: one warp per column j solves R x = e_j by back
+// substitution, x staged in shared memory (wpc warps per CTA).
+__global__ void __launch_bounds__(256) tri_inv_upper_kernel(const double *R, int64_t l, double *Ri, int wpc) {
+    extern __shared__ double xs_all[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int64_t j = (int64_t)blockIdx.x * wpc + wib;
     if (j >= l) return;
-    double *x = Ri + j * l;
-    for (int64_t i = j + 1; i < l; ++i) x[i] = 0.0;
-    x[j] = 1.0 / R[j + j * l];
+    double *x = xs_all + (int64_t)wib * l;
+    for (int64_t i = lane; i <= j; i += 32) x[i] = 0.0;
+    __syncwarp();
+    if (lane == 0) x[j] = 1.0 / R[j + j * l];
+    __syncwarp();
     for (int64_t i = j - 1; i >= 0; --i) {
-        double s = 0.0;
-        for (int64_t k = i + 1; k <= j; ++k) s += R[i + k * l] * x[k];
-        x[i] = -s / R[i + i * l];
+        double d = 0.0;
+        for (int64_t k = i + 1 + lane; k <= j; k += 32) d += R[i + k * l] * x[k];
+        d = warp_sum(d);
+        if (lane == 0) x[i] = -d / R[i + i * l];
+        __syncwarp();
     }
+    double *out = Ri + j * l;
+    for (int64_t i = lane; i < l; i += 32) out[i] = i <= j ? x[i] : 0.0;
 }
 
-__device__ inline double warp_sum(double v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
-    return v;
-}
 
 // Circle-method pairing: round r (0..n2-2), pair p (0..n2/2-1) over players 0..n2-1.
 __device__ inline void tourney_pair(int r, int p, int n2, int *i, int *j) {
@@ -79,7 +103,6 @@ __device__ inline void tourney_pair(int r, int p, int n2, int *i, int *j) {
 __global__ void __launch_bounds__(1024) jacobi_kernel(double *X, double *J, double *sigma, int64_t l, double *work,
                                                       int max_sweeps, double tol) {
     __shared__ unsigned long long off_bits;
-    __shared__ int perm_done;
     const int tid = threadIdx.x, nt = blockDim.x;
     const int lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
     for (int64_t idx = tid; idx < l * l; idx += nt) J[idx] = (idx % l == idx / l) ? 1.0 : 0.0;
@@ -133,6 +156,15 @@ __global__ void __launch_bounds__(1024) jacobi_kernel(double *X, double *J, doub
         __syncthreads();
     }
     __syncthreads();
+}
+
+// Column norms -> sigma, columns sorted by descending sigma (stable), X normalised, J
+// permuted alongside.  work: 2*l*l + 2*l doubles.
+__global__ void __launch_bounds__(1024) jacobi_finish_kernel(double *X, double *J, double *sigma, int64_t l,
+                                                             double *work) {
+    __shared__ int perm_done;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
     // column norms
     for (int c = warp; c < l; c += nwarps) {
         const double *xc = X + (int64_t)c * l;
@@ -174,6 +206,108 @@ __global__ void __launch_bounds__(1024) jacobi_kernel(double *X, double *J, doub
         J[idx] = Jt[idx];
     }
     for (int64_t c = tid; c < l; c += nt) sigma[c] = sg[perm[c]];
+}
+
+
+// ---- block one-sided Jacobi -------------------------------------------------------------
+// Columns in blocks of BJ_B; an outer round pairs blocks (circle method) and each CTA takes
+// one pair: it stages the pair's columns of X and J in shared memory, runs inner one-sided
+// (Hestenes) sweeps over them (one warp per column pair, circle-method rounds) until they
+// are mutually orthogonal to `tol` or BJ_INNER sweeps, and writes them back.  The largest
+// relative off-diagonal seen in a CTA's first inner sweep goes to *off (max over the outer
+// sweep), which the host reads to stop.
+constexpr int BJ_B = 16, BJ_INNER = 4, BJ_THREADS = 512;
+
+__global__ void jacobi_identity_kernel(double *J, int64_t l) {
+    const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (idx < l * l) J[idx] = (idx % l == idx / l) ? 1.0 : 0.0;
+}
+
+__global__ void __launch_bounds__(BJ_THREADS) block_jacobi_round_kernel(double *X, double *J, int64_t l, int nbp,
+                                                                        int round, double tol,
+                                                                        unsigned long long *off) {
+    extern __shared__ double bj_smem[];
+    __shared__ unsigned long long inner_off;
+    __shared__ int cols[2 * BJ_B];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = BJ_THREADS / 32;
+    const int nb = (int)((l + BJ_B - 1) / BJ_B);
+    int bi, bj;
+    tourney_pair(round, blockIdx.x, nbp, &bi, &bj);
+    int c = 0;
+    for (int q = 0; q < 2; ++q) {
+        const int blk = q == 0 ? bi : bj;
+        if (blk >= nb) continue;
+        const int c0 = blk * BJ_B, c1 = (int)(l < (int64_t)c0 + BJ_B ? l : (int64_t)c0 + BJ_B);
+        for (int cc = c0; cc < c1; ++cc) {
+            if (tid == 0) cols[c] = cc;
+            ++c;
+        }
+    }
+    __syncthreads();
+    if (c < 2) return;
+    double *Xs = bj_smem, *Js = bj_smem + (int64_t)2 * BJ_B * l;
+    for (int64_t idx = tid; idx < (int64_t)c * l; idx += BJ_THREADS) {
+        const int q = (int)(idx / l);
+        const int64_t r = idx % l;
+        Xs[idx] = X[r + (int64_t)cols[q] * l];
+        Js[idx] = J[r + (int64_t)cols[q] * l];
+    }
+    __syncthreads();
+    const int cp = c + (c & 1);
+    for (int sweep = 0; sweep < BJ_INNER; ++sweep) {
+        if (tid == 0) inner_off = 0ull;
+        __syncthreads();
+        for (int r = 0; r < cp - 1; ++r) {
+            for (int p = warp; p < cp / 2; p += nwarps) {
+                int i, j;
+                tourney_pair(r, p, cp, &i, &j);
+                if (i >= c || j >= c) continue;
+                if (i > j) {
+                    const int t = i;
+                    i = j;
+                    j = t;
+                }
+                double *xi = Xs + (int64_t)i * l, *xj = Xs + (int64_t)j * l;
+                double a = 0, b = 0, g = 0;
+                for (int64_t k = lane; k < l; k += 32) {
+                    const double u = xi[k], w = xj[k];
+                    a = fma(u, u, a);
+                    b = fma(w, w, b);
+                    g = fma(u, w, g);
+                }
+                a = warp_sum(a);
+                b = warp_sum(b);
+                g = warp_sum(g);
+                const double nrm = sqrt(a * b);
+                if (g != 0.0 && fabs(g) > tol * nrm) {
+                    if (lane == 0) atomicMax(&inner_off, (unsigned long long)__double_as_longlong(fabs(g) / nrm));
+                    const double zeta = (b - a) / (2.0 * g);
+                    const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+                    const double cs = 1.0 / sqrt(1.0 + t * t), sn = cs * t;
+                    double *ji = Js + (int64_t)i * l, *jj = Js + (int64_t)j * l;
+                    for (int64_t k = lane; k < l; k += 32) {
+                        const double u = xi[k], w = xj[k];
+                        xi[k] = cs * u - sn * w;
+                        xj[k] = sn * u + cs * w;
+                        const double uj = ji[k], wj = jj[k];
+                        ji[k] = cs * uj - sn * wj;
+                        jj[k] = sn * uj + cs * wj;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        if (sweep == 0 && tid == 0 && inner_off) atomicMax(off, inner_off);
+        const bool done = __longlong_as_double((long long)inner_off) <= tol;
+        __syncthreads();
+        if (done) break;
+    }
+    for (int64_t idx = tid; idx < (int64_t)c * l; idx += BJ_THREADS) {
+        const int q = (int)(idx / l);
+        const int64_t r = idx % l;
+        X[r + (int64_t)cols[q] * l] = Xs[idx];
+        J[r + (int64_t)cols[q] * l] = Js[idx];
+    }
 }
 
 // ---- Householder QR with LAPACK's conventions (dgeqr2 + dlarfg + dorg2r) --------------
@@ -264,18 +398,53 @@ template int householder_q<float>(rla_ctx *, float *, int64_t, int64_t, int64_t,
 template int householder_q<double>(rla_ctx *, double *, int64_t, int64_t, int64_t, double *);
 
 int cholesky_upper(rla_ctx *ctx, double *G, int64_t l, double shift, int *breakdown) {
-    chol_upper_kernel<<<1, 1024, 0, ctx->stream>>>(G, l, shift, breakdown);
+    const size_t smem = sizeof(double) * (size_t)std::max<int64_t>(l, 1);
+    if (smem > (size_t)ctx->smem_optin - 1024)
+        return set_error(ctx, RLA_E_UNSUPPORTED, "Cholesky of order %lld exceeds shared memory", (long long)l);
+    RLA_CUDA_TRY(ctx, cudaFuncSetAttribute(chol_upper_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    chol_upper_kernel<<<1, 1024, smem, ctx->stream>>>(G, l, shift, breakdown);
     return check_launch(ctx, "chol_upper");
 }
 
 int tri_inv_upper(rla_ctx *ctx, const double *R, int64_t l, double *Rinv) {
-    tri_inv_upper_kernel<<<ceil_div_i(l, 128), 128, 0, ctx->stream>>>(R, l, Rinv);
+    const int64_t per = sizeof(double) * std::max<int64_t>(l, 1);
+    const int wpc = (int)std::max<int64_t>(1, std::min<int64_t>(8, (ctx->smem_optin - 1024) / per));
+    if (per > ctx->smem_optin - 1024)
+        return set_error(ctx, RLA_E_UNSUPPORTED, "triangular inverse of order %lld exceeds shared memory", (long long)l);
+    const size_t smem = (size_t)per * wpc;
+    RLA_CUDA_TRY(ctx, cudaFuncSetAttribute(tri_inv_upper_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    tri_inv_upper_kernel<<<ceil_div_i(l, wpc), 32 * wpc, smem, ctx->stream>>>(R, l, Rinv, wpc);
     return check_launch(ctx, "tri_inv_upper");
 }
 
 int jacobi_svd(rla_ctx *ctx, double *X, double *J, double *sigma, int64_t l, double *work) {
-    jacobi_kernel<<<1, 1024, 0, ctx->stream>>>(X, J, sigma, l, work, 60, 1e-15);
-    return check_launch(ctx, "jacobi_svd");
+    const double tol = 1e-15;
+    const size_t smem = sizeof(double) * 4 * BJ_B * (size_t)l;
+    if (l <= 2 * BJ_B || smem > (size_t)ctx->smem_optin - 2048) {
+        jacobi_kernel<<<1, 1024, 0, ctx->stream>>>(X, J, sigma, l, work, 60, tol);
+        RLA_TRY(check_launch(ctx, "jacobi_svd"));
+    } else {
+        const int nb = (int)ceil_div(l, BJ_B), nbp = nb + (nb & 1);
+        jacobi_identity_kernel<<<ceil_div_i(l * l, 256), 256, 0, ctx->stream>>>(J, l);
+        RLA_TRY(check_launch(ctx, "jacobi_identity"));
+        RLA_CUDA_TRY(ctx, cudaFuncSetAttribute(block_jacobi_round_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)smem));
+        unsigned long long *off = reinterpret_cast<unsigned long long *>(work + 2 * l * l);
+        for (int sweep = 0; sweep < 40; ++sweep) {
+            RLA_CUDA_TRY(ctx, cudaMemsetAsync(off, 0, sizeof(unsigned long long), ctx->stream));
+            for (int r = 0; r < nbp - 1; ++r)
+                block_jacobi_round_kernel<<<nbp / 2, BJ_THREADS, smem, ctx->stream>>>(X, J, l, nbp, r, tol, off);
+            RLA_TRY(check_launch(ctx, "block_jacobi_round"));
+            unsigned long long h = 0;
+            RLA_CUDA_TRY(ctx, cudaMemcpyAsync(&h, off, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+            RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+            double v;
+            memcpy(&v, &h, sizeof(v));
+            if (v <= tol) break;
+        }
+    }
+    jacobi_finish_kernel<<<1, 1024, 0, ctx->stream>>>(X, J, sigma, l, work);
+    return check_launch(ctx, "jacobi_finish");
 }
 
 }  // namespace rla

@@ -47,7 +47,7 @@ static int lowrank_t(rla_ctx *ctx, int side, int trans_r, int64_t m, int64_t n, 
                                 beta);
     }
     double *tmp = nullptr;
-    RLA_CUDA_TRY(ctx, cudaMallocAsync((void **)&tmp, sizeof(double) * std::max<int64_t>(1, k * std::max(c_rows, c_cols)),
+    RLA_CUDA_TRY(ctx, pool_malloc_s(ctx, (void **)&tmp, sizeof(double) * std::max<int64_t>(1, k * std::max(c_rows, c_cols)),
                                       ctx->stream));
     int rc;
     if (side == RLA_SIDE_LEFT) {

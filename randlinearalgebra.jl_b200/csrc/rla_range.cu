@@ -204,9 +204,11 @@ struct OrthWork {
     void *tmp;  // rows x l of T
 };
 
-// In-place orthonormalisation of Y (rows x l, ld ldy); Q columns get Householder signs.
+// In-place orthonormalisation of Y (rows x l, ld ldy).  With `signs` the columns of Q get
+// the signs LAPACK's Householder QR of Y gives them (needed only where Q itself is
+// returned: column signs of intermediate bases cancel out of the final factors).
 template <class T>
-static int orth(rla_ctx *ctx, T *Y, int64_t rows, int64_t l, int64_t ldy, OrthWork &w) {
+static int orth(rla_ctx *ctx, T *Y, int64_t rows, int64_t l, int64_t ldy, OrthWork &w, bool signs = true) {
     if (l > rows)
         return set_error(ctx, RLA_E_UNSUPPORTED, "compression dimension %lld exceeds the %lld rows being orthogonalised",
                          (long long)l, (long long)rows);
@@ -247,6 +249,7 @@ static int orth(rla_ctx *ctx, T *Y, int64_t rows, int64_t l, int64_t ldy, OrthWo
         convert_kernel<T, T><<<ceil_div_i(rows * l, 256), 256, 0, ctx->stream>>>(tmp, rows, l, rows, Y, ldy);
         RLA_TRY(check_launch(ctx, "copy_back"));
     }
+    if (!signs) return RLA_OK;
     house_signs_kernel<T><<<1, 1024, 0, ctx->stream>>>(Y, rows, l, ldy, w.hw);
     return check_launch(ctx, "house_signs");
 }
@@ -254,7 +257,7 @@ static int orth(rla_ctx *ctx, T *Y, int64_t rows, int64_t l, int64_t ldy, OrthWo
 template <class T>
 static int alloc_orth(rla_ctx *ctx, OrthWork &w, int64_t rows, int64_t l, std::vector<void *> &owned) {
     auto get = [&](size_t bytes, void **p) -> int {
-        RLA_CUDA_TRY(ctx, cudaMallocAsync(p, std::max<size_t>(bytes, 16), ctx->stream));
+        RLA_CUDA_TRY(ctx, pool_malloc_s(ctx, p, std::max<size_t>(bytes, 16), ctx->stream));
         owned.push_back(*p);
         return RLA_OK;
     };
@@ -290,7 +293,7 @@ static int tc_ops_make(rla_ctx *ctx, const float *A, int64_t m, int64_t n, int64
     ops.lda = ceil_div(m, 8) * 8;
     const size_t na = (size_t)ops.lda * n, nx = (size_t)ceil_div(std::max(m, n), 8) * 8 * l;
     bf16 *buf = nullptr;
-    RLA_CUDA_TRY(ctx, cudaMallocAsync((void **)&buf, sizeof(bf16) * 2 * (na + nx), ctx->stream));
+    RLA_CUDA_TRY(ctx, pool_malloc_s(ctx, (void **)&buf, sizeof(bf16) * 2 * (na + nx), ctx->stream));
     own.ptrs.push_back(buf);
     ops.a_hi = buf;
     ops.a_lo = buf + na;
@@ -314,7 +317,8 @@ static int tc_apply(rla_ctx *ctx, const TcOps &ops, int at, int64_t m, int64_t n
 // only) the products with A run on the tensor cores in split BF16.
 template <class T>
 static int range_core(rla_ctx *ctx, const rla_sketch *om, int64_t m, int64_t n, const T *A, int64_t lda,
-                      const rla_range_params *pr, T *Q, int64_t ldq, Owned &own, const TcOps *tc = nullptr) {
+                      const rla_range_params *pr, T *Q, int64_t ldq, Owned &own, const TcOps *tc = nullptr,
+                      bool q_signs = true) {
     const int64_t l = om->n_cols;
     // Z = A'Q, Q = A Z
     auto at_q = [&](const T *Qp, T *Zp) -> int {
@@ -332,7 +336,7 @@ static int range_core(rla_ctx *ctx, const rla_sketch *om, int64_t m, int64_t n, 
     T *Z = nullptr;
     if (pr->power_its > 0) {
         RLA_TRY(alloc_orth<T>(ctx, wz, n, l, own.ptrs));
-        RLA_CUDA_TRY(ctx, cudaMallocAsync((void **)&Z, sizeof(T) * n * l, ctx->stream));
+        RLA_CUDA_TRY(ctx, pool_malloc_s(ctx, (void **)&Z, sizeof(T) * n * l, ctx->stream));
         own.ptrs.push_back(Z);
     }
     // Y = A * Omega (power_its.jl:21 / :59); a dense Gaussian Omega is a GEMM
@@ -345,19 +349,19 @@ static int range_core(rla_ctx *ctx, const rla_sketch *om, int64_t m, int64_t n, 
     }
     if (!done) RLA_TRY(sketch_mul_impl(ctx, om, RLA_SIDE_RIGHT, 0, m, l, Q, ldq, 0, m, n, A, lda, 0, 1.0, 0.0));
     if (pr->orthogonalize) {
-        RLA_TRY(orth<T>(ctx, Q, m, l, ldq, wq));
+        RLA_TRY(orth<T>(ctx, Q, m, l, ldq, wq, q_signs && pr->power_its == 0));
         for (int64_t it = 0; it < pr->power_its; ++it) {
             RLA_TRY(at_q(Q, Z));
-            RLA_TRY(orth<T>(ctx, Z, n, l, n, wz));
+            RLA_TRY(orth<T>(ctx, Z, n, l, n, wz, false));
             RLA_TRY(a_z(Z, Q));
-            RLA_TRY(orth<T>(ctx, Q, m, l, ldq, wq));
+            RLA_TRY(orth<T>(ctx, Q, m, l, ldq, wq, q_signs && it + 1 == pr->power_its));
         }
     } else {
         for (int64_t it = 0; it < pr->power_its; ++it) {
             RLA_TRY(at_q(Q, Z));
             RLA_TRY(a_z(Z, Q));
         }
-        RLA_TRY(orth<T>(ctx, Q, m, l, ldq, wq));
+        RLA_TRY(orth<T>(ctx, Q, m, l, ldq, wq, q_signs));
     }
     return RLA_OK;
 }
@@ -382,16 +386,16 @@ static int randsvd_t(rla_ctx *ctx, const rla_sketch *om, int64_t m, int64_t n, c
     const int64_t l = om->n_cols;
     Owned own{ctx, {}};
     T *Q;
-    RLA_CUDA_TRY(ctx, cudaMallocAsync((void **)&Q, sizeof(T) * m * l, ctx->stream));
+    RLA_CUDA_TRY(ctx, pool_malloc_s(ctx, (void **)&Q, sizeof(T) * m * l, ctx->stream));
     own.ptrs.push_back(Q);
     TcOps tc;
     const bool use_tc = pr->precision == RLA_PREC_SPLIT_BF16;
     if constexpr (std::is_same<T, float>::value)
         if (use_tc) RLA_TRY(tc_ops_make(ctx, A, m, n, lda, l, tc, own));
-    RLA_TRY(range_core<T>(ctx, om, m, n, A, lda, pr, Q, m, own, use_tc ? &tc : nullptr));
+    RLA_TRY(range_core<T>(ctx, om, m, n, A, lda, pr, Q, m, own, use_tc ? &tc : nullptr, false));
     // Bt = A'Q (n x l) in FP64 (randsvd.jl:183-185 forms QA in Float64)
     double *Bt, *X, *J, *sig, *jw;
-    RLA_CUDA_TRY(ctx, cudaMallocAsync((void **)&Bt, sizeof(double) * n * l, ctx->stream));
+    RLA_CUDA_TRY(ctx, pool_malloc_s(ctx, (void **)&Bt, sizeof(double) * n * l, ctx->stream));
     own.ptrs.push_back(Bt);
     bool bt_done = false;
     if constexpr (std::is_same<T, float>::value) {
@@ -402,19 +406,19 @@ static int randsvd_t(rla_ctx *ctx, const rla_sketch *om, int64_t m, int64_t n, c
     }
     if (!bt_done) RLA_TRY((gemm<T, T, double, double>(ctx, n, l, m, A, lda, 1, Q, m, 0, Bt, n, 1.0, 0.0)));
     double *Qb;
-    RLA_CUDA_TRY(ctx, cudaMallocAsync((void **)&Qb, sizeof(double) * n * l, ctx->stream));
+    RLA_CUDA_TRY(ctx, pool_malloc_s(ctx, (void **)&Qb, sizeof(double) * n * l, ctx->stream));
     own.ptrs.push_back(Qb);
     RLA_CUDA_TRY(ctx, cudaMemcpyAsync(Qb, Bt, sizeof(double) * n * l, cudaMemcpyDeviceToDevice, ctx->stream));
     OrthWork wb{};
     RLA_TRY(alloc_orth<double>(ctx, wb, n, l, own.ptrs));
-    RLA_TRY(orth<double>(ctx, Qb, n, l, n, wb));
-    RLA_CUDA_TRY(ctx, cudaMallocAsync((void **)&X, sizeof(double) * l * l, ctx->stream));
+    RLA_TRY(orth<double>(ctx, Qb, n, l, n, wb, false));
+    RLA_CUDA_TRY(ctx, pool_malloc_s(ctx, (void **)&X, sizeof(double) * l * l, ctx->stream));
     own.ptrs.push_back(X);
-    RLA_CUDA_TRY(ctx, cudaMallocAsync((void **)&J, sizeof(double) * l * l, ctx->stream));
+    RLA_CUDA_TRY(ctx, pool_malloc_s(ctx, (void **)&J, sizeof(double) * l * l, ctx->stream));
     own.ptrs.push_back(J);
-    RLA_CUDA_TRY(ctx, cudaMallocAsync((void **)&sig, sizeof(double) * l, ctx->stream));
+    RLA_CUDA_TRY(ctx, pool_malloc_s(ctx, (void **)&sig, sizeof(double) * l, ctx->stream));
     own.ptrs.push_back(sig);
-    RLA_CUDA_TRY(ctx, cudaMallocAsync((void **)&jw, sizeof(double) * (2 * l * l + 2 * l), ctx->stream));
+    RLA_CUDA_TRY(ctx, pool_malloc_s(ctx, (void **)&jw, sizeof(double) * (2 * l * l + 2 * l), ctx->stream));
     own.ptrs.push_back(jw);
     // X = Rb' = Bt' Qb (l x l)
     RLA_TRY((gemm<double, double, double, double>(ctx, l, l, n, Bt, n, 1, Qb, n, 0, X, l, 1.0, 0.0)));

@@ -465,8 +465,18 @@ int tc_gemm_bf16x3(rla_ctx *ctx, int64_t M, int64_t N, int64_t K, const bf16 *Ah
         TcParams p{(int)M, (int)nb, (int)K, pl.BN, pl.nch, a_kmajor, pl.nkb, pl.kbps, pl.stages, pl.tmem_cols,
                    out, ldo, sstride, status};
         RLA_CUDA_TRY(ctx, cudaFuncSetAttribute(tc_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem));
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        if (ctx->timing) {
+            RLA_CUDA_TRY(ctx, cudaEventCreate(&e0));
+            RLA_CUDA_TRY(ctx, cudaEventCreate(&e1));
+            RLA_CUDA_TRY(ctx, cudaEventRecord(e0, ctx->stream));
+        }
         tc_gemm_kernel<<<dim3(pl.mt, pl.splits), TC_THREADS, pl.smem, ctx->stream>>>(mah, mal, mbh, mbl, p);
         RLA_TRY(check_launch(ctx, "tc_gemm"));
+        if (ctx->timing) {
+            RLA_CUDA_TRY(ctx, cudaEventRecord(e1, ctx->stream));
+            ctx->timed[0].emplace_back(e0, e1);
+        }
         if (!direct) {
             const unsigned gx = (unsigned)std::min<int64_t>(ceil_div(M, 256), 1024);
             const unsigned gy = (unsigned)std::min<int64_t>(nb, 65535);
@@ -505,7 +515,7 @@ int rla_gemm_bf16x3(rla_ctx *ctx, int trans_a, int64_t m, int64_t n, int64_t k, 
     bf16 *buf = nullptr;
     const size_t na = (size_t)lda2 * a_cols, nb = (size_t)ldb2 * n;
     if (k > 0) {
-        RLA_CUDA_TRY(ctx, cudaMallocAsync((void **)&buf, sizeof(bf16) * 2 * (na + nb) + 64, ctx->stream));
+        RLA_CUDA_TRY(ctx, pool_malloc_s(ctx, (void **)&buf, sizeof(bf16) * 2 * (na + nb) + 64, ctx->stream));
     }
     int rc = RLA_OK;
     if (k == 0) {
