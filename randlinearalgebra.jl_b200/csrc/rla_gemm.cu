@@ -13,7 +13,7 @@ template <class TA, class TB, class TC, class TAcc, int BM, int BN, int BK, int 
 __global__ void __launch_bounds__((BM / TM) * (BN / TN))
 gemm_simt_kernel(int64_t M, int64_t N, int64_t K, const TA *__restrict__ A, int64_t lda, int ta,
                  const TB *__restrict__ B, int64_t ldb, int tb, TC *__restrict__ C, int64_t ldc, TAcc alpha,
-                 TAcc beta, int beta_zero) {
+                 TAcc beta, int beta_zero, int b_upper) {
     constexpr int NT = (BM / TM) * (BN / TN);
     __shared__ TAcc As[BK][BM + 1];
     __shared__ TAcc Bs[BK][BN + 1];
@@ -25,7 +25,9 @@ gemm_simt_kernel(int64_t M, int64_t N, int64_t K, const TA *__restrict__ A, int6
     for (int i = 0; i < TM; ++i)
 #pragma unroll
         for (int j = 0; j < TN; ++j) acc[i][j] = TAcc(0);
-    for (int64_t k0 = 0; k0 < K; k0 += BK) {
+    // an upper-triangular op(B) has no rows below the diagonal of this column block
+    const int64_t kend = b_upper ? min(K, n0 + BN) : K;
+    for (int64_t k0 = 0; k0 < kend; k0 += BK) {
         // A tile: BM x BK ; thread order follows the contiguous dimension of A
         for (int idx = tid; idx < BM * BK; idx += NT) {
             int i, k;
@@ -78,20 +80,20 @@ gemm_simt_kernel(int64_t M, int64_t N, int64_t K, const TA *__restrict__ A, int6
 
 template <class TA, class TB, class TC, class TAcc>
 int gemm(rla_ctx *ctx, int64_t M, int64_t N, int64_t K, const TA *A, int64_t lda, int ta, const TB *B, int64_t ldb,
-         int tb, TC *C, int64_t ldc, double alpha, double beta) {
+         int tb, TC *C, int64_t ldc, double alpha, double beta, int b_upper) {
     if (M <= 0 || N <= 0) return RLA_OK;
     constexpr int BM = 64, BN = 64, BK = 16, TM = 4, TN = 4;
     const int64_t gx = ceil_div(M, BM), gy = ceil_div(N, BN);
     if (gy > 65535) return set_error(ctx, RLA_E_UNSUPPORTED, "GEMM grid too large (N=%lld)", (long long)N);
     dim3 grid((unsigned)gx, (unsigned)gy);
     gemm_simt_kernel<TA, TB, TC, TAcc, BM, BN, BK, TM, TN><<<grid, (BM / TM) * (BN / TN), 0, ctx->stream>>>(
-        M, N, K, A, lda, ta, B, ldb, tb, C, ldc, (TAcc)alpha, (TAcc)beta, beta == 0.0);
+        M, N, K, A, lda, ta, B, ldb, tb, C, ldc, (TAcc)alpha, (TAcc)beta, beta == 0.0, b_upper);
     return check_launch(ctx, "gemm_simt");
 }
 
 #define RLA_GEMM_INST(TA, TB, TC, TAcc)                                                                  \
     template int gemm<TA, TB, TC, TAcc>(rla_ctx *, int64_t, int64_t, int64_t, const TA *, int64_t, int, \
-                                        const TB *, int64_t, int, TC *, int64_t, double, double);
+                                        const TB *, int64_t, int, TC *, int64_t, double, double, int);
 RLA_GEMM_INST(float, float, float, float)
 #define RLA_GEMM_INST_D(TA, TB) RLA_GEMM_INST(TA, TB, float, double) RLA_GEMM_INST(TA, TB, double, double)
 RLA_GEMM_INST_D(float, float)

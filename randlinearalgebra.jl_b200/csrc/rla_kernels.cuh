@@ -36,10 +36,11 @@ template <class T>
 int fjlt_expand(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_t x_es, int64_t x_vs, int64_t nv, T *Y,
                 int64_t y_es, int64_t y_vs, double alpha, double beta);
 
-// CUDA-core GEMM (rla_gemm.cu): C = alpha*op(A)*op(B) + beta*C, column-major.
+// CUDA-core GEMM (rla_gemm.cu): C = alpha*op(A)*op(B) + beta*C, column-major.  b_upper:
+// op(B) is upper triangular (its entries below the diagonal are not read).
 template <class TA, class TB, class TC, class TAcc>
 int gemm(rla_ctx *ctx, int64_t M, int64_t N, int64_t K, const TA *A, int64_t lda, int ta, const TB *B, int64_t ldb,
-         int tb, TC *C, int64_t ldc, double alpha, double beta);
+         int tb, TC *C, int64_t ldc, double alpha, double beta, int b_upper = 0);
 
 // Small dense FP64 kernels (rla_linalg.cu)
 // In place: G (l x l, ld l) -> upper Cholesky factor R (lower part zeroed).  `shift` is

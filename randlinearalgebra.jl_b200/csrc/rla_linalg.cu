@@ -48,12 +48,21 @@ __global__ void __launch_bounds__(1024) chol_upper_kernel(double *G, int64_t l, 
         }
         __syncthreads();
         const double rjj = rjj_s;
-        for (int64_t i = j + 1 + warp; i < l; i += nwarps) {
-            const double *ci = G + i * l;
-            double d = 0.0;
-            for (int64_t k = lane; k < j; k += 32) d += colj[k] * ci[k];
-            d = warp_sum(d);
-            if (lane == 0) G[j + i * l] = (G[j + i * l] - d) / rjj;
+        // four columns per warp at a time, so their loads overlap
+        for (int64_t i0 = j + 1 + 4 * warp; i0 < l; i0 += 4 * nwarps) {
+            double d[4] = {0.0, 0.0, 0.0, 0.0};
+            for (int64_t k = lane; k < j; k += 32) {
+                const double cj = colj[k];
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    if (i0 + q < l) d[q] = fma(cj, G[k + (i0 + q) * l], d[q]);
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) d[q] = warp_sum(d[q]);
+            if (lane < 4 && i0 + lane < l) {
+                const double dq = lane == 0 ? d[0] : lane == 1 ? d[1] : lane == 2 ? d[2] : d[3];
+                G[j + (i0 + lane) * l] = (G[j + (i0 + lane) * l] - dq) / rjj;
+            }
         }
         __syncthreads();
     }
@@ -216,7 +225,7 @@ __global__ void __launch_bounds__(1024) jacobi_finish_kernel(double *X, double *
 // are mutually orthogonal to `tol` or BJ_INNER sweeps, and writes them back.  The largest
 // relative off-diagonal seen in a CTA's first inner sweep goes to *off (max over the outer
 // sweep), which the host reads to stop.
-constexpr int BJ_B = 16, BJ_INNER = 4, BJ_THREADS = 512;
+constexpr int BJ_B = 16, BJ_INNER = 1, BJ_THREADS = 512;
 
 __global__ void jacobi_identity_kernel(double *J, int64_t l) {
     const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;

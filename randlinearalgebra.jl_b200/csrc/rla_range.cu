@@ -245,7 +245,7 @@ static int orth(rla_ctx *ctx, T *Y, int64_t rows, int64_t l, int64_t ldy, OrthWo
         RLA_TRY(tri_inv_upper(ctx, w.G, l, w.Rinv));
         row_scale_kernel<<<ceil_div_i(l * l, 256), 256, 0, ctx->stream>>>(w.Rinv, l, w.dscale);
         RLA_TRY(check_launch(ctx, "row_scale"));
-        RLA_TRY((gemm<T, double, T, double>(ctx, rows, l, l, Y, ldy, 0, w.Rinv, l, 0, tmp, rows, 1.0, 0.0)));
+        RLA_TRY((gemm<T, double, T, double>(ctx, rows, l, l, Y, ldy, 0, w.Rinv, l, 0, tmp, rows, 1.0, 0.0, 1)));
         convert_kernel<T, T><<<ceil_div_i(rows * l, 256), 256, 0, ctx->stream>>>(tmp, rows, l, rows, Y, ldy);
         RLA_TRY(check_launch(ctx, "copy_back"));
     }
