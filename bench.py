@@ -433,8 +433,8 @@ def randsvd_arm(args):
     rla = load_package()
     from randlinearalgebra_b200 import _lib as L
     dev = torch.device("cuda", local if world > 1 else 0)
-    m, n, l, q = RS_M, RS_N, RS_K + RS_P, RS_Q
-    A = rs_problem(torch, dev, m, n, RS_R, 3 + rank)
+    m, n, l, q = args.rs_m, args.rs_n, RS_K + RS_P, RS_Q
+    A = rs_problem(torch, dev, m, n, min(RS_R, n), 3 + rank)
     comp = rla.Gaussian(cardinality=rla.Right(), compression_dim=l, type=np.float32)
     rec = rla.complete_approximator(rla.RandSVD(compressor=comp, power_its=q, orthogonalize=True,
                                                 precision=rla.RLA_PREC_SPLIT_BF16, factor_type=np.float32),
@@ -526,7 +526,8 @@ def randsvd_arm(args):
             "warmup": args.warmup, "ms_per_step": round(ms / K, 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 data, bf16x3 products, f64 small factorizations",
             "data": "synthetic U diag(i^-1.5) V' + 1e-6 N(0,1) generated on device (seed 3+rank)",
-            "config": {"workload": RS_WORKLOAD, "m": m, "n": n, "k": RS_K, "p": RS_P, "q": q,
+            "config": {"workload": RS_WORKLOAD if (m, n) == (RS_M, RS_N) else
+                       RS_WORKLOAD.replace("65536x8192", f"{m}x{n}"), "m": m, "n": n, "k": RS_K, "p": RS_P, "q": q,
                        "parallelism": f"replicas x{world}", "l2": "A is 2.15 GB (larger than L2), no flush needed"},
             "roofline": roofline,
             "error": {"proj_err_split": e32, "proj_err_fp64": e64, "proj_err_diff": abs(e32 - e64),
@@ -550,6 +551,8 @@ def main():
                          "cases of the same kernels for profiler captures)")
     ap.add_argument("--workload", choices=["sketch", "randsvd"], default="sketch",
                     help="sketch: SRHT + CountSketch apply (default); randsvd: mixed-precision RandSVD")
+    ap.add_argument("--rs-m", type=int, default=RS_M, help="RandSVD rows (default 65536; smaller for profiler cases)")
+    ap.add_argument("--rs-n", type=int, default=RS_N, help="RandSVD columns (default 8192)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
