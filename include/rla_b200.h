@@ -195,6 +195,46 @@ int rla_lowrank_mul(rla_ctx *ctx, int factor_dtype, int dtype, int side, int tra
                     int64_t a_rows, int64_t a_cols, const void *A, int64_t lda, int trans_a,
                     double alpha, double beta);
 
+/* ---- batched RandSVD (grouped launches, CUDA graph) -------------------------------- */
+/* Many rapproximate!(RandSVD) calls at once (randsvd.jl:174-189 per instance, with the
+ * reference's defaults: Gaussian Right compressor with compression_dim = k, p = 0, the
+ * given power_its / orthogonalize).  Instance i: A (m x n, Float32, column-major, device)
+ * -> U (m x k, Float32), S (k, Float64, descending), V (n x k, Float32); k <= min(m, n, 128).
+ * Omega is drawn exactly as rla_sketch_create(RLA_GAUSSIAN, RLA_RIGHT, RLA_F32, k, n, seed)
+ * draws it.  Products with A accumulate in FP32, Gram/Cholesky/SVD in FP64.  No single
+ * reference function: the reference runs the instances one after another. */
+typedef struct rla_svd_problem {
+    int64_t m, n, k;
+    const float *A;
+    int64_t lda;
+    float *U;
+    int64_t ldu;
+    double *S;
+    float *V;
+    int64_t ldv;
+    uint64_t seed;
+} rla_svd_problem;
+
+typedef struct rla_batch rla_batch;
+#define RLA_BATCH_AUTOTUNE 1 /* time candidate tile shapes on the problem set at creation */
+
+/* Plan a batch: workspaces, per-rank-class grouped launch tables, tuned tile shapes.  The
+ * problem list (pointers included) is fixed for the plan's lifetime. */
+int rla_randsvd_batch_create(rla_ctx *ctx, int count, const rla_svd_problem *problems,
+                             const rla_range_params *params, int flags, rla_batch **out);
+/* Run the batch on the context's stream: the first run captures the grouped launch
+ * sequence as a CUDA graph, later runs replay it.  Returns when every instance is done
+ * (instances whose Cholesky broke down are recomputed by the single-instance path). */
+int rla_randsvd_batch_run(rla_ctx *ctx, rla_batch *batch);
+/* Tile shapes in use for rank class c (0: k <= 16, 1: <= 32, 2: <= 64, 3: <= 128): rows
+ * per CTA of A*Omega, columns of A per CTA of A'Q and its row chunk. */
+int rla_randsvd_batch_tiles(const rla_batch *batch, int c, int *rows_a_omega, int *cols_at_q,
+                            int64_t *chunk_at_q);
+int rla_randsvd_batch_destroy(rla_batch *batch);
+/* create (no tuning) + run + destroy */
+int rla_randsvd_grouped(rla_ctx *ctx, int count, const rla_svd_problem *problems,
+                        const rla_range_params *params);
+
 /* ---- kernel timing (tracing aid, no reference counterpart) ------------------------- */
 /* While enabled, the context records CUDA events around each launch of a timed kernel
  * class on its stream (class 0: the tensor-core GEMM kernel).  rla_ctx_kernel_time

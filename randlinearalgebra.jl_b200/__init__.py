@@ -11,7 +11,7 @@ from .compressors import (Cardinality, Left, Right, Undef, Compressor, Compresso
                           adjoint, transpose, size, seed_)
 from .approximators import (Approximator, RangeApproximator, ApproximatorRecipe, RangeApproximatorRecipe,
                             ApproximatorAdjoint, RangeFinder, RangeFinderRecipe, RandSVD, RandSVDRecipe,
-                            complete_approximator, rapproximate_, rapproximate)
+                            complete_approximator, rapproximate_, rapproximate, RandSVDBatch)
 from ._lib import RLA_PREC_NATIVE, RLA_PREC_SPLIT_BF16, lib, Context
 
 __version__ = "0.1.0"

@@ -43,6 +43,13 @@ class RangeParams(ctypes.Structure):
     _fields_ = [("power_its", i64), ("orthogonalize", ctypes.c_int), ("precision", ctypes.c_int)]
 
 
+class SvdProblem(ctypes.Structure):
+    _fields_ = [("m", i64), ("n", i64), ("k", i64), ("A", vp), ("lda", i64), ("U", vp), ("ldu", i64),
+                ("S", vp), ("V", vp), ("ldv", i64), ("seed", ctypes.c_uint64)]
+
+
+RLA_BATCH_AUTOTUNE = 1
+
 # name -> (restype, argtypes); every function declared in include/rla_b200.h
 SIGNATURES = {
     "rla_version": (ctypes.c_int, []),
@@ -71,6 +78,13 @@ SIGNATURES = {
                                        ctypes.c_int, ctypes.c_double, ctypes.c_double]),
     "rla_srht_mul_noalloc": (ctypes.c_int, [vp, vp, i64, i64, vp, i64, i64, i64, vp, i64, ctypes.c_double,
                                             ctypes.c_double]),
+    "rla_randsvd_batch_create": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(SvdProblem), ctypes.POINTER(RangeParams),
+                                                ctypes.c_int, ctypes.POINTER(vp)]),
+    "rla_randsvd_batch_run": (ctypes.c_int, [vp, vp]),
+    "rla_randsvd_batch_tiles": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                               ctypes.POINTER(ctypes.c_int), ctypes.POINTER(i64)]),
+    "rla_randsvd_batch_destroy": (ctypes.c_int, [vp]),
+    "rla_randsvd_grouped": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(SvdProblem), ctypes.POINTER(RangeParams)]),
     "rla_ctx_set_timing": (ctypes.c_int, [vp, ctypes.c_int]),
     "rla_ctx_kernel_time": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(i64)]),
     "rla_gemm_bf16x3": (ctypes.c_int, [vp, ctypes.c_int, i64, i64, i64, vp, i64, vp, i64, vp, i64,

@@ -227,3 +227,65 @@ def _times(X, Y):
 for _cls in (RangeFinderRecipe, RandSVDRecipe, ApproximatorAdjoint):
     _cls.__matmul__ = lambda self, A: _times(self, A)
     _cls.__rmatmul__ = lambda self, A: _times(A, self)
+
+
+class RandSVDBatch:
+    """Many RandSVD instances at once (rla_randsvd_batch_*): instance i is
+    rapproximate!(RandSVD(compressor=Gaussian(Right(), compression_dim=k_i), power_its,
+    orthogonalize), A_i) with Float32 A_i; the factors U_i (m_i x k_i, Float32), S_i (k_i,
+    Float64) and V_i (n_i x k_i, Float32) are allocated here.  Omega_i is the Gaussian
+    sketch complete_compressor would draw with seed seeds[i].  The first run() captures the
+    grouped launch sequence as a CUDA graph; later runs replay it."""
+
+    def __init__(self, As, ks, seeds, power_its: int = 0, orthogonalize: bool = False, autotune: bool = True):
+        import torch
+        if not (len(As) == len(ks) == len(seeds)):
+            raise ArgumentError("As, ks and seeds must have the same length.")
+        self.As, self.U, self.S, self.V = [], [], [], []
+        probs = (L.SvdProblem * max(1, len(As)))()
+        dev = None
+        for i, (A, k, sd) in enumerate(zip(As, ks, seeds)):
+            Aop = Operand(A, "col")
+            if Aop.host or Aop.dtype != 0:
+                raise ArgumentError("Batched RandSVD takes Float32 device matrices.")
+            if Aop.trans:
+                Aop = Operand(Aop.t.t().contiguous().t(), "col")
+            dev = Aop.t.device
+            m, n = Aop.rows, Aop.cols
+            U = torch.empty(k, m, dtype=torch.float32, device=dev).t()
+            S = torch.empty(k, dtype=torch.float64, device=dev)
+            V = torch.empty(k, n, dtype=torch.float32, device=dev).t()
+            self.As.append(Aop.t)
+            self.U.append(U)
+            self.S.append(S)
+            self.V.append(V)
+            probs[i] = L.SvdProblem(m, n, int(k), Aop.ptr, Aop.ld, U.data_ptr(), m, S.data_ptr(), V.data_ptr(), n,
+                                    int(sd) & (2**64 - 1))
+        self.ctx = L.Context.get(None if dev is None else dev.index)
+        p = L.RangeParams()
+        p.power_its = int(power_its)
+        p.orthogonalize = 1 if orthogonalize else 0
+        p.precision = L.RLA_PREC_NATIVE
+        h = ctypes.c_void_p()
+        L.check(L.lib().rla_randsvd_batch_create(self.ctx.handle, len(As), probs, ctypes.byref(p),
+                                                 L.RLA_BATCH_AUTOTUNE if autotune else 0, ctypes.byref(h)),
+                self.ctx.handle)
+        self.handle = h
+        self._probs = probs
+
+    def run(self) -> None:
+        ctx = L.Context.get(self.ctx.device)
+        L.check(L.lib().rla_randsvd_batch_run(ctx.handle, self.handle), ctx.handle)
+
+    def tiles(self, c: int):
+        a, b, ch = ctypes.c_int(), ctypes.c_int(), ctypes.c_int64()
+        L.check(L.lib().rla_randsvd_batch_tiles(self.handle, c, ctypes.byref(a), ctypes.byref(b), ctypes.byref(ch)))
+        return a.value, b.value, ch.value
+
+    def __del__(self):
+        try:
+            if getattr(self, "handle", None):
+                L.lib().rla_randsvd_batch_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass

@@ -166,6 +166,36 @@ __host__ __device__ inline double u01_open_d(uint32_t a, uint32_t b) {
     return ((double)v + 1.0) * (1.0 / 9007199254740992.0);
 }
 
+// Per-thread word source over one Philox stream position.
+struct WordStream {
+    Rng rng;
+    uint32_t stream;
+    uint64_t base;   // index of the first block
+    uint64_t block = 0;
+    int used = 4;
+    P4 cur{};
+    __device__ uint32_t operator()() {
+        if (used == 4) {
+            cur = rng.at(stream, base + block++);
+            used = 0;
+        }
+        uint32_t w = used == 0 ? cur.x : used == 1 ? cur.y : used == 2 ? cur.z : cur.w;
+        ++used;
+        return w;
+    }
+};
+
+// Two N(0,1) draws by Box-Muller from four 32-bit words (53-bit uniforms in (0, 1]).
+__device__ inline double normal_pair(WordStream &ws, double *second) {
+    double u1 = u01_open_d(ws(), ws());
+    double u2 = u01_open_d(ws(), ws());
+    double r = sqrt(-2.0 * log(u1));
+    double sn, cs;
+    sincospi(2.0 * u2, &sn, &cs);
+    *second = r * sn;
+    return r * cs;
+}
+
 // ------------------------------------------------------------------------------------
 // Element-type helpers
 // ------------------------------------------------------------------------------------

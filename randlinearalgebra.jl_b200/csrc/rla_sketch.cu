@@ -18,25 +18,6 @@
 
 namespace rla {
 
-// Per-thread word source over one Philox stream position.
-struct WordStream {
-    Rng rng;
-    uint32_t stream;
-    uint64_t base;   // index of the first block
-    uint64_t block = 0;
-    int used = 4;
-    P4 cur{};
-    __device__ uint32_t operator()() {
-        if (used == 4) {
-            cur = rng.at(stream, base + block++);
-            used = 0;
-        }
-        uint32_t w = used == 0 ? cur.x : used == 1 ? cur.y : used == 2 ? cur.z : cur.w;
-        ++used;
-        return w;
-    }
-};
-
 // SparseSign / CountSketch: per long index j, nnz distinct buckets (Floyd's algorithm,
 // then sorted ascending like StatsBase.sample!(...; ordered=true)) and nnz sign bits.
 __global__ void draw_sparse_kernel(Rng rng, uint32_t stream, int64_t L, int nnz, int64_t s,
@@ -301,15 +282,6 @@ __global__ void draw_rows_kernel(Rng rng, int64_t N, int64_t s, uint32_t *gbitma
     }
 }
 
-__device__ inline double normal_pair(WordStream &ws, double *second) {
-    double u1 = u01_open_d(ws(), ws());
-    double u2 = u01_open_d(ws(), ws());
-    double r = sqrt(-2.0 * log(u1));
-    double sn, cs;
-    sincospi(2.0 * u2, &sn, &cs);
-    *second = r * sn;
-    return r * cs;
-}
 
 // FJLT: rows of Kc (s x N) with a Bernoulli(q) pattern drawn by geometric gaps.
 // Pass 0 counts, pass 1 fills; both passes replay the same word stream.
