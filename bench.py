@@ -539,6 +539,172 @@ def randsvd_arm(args):
         dist.destroy_process_group()
 
 
+# --------------------------------------------------------------------------------------
+# Batched RandSVD workload
+# --------------------------------------------------------------------------------------
+BT_COUNT = 512
+BT_METRIC = "batched RandSVD throughput (instances/s; grouped launches in a CUDA graph)"
+BT_WORKLOAD = ("batched randsvd: 512 fp32 instances, m~U[2^12,2^16], n~U[64,1024], k in {16,32,64}, "
+               "s_i = 0.9^i + 1e-6 N(0,1), gaussian sketch, p=0, q=0")
+
+
+def bt_shapes(count, seed=4):
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    ms = rng.integers(2**12, 2**16 + 1, size=count)
+    ns = rng.integers(64, 1025, size=count)
+    ks = rng.choice([16, 32, 64], size=count)
+    return [(int(m), int(n), int(min(k, n))) for m, n, k in zip(ms, ns, ks)]
+
+
+def bt_matrix(torch, dev, m, n, g):
+    """m x n Float32 column-major: U diag(0.9^i) V' + 1e-6 N(0,1), U and V orthonormal with
+    min(n, 160) columns (0.9^160 < 1e-7, below the noise)."""
+    r = min(n, 160)
+    U = torch.linalg.qr(torch.randn(m, r, device=dev, generator=g))[0]
+    V = torch.linalg.qr(torch.randn(n, r, device=dev, generator=g))[0]
+    s = 0.9 ** torch.arange(r, device=dev, dtype=torch.float32)
+    At = (V * s) @ U.t()
+    At.add_(torch.randn(n, m, device=dev, generator=g), alpha=1e-6)
+    return At.t()
+
+
+def batched_arm(args):
+    import numpy as np
+    import torch
+
+    world, rank, local = dist_setup(args.gpus)
+    from __graft_entry__ import load_package
+    rla = load_package()
+    dev = torch.device("cuda", local if world > 1 else 0)
+    shapes = bt_shapes(args.batch_count)
+    g = torch.Generator(device=dev)
+    g.manual_seed(4 + rank)
+    As = [bt_matrix(torch, dev, m, n, g) for (m, n, k) in shapes]
+    ks = [k for (_, _, k) in shapes]
+    seeds = [4000 + 7 * i + 100000 * rank for i in range(len(shapes))]
+    bytes_alg = sum(4 * 2 * m * n for (m, n, _) in shapes)   # A read twice (A*Omega, A'Q)
+    flops = sum(4.0 * m * n * k for (m, n, k) in shapes)
+    t_plan = time.perf_counter()
+    B = rla.RandSVDBatch(As, ks, seeds, autotune=True)
+    t_plan = time.perf_counter() - t_plan
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(args.warmup):
+        B.run()
+    torch.cuda.synchronize()
+    K = args.steps
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    props = torch.cuda.get_device_properties(dev)
+    clocks = ClockSampler(f"GPU-{props.uuid}" if getattr(props, "uuid", None) else dev.index)
+    barrier(world)
+    clocks.start()
+    t0.record(stream)
+    for _ in range(K):
+        B.run()
+    t1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = allreduce_max(t0.elapsed_time(t1) / K, world)
+    n_inst = len(shapes)
+    value = world * n_inst / (ms / 1e3)
+
+    # ---- plain path: one rapproximate! (its own launch sequence) per instance ---------------
+    def plain_once():
+        out = []
+        for A, k, sd in zip(As, ks, seeds):
+            comp = rla.Gaussian(cardinality=rla.Right(), compression_dim=k, type=np.float32)
+            out.append(rla.rapproximate(rla.RandSVD(compressor=comp, factor_type=np.float32), A, seed=sd))
+        return out
+    plain_once()
+    torch.cuda.synchronize()
+    p0 = time.perf_counter()
+    recs = plain_once()
+    torch.cuda.synchronize()
+    plain_s = time.perf_counter() - p0
+
+    # ---- error on a sample against the FP64 run of the same algorithm on the same draws --------
+    errs = []
+    for i in range(0, n_inst, max(1, n_inst // 12)):
+        A64 = As[i].t().double().t()
+        comp = rla.Gaussian(cardinality=rla.Right(), compression_dim=ks[i])
+        r64 = rla.complete_approximator(rla.RandSVD(compressor=comp), A64, seed=1)
+        r64.compressor.load_draws(vals=recs[i].compressor.draws()["op"].astype(np.float64))
+        rla.rapproximate_(r64, A64)
+        U = B.U[i].double()
+        nA = torch.linalg.norm(A64)
+        e_b = float(torch.linalg.norm(A64 - U @ (U.t() @ A64)) / nA)
+        e_r = float(torch.linalg.norm(A64 - r64.U @ (r64.U.t() @ A64)) / nA)
+        s_err = float(torch.linalg.norm(B.S[i] - r64.S) / torch.linalg.norm(r64.S))
+        errs.append((abs(e_b - e_r), s_err))
+        del A64, r64
+    del recs
+
+    # ---- end to end: host inputs in, factors out -----------------------------------------
+    e2e = None
+    try:
+        Ah = [torch.empty(n, m, dtype=torch.float32, pin_memory=True).t() for (m, n, _) in shapes]
+        for a, h in zip(As, Ah):
+            h.copy_(a)
+        torch.cuda.synchronize()
+        w0 = time.perf_counter()
+        for a, h in zip(As, Ah):
+            a.copy_(h, non_blocking=True)
+        B.run()
+        outs = [(u.cpu(), s_.cpu(), v.cpu()) for u, s_, v in zip(B.U, B.S, B.V)]
+        e2e_s = time.perf_counter() - w0
+        e2e = {"value": round(world * n_inst / e2e_s, 3), "unit": "instances/s",
+               "h2d_bytes_per_step": sum(4 * m * n for (m, n, _) in shapes),
+               "d2h_bytes_per_step": sum(4 * (m + n) * k + 8 * k for (m, n, k) in shapes),
+               "ms_per_step": round(e2e_s * 1e3, 3)}
+        del Ah, outs
+    except RuntimeError as ex:  # host memory for pinned copies of every A
+        e2e = {"unavailable": f"pinned host copies of all inputs: {ex}"[:200]}
+    barrier(world)
+    if rank != 0:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    peak, peak_kind = peaks()
+    gbs = bytes_alg / (ms / 1e3) / 1e9
+    tiles = {c: dict(zip(("rows_a_omega", "cols_at_q", "chunk_at_q"), B.tiles(c))) for c in range(3)}
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        from __graft_entry__ import load_oracle
+        orc = load_oracle()
+        idx = list(range(0, n_inst, max(1, n_inst // 8)))
+        c0 = time.perf_counter()
+        for i in idx:
+            A = As[i].cpu().numpy().astype(np.float64)
+            R = orc.Recipe("gaussian", "right", A.shape[1], ks[i], np.float64,
+                           dense_op=np.random.default_rng(i).standard_normal((A.shape[1], ks[i])) / np.sqrt(ks[i]),
+                           scale=1.0 / np.sqrt(ks[i]))
+            orc.randsvd(A, R)
+        cdt = (time.perf_counter() - c0) / len(idx)
+        cpu = {"value": round(1.0 / cdt, 3), "unit": "instances/s", "cores": os.cpu_count(), "kind": "port",
+               "sample": f"FP64 RandSVD of the oracle (numpy/LAPACK, all BLAS threads) on {len(idx)} of the instances"}
+    line = {"metric": BT_METRIC, "value": round(value, 2), "unit": "instances/s", "n_gpus": world, "steps": K,
+            "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 data, f32 products, f64 small factorizations",
+            "data": "synthetic low-rank + noise generated on device (seed 4+rank)",
+            "config": {"workload": BT_WORKLOAD if n_inst == BT_COUNT else BT_WORKLOAD.replace("512", str(n_inst)),
+                       "instances": n_inst, "parallelism": f"replicas x{world}",
+                       "l2": f"{bytes_alg / 2 / 1e9:.1f} GB of A per pass, larger than L2"},
+            "roofline": {"bound": "hbm", "kernel": "whole batch (grouped launches)", "achieved": round(gbs, 2),
+                         "peak": peak, "peak_source": peak_kind, "unit": "GB/s", "frac": round(gbs / peak, 4),
+                         "traffic": None, "algorithmic_bytes_per_step": bytes_alg, "gflops": round(flops / ms / 1e6, 1)},
+            "plain": {"instances_per_s": round(n_inst / plain_s, 2), "ms": round(plain_s * 1e3, 2),
+                      "speedup_batched": round(plain_s * 1e3 / ms, 2)},
+            "error": {"max_proj_err_diff": max(e[0] for e in errs), "max_sigma_rel_err": max(e[1] for e in errs),
+                      "instances_checked": len(errs), "tolerance": 1e-4},
+            "autotuned_tiles": tiles, "plan_s": round(t_plan, 3),
+            "cpu_baseline": cpu, "e2e": e2e, "clocks": clk}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -549,14 +715,22 @@ def main():
     ap.add_argument("--cols", type=int, default=NCOL,
                     help="columns of A (default 512, the benchmark workload; smaller values make small "
                          "cases of the same kernels for profiler captures)")
-    ap.add_argument("--workload", choices=["sketch", "randsvd"], default="sketch",
-                    help="sketch: SRHT + CountSketch apply (default); randsvd: mixed-precision RandSVD")
+    ap.add_argument("--workload", choices=["sketch", "randsvd", "batched"], default="sketch",
+                    help="sketch: SRHT + CountSketch apply (default); randsvd: mixed-precision RandSVD; "
+                         "batched: 512 uneven RandSVD instances")
+    ap.add_argument("--batch-count", type=int, default=BT_COUNT, help="instances of the batched workload")
     ap.add_argument("--rs-m", type=int, default=RS_M, help="RandSVD rows (default 65536; smaller for profiler cases)")
     ap.add_argument("--rs-n", type=int, default=RS_N, help="RandSVD columns (default 8192)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.workload == "randsvd":
+    if args.workload == "batched":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "batched workload: the reference arm is timed "
+                              "for the sketch and randsvd workloads only"}), flush=True)
+        else:
+            batched_arm(args)
+    elif args.workload == "randsvd":
         if args.impl == "reference":
             randsvd_reference_arm(args)
         else:
