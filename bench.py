@@ -586,7 +586,7 @@ def batched_arm(args):
     bytes_alg = sum(4 * 2 * m * n for (m, n, _) in shapes)   # A read twice (A*Omega, A'Q)
     flops = sum(4.0 * m * n * k for (m, n, k) in shapes)
     t_plan = time.perf_counter()
-    B = rla.RandSVDBatch(As, ks, seeds, autotune=True)
+    B = rla.RandSVDBatch(As, ks, seeds, autotune=not args.no_autotune)
     t_plan = time.perf_counter() - t_plan
     stream = torch.cuda.current_stream(dev)
     for _ in range(args.warmup):
@@ -719,6 +719,7 @@ def main():
                     help="sketch: SRHT + CountSketch apply (default); randsvd: mixed-precision RandSVD; "
                          "batched: 512 uneven RandSVD instances")
     ap.add_argument("--batch-count", type=int, default=BT_COUNT, help="instances of the batched workload")
+    ap.add_argument("--no-autotune", action="store_true", help="batched workload: default tile shapes")
     ap.add_argument("--rs-m", type=int, default=RS_M, help="RandSVD rows (default 65536; smaller for profiler cases)")
     ap.add_argument("--rs-n", type=int, default=RS_N, help="RandSVD columns (default 8192)")
     args = ap.parse_args()
