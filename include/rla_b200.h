@@ -217,9 +217,11 @@ typedef struct rla_svd_problem {
 
 typedef struct rla_batch rla_batch;
 #define RLA_BATCH_AUTOTUNE 1 /* time candidate tile shapes on the problem set at creation */
+#define RLA_BATCH_EAGER 2    /* launch directly on the context's stream, no CUDA graph */
 
 /* Plan a batch: workspaces, per-rank-class grouped launch tables, tuned tile shapes.  The
- * problem list (pointers included) is fixed for the plan's lifetime. */
+ * problem list (pointers included) is fixed for the plan's lifetime.  Its device memory
+ * comes from the context's pool, so the context must outlive the batch. */
 int rla_randsvd_batch_create(rla_ctx *ctx, int count, const rla_svd_problem *problems,
                              const rla_range_params *params, int flags, rla_batch **out);
 /* Run the batch on the context's stream: the first run captures the grouped launch
@@ -234,6 +236,60 @@ int rla_randsvd_batch_destroy(rla_batch *batch);
 /* create (no tuning) + run + destroy */
 int rla_randsvd_grouped(rla_ctx *ctx, int count, const rla_svd_problem *problems,
                         const rla_range_params *params);
+
+/* ---- sketch-and-solve least squares -------------------------------------------------- */
+/* x = argmin ||S(Ax - b)|| for a Left Float32 compressor S (s x m, s >= n), A (m x n),
+ * b (m), x (n): SA and Sb by the sketch kernels, then the sketched normal equations through
+ * the FP64 Cholesky factor of the equilibrated Gram matrix of SA.  The least-squares request
+ * of the serving loop; the reference's solvers reach the same sketch through mul!
+ * (src/Solvers/ihs.jl:231-236).  Device pointers; synchronous; RLA_E_NUMERIC when the
+ * sketched Gram matrix is not positive definite. */
+int rla_sketch_solve(rla_ctx *ctx, const rla_sketch *sk, int64_t m, int64_t n, const float *A,
+                     int64_t lda, const float *b, float *x);
+
+/* ---- serving loop ------------------------------------------------------------------------ */
+/* No reference counterpart (the reference is a library of one-call functions).  Mixed
+ * requests -- sketch-and-solve least squares (SparseSign Left, s = min(4n, m), nnz = 8) and
+ * RandSVD (Gaussian, compression_dim = k, p = 0, q = 0) -- on Float32 device buffers the
+ * caller owns and keeps alive until the request is polled as done. */
+#define RLA_REQ_LS 0
+#define RLA_REQ_SVD 1
+typedef struct rla_request {
+    int kind;                 /* RLA_REQ_LS or RLA_REQ_SVD */
+    int64_t m, n, k;          /* A is m x n; k: RandSVD rank (ignored for LS) */
+    const float *A;
+    int64_t lda;
+    const float *b;           /* LS: right-hand side (m) */
+    float *x;                 /* LS: solution (n) */
+    float *U;                 /* RandSVD: U (m x k), S (k, Float64), V (n x k) */
+    int64_t ldu;
+    double *S;
+    float *V;
+    int64_t ldv;
+    uint64_t seed;            /* sketch seed (sketches are kept resident per shape and seed) */
+    uint64_t tag;             /* returned by rla_server_poll */
+} rla_request;
+
+#define RLA_SERVE_BATCHED 0   /* continuous batching: slots work at once, RandSVD grouped */
+#define RLA_SERVE_PLAIN 1     /* baseline: one request at a time, single-instance path */
+typedef struct rla_server_config {
+    int device;
+    int slots;                /* concurrent workers (each with its own stream) */
+    int max_group;            /* RandSVD requests (k <= 128) run as one grouped batch */
+    int mode;                 /* RLA_SERVE_BATCHED or RLA_SERVE_PLAIN */
+    uint64_t memory_budget;   /* bytes of workspace admitted at once (0: 150 GB) */
+} rla_server_config;
+
+typedef struct rla_server rla_server;
+int rla_server_start(const rla_server_config *cfg, rla_server **out);
+/* Queue a request (returns at once). */
+int rla_server_submit(rla_server *srv, const rla_request *req);
+/* Up to `max` completed requests: tags, submit-to-done latency (s) and status. */
+int rla_server_poll(rla_server *srv, uint64_t *tags, double *latency_s, int *status, int max, int *count);
+/* Block until the queue is empty and nothing runs. */
+int rla_server_wait_idle(rla_server *srv);
+/* Finish queued work and shut the workers down. */
+int rla_server_stop(rla_server *srv);
 
 /* ---- kernel timing (tracing aid, no reference counterpart) ------------------------- */
 /* While enabled, the context records CUDA events around each launch of a timed kernel

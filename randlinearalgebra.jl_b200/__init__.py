@@ -13,5 +13,6 @@ from .approximators import (Approximator, RangeApproximator, ApproximatorRecipe,
                             ApproximatorAdjoint, RangeFinder, RangeFinderRecipe, RandSVD, RandSVDRecipe,
                             complete_approximator, rapproximate_, rapproximate, RandSVDBatch)
 from ._lib import RLA_PREC_NATIVE, RLA_PREC_SPLIT_BF16, lib, Context
+from .serving import Server, sketch_solve
 
 __version__ = "0.1.0"

@@ -48,7 +48,21 @@ class SvdProblem(ctypes.Structure):
                 ("S", vp), ("V", vp), ("ldv", i64), ("seed", ctypes.c_uint64)]
 
 
+class Request(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int), ("m", i64), ("n", i64), ("k", i64), ("A", vp), ("lda", i64), ("b", vp),
+                ("x", vp), ("U", vp), ("ldu", i64), ("S", vp), ("V", vp), ("ldv", i64), ("seed", ctypes.c_uint64),
+                ("tag", ctypes.c_uint64)]
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("slots", ctypes.c_int), ("max_group", ctypes.c_int), ("mode", ctypes.c_int),
+                ("memory_budget", ctypes.c_uint64)]
+
+
+RLA_REQ_LS, RLA_REQ_SVD = 0, 1
+RLA_SERVE_BATCHED, RLA_SERVE_PLAIN = 0, 1
 RLA_BATCH_AUTOTUNE = 1
+RLA_BATCH_EAGER = 2
 
 # name -> (restype, argtypes); every function declared in include/rla_b200.h
 SIGNATURES = {
@@ -85,6 +99,12 @@ SIGNATURES = {
                                                ctypes.POINTER(ctypes.c_int), ctypes.POINTER(i64)]),
     "rla_randsvd_batch_destroy": (ctypes.c_int, [vp]),
     "rla_randsvd_grouped": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(SvdProblem), ctypes.POINTER(RangeParams)]),
+    "rla_sketch_solve": (ctypes.c_int, [vp, vp, i64, i64, vp, i64, vp, vp]),
+    "rla_server_start": (ctypes.c_int, [ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]),
+    "rla_server_submit": (ctypes.c_int, [vp, ctypes.POINTER(Request)]),
+    "rla_server_poll": (ctypes.c_int, [vp, vp, vp, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
+    "rla_server_wait_idle": (ctypes.c_int, [vp]),
+    "rla_server_stop": (ctypes.c_int, [vp]),
     "rla_ctx_set_timing": (ctypes.c_int, [vp, ctypes.c_int]),
     "rla_ctx_kernel_time": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(i64)]),
     "rla_gemm_bf16x3": (ctypes.c_int, [vp, ctypes.c_int, i64, i64, i64, vp, i64, vp, i64, vp, i64,

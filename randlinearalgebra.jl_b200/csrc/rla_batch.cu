@@ -520,14 +520,16 @@ __global__ void __launch_bounds__(512) b_jacobi_kernel(BProb *P, const int *idx,
 // host side: plan, autotuner, graph
 // ------------------------------------------------------------------------------------
 struct rla_batch {
+    rla_ctx *ctx = nullptr;   // allocations come from this context's pool
     int device = 0;
+    int flags = 0;
     int count = 0;
     std::vector<rla_svd_problem> probs;
     rla_range_params params{};
     rla::BProb *d_probs = nullptr;
     std::vector<rla::BProb> h_probs;
     void *work = nullptr;
-    int *flags = nullptr;
+    int *flagbuf = nullptr;
     // per rank class: instance list (device) and host copy
     std::vector<int> cls_h[rla::B_NCLASS];
     int *cls_d[rla::B_NCLASS] = {nullptr, nullptr, nullptr, nullptr};
@@ -581,8 +583,9 @@ static int get_map(rla_ctx *ctx, rla_batch *b, int cls, int kind, int64_t sz, in
     ts[ids.size()] = (int)acc;
     if (acc >= (1ll << 31)) return set_error(ctx, RLA_E_UNSUPPORTED, "batch too large for one grouped launch");
     int *d = nullptr;
-    RLA_CUDA_TRY(ctx, cudaMalloc(&d, sizeof(int) * ts.size()));
-    RLA_CUDA_TRY(ctx, cudaMemcpy(d, ts.data(), sizeof(int) * ts.size(), cudaMemcpyHostToDevice));
+    RLA_CUDA_TRY(ctx, pool_malloc_s(b->ctx, &d, sizeof(int) * ts.size(), b->ctx->stream));
+    RLA_CUDA_TRY(ctx, cudaMemcpyAsync(d, ts.data(), sizeof(int) * ts.size(), cudaMemcpyHostToDevice, b->ctx->stream));
+    RLA_CUDA_TRY(ctx, cudaStreamSynchronize(b->ctx->stream));
     b->owned.push_back(d);
     b->maps[key] = d;
     b->map_total[key] = (int)acc;
@@ -782,6 +785,8 @@ int rla_randsvd_batch_create(rla_ctx *ctx, int count, const rla_svd_problem *pro
     }
     RLA_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
     rla_batch *b = new rla_batch();
+    b->ctx = ctx;
+    b->flags = flags;
     b->device = ctx->device;
     b->count = count;
     b->probs.assign(probs, probs + count);
@@ -817,9 +822,9 @@ int rla_randsvd_batch_create(rla_ctx *ctx, int count, const rla_svd_problem *pro
         rla_randsvd_batch_destroy(b);
         return r;
     };
-    if (cudaMalloc(&b->work, std::max<size_t>(total, 256)) != cudaSuccess)
+    if (pool_malloc_s(ctx, &b->work, std::max<size_t>(total, 256), ctx->stream) != cudaSuccess)
         return fail(set_error(ctx, RLA_E_OOM, "batch workspace of %zu bytes", total));
-    if (cudaMalloc((void **)&b->flags, sizeof(int) * std::max(count, 1)) != cudaSuccess)
+    if (pool_malloc_s(ctx, &b->flagbuf, sizeof(int) * std::max(count, 1), ctx->stream) != cudaSuccess)
         return fail(set_error(ctx, RLA_E_OOM, "batch flags"));
     char *w = (char *)b->work;
     for (int i = 0; i < count; ++i) {
@@ -829,26 +834,31 @@ int rla_randsvd_batch_create(rla_ctx *ctx, int count, const rla_svd_problem *pro
         p.G = (double *)(w + o[3]); p.Rinv = (double *)(w + o[4]); p.Bt = (double *)(w + o[5]);
         p.Bt0 = (double *)(w + o[6]); p.X = (double *)(w + o[7]); p.J = (double *)(w + o[8]);
         p.part = w + o[9];
-        p.flag = b->flags + i;
+        p.flag = b->flagbuf + i;
     }
-    if (cudaMalloc((void **)&b->d_probs, sizeof(BProb) * std::max(count, 1)) != cudaSuccess)
+    if (pool_malloc_s(ctx, &b->d_probs, sizeof(BProb) * std::max(count, 1), ctx->stream) != cudaSuccess)
         return fail(set_error(ctx, RLA_E_OOM, "batch table"));
-    if (count) cudaMemcpy(b->d_probs, b->h_probs.data(), sizeof(BProb) * count, cudaMemcpyHostToDevice);
+    if (count)
+        cudaMemcpyAsync(b->d_probs, b->h_probs.data(), sizeof(BProb) * count, cudaMemcpyHostToDevice, ctx->stream);
     for (int c = 0; c < B_NCLASS; ++c) {
         if (b->cls_h[c].empty()) continue;
-        if (cudaMalloc((void **)&b->cls_d[c], sizeof(int) * b->cls_h[c].size()) != cudaSuccess)
+        if (pool_malloc_s(ctx, &b->cls_d[c], sizeof(int) * b->cls_h[c].size(), ctx->stream) != cudaSuccess)
             return fail(set_error(ctx, RLA_E_OOM, "batch class table"));
-        cudaMemcpy(b->cls_d[c], b->cls_h[c].data(), sizeof(int) * b->cls_h[c].size(), cudaMemcpyHostToDevice);
+        cudaMemcpyAsync(b->cls_d[c], b->cls_h[c].data(), sizeof(int) * b->cls_h[c].size(), cudaMemcpyHostToDevice,
+                        ctx->stream);
     }
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return fail(set_error(ctx, RLA_E_CUDA, "batch tables"));
     {
         const int lim = ctx->smem_optin - 1024;
         if (cudaFuncSetAttribute(b_chol_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, lim) != cudaSuccess ||
             cudaFuncSetAttribute(b_jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, lim) != cudaSuccess)
             return fail(set_error(ctx, RLA_E_CUDA, "batch kernel attributes"));
     }
-    if (cudaStreamCreateWithFlags(&b->cs, cudaStreamNonBlocking) != cudaSuccess || cudaEventCreate(&b->ev0) != cudaSuccess ||
-        cudaEventCreate(&b->ev1) != cudaSuccess)
-        return fail(set_error(ctx, RLA_E_CUDA, "batch stream/events"));
+    if (!(flags & RLA_BATCH_EAGER) || (flags & RLA_BATCH_AUTOTUNE)) {
+        if (cudaStreamCreateWithFlags(&b->cs, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess)
+            return fail(set_error(ctx, RLA_E_CUDA, "batch stream/events"));
+    }
     if (flags & RLA_BATCH_AUTOTUNE) {
         rc = autotune(ctx, b);
         if (rc != RLA_OK) return fail(rc);
@@ -870,6 +880,10 @@ int rla_randsvd_batch_run(rla_ctx *ctx, rla_batch *b) {
     if (b->device != ctx->device) return set_error(ctx, RLA_E_ARG, "Batch lives on device %d, context on %d.", b->device, ctx->device);
     RLA_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
     if (b->count == 0) return RLA_OK;
+    if (b->flags & RLA_BATCH_EAGER) {
+        RLA_CUDA_TRY(ctx, cudaMemsetAsync(b->flagbuf, 0, sizeof(int) * b->count, ctx->stream));
+        RLA_TRY(enqueue_all(ctx, b, ctx->stream));
+    } else {
     if (!b->exec) {
         // first run: capture the grouped launch sequence (prefix tables and attributes are
         // created outside the capture by a dry enqueue)
@@ -884,16 +898,17 @@ int rla_randsvd_batch_run(rla_ctx *ctx, rla_batch *b) {
         b->graph = g;
         RLA_CUDA_TRY(ctx, cudaGraphInstantiate(&b->exec, g, 0));
     }
-    RLA_CUDA_TRY(ctx, cudaMemsetAsync(b->flags, 0, sizeof(int) * b->count, ctx->stream));
+    RLA_CUDA_TRY(ctx, cudaMemsetAsync(b->flagbuf, 0, sizeof(int) * b->count, ctx->stream));
     RLA_CUDA_TRY(ctx, cudaEventRecord(b->ev0, ctx->stream));
     RLA_CUDA_TRY(ctx, cudaStreamWaitEvent(b->cs, b->ev0, 0));
     RLA_CUDA_TRY(ctx, cudaGraphLaunch(b->exec, b->cs));
     RLA_CUDA_TRY(ctx, cudaEventRecord(b->ev1, b->cs));
     RLA_CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, b->ev1, 0));
+    }
     // instances whose Cholesky broke down: the single-instance path (shifted CholeskyQR /
     // Householder fallback) recomputes them with the same draws
     std::vector<int> fl(b->count);
-    RLA_CUDA_TRY(ctx, cudaMemcpyAsync(fl.data(), b->flags, sizeof(int) * b->count, cudaMemcpyDeviceToHost, ctx->stream));
+    RLA_CUDA_TRY(ctx, cudaMemcpyAsync(fl.data(), b->flagbuf, sizeof(int) * b->count, cudaMemcpyDeviceToHost, ctx->stream));
     RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     for (int i = 0; i < b->count; ++i) {
         if (!fl[i]) continue;
@@ -919,12 +934,13 @@ int rla_randsvd_batch_destroy(rla_batch *b) {
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
     if (b->cs) cudaStreamDestroy(b->cs);
-    for (void *p : b->owned) cudaFree(p);
+    cudaStream_t st = b->ctx->stream;
+    for (void *p : b->owned) cudaFreeAsync(p, st);
     for (int c = 0; c < B_NCLASS; ++c)
-        if (b->cls_d[c]) cudaFree(b->cls_d[c]);
-    if (b->d_probs) cudaFree(b->d_probs);
-    if (b->flags) cudaFree(b->flags);
-    if (b->work) cudaFree(b->work);
+        if (b->cls_d[c]) cudaFreeAsync(b->cls_d[c], st);
+    if (b->d_probs) cudaFreeAsync(b->d_probs, st);
+    if (b->flagbuf) cudaFreeAsync(b->flagbuf, st);
+    if (b->work) cudaFreeAsync(b->work, st);
     delete b;
     return RLA_OK;
 }

@@ -42,6 +42,10 @@ template <class TA, class TB, class TC, class TAcc>
 int gemm(rla_ctx *ctx, int64_t M, int64_t N, int64_t K, const TA *A, int64_t lda, int ta, const TB *B, int64_t ldb,
          int tb, TC *C, int64_t ldc, double alpha, double beta, int b_upper = 0);
 
+// G (l x l, ld l, FP64) = Y'Y for Y (rows x l, ld ldy), split over row chunks (rla_range.cu).
+template <class T>
+int gram_fp64(rla_ctx *ctx, const T *Y, int64_t rows, int64_t l, int64_t ldy, double *G);
+
 // Small dense FP64 kernels (rla_linalg.cu)
 // In place: G (l x l, ld l) -> upper Cholesky factor R (lower part zeroed).  `shift` is
 // added to the diagonal first.  *breakdown (device int) is set to 1 when a pivot is not

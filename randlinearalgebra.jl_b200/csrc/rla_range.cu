@@ -178,7 +178,7 @@ __global__ void gram_reduce_kernel(const double *__restrict__ part, int64_t nchu
 }
 
 template <class T>
-static int gram_fp64(rla_ctx *ctx, const T *Y, int64_t rows, int64_t l, int64_t ldy, double *G) {
+int gram_fp64(rla_ctx *ctx, const T *Y, int64_t rows, int64_t l, int64_t ldy, double *G) {
     const int nt = (int)ceil_div(l, GRAM_T);
     const int ntiles = nt * (nt + 1) / 2;
     int64_t nchunks = std::max<int64_t>(1, ceil_div(2 * (int64_t)ctx->sm_count * 2, ntiles));
@@ -197,6 +197,9 @@ static int gram_fp64(rla_ctx *ctx, const T *Y, int64_t rows, int64_t l, int64_t 
     gram_reduce_kernel<<<ceil_div_i(l * l, 256), 256, 0, ctx->stream>>>((const double *)ws, nchunks, ntiles, l, G);
     return check_launch(ctx, "gram_reduce");
 }
+
+template int gram_fp64<float>(rla_ctx *, const float *, int64_t, int64_t, int64_t, double *);
+template int gram_fp64<double>(rla_ctx *, const double *, int64_t, int64_t, int64_t, double *);
 
 struct OrthWork {
     double *G, *Rinv, *dscale, *diag, *hw;

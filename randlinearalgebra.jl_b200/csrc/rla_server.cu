@@ -1,0 +1,288 @@
+// rla_server.cu -- serving loop for mixed sketch-and-solve and RandSVD requests.
+//
+// `slots` worker threads, each with its own context (stream, memory pool, scratch), pull
+// requests from one FIFO queue.  A request is admitted when its estimated device workspace
+// fits the memory budget next to the work already running (a request is always admitted
+// when nothing runs, so none starves).  In RLA_SERVE_BATCHED mode a worker that takes a
+// RandSVD request with k <= 128 also takes the other pending ones that fit (up to
+// max_group) and runs them as one grouped batch (rla_batch.cu, eager launches); the other
+// workers keep taking requests meanwhile, so work that arrives while the GPU is busy
+// overlaps on the device.  Least-squares requests (sketch-and-solve, rla_ls.cu) and
+// RandSVD requests with k > 128 run one per worker; sketches stay resident per worker,
+// keyed by shape and seed.  RLA_SERVE_PLAIN is the baseline: one worker, one request at a
+// time, the single-instance RandSVD path.  Latency is submit-to-completion on the host
+// clock.  A request's result does not depend on what else runs: grouped kernels map every
+// tile to one instance and add partial sums in a fixed order.
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
+#include <tuple>
+
+#include "rla_internal.cuh"
+#include "rla_kernels.cuh"
+
+namespace rla {
+size_t ls_work_bytes(int64_t s, int64_t n);
+int ls_sketch_solve(rla_ctx *ctx, const rla_sketch *S, int64_t m, int64_t n, const float *A, int64_t lda,
+                    const float *b, float *x, void *work, int **bad_out);
+}  // namespace rla
+
+using namespace rla;
+
+namespace {
+
+struct Pending {
+    rla_request req;
+    double t_submit;
+    size_t bytes;
+};
+
+struct DoneRec {
+    uint64_t tag;
+    double latency;
+    int status;
+};
+
+size_t req_bytes(const rla_request &r) {
+    if (r.kind == RLA_REQ_LS) {
+        const int64_t s = std::min<int64_t>(4 * r.n, r.m);
+        return ls_work_bytes(s, r.n) + (size_t)r.m * 8 * 5 + (size_t)r.m * 8 * 4;
+    }
+    const int64_t m = r.m, n = r.n, k = r.k;
+    if (k <= 128)
+        return (size_t)(4 * m * k + 4 * n * k + 16 * n * k + 32 * k * k + 4 * ((m + 2047) / 2048) * n * k) + 4096;
+    return (size_t)(12 * m * k + 40 * n * k + 64 * k * k) + 4096;
+}
+
+}  // namespace
+
+struct rla_server {
+    rla_server_config cfg{};
+    std::vector<std::thread> workers;
+    std::vector<rla_ctx *> ctxs;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_idle;
+    std::deque<Pending> queue;
+    std::vector<DoneRec> done;
+    size_t in_use = 0;
+    int running = 0;
+    bool stopping = false;
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+    double now() const {
+        return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+};
+
+namespace {
+
+bool admissible(const rla_server *S) {
+    if (S->queue.empty()) return false;
+    return S->in_use == 0 || S->in_use + S->queue.front().bytes <= S->cfg.memory_budget;
+}
+
+using SketchKey = std::tuple<int, int64_t, int64_t, uint64_t>;
+
+int get_sketch(rla_ctx *ctx, std::map<SketchKey, rla_sketch *> &cache, int kind, int64_t s, int64_t L, uint64_t seed,
+               rla_sketch **out) {
+    const SketchKey key{kind, s, L, seed};
+    auto it = cache.find(key);
+    if (it != cache.end()) {
+        *out = it->second;
+        return RLA_OK;
+    }
+    rla_sketch_params p{};
+    p.kind = kind;
+    p.card = kind == RLA_GAUSSIAN ? RLA_RIGHT : RLA_LEFT;
+    p.dtype = RLA_F32;
+    p.compression_dim = s;
+    p.long_dim = L;
+    p.nnz = std::min<int64_t>(8, s);
+    p.seed = seed;
+    rla_sketch *sk = nullptr;
+    RLA_TRY(rla_sketch_create(ctx, &p, &sk));
+    cache[key] = sk;
+    *out = sk;
+    return RLA_OK;
+}
+
+int run_ls(rla_ctx *ctx, std::map<SketchKey, rla_sketch *> &cache, const rla_request &r) {
+    const int64_t s = std::min<int64_t>(4 * r.n, r.m);
+    rla_sketch *S = nullptr;
+    RLA_TRY(get_sketch(ctx, cache, RLA_SPARSE_SIGN, s, r.m, r.seed, &S));
+    void *work = nullptr;
+    RLA_CUDA_TRY(ctx, pool_malloc_s(ctx, &work, ls_work_bytes(s, r.n), ctx->stream));
+    int *bad = nullptr;
+    int rc = ls_sketch_solve(ctx, S, r.m, r.n, r.A, r.lda, r.b, r.x, work, &bad);
+    int hbad = 0;
+    if (rc == RLA_OK) {
+        cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+        if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) rc = RLA_E_CUDA;
+    }
+    cudaFreeAsync(work, ctx->stream);
+    RLA_TRY(rc);
+    return hbad ? RLA_E_NUMERIC : RLA_OK;
+}
+
+int run_svd_single(rla_ctx *ctx, std::map<SketchKey, rla_sketch *> &cache, const rla_request &r) {
+    rla_sketch *om = nullptr;
+    RLA_TRY(get_sketch(ctx, cache, RLA_GAUSSIAN, r.k, r.n, r.seed, &om));
+    rla_range_params pr{0, 0, RLA_PREC_NATIVE};
+    return rla_randsvd(ctx, om, RLA_F32, r.m, r.n, r.A, r.lda, &pr, RLA_F32, r.U, r.ldu, r.S, r.V, r.ldv);
+}
+
+int run_svd_group(rla_ctx *ctx, const std::vector<Pending> &job) {
+    std::vector<rla_svd_problem> probs;
+    for (const Pending &p : job) {
+        const rla_request &r = p.req;
+        probs.push_back(rla_svd_problem{r.m, r.n, r.k, r.A, r.lda, r.U, r.ldu, r.S, r.V, r.ldv, r.seed});
+    }
+    rla_range_params pr{0, 0, RLA_PREC_NATIVE};
+    rla_batch *b = nullptr;
+    RLA_TRY(rla_randsvd_batch_create(ctx, (int)probs.size(), probs.data(), &pr, RLA_BATCH_EAGER, &b));
+    const int rc = rla_randsvd_batch_run(ctx, b);
+    rla_randsvd_batch_destroy(b);
+    RLA_TRY(rc);
+    RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return RLA_OK;
+}
+
+void worker_main(rla_server *S, int w) {
+    cudaSetDevice(S->cfg.device);
+    rla_ctx *ctx = S->ctxs[w];
+    std::map<SketchKey, rla_sketch *> cache;
+    const bool batched = S->cfg.mode == RLA_SERVE_BATCHED;
+    for (;;) {
+        std::vector<Pending> job;
+        size_t bytes = 0;
+        {
+            std::unique_lock<std::mutex> lk(S->mu);
+            S->cv_work.wait(lk, [&] { return admissible(S) || (S->stopping && S->queue.empty()); });
+            if (S->queue.empty()) break;  // stopping
+            Pending f = S->queue.front();
+            S->queue.pop_front();
+            job.push_back(f);
+            bytes += f.bytes;
+            S->in_use += f.bytes;
+            const bool group = batched && f.req.kind == RLA_REQ_SVD && f.req.k <= 128;
+            if (group) {
+                for (auto it = S->queue.begin(); it != S->queue.end() && (int)job.size() < S->cfg.max_group;) {
+                    if (it->req.kind == RLA_REQ_SVD && it->req.k <= 128 &&
+                        S->in_use + it->bytes <= S->cfg.memory_budget) {
+                        job.push_back(*it);
+                        bytes += it->bytes;
+                        S->in_use += it->bytes;
+                        it = S->queue.erase(it);
+                    } else {
+                        ++it;
+                    }
+                }
+            }
+            ++S->running;
+        }
+        int rc = RLA_OK;
+        const rla_request &r0 = job.front().req;
+        if (r0.kind == RLA_REQ_LS) rc = run_ls(ctx, cache, r0);
+        else if (job.size() > 1 || (batched && r0.k <= 128)) rc = run_svd_group(ctx, job);
+        else rc = run_svd_single(ctx, cache, r0);
+        if (rc == RLA_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess) rc = RLA_E_CUDA;
+        {
+            std::lock_guard<std::mutex> lk(S->mu);
+            const double t = S->now();
+            for (const Pending &p : job) S->done.push_back(DoneRec{p.req.tag, t - p.t_submit, rc});
+            S->in_use -= bytes;
+            --S->running;
+        }
+        S->cv_work.notify_all();
+        S->cv_idle.notify_all();
+    }
+    for (auto &kv : cache) rla_sketch_destroy(kv.second);
+}
+
+}  // namespace
+
+extern "C" {
+
+int rla_server_start(const rla_server_config *cfg, rla_server **out) {
+    if (!cfg || !out) return RLA_E_ARG;
+    *out = nullptr;
+    if (cfg->slots <= 0 || cfg->max_group <= 0 || (cfg->mode != RLA_SERVE_BATCHED && cfg->mode != RLA_SERVE_PLAIN))
+        return RLA_E_ARG;
+    rla_server *S = new rla_server();
+    S->cfg = *cfg;
+    if (S->cfg.mode == RLA_SERVE_PLAIN) {
+        S->cfg.slots = 1;
+        S->cfg.max_group = 1;
+    }
+    if (S->cfg.memory_budget == 0) S->cfg.memory_budget = (uint64_t)150 << 30;
+    for (int w = 0; w < S->cfg.slots; ++w) {
+        rla_ctx *c = nullptr;
+        const int rc = rla_ctx_create(cfg->device, nullptr, &c);
+        if (rc != RLA_OK) {
+            for (rla_ctx *x : S->ctxs) rla_ctx_destroy(x);
+            delete S;
+            return rc;
+        }
+        S->ctxs.push_back(c);
+    }
+    for (int w = 0; w < S->cfg.slots; ++w) S->workers.emplace_back(worker_main, S, w);
+    *out = S;
+    return RLA_OK;
+}
+
+int rla_server_submit(rla_server *S, const rla_request *req) {
+    if (!S || !req) return RLA_E_ARG;
+    const rla_request &r = *req;
+    if (r.kind != RLA_REQ_LS && r.kind != RLA_REQ_SVD) return RLA_E_ARG;
+    if (r.m <= 0 || r.n <= 0 || !r.A || r.lda < r.m) return RLA_E_ARG;
+    if (r.kind == RLA_REQ_LS && (!r.b || !r.x || r.n > r.m || r.n > 4096)) return RLA_E_ARG;
+    if (r.kind == RLA_REQ_SVD && (r.k <= 0 || r.k > std::min(r.m, r.n) || !r.U || !r.S || !r.V || r.ldu < r.m ||
+                                  r.ldv < r.n))
+        return RLA_E_ARG;
+    Pending p{r, S->now(), req_bytes(r)};
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        if (S->stopping) return RLA_E_ARG;
+        S->queue.push_back(p);
+    }
+    S->cv_work.notify_one();
+    return RLA_OK;
+}
+
+int rla_server_poll(rla_server *S, uint64_t *tags, double *latency_s, int *status, int max, int *count) {
+    if (!S || !count || max < 0) return RLA_E_ARG;
+    std::lock_guard<std::mutex> lk(S->mu);
+    const int n = (int)std::min<size_t>((size_t)max, S->done.size());
+    for (int i = 0; i < n; ++i) {
+        if (tags) tags[i] = S->done[i].tag;
+        if (latency_s) latency_s[i] = S->done[i].latency;
+        if (status) status[i] = S->done[i].status;
+    }
+    S->done.erase(S->done.begin(), S->done.begin() + n);
+    *count = n;
+    return RLA_OK;
+}
+
+int rla_server_wait_idle(rla_server *S) {
+    if (!S) return RLA_E_ARG;
+    std::unique_lock<std::mutex> lk(S->mu);
+    S->cv_idle.wait(lk, [&] { return S->queue.empty() && S->running == 0; });
+    return RLA_OK;
+}
+
+int rla_server_stop(rla_server *S) {
+    if (!S) return RLA_OK;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->stopping = true;
+    }
+    S->cv_work.notify_all();
+    for (auto &t : S->workers) t.join();
+    for (rla_ctx *c : S->ctxs) rla_ctx_destroy(c);
+    delete S;
+    return RLA_OK;
+}
+
+}  // extern "C"
