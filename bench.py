@@ -705,6 +705,137 @@ def batched_arm(args):
         dist.destroy_process_group()
 
 
+# --------------------------------------------------------------------------------------
+# Serving workload
+# --------------------------------------------------------------------------------------
+SV_METRIC = "served requests/s (60% sketch-and-solve LS, 40% RandSVD; continuous batching)"
+SV_WORKLOAD = ("serving: Poisson arrivals, 60% LS m~U[2^14,2^18] n~U[32,512] s=4n SparseSign nnz=8, "
+               "40% RandSVD m<=32768 n<=4096 k in {32,64,128}; device-resident inputs (H2D excluded)")
+
+
+def sv_pool(torch, dev, n_ls, n_svd, seed=5):
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    ls, svd = [], []
+    for i in range(n_ls):
+        m, n = int(rng.integers(2**14, 2**18 + 1)), int(rng.integers(32, 513))
+        A = torch.randn(n, m, device=dev, generator=g).t()
+        x0 = torch.randn(n, device=dev, generator=g)
+        b = A @ x0 + 1e-3 * torch.randn(m, device=dev, generator=g)
+        ls.append((A, b, 50000 + i))
+    for i in range(n_svd):
+        m, n = int(rng.integers(4096, 32769)), int(rng.integers(256, 4097))
+        k = int(rng.choice([32, 64, 128]))
+        svd.append((bt_matrix(torch, dev, m, n, g), min(k, n), 60000 + i))
+    return ls, svd
+
+
+def sv_run(rla, torch, dev, ls, svd, lam, nreq, plain, slots, seed):
+    """Submit nreq requests with Poisson(lam) arrivals; returns (throughput, p50, p99, lat list)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    kinds = rng.random(nreq) < 0.6
+    picks = [int(rng.integers(0, len(ls) if k else len(svd))) for k in kinds]
+    arrivals = np.cumsum(rng.exponential(1.0 / lam, size=nreq))
+    srv = rla.Server(slots=slots, max_group=32, plain=plain)
+    outs, sched, lat = {}, {}, {}
+    t0 = time.perf_counter()
+    i = 0
+    while len(lat) < nreq:
+        now = time.perf_counter() - t0
+        while i < nreq and arrivals[i] <= now:
+            if kinds[i]:
+                A, b, sd = ls[picks[i]]
+                x = torch.empty(A.shape[1], dtype=torch.float32, device=dev)
+                outs[i] = (x,)
+                srv.submit_ls(A, b, x, sd, i)
+            else:
+                A, k, sd = svd[picks[i]]
+                m, n = A.shape
+                U = torch.empty(k, m, dtype=torch.float32, device=dev).t()
+                S = torch.empty(k, dtype=torch.float64, device=dev)
+                V = torch.empty(k, n, dtype=torch.float32, device=dev).t()
+                outs[i] = (U, S, V)
+                srv.submit_svd(A, k, U, S, V, sd, i)
+            sched[i] = now - arrivals[i]  # submission lag behind the scheduled arrival
+            i += 1
+        for tag, l, st in srv.poll():
+            if st != 0:
+                raise RuntimeError(f"request {tag} failed with status {st}: {srv.last_error()}")
+            lat[tag] = l + sched[tag]
+            outs.pop(tag, None)
+        if i < nreq:
+            time.sleep(min(2e-4, max(0.0, arrivals[i] - (time.perf_counter() - t0))))
+        else:
+            time.sleep(2e-4)
+    t_end = time.perf_counter() - t0
+    srv.stop()
+    ls_lat = sorted(lat.values())
+    thr = nreq / (t_end - arrivals[0])
+    return thr, float(np.percentile(ls_lat, 50)), float(np.percentile(ls_lat, 99))
+
+
+def serve_arm(args):
+    import numpy as np
+    import torch
+
+    world, rank, local = dist_setup(args.gpus)
+    from __graft_entry__ import load_package
+    rla = load_package()
+    dev = torch.device("cuda", local if world > 1 else 0)
+    ls, svd = sv_pool(torch, dev, 24, 16, seed=5 + rank)
+    torch.cuda.synchronize()
+    lams = [2000, 5000, 10000, 20000]
+    # warm both modes (sketches, pools, module loading)
+    sv_run(rla, torch, dev, ls, svd, 5000, 60, False, args.slots, 1)
+    sv_run(rla, torch, dev, ls, svd, 5000, 30, True, 1, 2)
+    res = {"batched": {}, "plain": {}}
+    props = torch.cuda.get_device_properties(dev)
+    clocks = ClockSampler(f"GPU-{props.uuid}" if getattr(props, "uuid", None) else dev.index)
+    clocks.start()
+    for lam in lams:
+        thr, p50, p99 = sv_run(rla, torch, dev, ls, svd, lam, args.serve_requests, False, args.slots, 10 + lam)
+        res["batched"][lam] = {"req_per_s": round(thr, 1), "p50_ms": round(1e3 * p50, 3), "p99_ms": round(1e3 * p99, 3)}
+        thr, p50, p99 = sv_run(rla, torch, dev, ls, svd, lam, args.serve_requests, True, 1, 10 + lam)
+        res["plain"][lam] = {"req_per_s": round(thr, 1), "p50_ms": round(1e3 * p50, 3), "p99_ms": round(1e3 * p99, 3)}
+    clk = clocks.stop()
+    barrier(world)
+    if rank != 0:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    top = max(lams)
+    value = world * res["batched"][top]["req_per_s"]
+    # throughput at equal p99: the plain path's best rate against the batched rate whose p99
+    # is not above the plain path's p99 at that rate
+    pl_best = max(lams, key=lambda L: res["plain"][L]["req_per_s"])
+    p99_budget = res["plain"][pl_best]["p99_ms"]
+    ok = [L for L in lams if res["batched"][L]["p99_ms"] <= p99_budget]
+    b_at = max((res["batched"][L]["req_per_s"] for L in ok), default=None)
+    line = {"metric": SV_METRIC, "value": round(value, 1), "unit": "req/s", "n_gpus": world,
+            "steps": args.serve_requests, "warmup": 2, "ms_per_step": round(1e3 / max(value, 1e-9), 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 data, f32/f64 as in the request kernels",
+            "data": "synthetic device-resident pool (24 LS, 16 RandSVD problems, seed 5+rank)",
+            "config": {"workload": SV_WORKLOAD, "arrival_rates": lams, "requests_per_rate": args.serve_requests,
+                       "slots": args.slots, "max_group": 32, "memory_budget_gb": 150,
+                       "parallelism": f"replicas x{world}"},
+            "serving": res,
+            "equal_p99": {"plain_req_per_s": res["plain"][pl_best]["req_per_s"], "p99_budget_ms": p99_budget,
+                          "batched_req_per_s": b_at,
+                          "ratio": None if b_at is None else round(b_at / res["plain"][pl_best]["req_per_s"], 2)},
+            "e2e": {"value": round(value, 1), "unit": "req/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                    "note": "inputs come from a device-resident pool by the workload's definition"},
+            "clocks": clk}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -715,17 +846,25 @@ def main():
     ap.add_argument("--cols", type=int, default=NCOL,
                     help="columns of A (default 512, the benchmark workload; smaller values make small "
                          "cases of the same kernels for profiler captures)")
-    ap.add_argument("--workload", choices=["sketch", "randsvd", "batched"], default="sketch",
+    ap.add_argument("--workload", choices=["sketch", "randsvd", "batched", "serve"], default="sketch",
                     help="sketch: SRHT + CountSketch apply (default); randsvd: mixed-precision RandSVD; "
                          "batched: 512 uneven RandSVD instances")
     ap.add_argument("--batch-count", type=int, default=BT_COUNT, help="instances of the batched workload")
     ap.add_argument("--no-autotune", action="store_true", help="batched workload: default tile shapes")
+    ap.add_argument("--serve-requests", type=int, default=600, help="serving workload: requests per arrival rate")
+    ap.add_argument("--slots", type=int, default=4, help="serving workload: concurrent workers")
     ap.add_argument("--rs-m", type=int, default=RS_M, help="RandSVD rows (default 65536; smaller for profiler cases)")
     ap.add_argument("--rs-n", type=int, default=RS_N, help="RandSVD columns (default 8192)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.workload == "batched":
+    if args.workload == "serve":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "serving workload: the reference arm is timed "
+                              "for the sketch and randsvd workloads only"}), flush=True)
+        else:
+            serve_arm(args)
+    elif args.workload == "batched":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "batched workload: the reference arm is timed "
                               "for the sketch and randsvd workloads only"}), flush=True)

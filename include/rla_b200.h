@@ -286,6 +286,8 @@ int rla_server_start(const rla_server_config *cfg, rla_server **out);
 int rla_server_submit(rla_server *srv, const rla_request *req);
 /* Up to `max` completed requests: tags, submit-to-done latency (s) and status. */
 int rla_server_poll(rla_server *srv, uint64_t *tags, double *latency_s, int *status, int max, int *count);
+/* Message of the first failed request ("" when none failed); valid until the next call. */
+const char *rla_server_last_error(rla_server *srv);
 /* Block until the queue is empty and nothing runs. */
 int rla_server_wait_idle(rla_server *srv);
 /* Finish queued work and shut the workers down. */

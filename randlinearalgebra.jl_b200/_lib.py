@@ -104,6 +104,7 @@ SIGNATURES = {
     "rla_server_submit": (ctypes.c_int, [vp, ctypes.POINTER(Request)]),
     "rla_server_poll": (ctypes.c_int, [vp, vp, vp, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     "rla_server_wait_idle": (ctypes.c_int, [vp]),
+    "rla_server_last_error": (ctypes.c_char_p, [vp]),
     "rla_server_stop": (ctypes.c_int, [vp]),
     "rla_ctx_set_timing": (ctypes.c_int, [vp, ctypes.c_int]),
     "rla_ctx_kernel_time": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(i64)]),

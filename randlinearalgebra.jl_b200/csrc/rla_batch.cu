@@ -850,8 +850,8 @@ int rla_randsvd_batch_create(rla_ctx *ctx, int count, const rla_svd_problem *pro
     if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return fail(set_error(ctx, RLA_E_CUDA, "batch tables"));
     {
         const int lim = ctx->smem_optin - 1024;
-        if (cudaFuncSetAttribute(b_chol_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, lim) != cudaSuccess ||
-            cudaFuncSetAttribute(b_jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, lim) != cudaSuccess)
+        if (set_smem_max(b_chol_inv_kernel) != cudaSuccess ||
+            set_smem_max(b_jacobi_kernel) != cudaSuccess)
             return fail(set_error(ctx, RLA_E_CUDA, "batch kernel attributes"));
     }
     if (!(flags & RLA_BATCH_EAGER) || (flags & RLA_BATCH_AUTOTUNE)) {

@@ -17,6 +17,8 @@ int set_error(rla_ctx *ctx, int code, const char *fmt, ...) {
     return code;
 }
 
+int g_smem_optin = 227 * 1024;
+
 int check_launch(rla_ctx *ctx, const char *what) {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess)
@@ -116,6 +118,7 @@ int rla_ctx_create(int device, void *stream, rla_ctx **out) {
     }
     ctx->sm_count = prop.multiProcessorCount;
     ctx->smem_optin = (int)prop.sharedMemPerBlockOptin;
+    g_smem_optin = ctx->smem_optin;
     if (stream) {
         ctx->stream = (cudaStream_t)stream;
         ctx->owns_stream = false;

@@ -74,6 +74,18 @@ int scratch_get(rla_ctx *ctx, size_t bytes, void **out);
 // Zero-initialised int32 counters (at least n); kernels leave them at zero on exit.
 int counters_get(rla_ctx *ctx, size_t n, int **out);
 int check_launch(rla_ctx *ctx, const char *what);
+// Largest dynamic shared memory a block may use on this device (set by rla_ctx_create).
+// Kernels' MaxDynamicSharedMemorySize attribute is process-wide and shared by every host
+// thread, so set_smem_max always raises it to the most the kernel can take (never to a
+// per-call size another thread could lower before its own launch).
+extern int g_smem_optin;
+template <class K>
+inline cudaError_t set_smem_max(K kern) {
+    cudaFuncAttributes a;
+    cudaError_t e = cudaFuncGetAttributes(&a, reinterpret_cast<const void *>(kern));
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, g_smem_optin - (int)a.sharedSizeBytes);
+}
 // Stream-ordered allocation from the context's pool (memory stays mapped between calls, so
 // repeated calls of the same size do not remap device memory).
 template <class P>

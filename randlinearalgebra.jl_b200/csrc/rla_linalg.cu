@@ -410,7 +410,7 @@ int cholesky_upper(rla_ctx *ctx, double *G, int64_t l, double shift, int *breakd
     const size_t smem = sizeof(double) * (size_t)std::max<int64_t>(l, 1);
     if (smem > (size_t)ctx->smem_optin - 1024)
         return set_error(ctx, RLA_E_UNSUPPORTED, "Cholesky of order %lld exceeds shared memory", (long long)l);
-    RLA_CUDA_TRY(ctx, cudaFuncSetAttribute(chol_upper_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    RLA_CUDA_TRY(ctx, set_smem_max(chol_upper_kernel));
     chol_upper_kernel<<<1, 1024, smem, ctx->stream>>>(G, l, shift, breakdown);
     return check_launch(ctx, "chol_upper");
 }
@@ -421,7 +421,7 @@ int tri_inv_upper(rla_ctx *ctx, const double *R, int64_t l, double *Rinv) {
     if (per > ctx->smem_optin - 1024)
         return set_error(ctx, RLA_E_UNSUPPORTED, "triangular inverse of order %lld exceeds shared memory", (long long)l);
     const size_t smem = (size_t)per * wpc;
-    RLA_CUDA_TRY(ctx, cudaFuncSetAttribute(tri_inv_upper_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    RLA_CUDA_TRY(ctx, set_smem_max(tri_inv_upper_kernel));
     tri_inv_upper_kernel<<<ceil_div_i(l, wpc), 32 * wpc, smem, ctx->stream>>>(R, l, Rinv, wpc);
     return check_launch(ctx, "tri_inv_upper");
 }
@@ -436,8 +436,7 @@ int jacobi_svd(rla_ctx *ctx, double *X, double *J, double *sigma, int64_t l, dou
         const int nb = (int)ceil_div(l, BJ_B), nbp = nb + (nb & 1);
         jacobi_identity_kernel<<<ceil_div_i(l * l, 256), 256, 0, ctx->stream>>>(J, l);
         RLA_TRY(check_launch(ctx, "jacobi_identity"));
-        RLA_CUDA_TRY(ctx, cudaFuncSetAttribute(block_jacobi_round_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)smem));
+        RLA_CUDA_TRY(ctx, set_smem_max(block_jacobi_round_kernel));
         unsigned long long *off = reinterpret_cast<unsigned long long *>(work + 2 * l * l);
         for (int sweep = 0; sweep < 40; ++sweep) {
             RLA_CUDA_TRY(ctx, cudaMemsetAsync(off, 0, sizeof(unsigned long long), ctx->stream));

@@ -87,7 +87,7 @@ int ls_sketch_solve(rla_ctx *ctx, const rla_sketch *S, int64_t m, int64_t n, con
     RLA_TRY(cholesky_upper(ctx, G, n, 0.0, bad));
     const size_t smem = sizeof(double) * (size_t)n;
     if (smem > 48 * 1024)
-        RLA_CUDA_TRY(ctx, cudaFuncSetAttribute(ls_trisolve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        RLA_CUDA_TRY(ctx, set_smem_max(ls_trisolve_kernel));
     ls_trisolve_kernel<<<1, 1024, smem, ctx->stream>>>(G, n, tmp, c, x);
     RLA_TRY(check_launch(ctx, "ls_trisolve"));
     *bad_out = bad;

@@ -70,6 +70,7 @@ struct rla_server {
     size_t in_use = 0;
     int running = 0;
     bool stopping = false;
+    std::string first_error;
     std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
     double now() const {
         return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -190,6 +191,8 @@ void worker_main(rla_server *S, int w) {
         if (rc == RLA_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess) rc = RLA_E_CUDA;
         {
             std::lock_guard<std::mutex> lk(S->mu);
+            if (rc != RLA_OK && S->first_error.empty())
+                S->first_error = std::string(rla_status_string(rc)) + ": " + ctx->last_error;
             const double t = S->now();
             for (const Pending &p : job) S->done.push_back(DoneRec{p.req.tag, t - p.t_submit, rc});
             S->in_use -= bytes;
@@ -263,6 +266,12 @@ int rla_server_poll(rla_server *S, uint64_t *tags, double *latency_s, int *statu
     S->done.erase(S->done.begin(), S->done.begin() + n);
     *count = n;
     return RLA_OK;
+}
+
+const char *rla_server_last_error(rla_server *S) {
+    if (!S) return "";
+    std::lock_guard<std::mutex> lk(S->mu);
+    return S->first_error.c_str();
 }
 
 int rla_server_wait_idle(rla_server *S) {

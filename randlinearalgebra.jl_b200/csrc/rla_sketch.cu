@@ -424,7 +424,7 @@ static int build_meta(rla_ctx *ctx, rla_sketch *sk) {
             sk->extra_rounds_cap = 2 * nb;
         }
         if (bm_bytes > 48 * 1024)
-            RLA_CUDA_TRY(ctx, cudaFuncSetAttribute(cs_sched_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bm_bytes));
+            RLA_CUDA_TRY(ctx, set_smem_max(cs_sched_kernel));
         cs_sched_kernel<<<ceil_div_i(nb, CS_SCHED_WARPS), CS_SCHED_WARPS * 32, bm_bytes, ctx->stream>>>(
             sk->bucket, sk->negative, sk->L, sk->s, (uint32_t)dtype_size(sk->p.dtype), sk->meta, sk->tile_flags,
             sk->extra);
@@ -496,8 +496,7 @@ static int draw(rla_ctx *ctx, rla_sketch *sk) {
                 RLA_TRY(scratch_get(ctx, bm_bytes, &p));
                 gbm = (uint32_t *)p;
             } else {
-                RLA_CUDA_TRY(ctx, cudaFuncSetAttribute(draw_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                       (int)bm_bytes));
+                RLA_CUDA_TRY(ctx, set_smem_max(draw_rows_kernel));
             }
             draw_rows_kernel<<<1, 256, use_smem ? bm_bytes : 0, ctx->stream>>>(rng, sk->N, sk->s, gbm, use_smem, sk->rows);
             RLA_TRY(check_launch(ctx, "draw_rows"));

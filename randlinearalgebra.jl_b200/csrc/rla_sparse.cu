@@ -693,7 +693,7 @@ int sparse_compress(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_t x_es
             const bool win = bins_cs < s;
             auto kern = win ? (vec ? cs_compress_kernel<T, true, true> : cs_compress_kernel<T, false, true>)
                             : (vec ? cs_compress_kernel<T, true, false> : cs_compress_kernel<T, false, false>);
-            RLA_CUDA_TRY(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            RLA_CUDA_TRY(ctx, set_smem_max(kern));
             int per_sm = 1;
             RLA_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32, smem));
             int64_t W = (int64_t)ctx->sm_count * std::max(per_sm, 1);
@@ -729,7 +729,7 @@ int sparse_compress(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_t x_es
             p.bin_lo = lo;
             p.bin_cnt = (int)std::min<int64_t>(bin_cnt, s - lo);
             auto launch = [&](auto kern) {
-                cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                set_smem_max(kern);
                 kern<<<blocks, warps * 32, smem, ctx->stream>>>(p);
             };
             const bool win = p.bin_cnt < s;
@@ -769,7 +769,7 @@ int sparse_compress(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_t x_es
         p.bin_lo = lo;
         p.bin_cnt = (int)std::min<int64_t>(bin_cnt, s - lo);
         const int64_t units = ngroups * P;
-        cudaFuncSetAttribute(compress_strided_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        set_smem_max(compress_strided_kernel<T>);
         compress_strided_kernel<T><<<ceil_div_i(units, warps), warps * 32, smem, ctx->stream>>>(p);
         RLA_TRY(check_launch(ctx, "compress_strided"));
         if (P > 1) {

@@ -464,7 +464,7 @@ int tc_gemm_bf16x3(rla_ctx *ctx, int64_t M, int64_t N, int64_t K, const bf16 *Ah
         }
         TcParams p{(int)M, (int)nb, (int)K, pl.BN, pl.nch, a_kmajor, pl.nkb, pl.kbps, pl.stages, pl.tmem_cols,
                    out, ldo, sstride, status};
-        RLA_CUDA_TRY(ctx, cudaFuncSetAttribute(tc_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem));
+        RLA_CUDA_TRY(ctx, set_smem_max(tc_gemm_kernel));
         cudaEvent_t e0 = nullptr, e1 = nullptr;
         if (ctx->timing) {
             RLA_CUDA_TRY(ctx, cudaEventCreate(&e0));

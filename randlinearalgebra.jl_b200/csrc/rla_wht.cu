@@ -280,7 +280,7 @@ template <class T, bool VEC>
 static void launch_srht_fused(const SrhtParams<T> &p, int grid, size_t smem, cudaStream_t st) {
     constexpr int NT = 1 << WhtCfg<T>::TB;
     auto go = [&](auto kern) {
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        set_smem_max(kern);
         kern<<<grid, NT, smem, st>>>(p);
     };
     const int spt = (p.s_cnt + NT - 1) / NT;
@@ -569,7 +569,7 @@ int srht_compress(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_t x_es, 
     }
     if (N < ((int64_t)1 << CH)) {
         const size_t smem = (size_t)N * es;
-        cudaFuncSetAttribute(srht_small_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        set_smem_max(srht_small_kernel<T>);
         const int grid = (int)std::min<int64_t>(nv, (int64_t)ctx->sm_count * 8);
         srht_small_kernel<T><<<grid, 256, smem, ctx->stream>>>(Xc, ldx, L, N, nv, sk->signbits, sk->rows, s, Y, y_es,
                                                                y_vs, a, (T)beta, beta_zero);
@@ -709,7 +709,7 @@ static int srht_noalloc_t(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_
     const bool beta_zero = beta == 0.0;
     if (N < ((int64_t)1 << CH)) {
         const size_t smem = (size_t)N * es;
-        cudaFuncSetAttribute(srht_small_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        set_smem_max(srht_small_kernel<T>);
         const int grid = (int)std::min<int64_t>(nv, (int64_t)ctx->sm_count * 8);
         srht_small_kernel<T><<<grid, 256, smem, ctx->stream>>>(X, ldx, L, N, nv, sk->signbits, sk->rows, s, Y, 1, ldy,
                                                                a, (T)beta, beta_zero);

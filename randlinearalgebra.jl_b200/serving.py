@@ -67,6 +67,10 @@ class Server:
             self._keep.pop(int(tags[i]), None)
         return out
 
+    def last_error(self) -> str:
+        raw = L.lib().rla_server_last_error(self.handle)
+        return raw.decode() if raw else ""
+
     def wait_idle(self) -> None:
         L.lib().rla_server_wait_idle(self.handle)
 
