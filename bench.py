@@ -732,11 +732,11 @@ def sv_pool(torch, dev, n_ls, n_svd, seed=5):
     return ls, svd
 
 
-def sv_run(rla, torch, dev, ls, svd, lam, nreq, plain, slots, seed):
-    """Submit nreq requests with Poisson(lam) arrivals; returns (throughput, p50, p99, lat list)."""
+def sv_run(rla, torch, dev, ls, svd, lam, nreq, plain, slots, seed, ls_frac=0.6):
+    """Submit nreq requests with Poisson(lam) arrivals; returns (throughput, p50, p99)."""
     import numpy as np
     rng = np.random.default_rng(seed)
-    kinds = rng.random(nreq) < 0.6
+    kinds = rng.random(nreq) < ls_frac
     picks = [int(rng.integers(0, len(ls) if k else len(svd))) for k in kinds]
     arrivals = np.cumsum(rng.exponential(1.0 / lam, size=nreq))
     srv = rla.Server(slots=slots, max_group=32, plain=plain)
@@ -787,7 +787,14 @@ def serve_arm(args):
     dev = torch.device("cuda", local if world > 1 else 0)
     ls, svd = sv_pool(torch, dev, 24, 16, seed=5 + rank)
     torch.cuda.synchronize()
-    lams = [2000, 5000, 10000, 20000]
+    lams = [int(x) for x in args.serve_rates.split(",")]
+    if args.serve_mix is not None:  # capacity of one request type (diagnostics)
+        for plain in (False, True):
+            thr, p50, p99 = sv_run(rla, torch, dev, ls, svd, max(lams), args.serve_requests, plain,
+                                   1 if plain else args.slots, 3, ls_frac=args.serve_mix)
+            print(json.dumps({"ls_fraction": args.serve_mix, "plain": plain, "req_per_s": round(thr, 1),
+                              "p50_ms": round(1e3 * p50, 2), "p99_ms": round(1e3 * p99, 2)}), flush=True)
+        return
     # warm both modes (sketches, pools, module loading)
     sv_run(rla, torch, dev, ls, svd, 5000, 60, False, args.slots, 1)
     sv_run(rla, torch, dev, ls, svd, 5000, 30, True, 1, 2)
@@ -853,6 +860,9 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="batched workload: default tile shapes")
     ap.add_argument("--serve-requests", type=int, default=600, help="serving workload: requests per arrival rate")
     ap.add_argument("--slots", type=int, default=4, help="serving workload: concurrent workers")
+    ap.add_argument("--serve-rates", default="2000,5000,10000,20000", help="serving workload: arrival rates (req/s)")
+    ap.add_argument("--serve-mix", type=float, default=None,
+                    help="serving diagnostics: fraction of LS requests (prints per-type capacity only)")
     ap.add_argument("--rs-m", type=int, default=RS_M, help="RandSVD rows (default 65536; smaller for profiler cases)")
     ap.add_argument("--rs-n", type=int, default=RS_N, help="RandSVD columns (default 8192)")
     args = ap.parse_args()

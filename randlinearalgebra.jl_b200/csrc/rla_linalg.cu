@@ -73,6 +73,112 @@ __global__ void __launch_bounds__(1024) chol_upper_kernel(double *G, int64_t l, 
     if (tid == 0) *breakdown = bad;
 }
 
+// Blocked right-looking upper Cholesky in one CTA for l <= CB_MAXL.  Per panel of CB
+// columns: (1) the diagonal block is factored by one warp in shared memory, (2) the panel's
+// rows of R, R(p, p+CB:l) = R_pp^-T G(p, p+CB:l), by forward substitution with one thread
+// per column (the column in registers), staged in shared memory, (3) the trailing upper
+// triangle G(a, b) -= R(p, a)' R(p, b), one 4x4 block of entries per thread.
+constexpr int CB = 32, CB_MAXL = 512, CB_THREADS = 512;
+
+__global__ void __launch_bounds__(CB_THREADS) chol_blocked_kernel(double *G, int64_t l, double shift, int *breakdown,
+                                                                  int ldp) {
+    extern __shared__ double cb_sm[];
+    double *D = cb_sm;             // CB x CB, column-major (ld CB)
+    double *P = cb_sm + CB * CB;   // panel rows: P[c + t*ldp] = R(p+t, p+CB+c)
+    __shared__ int bad;
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) bad = 0;
+    for (int64_t i = tid; i < l; i += nt) G[i + i * l] += shift;
+    __syncthreads();
+    for (int64_t p = 0; p < l; p += CB) {
+        const int pb = (int)(l - p < CB ? l - p : CB);
+        const int64_t c0 = p + pb, rest = l - c0;
+        for (int e = tid; e < pb * pb; e += nt) {
+            const int r = e % pb, c = e / pb;
+            D[r + c * CB] = r <= c ? G[(p + r) + (p + c) * l] : 0.0;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            for (int t = 0; t < pb; ++t) {
+                double v = D[t + t * CB];
+                if (!(v > 0.0) || !isfinite(v)) {
+                    if (lane == 0) bad = 1;
+                    v = 1.0;
+                }
+                const double piv = sqrt(v);
+                __syncwarp();
+                if (lane == t) D[t + t * CB] = piv;
+                if (lane > t && lane < pb) D[t + lane * CB] /= piv;
+                __syncwarp();
+                if (lane > t && lane < pb)
+                    for (int a = t + 1; a <= lane; ++a) D[a + lane * CB] -= D[t + a * CB] * D[t + lane * CB];
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        for (int e = tid; e < pb * pb; e += nt) {
+            const int r = e % pb, c = e / pb;
+            if (r <= c) G[(p + r) + (p + c) * l] = D[r + c * CB];
+        }
+        for (int64_t c = tid; c < rest; c += nt) {
+            double y[CB];
+#pragma unroll
+            for (int t = 0; t < CB; ++t) y[t] = t < pb ? G[(p + t) + (c0 + c) * l] : 0.0;
+#pragma unroll
+            for (int t = 0; t < CB; ++t) {
+                if (t < pb) {
+                    double acc = y[t];
+#pragma unroll
+                    for (int q = 0; q < t; ++q) acc -= D[q + t * CB] * y[q];
+                    y[t] = acc / D[t + t * CB];
+                }
+            }
+#pragma unroll
+            for (int t = 0; t < CB; ++t)
+                if (t < pb) {
+                    G[(p + t) + (c0 + c) * l] = y[t];
+                    P[c + (int64_t)t * ldp] = y[t];
+                }
+        }
+        __syncthreads();
+        const int nb = (int)((rest + 3) / 4);
+        for (int blk = tid; blk < nb * nb; blk += nt) {
+            const int ia = blk % nb, ib = blk / nb;
+            if (ia > ib) continue;
+            double acc[4][4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+            for (int t = 0; t < pb; ++t) {
+                const double *pt = P + (int64_t)t * ldp;
+                const double2 a01 = *reinterpret_cast<const double2 *>(pt + 4 * ia);
+                const double2 a23 = *reinterpret_cast<const double2 *>(pt + 4 * ia + 2);
+                const double2 b01 = *reinterpret_cast<const double2 *>(pt + 4 * ib);
+                const double2 b23 = *reinterpret_cast<const double2 *>(pt + 4 * ib + 2);
+                const double a[4] = {a01.x, a01.y, a23.x, a23.y}, b[4] = {b01.x, b01.y, b23.x, b23.y};
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int64_t a = 4 * ia + i, b = 4 * ib + j;
+                    if (a <= b && b < rest) G[(c0 + a) + (c0 + b) * l] -= acc[i][j];
+                }
+        }
+        __syncthreads();
+    }
+    for (int64_t idx = tid; idx < l * l; idx += nt) {
+        const int64_t r = idx % l, c = idx / l;
+        if (r > c) G[idx] = 0.0;
+    }
+    if (tid == 0) *breakdown = bad;
+}
+
 // Rinv = R^-1 for upper-triangular R: one warp per column j solves R x = e_j by back
 // substitution, x staged in shared memory (wpc warps per CTA).
 __global__ void __launch_bounds__(256) tri_inv_upper_kernel(const double *R, int64_t l, double *Ri, int wpc) {
@@ -407,6 +513,14 @@ template int householder_q<float>(rla_ctx *, float *, int64_t, int64_t, int64_t,
 template int householder_q<double>(rla_ctx *, double *, int64_t, int64_t, int64_t, double *);
 
 int cholesky_upper(rla_ctx *ctx, double *G, int64_t l, double shift, int *breakdown) {
+    if (l <= CB_MAXL) {
+        // panel rows padded so every 4-entry group is a whole 16-byte pair
+        const int ldp = (int)(ceil_div(std::max<int64_t>(l, 1), 4) * 4 + 4);
+        const size_t smem = sizeof(double) * ((size_t)CB * CB + (size_t)CB * ldp);
+        RLA_CUDA_TRY(ctx, set_smem_max(chol_blocked_kernel));
+        chol_blocked_kernel<<<1, CB_THREADS, smem, ctx->stream>>>(G, l, shift, breakdown, ldp);
+        return check_launch(ctx, "chol_blocked");
+    }
     const size_t smem = sizeof(double) * (size_t)std::max<int64_t>(l, 1);
     if (smem > (size_t)ctx->smem_optin - 1024)
         return set_error(ctx, RLA_E_UNSUPPORTED, "Cholesky of order %lld exceeds shared memory", (long long)l);

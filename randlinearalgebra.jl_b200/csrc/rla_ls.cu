@@ -27,28 +27,70 @@ __global__ void ls_scale_kernel(double *G, int64_t l, const double *d) {
     for (int64_t i = threadIdx.x; i < l; i += blockDim.x) G[i + j * l] *= d[i] * d[j];
 }
 
-// With R upper (l x l): y = R^-T (d .* c), z = R^-1 y, x = d .* z, in column (axpy) form so
-// every step is one parallel update plus a barrier.  One CTA; vectors in shared memory.
+// c(i) = sum_r X(r, i) y(r) in FP64, one warp per output (X rows x n, ld ldx; Float32).
+__global__ void ls_gemv_t_kernel(const float *X, int64_t rows, int64_t n, int64_t ldx, const float *y, double *c) {
+    const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= n) return;
+    const float *xi = X + i * ldx;
+    double acc = 0.0;
+    for (int64_t r = lane; r < rows; r += 32) acc += (double)xi[r] * (double)y[r];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(FULL, acc, o);
+    if (lane == 0) c[i] = acc;
+}
+
+// With R upper (l x l): y = R^-T (d .* c), z = R^-1 y, x = d .* z.  Blocked by 32: warp 0
+// solves a 32 x 32 diagonal triangle with shuffles (the block's entries in registers), then
+// all threads apply the block to the rest of the vector; two barriers per block.  One CTA;
+// the vector in shared memory.
 __global__ void __launch_bounds__(1024) ls_trisolve_kernel(const double *R, int64_t l, const double *d,
                                                           const double *c, float *x) {
     extern __shared__ double v[];
-    const int tid = threadIdx.x, nt = blockDim.x;
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
     for (int64_t i = tid; i < l; i += nt) v[i] = d[i] * c[i];
     __syncthreads();
-    // forward, R' lower: y_i = v_i / r_ii; v(i+1:) -= y_i * R(i, i+1:)
-    for (int64_t i = 0; i < l; ++i) {
-        const double yi = v[i] / R[i + i * l];
+    // forward: R' y = v, R' lower; block rows [b, b+32)
+    for (int64_t b = 0; b < l; b += 32) {
+        const int nb = (int)min((int64_t)32, l - b);
+        if (warp == 0) {
+            double yv = lane < nb ? v[b + lane] : 0.0;
+            for (int t = 0; t < nb; ++t) {
+                const double yt = __shfl_sync(FULL, yv, t) / R[(b + t) + (b + t) * l];
+                if (lane == t) yv = yt;
+                if (lane > t && lane < nb) yv -= yt * R[(b + t) + (b + lane) * l];
+            }
+            if (lane < nb) v[b + lane] = yv;
+        }
         __syncthreads();
-        for (int64_t j = i + 1 + tid; j < l; j += nt) v[j] -= yi * R[i + j * l];
-        if (tid == 0) v[i] = yi;
+        // v(j) -= sum_{t in block} R(b+t, j) y(b+t) for j >= b+nb
+        for (int64_t j = b + nb + tid; j < l; j += nt) {
+            double acc = 0.0;
+            for (int t = 0; t < nb; ++t) acc += R[(b + t) + j * l] * v[b + t];
+            v[j] -= acc;
+        }
         __syncthreads();
     }
-    // backward: z_i = v_i / r_ii; v(0:i) -= z_i * R(0:i, i)
-    for (int64_t i = l - 1; i >= 0; --i) {
-        const double zi = v[i] / R[i + i * l];
+    // backward: R z = y; block rows [b, b+nb) from the bottom
+    for (int64_t e = l; e > 0; e -= 32) {
+        const int nb = (int)min((int64_t)32, e);
+        const int64_t b = e - nb;
+        if (warp == 0) {
+            double zv = lane < nb ? v[b + lane] : 0.0;
+            for (int t = nb - 1; t >= 0; --t) {
+                const double zt = __shfl_sync(FULL, zv, t) / R[(b + t) + (b + t) * l];
+                if (lane == t) zv = zt;
+                if (lane < t) zv -= zt * R[(b + lane) + (b + t) * l];
+            }
+            if (lane < nb) v[b + lane] = zv;
+        }
         __syncthreads();
-        for (int64_t j = tid; j < i; j += nt) v[j] -= zi * R[j + i * l];
-        if (tid == 0) v[i] = zi;
+        // v(j) -= sum_{t in block} R(j, b+t) z(b+t) for j < b
+        for (int64_t j = tid; j < b; j += nt) {
+            double acc = 0.0;
+            for (int t = 0; t < nb; ++t) acc += R[j + (b + t) * l] * v[b + t];
+            v[j] -= acc;
+        }
         __syncthreads();
     }
     for (int64_t i = tid; i < l; i += nt) x[i] = (float)(d[i] * v[i]);
@@ -80,7 +122,8 @@ int ls_sketch_solve(rla_ctx *ctx, const rla_sketch *S, int64_t m, int64_t n, con
     RLA_TRY(sketch_mul_impl(ctx, S, RLA_SIDE_LEFT, 0, s, n, SA, s, 0, m, n, A, lda, 0, 1.0, 0.0));
     RLA_TRY(sketch_mul_impl(ctx, S, RLA_SIDE_LEFT, 0, s, 1, Sb, s, 0, m, 1, b, m, 0, 1.0, 0.0));
     RLA_TRY(gram_fp64<float>(ctx, SA, s, n, s, G));
-    RLA_TRY((gemm<float, float, double, double>(ctx, n, 1, s, SA, s, 1, Sb, s, 0, c, n, 1.0, 0.0)));
+    ls_gemv_t_kernel<<<ceil_div_i(n * 32, 256), 256, 0, ctx->stream>>>(SA, s, n, s, Sb, c);
+    RLA_TRY(check_launch(ctx, "ls_gemv_t"));
     ls_diag_kernel<<<ceil_div_i(n, 256), 256, 0, ctx->stream>>>(G, n, tmp);
     ls_scale_kernel<<<(unsigned)n, 256, 0, ctx->stream>>>(G, n, tmp);
     RLA_TRY(check_launch(ctx, "ls_equilibrate"));

@@ -8,8 +8,8 @@
 // max_group) and runs them as one grouped batch (rla_batch.cu, eager launches); the other
 // workers keep taking requests meanwhile, so work that arrives while the GPU is busy
 // overlaps on the device.  Least-squares requests (sketch-and-solve, rla_ls.cu) and
-// RandSVD requests with k > 128 run one per worker; sketches stay resident per worker,
-// keyed by shape and seed.  RLA_SERVE_PLAIN is the baseline: one worker, one request at a
+// RandSVD requests with k > 128 run one per worker; sketches stay resident (shared by the
+// workers), keyed by shape and seed.  RLA_SERVE_PLAIN is the baseline: one worker, one request at a
 // time, the single-instance RandSVD path.  Latency is submit-to-completion on the host
 // clock.  A request's result does not depend on what else runs: grouped kernels map every
 // tile to one instance and add partial sums in a fixed order.
@@ -71,6 +71,10 @@ struct rla_server {
     int running = 0;
     bool stopping = false;
     std::string first_error;
+    // resident sketches shared by all workers (read-only once created; creation synchronises
+    // its stream), keyed by kind, dimensions and seed
+    std::mutex sk_mu;
+    std::map<std::tuple<int, int64_t, int64_t, uint64_t>, rla_sketch *> sketches;
     std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
     double now() const {
         return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -86,9 +90,12 @@ bool admissible(const rla_server *S) {
 
 using SketchKey = std::tuple<int, int64_t, int64_t, uint64_t>;
 
-int get_sketch(rla_ctx *ctx, std::map<SketchKey, rla_sketch *> &cache, int kind, int64_t s, int64_t L, uint64_t seed,
-               rla_sketch **out) {
+// Sketches are created once per key for the whole server: creation allocates device memory,
+// which can synchronise the device, so doing it per worker would serialise the workers.
+int get_sketch(rla_server *S, rla_ctx *ctx, int kind, int64_t s, int64_t L, uint64_t seed, rla_sketch **out) {
     const SketchKey key{kind, s, L, seed};
+    std::lock_guard<std::mutex> lk(S->sk_mu);
+    auto &cache = S->sketches;
     auto it = cache.find(key);
     if (it != cache.end()) {
         *out = it->second;
@@ -109,10 +116,10 @@ int get_sketch(rla_ctx *ctx, std::map<SketchKey, rla_sketch *> &cache, int kind,
     return RLA_OK;
 }
 
-int run_ls(rla_ctx *ctx, std::map<SketchKey, rla_sketch *> &cache, const rla_request &r) {
+int run_ls(rla_server *srv, rla_ctx *ctx, const rla_request &r) {
     const int64_t s = std::min<int64_t>(4 * r.n, r.m);
     rla_sketch *S = nullptr;
-    RLA_TRY(get_sketch(ctx, cache, RLA_SPARSE_SIGN, s, r.m, r.seed, &S));
+    RLA_TRY(get_sketch(srv, ctx, RLA_SPARSE_SIGN, s, r.m, r.seed, &S));
     void *work = nullptr;
     RLA_CUDA_TRY(ctx, pool_malloc_s(ctx, &work, ls_work_bytes(s, r.n), ctx->stream));
     int *bad = nullptr;
@@ -127,9 +134,9 @@ int run_ls(rla_ctx *ctx, std::map<SketchKey, rla_sketch *> &cache, const rla_req
     return hbad ? RLA_E_NUMERIC : RLA_OK;
 }
 
-int run_svd_single(rla_ctx *ctx, std::map<SketchKey, rla_sketch *> &cache, const rla_request &r) {
+int run_svd_single(rla_server *srv, rla_ctx *ctx, const rla_request &r) {
     rla_sketch *om = nullptr;
-    RLA_TRY(get_sketch(ctx, cache, RLA_GAUSSIAN, r.k, r.n, r.seed, &om));
+    RLA_TRY(get_sketch(srv, ctx, RLA_GAUSSIAN, r.k, r.n, r.seed, &om));
     rla_range_params pr{0, 0, RLA_PREC_NATIVE};
     return rla_randsvd(ctx, om, RLA_F32, r.m, r.n, r.A, r.lda, &pr, RLA_F32, r.U, r.ldu, r.S, r.V, r.ldv);
 }
@@ -153,7 +160,6 @@ int run_svd_group(rla_ctx *ctx, const std::vector<Pending> &job) {
 void worker_main(rla_server *S, int w) {
     cudaSetDevice(S->cfg.device);
     rla_ctx *ctx = S->ctxs[w];
-    std::map<SketchKey, rla_sketch *> cache;
     const bool batched = S->cfg.mode == RLA_SERVE_BATCHED;
     for (;;) {
         std::vector<Pending> job;
@@ -185,9 +191,9 @@ void worker_main(rla_server *S, int w) {
         }
         int rc = RLA_OK;
         const rla_request &r0 = job.front().req;
-        if (r0.kind == RLA_REQ_LS) rc = run_ls(ctx, cache, r0);
+        if (r0.kind == RLA_REQ_LS) rc = run_ls(S, ctx, r0);
         else if (job.size() > 1 || (batched && r0.k <= 128)) rc = run_svd_group(ctx, job);
-        else rc = run_svd_single(ctx, cache, r0);
+        else rc = run_svd_single(S, ctx, r0);
         if (rc == RLA_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess) rc = RLA_E_CUDA;
         {
             std::lock_guard<std::mutex> lk(S->mu);
@@ -201,7 +207,6 @@ void worker_main(rla_server *S, int w) {
         S->cv_work.notify_all();
         S->cv_idle.notify_all();
     }
-    for (auto &kv : cache) rla_sketch_destroy(kv.second);
 }
 
 }  // namespace
@@ -289,6 +294,7 @@ int rla_server_stop(rla_server *S) {
     }
     S->cv_work.notify_all();
     for (auto &t : S->workers) t.join();
+    for (auto &kv : S->sketches) rla_sketch_destroy(kv.second);
     for (rla_ctx *c : S->ctxs) rla_ctx_destroy(c);
     delete S;
     return RLA_OK;

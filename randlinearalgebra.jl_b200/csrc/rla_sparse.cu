@@ -714,7 +714,8 @@ int sparse_compress(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_t x_es
         }
         const int blocks_per_sm = std::max(1, cap / (int)(warps * (bin_cnt + 64) * es + 1));
         int64_t W = (int64_t)ctx->sm_count * blocks_per_sm * warps;
-        W = std::min<int64_t>(W, nv * 8);
+        // few vectors: still split each over enough warps (the last warp adds <= W/nv partials)
+        W = std::min<int64_t>(W, std::max<int64_t>(nv * 8, 128));
         W = std::min<int64_t>(W, ceil_div(total, 4));
         W = std::max<int64_t>(W, 1);
         const int blocks = ceil_div_i(W, warps);
