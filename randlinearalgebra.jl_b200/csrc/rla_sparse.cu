@@ -714,9 +714,9 @@ int sparse_compress(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_t x_es
         }
         const int blocks_per_sm = std::max(1, cap / (int)(warps * (bin_cnt + 64) * es + 1));
         int64_t W = (int64_t)ctx->sm_count * blocks_per_sm * warps;
-        // few vectors: still split each over enough warps (the last warp adds <= W/nv partials)
-        W = std::min<int64_t>(W, std::max<int64_t>(nv * 8, 128));
-        W = std::min<int64_t>(W, ceil_div(total, 4));
+        // fill the GPU even with few vectors (at least two tiles per warp), but split one
+        // vector over at most 64 warps: its last warp adds all of their partial bin arrays
+        W = std::min<int64_t>(W, std::min<int64_t>(ceil_div(total, 2), nv * 64));
         W = std::max<int64_t>(W, 1);
         const int blocks = ceil_div_i(W, warps);
         const size_t smem = (size_t)warps * (bin_cnt + 64) * es;
