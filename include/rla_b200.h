@@ -229,7 +229,8 @@ int rla_randsvd_batch_create(rla_ctx *ctx, int count, const rla_svd_problem *pro
  * (instances whose Cholesky broke down are recomputed by the single-instance path). */
 int rla_randsvd_batch_run(rla_ctx *ctx, rla_batch *batch);
 /* Tile shapes in use for rank class c (0: k <= 16, 1: <= 32, 2: <= 64, 3: <= 128): rows
- * per CTA of A*Omega, columns of A per CTA of A'Q and its row chunk. */
+ * per CTA of A*Omega (64, 128 or 256), columns of A per CTA of A'Q (64, 128 or 256) and its
+ * row chunk. */
 int rla_randsvd_batch_tiles(const rla_batch *batch, int c, int *rows_a_omega, int *cols_at_q,
                             int64_t *chunk_at_q);
 int rla_randsvd_batch_destroy(rla_batch *batch);

@@ -140,6 +140,21 @@ struct AxOps<AX_QB_J> {
     __device__ static TO *O(const BProb &p, int64_t &ld) { ld = p.ldv; return p.V; }
 };
 
+// Register tiling shared by the grouped products: a CTA computes a BM x KT output tile with
+// B_THREADS threads, KT/4 threads across the columns (4 consecutive columns each) and the rest
+// down the rows (TM rows each, strided so a warp's shared-memory reads are broadcasts or
+// consecutive).  The reduction runs over BK-deep slices staged in shared memory; the next
+// slice is read from global memory into registers while the current one is multiplied.
+template <class TAcc, int KT, int BM>
+struct Tile {
+    static constexpr int TN = 4, TXN = KT / TN, TYM = B_THREADS / TXN, TM = BM / TYM;
+    static constexpr int BK = (sizeof(TAcc) == 8 && (KT >= 128 || BM >= 128)) ? 16 : 32;
+    static constexpr int NP = BK * BM / B_THREADS;  // P-slice elements per thread
+    static constexpr int NW = (BK * KT + B_THREADS - 1) / B_THREADS;
+    static_assert(TM >= 1 && TYM * TM == BM, "tile shape");
+    static_assert(NP * B_THREADS == BK * BM, "slice shape");
+};
+
 // out (rows x k) = X (rows x K) * W (K x k); CTA = BM rows of one instance, all k columns.
 // In-place use (out == X) is safe: a CTA reads all of its rows before it writes them.
 template <int KIND, int KT, int BM>
@@ -149,9 +164,10 @@ __global__ void __launch_bounds__(B_THREADS) b_ax_kernel(BProb *P, const int *id
     using TW = typename O::TW;
     using TAcc = typename O::TAcc;
     using TO = typename O::TO;
-    constexpr int BK = (sizeof(TAcc) == 8 && KT >= 128) ? 16 : 32, TM = BM / 16, TN = KT / 16;
-    __shared__ TAcc Xs[BK][BM + 1];
-    __shared__ TAcc Ws[BK][KT];
+    using Tl = Tile<TAcc, KT, BM>;
+    constexpr int BK = Tl::BK, TM = Tl::TM, TN = Tl::TN, TXN = Tl::TXN, TYM = Tl::TYM, NP = Tl::NP, NW = Tl::NW;
+    __shared__ __align__(16) TAcc Xs[BK][BM + 4];
+    __shared__ __align__(16) TAcc Ws[BK][KT];
     const int t = blockIdx.x;
     const int q = b_find(tstart, count, t);
     const BProb &p = P[idx[q]];
@@ -161,31 +177,51 @@ __global__ void __launch_bounds__(B_THREADS) b_ax_kernel(BProb *P, const int *id
     const TW *W = O::W(p, ldw);
     TO *Out = O::O(p, ldo);
     const int64_t r0 = (int64_t)(t - tstart[q]) * BM;
-    const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
+    const int tid = threadIdx.x, tx = tid % TXN, ty = tid / TXN;
     TAcc acc[TM][TN];
 #pragma unroll
     for (int i = 0; i < TM; ++i)
 #pragma unroll
         for (int j = 0; j < TN; ++j) acc[i][j] = TAcc(0);
-    for (int64_t c0 = 0; c0 < K; c0 += BK) {
-        for (int e = tid; e < BK * BM; e += B_THREADS) {
-            const int r = e % BM, c = e / BM;
+    TAcc px[NP], pw[NW];
+    auto fetch = [&](int64_t c0) {
+#pragma unroll
+        for (int u = 0; u < NP; ++u) {
+            const int e = tid + u * B_THREADS, r = e % BM, c = e / BM;
             const int64_t gr = r0 + r, gc = c0 + c;
-            Xs[c][r] = (gr < rows && gc < K) ? (TAcc)X[gr + gc * ldx] : TAcc(0);
+            px[u] = (gr < rows && gc < K) ? (TAcc)X[gr + gc * ldx] : TAcc(0);
         }
-        for (int e = tid; e < BK * KT; e += B_THREADS) {
-            const int c = e % BK, j = e / BK;
+#pragma unroll
+        for (int u = 0; u < NW; ++u) {
+            const int e = tid + u * B_THREADS, c = e % BK, j = e / BK;
             const int64_t gc = c0 + c;
-            Ws[c][j] = (gc < K && j < kk) ? (TAcc)W[gc + j * ldw] : TAcc(0);
+            pw[u] = (e < BK * KT && gc < K && j < kk) ? (TAcc)W[gc + j * ldw] : TAcc(0);
         }
+    };
+    auto stash = [&]() {
+#pragma unroll
+        for (int u = 0; u < NP; ++u) {
+            const int e = tid + u * B_THREADS;
+            Xs[e / BM][e % BM] = px[u];
+        }
+#pragma unroll
+        for (int u = 0; u < NW; ++u) {
+            const int e = tid + u * B_THREADS;
+            if (e < BK * KT) Ws[e % BK][e / BK] = pw[u];
+        }
+    };
+    fetch(0);
+    for (int64_t c0 = 0; c0 < K; c0 += BK) {
+        stash();
         __syncthreads();
+        if (c0 + BK < K) fetch(c0 + BK);
 #pragma unroll 8
         for (int c = 0; c < BK; ++c) {
             TAcc a[TM], b[TN];
 #pragma unroll
-            for (int i = 0; i < TM; ++i) a[i] = Xs[c][ty + 16 * i];
+            for (int i = 0; i < TM; ++i) a[i] = Xs[c][ty + TYM * i];
 #pragma unroll
-            for (int j = 0; j < TN; ++j) b[j] = Ws[c][tx + 16 * j];
+            for (int j = 0; j < TN; ++j) b[j] = Ws[c][tx * TN + j];
 #pragma unroll
             for (int i = 0; i < TM; ++i)
 #pragma unroll
@@ -195,11 +231,11 @@ __global__ void __launch_bounds__(B_THREADS) b_ax_kernel(BProb *P, const int *id
     }
 #pragma unroll
     for (int j = 0; j < TN; ++j) {
-        const int64_t gj = tx + 16 * j;
+        const int64_t gj = tx * TN + j;
         if (gj >= kk) continue;
 #pragma unroll
         for (int i = 0; i < TM; ++i) {
-            const int64_t gr = r0 + ty + 16 * i;
+            const int64_t gr = r0 + ty + TYM * i;
             if (gr < rows) Out[gr + gj * ldo] = (TO)acc[i][j];
         }
     }
@@ -243,16 +279,18 @@ struct XtyOps<XT_BT0_QB> {
 };
 
 // part[s][i][j] = sum over rows r of chunk s of X(r, i) Y(r, j), i in a BR-column block of
-// X, j < k.  Tiles of an instance: (column block, chunk), chunk-major.
+// X, j < k.  Tiles of an instance: (column block, chunk), chunk-major.  Same register tiling
+// and slice prefetch as b_ax_kernel, with the X slice transposed into shared memory.
 template <int KIND, int KT, int BR>
 __global__ void __launch_bounds__(B_THREADS) b_xty_kernel(BProb *P, const int *idx, const int *tstart, int count,
                                                           int64_t chunk) {
     using O = XtyOps<KIND>;
     using TX = typename O::TX;
     using TAcc = typename O::TAcc;
-    constexpr int BK = (sizeof(TAcc) == 8 && KT * BR >= 128 * 64) ? 16 : 32, TM = BR / 16, TN = KT / 16;
-    __shared__ TAcc Xs[BK][BR + 1];
-    __shared__ TAcc Ys[BK][KT + 1];
+    using Tl = Tile<TAcc, KT, BR>;
+    constexpr int BK = Tl::BK, TM = Tl::TM, TN = Tl::TN, TXN = Tl::TXN, TYM = Tl::TYM, NP = Tl::NP, NW = Tl::NW;
+    __shared__ __align__(16) TAcc Xs[BK][BR + 4];
+    __shared__ __align__(16) TAcc Ys[BK][KT];
     const int t = blockIdx.x;
     const int q = b_find(tstart, count, t);
     const BProb &p = P[idx[q]];
@@ -264,31 +302,51 @@ __global__ void __launch_bounds__(B_THREADS) b_xty_kernel(BProb *P, const int *i
     const int64_t lt = t - tstart[q];
     const int64_t cb = lt % ncb, split = lt / ncb;
     const int64_t i0 = cb * BR, rs = split * chunk, re = min(rows, rs + chunk);
-    const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
+    const int tid = threadIdx.x, tx = tid % TXN, ty = tid / TXN;
     TAcc acc[TM][TN];
 #pragma unroll
     for (int i = 0; i < TM; ++i)
 #pragma unroll
         for (int j = 0; j < TN; ++j) acc[i][j] = TAcc(0);
-    for (int64_t r0 = rs; r0 < re; r0 += BK) {
-        for (int e = tid; e < BK * BR; e += B_THREADS) {
-            const int r = e % BK, c = e / BK;
+    TAcc px[NP], py[NW];
+    auto fetch = [&](int64_t r0) {
+#pragma unroll
+        for (int u = 0; u < NP; ++u) {
+            const int e = tid + u * B_THREADS, r = e % BK, c = e / BK;
             const int64_t gr = r0 + r, gc = i0 + c;
-            Xs[r][c] = (gr < re && gc < nx) ? (TAcc)X[gr + gc * ldx] : TAcc(0);
+            px[u] = (gr < re && gc < nx) ? (TAcc)X[gr + gc * ldx] : TAcc(0);
         }
-        for (int e = tid; e < BK * KT; e += B_THREADS) {
-            const int r = e % BK, j = e / BK;
+#pragma unroll
+        for (int u = 0; u < NW; ++u) {
+            const int e = tid + u * B_THREADS, r = e % BK, j = e / BK;
             const int64_t gr = r0 + r;
-            Ys[r][j] = (gr < re && j < kk) ? (TAcc)Yp[gr + j * ldy] : TAcc(0);
+            py[u] = (e < BK * KT && gr < re && j < kk) ? (TAcc)Yp[gr + j * ldy] : TAcc(0);
         }
+    };
+    auto stash = [&]() {
+#pragma unroll
+        for (int u = 0; u < NP; ++u) {
+            const int e = tid + u * B_THREADS;
+            Xs[e % BK][e / BK] = px[u];
+        }
+#pragma unroll
+        for (int u = 0; u < NW; ++u) {
+            const int e = tid + u * B_THREADS;
+            if (e < BK * KT) Ys[e % BK][e / BK] = py[u];
+        }
+    };
+    if (rs < re) fetch(rs);
+    for (int64_t r0 = rs; r0 < re; r0 += BK) {
+        stash();
         __syncthreads();
+        if (r0 + BK < re) fetch(r0 + BK);
 #pragma unroll 8
         for (int r = 0; r < BK; ++r) {
             TAcc a[TM], b[TN];
 #pragma unroll
-            for (int i = 0; i < TM; ++i) a[i] = Xs[r][ty + 16 * i];
+            for (int i = 0; i < TM; ++i) a[i] = Xs[r][ty + TYM * i];
 #pragma unroll
-            for (int j = 0; j < TN; ++j) b[j] = Ys[r][tx + 16 * j];
+            for (int j = 0; j < TN; ++j) b[j] = Ys[r][tx * TN + j];
 #pragma unroll
             for (int i = 0; i < TM; ++i)
 #pragma unroll
@@ -299,11 +357,11 @@ __global__ void __launch_bounds__(B_THREADS) b_xty_kernel(BProb *P, const int *i
     TAcc *part = reinterpret_cast<TAcc *>(p.part) + split * nx * kk;
 #pragma unroll
     for (int i = 0; i < TM; ++i) {
-        const int64_t gi = i0 + ty + 16 * i;
+        const int64_t gi = i0 + ty + TYM * i;
         if (gi >= nx) continue;
 #pragma unroll
         for (int j = 0; j < TN; ++j) {
-            const int64_t gj = tx + 16 * j;
+            const int64_t gj = tx * TN + j;
             if (gj < kk) part[gi * kk + gj] = acc[i][j];
         }
     }
@@ -537,11 +595,13 @@ struct rla_batch {
     std::map<std::tuple<int, int, int64_t>, int *> maps;
     std::map<std::tuple<int, int, int64_t>, int> map_total;
     int64_t chunk_m = 4096, chunk_n = 1 << 20;
-    int bm_ax[rla::B_NCLASS] = {128, 128, 128, 128};  // rows per CTA of A*Omega / A*Z
-    int br_aq[rla::B_NCLASS] = {64, 64, 64, 64};      // columns of A per CTA of A'Q
+    int bm_ax[rla::B_NCLASS] = {256, 256, 256, 128};  // rows per CTA of A*Omega / A*Z (64, 128, 256)
+    int br_aq[rla::B_NCLASS] = {256, 256, 256, 128};  // columns of A per CTA of A'Q (64, 128, 256)
     int64_t chunk_aq[rla::B_NCLASS] = {8192, 8192, 8192, 8192};
     bool tuned = false;
     cudaStream_t cs = nullptr;
+    cudaStream_t side[rla::B_NCLASS] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t fork = nullptr, join[rla::B_NCLASS] = {nullptr, nullptr, nullptr, nullptr};
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -604,13 +664,33 @@ static int launch_ax(rla_ctx *ctx, rla_batch *b, int cls, cudaStream_t st) {
     return check_launch(ctx, "batch_ax");
 }
 
+// Rows per CTA of the A*X products: candidates 64, 128, 256 (256 only while the register tile
+// stays small, KT <= 64).
 template <int KIND, int KT>
 static int launch_ax_bm(rla_ctx *ctx, rla_batch *b, int cls, int bm, cudaStream_t st) {
-    switch (bm) {
-        case 32: return launch_ax<KIND, KT, 32>(ctx, b, cls, st);
-        case 64: return launch_ax<KIND, KT, 64>(ctx, b, cls, st);
-        default: return launch_ax<KIND, KT, 128>(ctx, b, cls, st);
+    if (bm <= 64) return launch_ax<KIND, KT, 64>(ctx, b, cls, st);
+    if constexpr (KT <= 64) {
+        if (bm > 128) return launch_ax<KIND, KT, 256>(ctx, b, cls, st);
     }
+    return launch_ax<KIND, KT, 128>(ctx, b, cls, st);
+}
+
+// Smallest column block of an X'Y product with a full register tile (Tile<.., KT, BR>).
+template <int KT>
+constexpr int min_br() { return 1024 / KT > KT ? 1024 / KT : KT; }
+
+template <int KIND, int KT, int BR>
+static int launch_xty(rla_ctx *ctx, rla_batch *b, int cls, int64_t chunk, cudaStream_t st);
+
+// Columns of A per CTA of A'Q: candidates 64, 128, 256 (256 only while the register tile stays
+// small, KT <= 64).
+template <int KIND, int KT>
+static int launch_xty_br(rla_ctx *ctx, rla_batch *b, int cls, int br, int64_t chunk, cudaStream_t st) {
+    if (br <= 64) return launch_xty<KIND, KT, 64>(ctx, b, cls, chunk, st);
+    if constexpr (KT <= 64) {
+        if (br > 128) return launch_xty<KIND, KT, 256>(ctx, b, cls, chunk, st);
+    }
+    return launch_xty<KIND, KT, 128>(ctx, b, cls, chunk, st);
 }
 
 template <int KIND, int KT, int BR>
@@ -649,7 +729,7 @@ static int run_class(rla_ctx *ctx, rla_batch *b, int cls, cudaStream_t st) {
     // (dynamic shared-memory limits of b_chol_inv_kernel / b_jacobi_kernel are raised at plan creation)
     auto orth_m = [&]() -> int {  // CholeskyQR2 of Y (m x k, FP32 data, FP64 Gram)
         for (int pass = 0; pass < 2; ++pass) {
-            RLA_TRY((launch_xty<XT_GRAM_Y, KT, KT>(ctx, b, cls, b->chunk_m, st)));
+            RLA_TRY((launch_xty<XT_GRAM_Y, KT, min_br<KT>()>(ctx, b, cls, b->chunk_m, st)));
             RLA_TRY((launch_reduce<RED_G_M, double>(ctx, b, cls, b->chunk_m, b->chunk_n, st)));
             b_chol_inv_kernel<<<nq, 512, chol_smem, st>>>(b->d_probs, b->cls_d[cls]);
             RLA_TRY(check_launch(ctx, "batch_chol"));
@@ -663,32 +743,24 @@ static int run_class(rla_ctx *ctx, rla_batch *b, int cls, cudaStream_t st) {
     if (ortho || b->params.power_its == 0) RLA_TRY(orth_m());
     for (int64_t it = 0; it < b->params.power_its; ++it) {
         // Z = A'Q (split over row chunks), optionally orthonormalised, then Q = A Z
-        switch (b->br_aq[cls]) {
-            case 32: RLA_TRY((launch_xty<XT_A_Q_Z, KT, 32>(ctx, b, cls, b->chunk_aq[cls], st))); break;
-            case 128: RLA_TRY((launch_xty<XT_A_Q_Z, KT, 128>(ctx, b, cls, b->chunk_aq[cls], st))); break;
-            default: RLA_TRY((launch_xty<XT_A_Q_Z, KT, 64>(ctx, b, cls, b->chunk_aq[cls], st)));
-        }
+        RLA_TRY((launch_xty_br<XT_A_Q_Z, KT>(ctx, b, cls, b->br_aq[cls], b->chunk_aq[cls], st)));
         RLA_TRY((launch_reduce<RED_Z, float>(ctx, b, cls, b->chunk_aq[cls], b->chunk_n, st)));
         RLA_TRY((launch_ax_bm<AX_A_Z, KT>(ctx, b, cls, b->bm_ax[cls], st)));
         if (ortho || it + 1 == b->params.power_its) RLA_TRY(orth_m());
     }
     // Bt = A'Q in FP64 (partials FP32, added in FP64)
-    switch (b->br_aq[cls]) {
-        case 32: RLA_TRY((launch_xty<XT_A_Q, KT, 32>(ctx, b, cls, b->chunk_aq[cls], st))); break;
-        case 128: RLA_TRY((launch_xty<XT_A_Q, KT, 128>(ctx, b, cls, b->chunk_aq[cls], st))); break;
-        default: RLA_TRY((launch_xty<XT_A_Q, KT, 64>(ctx, b, cls, b->chunk_aq[cls], st)));
-    }
+    RLA_TRY((launch_xty_br<XT_A_Q, KT>(ctx, b, cls, b->br_aq[cls], b->chunk_aq[cls], st)));
     RLA_TRY((launch_reduce<RED_BT, float>(ctx, b, cls, b->chunk_aq[cls], b->chunk_n, st)));
     // CholeskyQR2 of Bt (n x k, FP64)
     for (int pass = 0; pass < 2; ++pass) {
-        RLA_TRY((launch_xty<XT_GRAM_BT, KT, KT>(ctx, b, cls, b->chunk_n, st)));
+        RLA_TRY((launch_xty<XT_GRAM_BT, KT, min_br<KT>()>(ctx, b, cls, b->chunk_n, st)));
         RLA_TRY((launch_reduce<RED_G_N, double>(ctx, b, cls, b->chunk_m, b->chunk_n, st)));
         b_chol_inv_kernel<<<nq, 512, chol_smem, st>>>(b->d_probs, b->cls_d[cls]);
         RLA_TRY(check_launch(ctx, "batch_chol"));
         RLA_TRY((launch_ax<AX_BT_RINV, KT, 64>(ctx, b, cls, st)));
     }
     // X = Bt0' Qb = Rb', SVD, U = Q W, V = Qb J
-    RLA_TRY((launch_xty<XT_BT0_QB, KT, KT>(ctx, b, cls, b->chunk_n, st)));
+    RLA_TRY((launch_xty<XT_BT0_QB, KT, min_br<KT>()>(ctx, b, cls, b->chunk_n, st)));
     RLA_TRY((launch_reduce<RED_X, double>(ctx, b, cls, b->chunk_m, b->chunk_n, st)));
     b_jacobi_kernel<<<nq, 512, jac_smem, st>>>(b->d_probs, b->cls_d[cls], 1e-15, 60, j_in_smem);
     RLA_TRY(check_launch(ctx, "batch_jacobi"));
@@ -697,11 +769,23 @@ static int run_class(rla_ctx *ctx, rla_batch *b, int cls, cudaStream_t st) {
     return RLA_OK;
 }
 
+// The rank classes share nothing, so each runs on its own stream forked from `st` (their
+// launch tails overlap); `st` waits for all of them.
 static int enqueue_all(rla_ctx *ctx, rla_batch *b, cudaStream_t st) {
-    RLA_TRY(run_class<16>(ctx, b, 0, st));
-    RLA_TRY(run_class<32>(ctx, b, 1, st));
-    RLA_TRY(run_class<64>(ctx, b, 2, st));
-    RLA_TRY(run_class<128>(ctx, b, 3, st));
+    RLA_CUDA_TRY(ctx, cudaEventRecord(b->fork, st));
+    for (int c = 0; c < B_NCLASS; ++c) {
+        if (b->cls_h[c].empty()) continue;
+        cudaStream_t sc = b->side[c];
+        RLA_CUDA_TRY(ctx, cudaStreamWaitEvent(sc, b->fork, 0));
+        switch (c) {
+            case 0: RLA_TRY(run_class<16>(ctx, b, 0, sc)); break;
+            case 1: RLA_TRY(run_class<32>(ctx, b, 1, sc)); break;
+            case 2: RLA_TRY(run_class<64>(ctx, b, 2, sc)); break;
+            default: RLA_TRY(run_class<128>(ctx, b, 3, sc));
+        }
+        RLA_CUDA_TRY(ctx, cudaEventRecord(b->join[c], sc));
+        RLA_CUDA_TRY(ctx, cudaStreamWaitEvent(st, b->join[c], 0));
+    }
     return RLA_OK;
 }
 
@@ -733,14 +817,14 @@ static int autotune(rla_ctx *ctx, rla_batch *b) {
         float best = 1e30f;
         int bbm = b->bm_ax[c], bbr = b->br_aq[c];
         int64_t bch = b->chunk_aq[c];
-        for (int bm : {32, 64, 128}) {
+        for (int bm : {64, 128, 256}) {
             b->bm_ax[c] = bm;
             float ms;
             RLA_TRY(time_class(ctx, b, c, &ms));
             if (ms < best) { best = ms; bbm = bm; }
         }
         b->bm_ax[c] = bbm;
-        for (int br : {32, 64, 128})
+        for (int br : {64, 128, 256})
             for (int64_t ch : {2048, 8192, 32768}) {
                 b->br_aq[c] = br;
                 b->chunk_aq[c] = ch;
@@ -854,6 +938,12 @@ int rla_randsvd_batch_create(rla_ctx *ctx, int count, const rla_svd_problem *pro
             set_smem_max(b_jacobi_kernel) != cudaSuccess)
             return fail(set_error(ctx, RLA_E_CUDA, "batch kernel attributes"));
     }
+    if (cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess)
+        return fail(set_error(ctx, RLA_E_CUDA, "batch events"));
+    for (int c = 0; c < B_NCLASS; ++c)
+        if (cudaStreamCreateWithFlags(&b->side[c], cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&b->join[c], cudaEventDisableTiming) != cudaSuccess)
+            return fail(set_error(ctx, RLA_E_CUDA, "batch class streams"));
     if (!(flags & RLA_BATCH_EAGER) || (flags & RLA_BATCH_AUTOTUNE)) {
         if (cudaStreamCreateWithFlags(&b->cs, cudaStreamNonBlocking) != cudaSuccess ||
             cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess)
@@ -934,6 +1024,14 @@ int rla_randsvd_batch_destroy(rla_batch *b) {
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
     if (b->cs) cudaStreamDestroy(b->cs);
+    for (int c = 0; c < B_NCLASS; ++c) {
+        if (b->side[c]) {
+            cudaStreamSynchronize(b->side[c]);
+            cudaStreamDestroy(b->side[c]);
+        }
+        if (b->join[c]) cudaEventDestroy(b->join[c]);
+    }
+    if (b->fork) cudaEventDestroy(b->fork);
     cudaStream_t st = b->ctx->stream;
     for (void *p : b->owned) cudaFreeAsync(p, st);
     for (int c = 0; c < B_NCLASS; ++c)

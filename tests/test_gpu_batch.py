@@ -79,7 +79,7 @@ def test_batch_graph_replay_and_autotune(rla, dev):
         assert np.array_equal(a, s.cpu().numpy())
     for c in range(4):
         bm, br, ch = B.tiles(c)
-        assert bm in (32, 64, 128) and br in (32, 64, 128) and ch in (2048, 8192, 32768)
+        assert bm in (64, 128, 256) and br in (64, 128, 256) and ch in (2048, 8192, 32768)
 
 
 def test_batch_rank_deficient_falls_back(rla, dev):
