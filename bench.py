@@ -191,7 +191,7 @@ def cpu_sample(threads: int, budget_s: float, srht_draws=None, cs_draws=None):
     ts = run("srht", n_s)
     tc = run("count_sketch", n_c)
     gbs = 4 * (M + S) * (n_s + n_c) / (ts + tc) / 1e9
-    desc = (f"SRHT on {n_s} and CountSketch on {n_c} of the 512 columns of the 2^20-row A "
+    desc = (f"SRHT on {n_s} and CountSketch on {n_c} columns of a {M}-row A "
             f"({threads} thread(s), column blocks of 10 as srht.jl:240 walks them)")
     return gbs, desc, ts + tc
 
@@ -317,7 +317,7 @@ def b200_arm(args):
     peak, peak_kind = peaks()
     dom_name, dom_ms = ("srht_fused_kernel", srht_ms) if srht_ms >= cs_ms else ("cs_compress_kernel", cs_ms)
     achieved = BYTES_PER_APPLY / (dom_ms / 1e3) / 1e9
-    traffic = TRAFFIC_PER_LAUNCH.get(dom_name)
+    traffic = TRAFFIC_PER_LAUNCH.get(dom_name) if (M, NCOL) == (2**20, 512) else None
     roofline = {"bound": "hbm", "kernel": dom_name, "achieved": round(achieved, 2), "peak": peak,
                 "peak_source": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
                 "algorithmic_bytes_per_launch": BYTES_PER_APPLY}
@@ -338,7 +338,9 @@ def b200_arm(args):
     line = {"metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": K,
             "warmup": args.warmup, "ms_per_step": round(ms / K, 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic N(0,1) generated on device (torch.randn, seed 2+rank)",
-            "config": {"workload": WORKLOAD if NCOL == 512 else WORKLOAD.replace("512", str(NCOL)), "m": M, "n": NCOL,
+            "config": {"workload": WORKLOAD if (NCOL, M) == (512, 2**20) else
+                       WORKLOAD.replace("2^20x512", f"{M}x{NCOL}").replace("512 ->", f"{NCOL} ->").replace("4096x512", f"4096x{NCOL}"),
+                       "m": M, "n": NCOL,
                        "s": S, "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (2.15 GB per A), no flush needed"},
             "roofline": roofline, "kernels": kernels, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
@@ -844,12 +846,15 @@ def serve_arm(args):
 
 
 def main():
+    global M, BYTES_PER_APPLY
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--rows", type=int, default=M,
+                    help="rows of A (default 2^20; 4194304 with --cols 128 is the tall-skinny variant)")
     ap.add_argument("--cols", type=int, default=NCOL,
                     help="columns of A (default 512, the benchmark workload; smaller values make small "
                          "cases of the same kernels for profiler captures)")
@@ -866,6 +871,9 @@ def main():
     ap.add_argument("--rs-m", type=int, default=RS_M, help="RandSVD rows (default 65536; smaller for profiler cases)")
     ap.add_argument("--rs-n", type=int, default=RS_N, help="RandSVD columns (default 8192)")
     args = ap.parse_args()
+    if args.rows != M:
+        M = args.rows
+        BYTES_PER_APPLY = bytes_per_apply()
     if args.warmup < 3:
         args.warmup = 3
     if args.workload == "serve":
