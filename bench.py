@@ -112,29 +112,43 @@ class ClockSampler:
 
 
 def dist_setup(gpus):
+    """One rank per GPU over NCCL (RANK / LOCAL_RANK / WORLD_SIZE / MASTER_* from the
+    launcher).  Without a GPU the same plumbing runs over gloo, which is how the host-side
+    logic of the N > 1 path is tested."""
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    cuda = torch.cuda.is_available()
     if world > 1:
         import datetime
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180),
-                                device_id=torch.device("cuda", local))
-    else:
+        if cuda:
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+    elif cuda:
         torch.cuda.set_device(0)
     return world, rank, local
 
 
 def allreduce_max(x: float, world: int) -> float:
+    """Max over ranks (the step time every rank reports is the slowest rank's)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def job_throughput(world: int, bytes_per_rank: float, seconds: float) -> float:
+    """Whole-job GB/s: every rank processed `bytes_per_rank`; `seconds` is the max over ranks."""
+    return world * bytes_per_rank / seconds / 1e9
 
 
 def barrier(world):
@@ -281,7 +295,7 @@ def b200_arm(args):
     ms = allreduce_max(ms_local, world)
     srht_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in ev)
     cs_ms = statistics.mean(e[2].elapsed_time(e[3]) for e in ev)
-    value = world * 2 * BYTES_PER_APPLY * K / (ms / 1e3) / 1e9
+    value = job_throughput(world, 2 * BYTES_PER_APPLY * K, ms / 1e3)
 
     # correctness guard on a few columns (no oracle: S*A for a column subset must agree)
     sub = A[:, :8]
@@ -303,7 +317,7 @@ def b200_arm(args):
         rla.mul_(Ch2, cs, A_h)
     torch.cuda.synchronize()
     e2e_s = allreduce_max((time.perf_counter() - w0) / e2e_steps, world)
-    e2e = {"value": round(world * 2 * BYTES_PER_APPLY / e2e_s / 1e9, 3), "unit": "GB/s",
+    e2e = {"value": round(job_throughput(world, 2 * BYTES_PER_APPLY, e2e_s), 3), "unit": "GB/s",
            "h2d_bytes_per_step": 2 * (4 * M * NCOL + 4 * S * NCOL), "d2h_bytes_per_step": 2 * 4 * S * NCOL,
            "ms_per_step": round(e2e_s * 1e3, 3)}
     del A_h
@@ -876,6 +890,8 @@ def main():
         BYTES_PER_APPLY = bytes_per_apply()
     if args.warmup < 3:
         args.warmup = 3
+    if args.impl == "reference" and int(os.environ.get("RANK", "0")) != 0:
+        return  # the reference arm runs on rank 0 alone; other ranks exit without work
     if args.workload == "serve":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "serving workload: the reference arm is timed "
