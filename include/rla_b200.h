@@ -248,6 +248,48 @@ int rla_randsvd_grouped(rla_ctx *ctx, int count, const rla_svd_problem *problems
 int rla_sketch_solve(rla_ctx *ctx, const rla_sketch *sk, int64_t m, int64_t n, const float *A,
                      int64_t lda, const float *b, float *x);
 
+/* ---- Iterative Hessian Sketch solver ------------------------------------------------------
+ * IHS (src/Solvers/ihs.jl:40-254) for min ||Ax - b|| with A (m x n, m > n), a Left compressor S
+ * (s x m, n <= s <= m) of the same element type, step size alpha.  All vectors are device
+ * buffers the caller owns: b (m), x (n, the solution_vec, updated in place), r (m, the
+ * residual_vec), g (n, the gradient_vec).
+ *   rla_ihs_create  complete_solver (ihs.jl:127-206): its ArgumentError checks, same wording
+ *                   and order; workspaces (compressed_mat s x n, Gram, partial sums).
+ *   rla_ihs_start   the start of rsolve! (ihs.jl:214-223): r = b - A x, then iteration 1's
+ *                   gradient g = A'r and error values.
+ *   rla_ihs_step    the rest of an iteration (ihs.jl:231-249): update_compressor!, S*A, the
+ *                   R'R of S*A (FP64 Cholesky of the equilibrated Gram matrix; the same R'R as
+ *                   qr!(S*A).R), u = R \ (R' \ g), x += alpha*u, r -= A*u (by A*u also when
+ *                   alpha != 1, as the reference does), then the next iteration's g and errors.
+ *   rla_ihs_errors  the error values of the current iteration (synchronises): FullResidual
+ *                   ||b - Ax|| (full_residual.jl) and LSGradient ||A'r|| (ls_gradient.jl);
+ *                   RLA_E_NUMERIC if the last step's sketched Gram matrix was not positive
+ *                   definite.
+ *   rla_ihs_solve   rsolve! with BasicLogger(max_it, collection_rate, threshold) and
+ *                   threshold_stop (src/Solvers/Loggers/basic_logger.jl:84-130): hist gets
+ *                   ceil(max_it/collection_rate)+1 entries; *iterations = the last logged
+ *                   iteration, *converged = the logger's converged flag.
+ * Asynchronous on the context's stream except rla_ihs_errors and rla_ihs_solve. */
+typedef struct rla_ihs rla_ihs;
+#define RLA_IHS_FULL_RESIDUAL 0
+#define RLA_IHS_LS_GRADIENT 1
+int rla_ihs_create(rla_ctx *ctx, rla_sketch *compressor, int dtype, int64_t m, int64_t n, double alpha,
+                   rla_ihs **out);
+int rla_ihs_start(rla_ctx *ctx, rla_ihs *h, const void *A, int64_t lda, const void *b, const void *x,
+                  void *r, void *g);
+int rla_ihs_step(rla_ctx *ctx, rla_ihs *h, const void *A, int64_t lda, const void *b, void *x, void *r,
+                 void *g);
+int rla_ihs_errors(rla_ctx *ctx, rla_ihs *h, double *full_residual, double *ls_gradient);
+int rla_ihs_solve(rla_ctx *ctx, rla_ihs *h, const void *A, int64_t lda, const void *b, void *x, void *r,
+                  void *g, int64_t max_it, int64_t collection_rate, double threshold, int error_kind,
+                  double *hist, int64_t hist_len, int64_t *iterations, int *converged);
+/* Device workspaces of the solver (owned by it): compressed_mat (s x n, ld s, the element
+ * type; the last S*A), update (n; the last u), R_equilibrated (n x n FP64, upper triangle; the
+ * Cholesky factor of D (SA)'(SA) D) and d (n FP64; D = diag(d)), so R = R_equilibrated D^-1. */
+int rla_ihs_workspace(const rla_ihs *h, void **compressed_mat, void **update, double **R_equilibrated,
+                      double **d);
+int rla_ihs_destroy(rla_ihs *h);
+
 /* ---- serving loop ------------------------------------------------------------------------ */
 /* No reference counterpart (the reference is a library of one-call functions).  Mixed
  * requests -- sketch-and-solve least squares (SparseSign Left, s = min(4n, m), nnz = 8) and

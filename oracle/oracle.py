@@ -507,3 +507,72 @@ def randsvd_mul_right(C, A, R: RandSVDResult, alpha, beta, bs):
         buf = alpha * (A[r0:r1, :] @ R.U)
         buf *= R.S[None, :]
         C[r0:r1, :] = buf @ R.V.T + beta * C[r0:r1, :]
+
+
+# ----------------------------------------------------------------------------------
+# Solvers: IHS (src/Solvers/ihs.jl), BasicLogger (src/Solvers/Loggers/basic_logger.jl),
+# FullResidual / LSGradient (src/Solvers/ErrorMethods/*.jl)
+# ----------------------------------------------------------------------------------
+@dataclass
+class IHSResult:
+    x: np.ndarray
+    residual_vec: np.ndarray
+    gradient_vec: np.ndarray
+    hist: np.ndarray
+    iteration: int
+    converged: bool
+    errors: list
+
+
+def ihs_rsolve(A: np.ndarray, b: np.ndarray, x0: np.ndarray, sketches, alpha: float = 1.0, max_it: int = 0,
+               threshold: float = 0.0, collection_rate: int = 1, error: str = "full") -> IHSResult:
+    """rsolve!(::IHSRecipe, x, A, b) (ihs.jl:214-254) with a BasicLogger (threshold_stop,
+    basic_logger.jl:84-130) in float64.  ``sketches(i)`` returns the Left compressor recipe
+    drawn by update_compressor! in iteration i (1-based).  R comes from Householder QR of
+    the sketched matrix (LAPACK geqrf, as qr!), the two solves are triangular solves.
+    ``error``: "full" = FullResidual (||b - Ax||), "gradient" = ||A'r|| of the maintained
+    residual (LSGradient)."""
+    A = A.astype(np.float64)
+    b = b.astype(np.float64)
+    x = x0.astype(np.float64).copy()
+    m, n = A.shape
+    hist = np.zeros(int(math.ceil(max_it / collection_rate)) + 1 if max_it > 0 else 1)
+    rec, it, conv = 0, 0, False
+    errs = []
+    r = b - A @ x                                   # :219-220
+    g = np.zeros(n)
+    for i in range(1, max_it + 1):
+        g = A.T @ r                                 # :223
+        err = float(np.linalg.norm(b - A @ x)) if error == "full" else float(np.linalg.norm(A.T @ r))
+        errs.append(err)
+        it = i                                      # update_logger! (basic_logger.jl:84-101)
+        conv = (err < threshold) if i < max_it else True
+        if conv:
+            hist[rec] = err
+        elif i % collection_rate == 0:
+            hist[rec] = err
+            rec += 1
+        if conv:
+            break
+        S = _as_f64(sketches(i))                    # :231
+        SA = np.zeros((S.n_rows, n))
+        mul_SA(SA, S, A)                            # :236
+        R = np.linalg.qr(SA, mode="r")              # :239
+        y = _solve_tri(R.T, g, lower=True)          # :241
+        u = _solve_tri(R, y, lower=False)           # :243
+        x += alpha * u                              # :246
+        r -= A @ u                                  # :249 (by A*u, not alpha*A*u)
+    return IHSResult(x, r, g, hist, it, conv, errs)
+
+
+def _solve_tri(T: np.ndarray, v: np.ndarray, lower: bool) -> np.ndarray:
+    """ldiv! with a triangular matrix (plain substitution, float64)."""
+    n = T.shape[0]
+    out = np.zeros(n)
+    rng = range(n) if lower else range(n - 1, -1, -1)
+    for i in rng:
+        if lower:
+            out[i] = (v[i] - T[i, :i] @ out[:i]) / T[i, i]
+        else:
+            out[i] = (v[i] - T[i, i + 1:] @ out[i + 1:]) / T[i, i]
+    return out

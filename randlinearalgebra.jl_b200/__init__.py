@@ -14,5 +14,9 @@ from .approximators import (Approximator, RangeApproximator, ApproximatorRecipe,
                             complete_approximator, rapproximate_, rapproximate, RandSVDBatch)
 from ._lib import RLA_PREC_NATIVE, RLA_PREC_SPLIT_BF16, lib, Context
 from .serving import Server, sketch_solve
+from .solvers import (Solver, SolverRecipe, Logger, LoggerRecipe, SolverError, SolverErrorRecipe, BasicLogger,
+                      BasicLoggerRecipe, threshold_stop, complete_logger, update_logger_, reset_logger_, FullResidual,
+                      FullResidualRecipe, LSGradient, LSGradientRecipe, CompressedResidual, CompressedResidualRecipe,
+                      complete_error, compute_error, IHS, IHSRecipe, complete_solver, rsolve_)
 
 __version__ = "0.1.0"

@@ -100,6 +100,15 @@ SIGNATURES = {
     "rla_randsvd_batch_destroy": (ctypes.c_int, [vp]),
     "rla_randsvd_grouped": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(SvdProblem), ctypes.POINTER(RangeParams)]),
     "rla_sketch_solve": (ctypes.c_int, [vp, vp, i64, i64, vp, i64, vp, vp]),
+    "rla_ihs_create": (ctypes.c_int, [vp, vp, ctypes.c_int, i64, i64, ctypes.c_double, ctypes.POINTER(vp)]),
+    "rla_ihs_start": (ctypes.c_int, [vp, vp, vp, i64, vp, vp, vp, vp]),
+    "rla_ihs_step": (ctypes.c_int, [vp, vp, vp, i64, vp, vp, vp, vp]),
+    "rla_ihs_errors": (ctypes.c_int, [vp, vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+    "rla_ihs_solve": (ctypes.c_int, [vp, vp, vp, i64, vp, vp, vp, vp, i64, i64, ctypes.c_double, ctypes.c_int,
+                                     vp, i64, ctypes.POINTER(i64), ctypes.POINTER(ctypes.c_int)]),
+    "rla_ihs_workspace": (ctypes.c_int, [vp, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp),
+                                         ctypes.POINTER(vp)]),
+    "rla_ihs_destroy": (ctypes.c_int, [vp]),
     "rla_server_start": (ctypes.c_int, [ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]),
     "rla_server_submit": (ctypes.c_int, [vp, ctypes.POINTER(Request)]),
     "rla_server_poll": (ctypes.c_int, [vp, vp, vp, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
