@@ -556,6 +556,154 @@ def randsvd_arm(args):
 
 
 # --------------------------------------------------------------------------------------
+# IHS workload
+# --------------------------------------------------------------------------------------
+IHS_M, IHS_N = 2**18, 512
+IHS_METRIC = "IHS iterations/s (sketch, sketched Cholesky solve, fused residual/gradient pass)"
+# kernel launches of one IHS step at the default shape (ncu launch list, profiles/)
+IHS_LAUNCHES_PER_STEP = 28
+
+
+def ihs_arm(args):
+    """rsolve!(IHS) on A 2^18 x 512 Float32 ~ N(0,1), b = A x* + 1e-3 N(0,1), SparseSign Left
+    s = 4n = 2048, nnz = 8 (the largest least-squares request shape of the serving workload).
+    One step = one IHS iteration: update_compressor!, S*A, the sketched Cholesky solve, x += u,
+    and the fused pass r -= A u, ||b - Ax||, g = A'r."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    world, rank, local = dist_setup(args.gpus)
+    from __graft_entry__ import load_package
+    rla = load_package()
+    from randlinearalgebra_b200 import _lib as L
+    dev = torch.device("cuda", local if world > 1 else 0)
+    m, n = args.ihs_m, args.ihs_n
+    s = 4 * n
+    g = torch.Generator(device=dev)
+    g.manual_seed(6 + rank)
+    A = torch.randn(n, m, device=dev, generator=g, dtype=torch.float32).t()
+    xs = torch.randn(n, device=dev, generator=g, dtype=torch.float32)
+    b = A @ xs + 1e-3 * torch.randn(m, device=dev, generator=g, dtype=torch.float32)
+    x = torch.zeros(n, device=dev, dtype=torch.float32)
+    solver = rla.complete_solver(rla.IHS(compressor=rla.SparseSign(compression_dim=s, nnz=8, type=np.float32),
+                                         log=rla.BasicLogger(max_it=args.steps + args.warmup + 1)),
+                                 x, A, b, seed=6000 + rank)
+    ctx = L.Context.get(dev.index)
+    lib = L.lib()
+    stream = torch.cuda.current_stream(dev)
+    cargs = (ctx.handle, solver._h, A.data_ptr(), A.stride(1), b.data_ptr())
+    vecs = (x.data_ptr(), solver.residual_vec.data_ptr(), solver.gradient_vec.data_ptr())
+    L.check(lib.rla_ihs_start(*cargs, *vecs), ctx.handle)
+    for _ in range(args.warmup):
+        L.check(lib.rla_ihs_step(*cargs, *vecs), ctx.handle)
+    torch.cuda.synchronize()
+    lib.rla_ctx_set_timing(ctx.handle, 1)
+    for c in (1, 2):
+        lib.rla_ctx_kernel_time(ctx.handle, c, ctypes.byref(ctypes.c_double()), ctypes.byref(ctypes.c_int64()))
+    K = args.steps
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    props = torch.cuda.get_device_properties(dev)
+    clocks = ClockSampler(f"GPU-{props.uuid}" if getattr(props, "uuid", None) else dev.index)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    t0.record(stream)
+    for _ in range(K):
+        L.check(lib.rla_ihs_step(*cargs, *vecs), ctx.handle)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    barrier(world)
+    ms = allreduce_max(t0.elapsed_time(t1), world)
+    kt = {}
+    for c in (1, 2):
+        tot, cnt = ctypes.c_double(), ctypes.c_int64()
+        L.check(lib.rla_ctx_kernel_time(ctx.handle, c, ctypes.byref(tot), ctypes.byref(cnt)), ctx.handle)
+        kt[c] = (tot.value / max(cnt.value, 1), cnt.value)
+    lib.rla_ctx_set_timing(ctx.handle, 0)
+    ef, eg = solver._errors()
+    value = world * K / (ms / 1e3)
+    # least-squares optimality of the final iterate: ||A'(b - Ax)|| relative to ||A'b||
+    grad_rel = float(torch.linalg.vector_norm(A.t() @ (b - A @ x)) / torch.linalg.vector_norm(A.t() @ b))
+
+    # ---- end to end: host A, b in (pinned), x out, through rsolve_ ------------------------
+    A_h = torch.empty(n, m, dtype=torch.float32, pin_memory=True).t()
+    A_h.copy_(A)
+    b_h = b.cpu().pin_memory()
+    e2e_it = max(3, min(K, 10))
+    x_h = torch.zeros(n, dtype=torch.float32, pin_memory=True)
+    sol_h = rla.complete_solver(rla.IHS(compressor=rla.SparseSign(compression_dim=s, nnz=8, type=np.float32),
+                                        log=rla.BasicLogger(max_it=e2e_it)), x_h, A_h, b_h, seed=7000 + rank)
+    torch.cuda.synchronize()
+    barrier(world)
+    w0 = time.perf_counter()
+    rla.rsolve_(sol_h, x_h, A_h, b_h)
+    torch.cuda.synchronize()
+    e2e_s = allreduce_max(time.perf_counter() - w0, world)
+    e2e = {"value": round(world * e2e_it / e2e_s, 3), "unit": "iterations/s",
+           "h2d_bytes_per_step": round(4 * (m * n + m + n) / e2e_it), "d2h_bytes_per_step": round(4 * n / e2e_it + 24),
+           "ms_per_step": round(e2e_s * 1e3 / e2e_it, 3),
+           "note": f"one rsolve_ of {e2e_it} iterations from pinned host A, b, x (A copied once per solve)"}
+    del A_h
+    if rank != 0:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    peak, peak_kind = peaks()
+    pass_ms, pass_n = kt[1]
+    pass_bytes = 4 * (m * n + 3 * m + 2 * n)
+    achieved = pass_bytes / (pass_ms / 1e3) / 1e9
+    sk_ms, sk_n = kt[2]
+    sk_bytes = 4 * (m * n + s * n)
+    roofline = {"bound": "hbm", "kernel": "ihs_pass_kernel", "achieved": round(achieved, 2), "peak": peak,
+                "peak_source": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                "algorithmic_bytes_per_launch": pass_bytes, "avg_launch_ms": round(pass_ms, 4),
+                "launches_timed": pass_n}
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        cpu = ihs_cpu_sample(m, n, s)
+    line = {"metric": IHS_METRIC, "value": round(value, 3), "unit": "iterations/s", "n_gpus": world, "steps": K,
+            "warmup": args.warmup, "ms_per_step": round(ms / K, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (Gram, Cholesky and triangular solves f64)",
+            "data": "synthetic A ~ N(0,1), b = A x* + 1e-3 N(0,1), generated on device (seed 6+rank)",
+            "config": {"workload": f"ihs: A {m}x{n} f32, sparse_sign left s={s} nnz=8", "m": m, "n": n, "s": s,
+                       "parallelism": f"replicas x{world}", "l2": f"A is {4 * m * n / 1e9:.2f} GB (larger than L2)"},
+            "roofline": roofline,
+            "kernels": {"ihs_pass": {"ms": round(pass_ms, 4), "gbs": round(achieved, 1),
+                                     "frac": round(achieved / peak, 4)},
+                        "sketch_apply": {"ms": round(sk_ms, 4), "gbs": round(sk_bytes / (sk_ms / 1e3) / 1e9, 1),
+                                         "frac": round(sk_bytes / (sk_ms / 1e3) / 1e9 / peak, 4)}},
+            "solution": {"full_residual": ef, "ls_gradient": eg, "rel_normal_eq_residual": grad_rel},
+            "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": IHS_LAUNCHES_PER_STEP * K}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def ihs_cpu_sample(m, n, s, iters=2):
+    """The oracle's rsolve! (float64 numpy + the C SparseSign loop, 1 thread for the sparse
+    product, all cores for numpy BLAS/LAPACK) for `iters` iterations of the same shape."""
+    import numpy as np
+
+    from __graft_entry__ import load_oracle
+    orc = load_oracle()
+    rng = np.random.default_rng(6)
+    A = np.asfortranarray(rng.standard_normal((m, n), dtype=np.float32))
+    b = (A @ rng.standard_normal(n).astype(np.float32)).astype(np.float32)
+    sk = [orc.draw_sparse_sign(rng, "left", s, m, 8, dtype=np.float32) for _ in range(iters)]
+    t0 = time.perf_counter()
+    orc.ihs_rsolve(A, b, np.zeros(n, np.float32), lambda i: sk[i - 1], max_it=iters + 1, threshold=-1.0)
+    dt = time.perf_counter() - t0
+    return {"value": round(iters / dt, 4), "unit": "iterations/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"{iters} iterations of the oracle's rsolve! on the same {m}x{n} shape (float64 numpy "
+                      "BLAS/LAPACK on all cores, single-threaded C SparseSign product)"}
+
+
+# --------------------------------------------------------------------------------------
 # Batched RandSVD workload
 # --------------------------------------------------------------------------------------
 BT_COUNT = 512
@@ -872,7 +1020,7 @@ def main():
     ap.add_argument("--cols", type=int, default=NCOL,
                     help="columns of A (default 512, the benchmark workload; smaller values make small "
                          "cases of the same kernels for profiler captures)")
-    ap.add_argument("--workload", choices=["sketch", "randsvd", "batched", "serve"], default="sketch",
+    ap.add_argument("--workload", choices=["sketch", "randsvd", "batched", "serve", "ihs"], default="sketch",
                     help="sketch: SRHT + CountSketch apply (default); randsvd: mixed-precision RandSVD; "
                          "batched: 512 uneven RandSVD instances")
     ap.add_argument("--batch-count", type=int, default=BT_COUNT, help="instances of the batched workload")
@@ -882,6 +1030,8 @@ def main():
     ap.add_argument("--serve-rates", default="2000,5000,10000,20000", help="serving workload: arrival rates (req/s)")
     ap.add_argument("--serve-mix", type=float, default=None,
                     help="serving diagnostics: fraction of LS requests (prints per-type capacity only)")
+    ap.add_argument("--ihs-m", type=int, default=IHS_M, help="IHS rows (default 2^18)")
+    ap.add_argument("--ihs-n", type=int, default=IHS_N, help="IHS columns (default 512; s = 4n)")
     ap.add_argument("--rs-m", type=int, default=RS_M, help="RandSVD rows (default 65536; smaller for profiler cases)")
     ap.add_argument("--rs-n", type=int, default=RS_N, help="RandSVD columns (default 8192)")
     args = ap.parse_args()
@@ -904,6 +1054,13 @@ def main():
                               "for the sketch and randsvd workloads only"}), flush=True)
         else:
             batched_arm(args)
+    elif args.workload == "ihs":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "ihs workload: the reference arm is timed "
+                              "for the sketch and randsvd workloads only (the CPU restatement is in cpu_baseline)"}),
+                  flush=True)
+        else:
+            ihs_arm(args)
     elif args.workload == "randsvd":
         if args.impl == "reference":
             randsvd_reference_arm(args)

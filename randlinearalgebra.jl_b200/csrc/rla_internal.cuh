@@ -45,7 +45,8 @@ struct rla_ctx {
     cudaMemPool_t pool = nullptr;  // context-owned stream-ordered pool, keeps freed memory mapped
     int *tc_status = nullptr;  // non-zero after a tensor-core kernel's bounded wait ran out
     bool timing = false;       // record CUDA events around timed kernel classes
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> timed[1];  // class 0: tensor-core GEMM
+    // classes: 0 tensor-core GEMM, 1 IHS fused pass over A, 2 IHS compressor apply
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> timed[3];
 };
 
 namespace rla {
@@ -247,6 +248,24 @@ struct Split {
     // first segment uses slot 2g, its last (when it started in an earlier segment) 2g+1.
     __host__ __device__ int slot(int g, int64_t vbeg) const { return 2 * g + (start(g) < vbeg ? 1 : 0); }
 };
+
+
+// CUDA events around a timed launch (rla_ctx_set_timing); no-ops while timing is off.
+inline cudaEvent_t timing_begin(rla_ctx *ctx) {
+    cudaEvent_t e0 = nullptr;
+    if (ctx->timing && cudaEventCreate(&e0) == cudaSuccess) cudaEventRecord(e0, ctx->stream);
+    return e0;
+}
+inline void timing_end(rla_ctx *ctx, int cls, cudaEvent_t e0) {
+    if (!e0) return;
+    cudaEvent_t e1 = nullptr;
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return;
+    }
+    cudaEventRecord(e1, ctx->stream);
+    ctx->timed[cls].emplace_back(e0, e1);
+}
 
 }  // namespace rla
 

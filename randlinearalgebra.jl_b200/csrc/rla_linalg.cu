@@ -512,7 +512,155 @@ int householder_q(rla_ctx *ctx, T *Y, int64_t m, int64_t l, int64_t ldy, double 
 template int householder_q<float>(rla_ctx *, float *, int64_t, int64_t, int64_t, double *);
 template int householder_q<double>(rla_ctx *, double *, int64_t, int64_t, int64_t, double *);
 
+// ---- multi-CTA blocked right-looking Cholesky (l >= MC_MIN) ------------------------------
+// Panel step p (MB columns): chol_panel_kernel factors the diagonal block in every CTA
+// (redundantly; CTA 0 writes it back) and solves R_pp' X = G(p:p+pb, cols) for the CTA's
+// 256 columns of the panel rows (one thread per column), zeroing the mirrored lower entries
+// G(cols, p:p+pb); chol_syrk_kernel then updates the trailing upper triangle,
+// G(I, J) -= R(p, I)' R(p, J), in 64 x 64 tiles (I <= J) spread over the GPU.
+constexpr int MB = 64, MC_MIN = 128, MP_THREADS = 256;
+
+// Upper Cholesky of the pb x pb block D into R (both ld MB+1), one barrier per step: step t
+// reads row t of the trailing block, writes row t of R and updates rows > t.
+__device__ void chol_diag_block(double (*D)[MB + 1], double (*R)[MB + 1], int pb, int *bad) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int t = 0; t < pb; ++t) {
+        double v = D[t][t];
+        if (!(v > 0.0) || !isfinite(v)) {
+            if (tid == 0) *bad = 1;
+            v = 1.0;
+        }
+        const double piv = sqrt(v), rp = 1.0 / piv;
+        const int w = pb - t;  // trailing width including t
+        for (int e = tid; e < w; e += nt) {
+            const int c = t + e;
+            R[t][c] = c == t ? piv : D[t][c] * rp;
+        }
+        // (a, c) with t < a <= c < pb
+        const int m1 = w - 1;
+        for (int e = tid; e < m1 * m1; e += nt) {
+            const int a = t + 1 + e / m1, c = t + 1 + e % m1;
+            if (a <= c) D[a][c] -= D[t][a] * D[t][c] * rp * rp;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(MP_THREADS) chol_panel_kernel(double *G, int64_t l, int64_t p, double shift,
+                                                                int *breakdown) {
+    extern __shared__ double mc_sm[];
+    double(*D)[MB + 1] = reinterpret_cast<double(*)[MB + 1]>(mc_sm);
+    double(*R)[MB + 1] = reinterpret_cast<double(*)[MB + 1]>(mc_sm + MB * (MB + 1));
+    __shared__ int bad;
+    const int tid = threadIdx.x;
+    const int pb = (int)min((int64_t)MB, l - p);
+    if (tid == 0) bad = 0;
+    for (int e = tid; e < MB * MB; e += blockDim.x) {
+        const int r = e % MB, c = e / MB;
+        double v = 0.0;
+        if (r < pb && c < pb && r <= c) v = G[(p + r) + (p + c) * l] + (r == c ? shift : 0.0);
+        D[r][c] = v;
+        R[r][c] = 0.0;
+    }
+    __syncthreads();
+    chol_diag_block(D, R, pb, &bad);
+    if (blockIdx.x == 0) {
+        for (int e = tid; e < pb * pb; e += blockDim.x) {
+            const int r = e % pb, c = e / pb;
+            G[(p + r) + (p + c) * l] = r <= c ? R[r][c] : 0.0;
+        }
+        if (tid == 0 && bad) *breakdown = 1;
+    }
+    // panel rows: thread = one column of the trailing part
+    const int64_t c0 = p + pb;
+    const int64_t col = c0 + (int64_t)blockIdx.x * MP_THREADS + tid;
+    if (col >= l) return;
+    double y[MB];
+#pragma unroll
+    for (int t = 0; t < MB; ++t) y[t] = t < pb ? G[(p + t) + col * l] : 0.0;
+#pragma unroll
+    for (int t = 0; t < MB; ++t) {
+        if (t < pb) {
+            double acc = y[t];
+#pragma unroll
+            for (int q = 0; q < t; ++q) acc -= R[q][t] * y[q];
+            y[t] = acc / R[t][t];
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < MB; ++t)
+        if (t < pb) {
+            G[(p + t) + col * l] = y[t];
+            G[col + (p + t) * l] = 0.0;
+        }
+}
+
+__global__ void __launch_bounds__(256) chol_syrk_kernel(double *G, int64_t l, int64_t p, int pb) {
+    extern __shared__ double mc_sm[];
+    double(*As)[MB + 1] = reinterpret_cast<double(*)[MB + 1]>(mc_sm);
+    double(*Bs)[MB + 1] = reinterpret_cast<double(*)[MB + 1]>(mc_sm + MB * (MB + 1));
+    // tile (ti, tj), ti <= tj, from the linear index over the upper triangle (by columns)
+    int idx = blockIdx.x, tj = 0;
+    while (idx >= tj + 1) {
+        idx -= tj + 1;
+        ++tj;
+    }
+    const int ti = idx;
+    const int64_t c0 = p + pb, I0 = c0 + (int64_t)ti * MB, J0 = c0 + (int64_t)tj * MB;
+    const int tid = threadIdx.x;
+    for (int e = tid; e < MB * MB; e += blockDim.x) {
+        const int t = e % MB, i = e / MB;
+        As[t][i] = (t < pb && I0 + i < l) ? G[(p + t) + (I0 + i) * l] : 0.0;
+        Bs[t][i] = (t < pb && J0 + i < l) ? G[(p + t) + (J0 + i) * l] : 0.0;
+    }
+    __syncthreads();
+    const int tx = tid & 15, ty = tid >> 4;  // outputs (4tx + ii, 4ty + jj)
+    double acc[4][4];
+#pragma unroll
+    for (int ii = 0; ii < 4; ++ii)
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) acc[ii][jj] = 0.0;
+    for (int t = 0; t < pb; ++t) {
+        double a[4], b[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            a[q] = As[t][4 * tx + q];
+            b[q] = Bs[t][4 * ty + q];
+        }
+#pragma unroll
+        for (int ii = 0; ii < 4; ++ii)
+#pragma unroll
+            for (int jj = 0; jj < 4; ++jj) acc[ii][jj] = fma(a[ii], b[jj], acc[ii][jj]);
+    }
+#pragma unroll
+    for (int ii = 0; ii < 4; ++ii)
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) {
+            const int64_t r = I0 + 4 * tx + ii, c = J0 + 4 * ty + jj;
+            if (r < l && c < l) G[r + c * l] -= acc[ii][jj];
+        }
+}
+
+static int cholesky_upper_mc(rla_ctx *ctx, double *G, int64_t l, double shift, int *breakdown) {
+    RLA_CUDA_TRY(ctx, cudaMemsetAsync(breakdown, 0, sizeof(int), ctx->stream));
+    const size_t smem = sizeof(double) * 2 * MB * (MB + 1);
+    RLA_CUDA_TRY(ctx, set_smem_max(chol_panel_kernel));
+    RLA_CUDA_TRY(ctx, set_smem_max(chol_syrk_kernel));
+    for (int64_t p = 0; p < l; p += MB) {
+        const int pb = (int)std::min<int64_t>(MB, l - p);
+        const int64_t rest = l - p - pb;
+        const unsigned gp = (unsigned)std::max<int64_t>(1, ceil_div(rest, MP_THREADS));
+        chol_panel_kernel<<<gp, MP_THREADS, smem, ctx->stream>>>(G, l, p, shift, breakdown);
+        if (rest > 0) {
+            const int T = (int)ceil_div(rest, MB);
+            chol_syrk_kernel<<<(unsigned)(T * (T + 1) / 2), 256, smem, ctx->stream>>>(G, l, p, pb);
+        }
+    }
+    return check_launch(ctx, "chol_multi_cta");
+}
+
 int cholesky_upper(rla_ctx *ctx, double *G, int64_t l, double shift, int *breakdown) {
+    if (l >= MC_MIN) return cholesky_upper_mc(ctx, G, l, shift, breakdown);
     if (l <= CB_MAXL) {
         // panel rows padded so every 4-entry group is a whole 16-byte pair
         const int ldp = (int)(ceil_div(std::max<int64_t>(l, 1), 4) * 4 + 4);

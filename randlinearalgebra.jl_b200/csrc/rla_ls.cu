@@ -42,12 +42,13 @@ __global__ void ls_gemv_t_kernel(const float *X, int64_t rows, int64_t n, int64_
 }
 
 // With R upper (l x l): y = R^-T (d .* c), z = R^-1 y, x = d .* z.  Blocked by 32: warp 0
-// solves a 32 x 32 diagonal triangle with shuffles (the block's entries in registers), then
-// all threads apply the block to the rest of the vector; two barriers per block.  One CTA;
-// the vector in shared memory.
+// solves a 32 x 32 diagonal triangle with shuffles, its lane holding the block's column
+// (forward) or row (backward) of R in registers with the pivot reciprocal, so the serial
+// steps wait on no memory; then all threads apply the block to the rest of the vector.  Two
+// barriers per block.  One CTA; the vector in shared memory.
 template <class TX>
-__global__ void __launch_bounds__(1024) ls_trisolve_kernel(const double *R, int64_t l, const double *d,
-                                                          const double *c, TX *x) {
+__global__ void __launch_bounds__(512) ls_trisolve_kernel(const double *R, int64_t l, const double *d,
+                                                         const double *c, TX *x) {
     extern __shared__ double v[];
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
     for (int64_t i = tid; i < l; i += nt) v[i] = d[i] * c[i];
@@ -56,19 +57,27 @@ __global__ void __launch_bounds__(1024) ls_trisolve_kernel(const double *R, int6
     for (int64_t b = 0; b < l; b += 32) {
         const int nb = (int)min((int64_t)32, l - b);
         if (warp == 0) {
+            double col[32];  // col[t] = R(b+t, b+lane) = R'(b+lane, b+t)
+#pragma unroll
+            for (int t = 0; t < 32; ++t) col[t] = (t < nb && lane < nb) ? R[(b + t) + (b + lane) * l] : 1.0;
+            const double rinv = 1.0 / (lane < nb ? R[(b + lane) + (b + lane) * l] : 1.0);
             double yv = lane < nb ? v[b + lane] : 0.0;
-            for (int t = 0; t < nb; ++t) {
-                const double yt = __shfl_sync(FULL, yv, t) / R[(b + t) + (b + t) * l];
-                if (lane == t) yv = yt;
-                if (lane > t && lane < nb) yv -= yt * R[(b + t) + (b + lane) * l];
+#pragma unroll
+            for (int t = 0; t < 32; ++t) {
+                if (t < nb) {
+                    if (lane == t) yv *= rinv;
+                    const double yt = __shfl_sync(FULL, yv, t);
+                    if (lane > t) yv -= yt * col[t];
+                }
             }
             if (lane < nb) v[b + lane] = yv;
         }
         __syncthreads();
         // v(j) -= sum_{t in block} R(b+t, j) y(b+t) for j >= b+nb
         for (int64_t j = b + nb + tid; j < l; j += nt) {
+            const double *rj = R + b + j * l;
             double acc = 0.0;
-            for (int t = 0; t < nb; ++t) acc += R[(b + t) + j * l] * v[b + t];
+            for (int t = 0; t < nb; ++t) acc += rj[t] * v[b + t];
             v[j] -= acc;
         }
         __syncthreads();
@@ -78,11 +87,18 @@ __global__ void __launch_bounds__(1024) ls_trisolve_kernel(const double *R, int6
         const int nb = (int)min((int64_t)32, e);
         const int64_t b = e - nb;
         if (warp == 0) {
+            double row[32];  // row[t] = R(b+lane, b+t)
+#pragma unroll
+            for (int t = 0; t < 32; ++t) row[t] = (t < nb && lane < nb) ? R[(b + lane) + (b + t) * l] : 1.0;
+            const double rinv = 1.0 / (lane < nb ? R[(b + lane) + (b + lane) * l] : 1.0);
             double zv = lane < nb ? v[b + lane] : 0.0;
-            for (int t = nb - 1; t >= 0; --t) {
-                const double zt = __shfl_sync(FULL, zv, t) / R[(b + t) + (b + t) * l];
-                if (lane == t) zv = zt;
-                if (lane < t) zv -= zt * R[(b + lane) + (b + t) * l];
+#pragma unroll
+            for (int t = 31; t >= 0; --t) {
+                if (t < nb) {
+                    if (lane == t) zv *= rinv;
+                    const double zt = __shfl_sync(FULL, zv, t);
+                    if (lane < t) zv -= zt * row[t];
+                }
             }
             if (lane < nb) v[b + lane] = zv;
         }
@@ -133,7 +149,7 @@ int ls_sketch_solve(rla_ctx *ctx, const rla_sketch *S, int64_t m, int64_t n, con
     const size_t smem = sizeof(double) * (size_t)n;
     if (smem > 48 * 1024)
         RLA_CUDA_TRY(ctx, set_smem_max(ls_trisolve_kernel<float>));
-    ls_trisolve_kernel<float><<<1, 1024, smem, ctx->stream>>>(G, n, tmp, c, x);
+    ls_trisolve_kernel<float><<<1, 512, smem, ctx->stream>>>(G, n, tmp, c, x);
     RLA_TRY(check_launch(ctx, "ls_trisolve"));
     *bad_out = bad;
     return RLA_OK;
@@ -353,7 +369,9 @@ template <class T, int WARPS>
 static int ihs_pass_fused(rla_ctx *ctx, rla_ihs *h, const T *A, int64_t lda, T *r, const T *u, const T *x,
                           const T *b) {
     auto go = [&](auto kern) {
+        cudaEvent_t e0 = timing_begin(ctx);
         kern<<<h->nblk, WARPS * 32, 0, ctx->stream>>>(A, lda, h->m, (int)h->n, r, u, x, b, h->g_part, h->e_part);
+        timing_end(ctx, 1, e0);
     };
     switch (h->cpw) {
     case 1: go(ihs_pass_kernel<T, WARPS, 1>); break;
@@ -403,7 +421,9 @@ static int ihs_step_t(rla_ctx *ctx, rla_ihs *h, const T *A, int64_t lda, const T
     // update_compressor! (ihs.jl:231) and mat_view = S*A (:236)
     RLA_TRY(rla_sketch_update(ctx, h->S));
     T *SA = (T *)h->SA;
+    cudaEvent_t e0 = timing_begin(ctx);
     RLA_TRY(sketch_mul_impl(ctx, h->S, RLA_SIDE_LEFT, 0, s, n, SA, s, 0, h->m, n, A, lda, 0, 1.0, 0.0));
+    timing_end(ctx, 2, e0);
     // R'R = (SA)'(SA) (ihs.jl:239), equilibrated: D G D = R'R
     RLA_TRY(gram_fp64<T>(ctx, SA, s, n, s, h->G));
     ls_diag_kernel<<<ceil_div_i(n, 256), 256, 0, ctx->stream>>>(h->G, n, h->d);
@@ -414,7 +434,7 @@ static int ihs_step_t(rla_ctx *ctx, rla_ihs *h, const T *A, int64_t lda, const T
     const size_t smem = sizeof(double) * (size_t)n;
     if (smem > 48 * 1024) RLA_CUDA_TRY(ctx, set_smem_max(ls_trisolve_kernel<T>));
     T *u = (T *)h->u;
-    ls_trisolve_kernel<T><<<1, 1024, smem, ctx->stream>>>(h->G, n, h->d, h->gd, u);
+    ls_trisolve_kernel<T><<<1, 512, smem, ctx->stream>>>(h->G, n, h->d, h->gd, u);
     ihs_axpy_kernel<T><<<ceil_div_i(n, 256), 256, 0, ctx->stream>>>(n, h->alpha, u, x);
     RLA_TRY(check_launch(ctx, "ihs_solve"));
     // r -= A*u (:249) with the next iteration's error and gradient
