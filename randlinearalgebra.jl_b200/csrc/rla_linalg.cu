@@ -520,50 +520,74 @@ template int householder_q<double>(rla_ctx *, double *, int64_t, int64_t, int64_
 // G(I, J) -= R(p, I)' R(p, J), in 64 x 64 tiles (I <= J) spread over the GPU.
 constexpr int MB = 64, MC_MIN = 128, MP_THREADS = 256;
 
-// Upper Cholesky of the pb x pb block D into R (both ld MB+1), one barrier per step: step t
-// reads row t of the trailing block, writes row t of R and updates rows > t.
-__device__ void chol_diag_block(double (*D)[MB + 1], double (*R)[MB + 1], int pb, int *bad) {
-    const int tid = threadIdx.x, nt = blockDim.x;
+// Upper Cholesky of the diagonal block G(p:p+pb, p:p+pb) (+ shift on its diagonal) into R
+// (shared, ld MB+2, rows t < pb, zero below the diagonal) and rinv[t] = 1/R(t,t).  The 256
+// threads form a 16 x 16 grid; thread (ty, tx) keeps the block's entries (4ty+i, 4tx+j) in
+// registers.  Step t: the owners of row t publish it in a double-buffered shared row, then
+// every thread applies the rank-1 update to its entries -- one barrier per step.
+__device__ void chol_diag_block(const double *G, int64_t l, int64_t p, int pb, double shift, double (*R)[MB + 2],
+                                double *rinv, double *rowbuf, int *bad) {
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    double d[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int r = 4 * ty + i, c = 4 * tx + j;
+            double v = 0.0;
+            if (r < pb && c < pb && r <= c) v = G[(p + r) + (p + c) * l] + (r == c ? shift : 0.0);
+            d[i][j] = v;
+        }
     for (int t = 0; t < pb; ++t) {
-        double v = D[t][t];
+        double *buf = rowbuf + (t & 1) * MB;
+        if (ty == (t >> 2)) {
+            const int i = t & 3;
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                buf[4 * tx + j] = i == 0 ? d[0][j] : i == 1 ? d[1][j] : i == 2 ? d[2][j] : d[3][j];
+        }
+        __syncthreads();
+        double v = buf[t];
         if (!(v > 0.0) || !isfinite(v)) {
             if (tid == 0) *bad = 1;
             v = 1.0;
         }
-        const double piv = sqrt(v), rp = 1.0 / piv;
-        const int w = pb - t;  // trailing width including t
-        for (int e = tid; e < w; e += nt) {
-            const int c = t + e;
-            R[t][c] = c == t ? piv : D[t][c] * rp;
+        const double piv = sqrt(v), rp = 1.0 / piv, rp2 = rp * rp;
+        if (tid < MB) {
+            const int c = tid;
+            if (c >= t && c < pb) R[t][c] = c == t ? piv : buf[c] * rp;
+            if (c == t) rinv[t] = rp;
         }
-        // (a, c) with t < a <= c < pb
-        const int m1 = w - 1;
-        for (int e = tid; e < m1 * m1; e += nt) {
-            const int a = t + 1 + e / m1, c = t + 1 + e % m1;
-            if (a <= c) D[a][c] -= D[t][a] * D[t][c] * rp * rp;
+        double ba[4], bc[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            ba[q] = buf[4 * ty + q] * rp2;
+            bc[q] = buf[4 * tx + q];
         }
-        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int a = 4 * ty + i, c = 4 * tx + j;
+                if (t < a && a <= c) d[i][j] -= ba[i] * bc[j];
+            }
     }
+    __syncthreads();
 }
 
 __global__ void __launch_bounds__(MP_THREADS) chol_panel_kernel(double *G, int64_t l, int64_t p, double shift,
                                                                 int *breakdown) {
     extern __shared__ double mc_sm[];
-    double(*D)[MB + 1] = reinterpret_cast<double(*)[MB + 1]>(mc_sm);
-    double(*R)[MB + 1] = reinterpret_cast<double(*)[MB + 1]>(mc_sm + MB * (MB + 1));
+    double(*R)[MB + 2] = reinterpret_cast<double(*)[MB + 2]>(mc_sm);
+    double *rinv = mc_sm + MB * (MB + 2);
+    double *rowbuf = rinv + MB;
     __shared__ int bad;
     const int tid = threadIdx.x;
     const int pb = (int)min((int64_t)MB, l - p);
     if (tid == 0) bad = 0;
-    for (int e = tid; e < MB * MB; e += blockDim.x) {
-        const int r = e % MB, c = e / MB;
-        double v = 0.0;
-        if (r < pb && c < pb && r <= c) v = G[(p + r) + (p + c) * l] + (r == c ? shift : 0.0);
-        D[r][c] = v;
-        R[r][c] = 0.0;
-    }
+    for (int e = tid; e < MB * (MB + 2); e += blockDim.x) (&R[0][0])[e] = 0.0;
     __syncthreads();
-    chol_diag_block(D, R, pb, &bad);
+    chol_diag_block(G, l, p, pb, shift, R, rinv, rowbuf, &bad);
     if (blockIdx.x == 0) {
         for (int e = tid; e < pb * pb; e += blockDim.x) {
             const int r = e % pb, c = e / pb;
@@ -571,7 +595,9 @@ __global__ void __launch_bounds__(MP_THREADS) chol_panel_kernel(double *G, int64
         }
         if (tid == 0 && bad) *breakdown = 1;
     }
-    // panel rows: thread = one column of the trailing part
+    // panel rows X = R_pp^-T G(p, cols): thread = one column of the trailing part, solved
+    // column-oriented (y_t = y_t / r_tt, then y_q -= r_tq y_t for q > t) so that the
+    // updates of one step are independent.
     const int64_t c0 = p + pb;
     const int64_t col = c0 + (int64_t)blockIdx.x * MP_THREADS + tid;
     if (col >= l) return;
@@ -581,10 +607,9 @@ __global__ void __launch_bounds__(MP_THREADS) chol_panel_kernel(double *G, int64
 #pragma unroll
     for (int t = 0; t < MB; ++t) {
         if (t < pb) {
-            double acc = y[t];
+            y[t] *= rinv[t];
 #pragma unroll
-            for (int q = 0; q < t; ++q) acc -= R[q][t] * y[q];
-            y[t] = acc / R[t][t];
+            for (int q = t + 1; q < MB; ++q) y[q] -= R[t][q] * y[t];
         }
     }
 #pragma unroll
@@ -644,13 +669,14 @@ __global__ void __launch_bounds__(256) chol_syrk_kernel(double *G, int64_t l, in
 static int cholesky_upper_mc(rla_ctx *ctx, double *G, int64_t l, double shift, int *breakdown) {
     RLA_CUDA_TRY(ctx, cudaMemsetAsync(breakdown, 0, sizeof(int), ctx->stream));
     const size_t smem = sizeof(double) * 2 * MB * (MB + 1);
+    const size_t smem_panel = sizeof(double) * (MB * (MB + 2) + 3 * MB);
     RLA_CUDA_TRY(ctx, set_smem_max(chol_panel_kernel));
     RLA_CUDA_TRY(ctx, set_smem_max(chol_syrk_kernel));
     for (int64_t p = 0; p < l; p += MB) {
         const int pb = (int)std::min<int64_t>(MB, l - p);
         const int64_t rest = l - p - pb;
         const unsigned gp = (unsigned)std::max<int64_t>(1, ceil_div(rest, MP_THREADS));
-        chol_panel_kernel<<<gp, MP_THREADS, smem, ctx->stream>>>(G, l, p, shift, breakdown);
+        chol_panel_kernel<<<gp, MP_THREADS, smem_panel, ctx->stream>>>(G, l, p, shift, breakdown);
         if (rest > 0) {
             const int T = (int)ceil_div(rest, MB);
             chol_syrk_kernel<<<(unsigned)(T * (T + 1) / 2), 256, smem, ctx->stream>>>(G, l, p, pb);

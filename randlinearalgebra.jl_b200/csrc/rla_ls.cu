@@ -44,11 +44,15 @@ __global__ void ls_gemv_t_kernel(const float *X, int64_t rows, int64_t n, int64_
 // With R upper (l x l): y = R^-T (d .* c), z = R^-1 y, x = d .* z.  Blocked by 32: warp 0
 // solves a 32 x 32 diagonal triangle with shuffles, its lane holding the block's column
 // (forward) or row (backward) of R in registers with the pivot reciprocal, so the serial
-// steps wait on no memory; then all threads apply the block to the rest of the vector.  Two
-// barriers per block.  One CTA; the vector in shared memory.
+// steps wait on no memory; then all threads apply the block to the rest of the vector.  The
+// R entries of a thread's first TS_PF update columns are loaded at the top of the block
+// step, together with warp 0's diagonal block, so one memory latency is paid per block.
+// Two barriers per block.  One CTA; the vector in shared memory.
+constexpr int TS_THREADS = 256, TS_PF = 2;
+
 template <class TX>
-__global__ void __launch_bounds__(512) ls_trisolve_kernel(const double *R, int64_t l, const double *d,
-                                                         const double *c, TX *x) {
+__global__ void __launch_bounds__(TS_THREADS) ls_trisolve_kernel(const double *R, int64_t l, const double *d,
+                                                                const double *c, TX *x) {
     extern __shared__ double v[];
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
     for (int64_t i = tid; i < l; i += nt) v[i] = d[i] * c[i];
@@ -56,6 +60,13 @@ __global__ void __launch_bounds__(512) ls_trisolve_kernel(const double *R, int64
     // forward: R' y = v, R' lower; block rows [b, b+32)
     for (int64_t b = 0; b < l; b += 32) {
         const int nb = (int)min((int64_t)32, l - b);
+        double pf[TS_PF][32];
+#pragma unroll
+        for (int k = 0; k < TS_PF; ++k) {
+            const int64_t j = b + nb + tid + (int64_t)k * nt;
+#pragma unroll
+            for (int t = 0; t < 32; ++t) pf[k][t] = (j < l && t < nb) ? R[(b + t) + j * l] : 0.0;
+        }
         if (warp == 0) {
             double col[32];  // col[t] = R(b+t, b+lane) = R'(b+lane, b+t)
 #pragma unroll
@@ -74,7 +85,17 @@ __global__ void __launch_bounds__(512) ls_trisolve_kernel(const double *R, int64
         }
         __syncthreads();
         // v(j) -= sum_{t in block} R(b+t, j) y(b+t) for j >= b+nb
-        for (int64_t j = b + nb + tid; j < l; j += nt) {
+#pragma unroll
+        for (int k = 0; k < TS_PF; ++k) {
+            const int64_t j = b + nb + tid + (int64_t)k * nt;
+            if (j < l) {
+                double acc = 0.0;
+#pragma unroll
+                for (int t = 0; t < 32; ++t) acc += pf[k][t] * v[b + min(t, nb - 1)];
+                v[j] -= acc;
+            }
+        }
+        for (int64_t j = b + nb + tid + (int64_t)TS_PF * nt; j < l; j += nt) {
             const double *rj = R + b + j * l;
             double acc = 0.0;
             for (int t = 0; t < nb; ++t) acc += rj[t] * v[b + t];
@@ -86,6 +107,13 @@ __global__ void __launch_bounds__(512) ls_trisolve_kernel(const double *R, int64
     for (int64_t e = l; e > 0; e -= 32) {
         const int nb = (int)min((int64_t)32, e);
         const int64_t b = e - nb;
+        double pf[TS_PF][32];
+#pragma unroll
+        for (int k = 0; k < TS_PF; ++k) {
+            const int64_t j = tid + (int64_t)k * nt;
+#pragma unroll
+            for (int t = 0; t < 32; ++t) pf[k][t] = (j < b && t < nb) ? R[j + (b + t) * l] : 0.0;
+        }
         if (warp == 0) {
             double row[32];  // row[t] = R(b+lane, b+t)
 #pragma unroll
@@ -104,7 +132,17 @@ __global__ void __launch_bounds__(512) ls_trisolve_kernel(const double *R, int64
         }
         __syncthreads();
         // v(j) -= sum_{t in block} R(j, b+t) z(b+t) for j < b
-        for (int64_t j = tid; j < b; j += nt) {
+#pragma unroll
+        for (int k = 0; k < TS_PF; ++k) {
+            const int64_t j = tid + (int64_t)k * nt;
+            if (j < b) {
+                double acc = 0.0;
+#pragma unroll
+                for (int t = 0; t < 32; ++t) acc += pf[k][t] * v[b + min(t, nb - 1)];
+                v[j] -= acc;
+            }
+        }
+        for (int64_t j = tid + (int64_t)TS_PF * nt; j < b; j += nt) {
             double acc = 0.0;
             for (int t = 0; t < nb; ++t) acc += R[j + (b + t) * l] * v[b + t];
             v[j] -= acc;
@@ -149,7 +187,7 @@ int ls_sketch_solve(rla_ctx *ctx, const rla_sketch *S, int64_t m, int64_t n, con
     const size_t smem = sizeof(double) * (size_t)n;
     if (smem > 48 * 1024)
         RLA_CUDA_TRY(ctx, set_smem_max(ls_trisolve_kernel<float>));
-    ls_trisolve_kernel<float><<<1, 512, smem, ctx->stream>>>(G, n, tmp, c, x);
+    ls_trisolve_kernel<float><<<1, TS_THREADS, smem, ctx->stream>>>(G, n, tmp, c, x);
     RLA_TRY(check_launch(ctx, "ls_trisolve"));
     *bad_out = bad;
     return RLA_OK;
@@ -361,6 +399,11 @@ struct rla_ihs {
     int *bad = nullptr;
     int ne = 0;
     double *hstat = nullptr;  // pinned host copy of stat
+    // update_compressor! runs on a private stream: building a sparse compressor's schedule
+    // waits on the host, and on the caller's stream that wait would drain the previous
+    // iteration's queued work.  ev_apply orders a redraw after the last S*A that read it.
+    rla_ctx *side = nullptr;
+    cudaEvent_t ev_apply = nullptr;
 };
 
 namespace rla {
@@ -412,6 +455,8 @@ template <class T>
 static int ihs_start_t(rla_ctx *ctx, rla_ihs *h, const T *A, int64_t lda, const T *b, const T *x, T *r, T *g) {
     RLA_CUDA_TRY(ctx, cudaMemcpyAsync(r, b, sizeof(T) * h->m, cudaMemcpyDeviceToDevice, ctx->stream));
     RLA_CUDA_TRY(ctx, cudaMemsetAsync(h->bad, 0, sizeof(int), ctx->stream));
+    // the first redraw waits for whatever the caller queued before the solve
+    RLA_CUDA_TRY(ctx, cudaEventRecord(h->ev_apply, ctx->stream));
     return ihs_pass<T>(ctx, h, A, lda, r, x, x, b, g);
 }
 
@@ -419,11 +464,13 @@ template <class T>
 static int ihs_step_t(rla_ctx *ctx, rla_ihs *h, const T *A, int64_t lda, const T *b, T *x, T *r, T *g) {
     const int64_t n = h->n, s = h->s;
     // update_compressor! (ihs.jl:231) and mat_view = S*A (:236)
-    RLA_TRY(rla_sketch_update(ctx, h->S));
+    RLA_CUDA_TRY(ctx, cudaStreamWaitEvent(h->side->stream, h->ev_apply, 0));
+    if (int rc = rla_sketch_update(h->side, h->S)) return set_error(ctx, rc, "%s", h->side->last_error.c_str());
     T *SA = (T *)h->SA;
     cudaEvent_t e0 = timing_begin(ctx);
     RLA_TRY(sketch_mul_impl(ctx, h->S, RLA_SIDE_LEFT, 0, s, n, SA, s, 0, h->m, n, A, lda, 0, 1.0, 0.0));
     timing_end(ctx, 2, e0);
+    RLA_CUDA_TRY(ctx, cudaEventRecord(h->ev_apply, ctx->stream));
     // R'R = (SA)'(SA) (ihs.jl:239), equilibrated: D G D = R'R
     RLA_TRY(gram_fp64<T>(ctx, SA, s, n, s, h->G));
     ls_diag_kernel<<<ceil_div_i(n, 256), 256, 0, ctx->stream>>>(h->G, n, h->d);
@@ -434,7 +481,7 @@ static int ihs_step_t(rla_ctx *ctx, rla_ihs *h, const T *A, int64_t lda, const T
     const size_t smem = sizeof(double) * (size_t)n;
     if (smem > 48 * 1024) RLA_CUDA_TRY(ctx, set_smem_max(ls_trisolve_kernel<T>));
     T *u = (T *)h->u;
-    ls_trisolve_kernel<T><<<1, 512, smem, ctx->stream>>>(h->G, n, h->d, h->gd, u);
+    ls_trisolve_kernel<T><<<1, TS_THREADS, smem, ctx->stream>>>(h->G, n, h->d, h->gd, u);
     ihs_axpy_kernel<T><<<ceil_div_i(n, 256), 256, 0, ctx->stream>>>(n, h->alpha, u, x);
     RLA_TRY(check_launch(ctx, "ihs_solve"));
     // r -= A*u (:249) with the next iteration's error and gradient
@@ -446,6 +493,8 @@ static void ihs_free(rla_ihs *h) {
     for (void *q : p)
         if (q) cudaFree(q);
     if (h->hstat) cudaFreeHost(h->hstat);
+    if (h->ev_apply) cudaEventDestroy(h->ev_apply);
+    if (h->side) rla_ctx_destroy(h->side);
 }
 
 }  // namespace rla
@@ -534,6 +583,8 @@ int rla_ihs_create(rla_ctx *ctx, rla_sketch *compressor, int dtype, int64_t m, i
     grab((void **)&h->stat, sizeof(double) * 4);
     grab((void **)&h->bad, sizeof(int));
     if (e == cudaSuccess) e = cudaMallocHost((void **)&h->hstat, sizeof(double) * 4);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_apply, cudaEventDisableTiming);
+    if (e == cudaSuccess && rla_ctx_create(ctx->device, nullptr, &h->side) != RLA_OK) e = cudaErrorUnknown;
     if (e == cudaSuccess) e = cudaMemsetAsync(h->bad, 0, sizeof(int), ctx->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(h->u, 0, (size_t)es * n, ctx->stream);
     if (e != cudaSuccess) {

@@ -146,6 +146,29 @@ __global__ void __launch_bounds__(SCHED_WARPS * 32) sparse_sched_kernel(const in
     }
 }
 
+// base[i] = sum_{k < i} nr[k] (exclusive scan of the per-tile extra-round counts), one CTA:
+// each thread sums a contiguous chunk, the chunk totals are scanned in shared memory.
+__global__ void __launch_bounds__(1024) sched_scan_kernel(const int32_t *nr, int64_t n, int64_t *base) {
+    __shared__ int64_t part[1024];
+    const int t = threadIdx.x, nt = blockDim.x;
+    const int64_t per = (n + nt - 1) / nt, lo = min(n, (int64_t)t * per), hi = min(n, lo + per);
+    int64_t sum = 0;
+    for (int64_t i = lo; i < hi; ++i) sum += nr[i];
+    part[t] = sum;
+    __syncthreads();
+    for (int off = 1; off < nt; off <<= 1) {
+        const int64_t v = t >= off ? part[t - off] : 0;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    int64_t run = part[t] - sum;
+    for (int64_t i = lo; i < hi; ++i) {
+        base[i] = run;
+        run += nr[i];
+    }
+}
+
 // CountSketch (nnz = 1, s <= 2^16): 512-element batches (4 tiles, 16 sub-rounds of 32
 // lanes).  An element is deferred when its bucket already occurred earlier in the batch,
 // in (sub-round, lane) order, so all non-deferred elements of a batch hit distinct bins and
@@ -439,6 +462,26 @@ static int build_meta(rla_ctx *ctx, rla_sketch *sk) {
     sparse_sched_kernel<0><<<blocks, SCHED_WARPS * 32, 0, ctx->stream>>>(sk->bucket, sk->negative, sk->L, (int)sk->nnz,
                                                                          sk->meta, nr, nullptr, nullptr, nullptr);
     RLA_TRY(check_launch(ctx, "sparse_sched(0)"));
+    if (ntile * MAX_XROUNDS < (int64_t(1) << 23)) {
+        // the schedule never needs more than MAX_XROUNDS rounds per tile: size `extra` for
+        // that once and scan the counts on the device, so a redraw waits on nothing
+        const int64_t cap = std::max<int64_t>(ntile * MAX_XROUNDS, 1);
+        if (sk->extra_rounds_cap < cap) {
+            if (sk->extra) RLA_CUDA_TRY(ctx, cudaFree(sk->extra));
+            sk->extra = nullptr;
+            RLA_CUDA_TRY(ctx, cudaMalloc(&sk->extra, sizeof(uint32_t) * 32 * cap));
+            sk->extra_rounds_cap = cap;
+        }
+        if (!sk->tile_flags) RLA_CUDA_TRY(ctx, cudaMalloc(&sk->tile_flags, sizeof(uint32_t) * std::max<int64_t>(ntile, 1)));
+        sched_scan_kernel<<<1, 1024, 0, ctx->stream>>>(nr, ntile, base);
+        RLA_TRY(check_launch(ctx, "sched_scan"));
+        sparse_sched_kernel<1><<<blocks, SCHED_WARPS * 32, 0, ctx->stream>>>(
+            sk->bucket, sk->negative, sk->L, (int)sk->nnz, sk->meta, nr, base, sk->tile_flags, sk->extra);
+        RLA_TRY(check_launch(ctx, "sparse_sched(1)"));
+        RLA_CUDA_TRY(ctx, cudaFreeAsync(nr, ctx->stream));
+        RLA_CUDA_TRY(ctx, cudaFreeAsync(base, ctx->stream));
+        return RLA_OK;
+    }
     std::vector<int32_t> hn(ntile);
     std::vector<int64_t> hb(ntile);
     RLA_CUDA_TRY(ctx, cudaMemcpyAsync(hn.data(), nr, sizeof(int32_t) * ntile, cudaMemcpyDeviceToHost, ctx->stream));
