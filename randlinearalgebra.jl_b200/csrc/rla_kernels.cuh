@@ -10,6 +10,9 @@ int sketch_mul_impl(rla_ctx *ctx, const rla_sketch *sk, int side, int trans_s, i
                     void *C, int64_t ldc, int trans_c, int64_t a_rows, int64_t a_cols, const void *A, int64_t lda,
                     int trans_a, double alpha, double beta);
 
+// update_compressor! ordered on ctx's stream, without waiting for it (rla_sketch.cu).
+int sketch_redraw_async(rla_ctx *ctx, rla_sketch *sk);
+
 // SparseSign / CountSketch (rla_sparse.cu).  Vectors of the input X: element (k, v) at
 // X[k*x_es + v*x_vs]; the output likewise.  Compress maps length-L vectors to length s,
 // expand maps length-s vectors to length L.

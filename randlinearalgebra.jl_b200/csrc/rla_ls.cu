@@ -237,12 +237,25 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
 #pragma unroll
         for (int k = 0; k < CPW; ++k) dst[k] = (rok && c0 + k < n) ? __ldcs(ap + (int64_t)k * lda) : T(0);
     };
+    // warp 0 also keeps the tile's r and b entries, prefetched one tile ahead like A
+    auto load_rb = [&](int64_t t, T &rv, T &bv) {
+        const int64_t row = t * 32 + lane;
+        rv = row < m ? r[row] : T(0);
+        bv = row < m ? b[row] : T(0);
+    };
     double e2 = 0.0;
+    T r_cur = T(0), b_cur = T(0), r_nx = T(0), b_nx = T(0);
     int64_t tile = blockIdx.x;
-    if (tile < ntiles) load(tile, a);
+    if (tile < ntiles) {
+        load(tile, a);
+        if (w == 0) load_rb(tile, r_cur, b_cur);
+    }
     for (; tile < ntiles; tile += gridDim.x) {
         const int64_t nxt = tile + gridDim.x;
-        if (nxt < ntiles) load(nxt, an);
+        if (nxt < ntiles) {
+            load(nxt, an);
+            if (w == 0) load_rb(nxt, r_nx, b_nx);
+        }
         T pu = T(0), px = T(0);
 #pragma unroll
         for (int k = 0; k < CPW; ++k) {
@@ -262,12 +275,14 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
             }
             T rv = T(0);
             if (row < m) {
-                rv = r[row] - au;
+                rv = r_cur - au;
                 r[row] = rv;
-                const double e = (double)b[row] - (double)ax;
+                const double e = (double)b_cur - (double)ax;
                 e2 += e * e;
             }
             rn[lane] = rv;
+            r_cur = r_nx;
+            b_cur = b_nx;
         }
         __syncthreads();
         const T rv = rn[lane];
@@ -399,11 +414,11 @@ struct rla_ihs {
     int *bad = nullptr;
     int ne = 0;
     double *hstat = nullptr;  // pinned host copy of stat
-    // update_compressor! runs on a private stream: building a sparse compressor's schedule
-    // waits on the host, and on the caller's stream that wait would drain the previous
-    // iteration's queued work.  ev_apply orders a redraw after the last S*A that read it.
+    // update_compressor! runs on a private stream, after the last S*A that read the draws
+    // (ev_apply) and before the next one (ev_draw), so it overlaps the previous iteration's
+    // tail and the host never waits for it.
     rla_ctx *side = nullptr;
-    cudaEvent_t ev_apply = nullptr;
+    cudaEvent_t ev_apply = nullptr, ev_draw = nullptr;
 };
 
 namespace rla {
@@ -465,7 +480,9 @@ static int ihs_step_t(rla_ctx *ctx, rla_ihs *h, const T *A, int64_t lda, const T
     const int64_t n = h->n, s = h->s;
     // update_compressor! (ihs.jl:231) and mat_view = S*A (:236)
     RLA_CUDA_TRY(ctx, cudaStreamWaitEvent(h->side->stream, h->ev_apply, 0));
-    if (int rc = rla_sketch_update(h->side, h->S)) return set_error(ctx, rc, "%s", h->side->last_error.c_str());
+    if (int rc = sketch_redraw_async(h->side, h->S)) return set_error(ctx, rc, "%s", h->side->last_error.c_str());
+    RLA_CUDA_TRY(ctx, cudaEventRecord(h->ev_draw, h->side->stream));
+    RLA_CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, h->ev_draw, 0));
     T *SA = (T *)h->SA;
     cudaEvent_t e0 = timing_begin(ctx);
     RLA_TRY(sketch_mul_impl(ctx, h->S, RLA_SIDE_LEFT, 0, s, n, SA, s, 0, h->m, n, A, lda, 0, 1.0, 0.0));
@@ -494,6 +511,7 @@ static void ihs_free(rla_ihs *h) {
         if (q) cudaFree(q);
     if (h->hstat) cudaFreeHost(h->hstat);
     if (h->ev_apply) cudaEventDestroy(h->ev_apply);
+    if (h->ev_draw) cudaEventDestroy(h->ev_draw);
     if (h->side) rla_ctx_destroy(h->side);
 }
 
@@ -584,6 +602,7 @@ int rla_ihs_create(rla_ctx *ctx, rla_sketch *compressor, int dtype, int64_t m, i
     grab((void **)&h->bad, sizeof(int));
     if (e == cudaSuccess) e = cudaMallocHost((void **)&h->hstat, sizeof(double) * 4);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_apply, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_draw, cudaEventDisableTiming);
     if (e == cudaSuccess && rla_ctx_create(ctx->device, nullptr, &h->side) != RLA_OK) e = cudaErrorUnknown;
     if (e == cudaSuccess) e = cudaMemsetAsync(h->bad, 0, sizeof(int), ctx->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(h->u, 0, (size_t)es * n, ctx->stream);

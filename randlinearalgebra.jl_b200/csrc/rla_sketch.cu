@@ -516,7 +516,7 @@ static Rng make_rng(const rla_sketch *sk) {
     return r;
 }
 
-static int draw(rla_ctx *ctx, rla_sketch *sk) {
+static int draw(rla_ctx *ctx, rla_sketch *sk, bool sync = true) {
     Rng rng = make_rng(sk);
     const int kind = sk->p.kind;
     if (kind == RLA_SPARSE_SIGN || kind == RLA_COUNT_SKETCH) {
@@ -564,8 +564,16 @@ static int draw(rla_ctx *ctx, rla_sketch *sk) {
                 rng, n, (double)sk->scale, (double *)sk->dense);
         RLA_TRY(check_launch(ctx, "draw_gaussian"));
     }
-    RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (sync) RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     return RLA_OK;
+}
+
+// update_compressor! without the final synchronisation: the new draws are complete when
+// the context's stream reaches this point.
+int sketch_redraw_async(rla_ctx *ctx, rla_sketch *sk) {
+    int rc = draw(ctx, sk, false);
+    if (rc == RLA_OK) sk->draw_count++;
+    return rc;
 }
 
 static void free_sketch_buffers(rla_sketch *sk) {
