@@ -58,6 +58,11 @@ extern "C" {
 #define RLA_SRHT 2           /* src/Compressors/srht.jl */
 #define RLA_FJLT 3           /* src/Compressors/fjlt.jl */
 #define RLA_GAUSSIAN 4       /* src/Compressors/gaussian.jl */
+#define RLA_SAMPLING 5       /* src/Compressors/sampling.jl (made by rla_sampling_create) */
+
+#define RLA_DIST_UNIFORM 0   /* src/Compressors/Distributions/uniform.jl */
+#define RLA_DIST_L2NORM 1    /* src/Compressors/Distributions/strohmer_vershynin.jl */
+#define RLA_DIST_AGMON 2     /* src/Compressors/Distributions/agmon.jl */
 
 #define RLA_SIDE_LEFT 0      /* C = alpha*op(S)*A + beta*C */
 #define RLA_SIDE_RIGHT 1     /* C = alpha*A*op(S) + beta*C */
@@ -129,6 +134,7 @@ int rla_sketch_get_info(const rla_sketch *sk, rla_sketch_info *out);
  *   SRHT         idx = op [compression_dim], signs = signs [padded] (1 = +1)
  *   FJLT         kptr = op.colptr, idx = op.rowval, vals = op.nzval, signs [padded]
  *   Gaussian     vals = op, column-major n_rows x n_cols
+ *   Sampling     idx = idx [compression_dim]
  * Pointers a kind does not use may be NULL. */
 int rla_sketch_get_draws(rla_ctx *ctx, const rla_sketch *sk, int64_t *idx, void *vals,
                          uint8_t *signs, int64_t *kptr);
@@ -136,6 +142,25 @@ int rla_sketch_get_draws(rla_ctx *ctx, const rla_sketch *sk, int64_t *idx, void 
  * For FJLT `k_nnz` is the number of stored entries of op; otherwise it is ignored. */
 int rla_sketch_set_draws(rla_ctx *ctx, rla_sketch *sk, const int64_t *idx, const void *vals,
                          const uint8_t *signs, const int64_t *kptr, int64_t k_nnz);
+
+/* complete_compressor(::Sampling, A) (src/Compressors/sampling.jl:98-121; constructor checks
+ * :50-61; Agmon's beta checks src/Compressors/Distributions/agmon.jl).  The recipe is an
+ * rla_sketch of kind RLA_SAMPLING: a selection of compression_dim indices of the long_dim
+ * rows (Left) or columns (Right); every rla_sketch_* call accepts it, and mul! gathers
+ * (compress) or scatter-adds (expand, repeated indices accumulate in order).  `replace`
+ * selects sampling with replacement; `beta` is Agmon's candidate count (compression_dim <=
+ * beta <= long_dim; compression_dim <= 1024).  Uniform draws at once; L2Norm and Agmon draw in
+ * rla_sampling_update. */
+int rla_sampling_create(rla_ctx *ctx, int card, int dtype, int64_t compression_dim, int64_t long_dim,
+                        int distribution, int replace, int64_t beta, uint64_t seed, rla_sketch **out);
+/* update_compressor!(S, x, A, b) for Sampling (sampling.jl:123-128): update_distribution!
+ * (L2Norm: squared row/column norms of A, strohmer_vershynin.jl; Agmon: x, A, b, agmon.jl)
+ * then sample_distribution!.  A (a_rows x a_cols, ld lda), x (x_len) and b (b_len) are device
+ * buffers of the recipe's element type; r (optional) is Agmon's precomputed residual.
+ * rla_sketch_update redraws Uniform and L2Norm (with the last weights) without data. */
+int rla_sampling_update(rla_ctx *ctx, rla_sketch *sk, int64_t a_rows, int64_t a_cols, const void *A,
+                        int64_t lda, const void *x, int64_t x_len, const void *b, int64_t b_len,
+                        const void *r);
 
 /* mul!(C, S, A, alpha, beta) / mul!(C, A, S, alpha, beta) and the adjoint forms
  * (src/Compressors.jl:331-384, sparse_sign.jl:339-361, count_sketch.jl:166-213,

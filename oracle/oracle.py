@@ -162,6 +162,7 @@ class Recipe:
     padded: int = 0
     block_size: int = 10
     dense_op: Optional[np.ndarray] = None  # Gaussian op
+    idx: Optional[np.ndarray] = None       # Sampling: selected indices (0-based)
 
     @property
     def shape(self):
@@ -169,6 +170,12 @@ class Recipe:
 
     def dense(self) -> np.ndarray:
         """Dense float64 re-materialisation of S, the way the reference tests compare."""
+        if self.kind == "sampling":
+            s = len(self.idx)
+            L = self.n_cols if self.card == "left" else self.n_rows
+            P = np.zeros((s, L))
+            P[np.arange(s), self.idx] = 1.0
+            return P if self.card == "left" else P.T
         if self.kind in ("sparse_sign",):
             D = self.csc.dense()
             return D if self.card == "left" else D.T
@@ -194,6 +201,36 @@ class Recipe:
 # ----------------------------------------------------------------------------------
 # Draws for CPU-only tests (numpy).  Parity tests load the library's own draws instead.
 # ----------------------------------------------------------------------------------
+def draw_sampling(rng: np.random.Generator, card: str, s: int, long_dim: int, replace: bool = False,
+                  weights: Optional[np.ndarray] = None, dtype=np.float64) -> Recipe:
+    """SamplingRecipe (src/Compressors/sampling.jl:98-121) with wsample!(..., ordered = true)
+    (Distributions/uniform.jl, strohmer_vershynin.jl): sorted 0-based indices."""
+    p = None if weights is None else np.asarray(weights, np.float64) / np.sum(weights)
+    idx = np.sort(rng.choice(long_dim, size=s, replace=replace, p=p))
+    n_rows, n_cols = (s, long_dim) if card == "left" else (long_dim, s)
+    return Recipe("sampling", card, n_rows, n_cols, dtype, idx=idx.astype(np.int64))
+
+
+def l2norm_weights(A: np.ndarray, card: str) -> np.ndarray:
+    """strohmer_vershynin.jl: squared row norms (Left) / column norms (Right)."""
+    A = A.astype(np.float64)
+    return np.sum(A * A, axis=1 if card == "left" else 0)
+
+
+def agmon_select(A: np.ndarray, x: np.ndarray, b: np.ndarray, card: str, candidates: np.ndarray, k: int,
+                 r: Optional[np.ndarray] = None) -> np.ndarray:
+    """sample_distribution!(indices, ::AgmonRecipe) after the candidate draw (agmon.jl): the k
+    candidates with the largest residual, ordered by (-residual, candidate)."""
+    A = A.astype(np.float64)
+    if card == "left":
+        res = np.abs(r[candidates]) if r is not None else np.abs(A[candidates, :] @ x - b[candidates])
+    else:
+        rv = r if r is not None else A @ x - b
+        res = np.abs(A[:, candidates].T @ rv)
+    order = sorted(range(len(candidates)), key=lambda i: (-res[i], candidates[i]))
+    return np.asarray([candidates[i] for i in order[:k]], np.int64)
+
+
 def draw_sparse_sign(rng: np.random.Generator, card: str, s: int, long_dim: int, nnz: int, dtype=np.float64) -> Recipe:
     """SparseSignRecipe (src/Compressors/sparse_sign.jl:229-295): per long index, nnz
     distinct sorted rows of 0:s-1, values +-1/sqrt(nnz) (rounded to T)."""
@@ -321,6 +358,16 @@ def mul_SA(C: np.ndarray, S: Recipe, A: np.ndarray, alpha: float = 1.0, beta: fl
     if C2.ndim == 2 and C.ndim == 1:
         ccs = 0
     n = A2.shape[1]
+    if S.kind == "sampling":
+        A64 = A2.astype(np.float64)
+        if S.card == "left":   # sampling.jl:145-157: C = alpha*A[idx, :] + beta*C
+            C2[...] = (alpha * A64[S.idx, :] + (beta * C2.astype(np.float64) if beta != 0 else 0)).astype(C2.dtype)
+        else:                  # sampling.jl:160-176: C .*= beta; C[idx, :] += alpha*A, in order
+            acc = beta * C2.astype(np.float64) if beta != 0 else np.zeros(C2.shape)
+            for i, t in enumerate(S.idx):
+                acc[t, :] += alpha * A64[i, :]
+            C2[...] = acc.astype(C2.dtype)
+        return
     if S.kind == "gaussian":
         # gaussian.jl:145-156 -- BLAS gemm
         res = alpha * (S.dense_op.astype(np.float64) @ A2.astype(np.float64))
@@ -370,6 +417,16 @@ def mul_AS(C: np.ndarray, A: np.ndarray, S: Recipe, alpha: float = 1.0, beta: fl
     cp_, crs, ccs = _view(C2)
     ap_, ars, acs = _view(A2)
     ar = A2.shape[0]
+    if S.kind == "sampling":
+        A64 = A2.astype(np.float64)
+        if S.card == "right":  # sampling.jl:178-188: C = alpha*A[:, idx] + beta*C
+            C2[...] = (alpha * A64[:, S.idx] + (beta * C2.astype(np.float64) if beta != 0 else 0)).astype(C2.dtype)
+        else:                  # sampling.jl:190-200: C .*= beta; C[:, idx] += alpha*A, in order
+            acc = beta * C2.astype(np.float64) if beta != 0 else np.zeros(C2.shape)
+            for i, t in enumerate(S.idx):
+                acc[:, t] += alpha * A64[:, i]
+            C2[...] = acc.astype(C2.dtype)
+        return
     if S.kind == "gaussian":
         # gaussian.jl:159-170
         res = alpha * (A2.astype(np.float64) @ S.dense_op.astype(np.float64))

@@ -14,6 +14,9 @@ from .approximators import (Approximator, RangeApproximator, ApproximatorRecipe,
                             complete_approximator, rapproximate_, rapproximate, RandSVDBatch)
 from ._lib import RLA_PREC_NATIVE, RLA_PREC_SPLIT_BF16, lib, Context
 from .serving import Server, sketch_solve
+from .sampling import (Sampling, SamplingRecipe, Distribution, DistributionRecipe, Uniform, UniformRecipe, L2Norm,
+                       L2NormRecipe, Agmon, AgmonRecipe, complete_distribution, update_distribution_,
+                       sample_distribution_)
 from .solvers import (Solver, SolverRecipe, Logger, LoggerRecipe, SolverError, SolverErrorRecipe, BasicLogger,
                       BasicLoggerRecipe, threshold_stop, complete_logger, update_logger_, reset_logger_, FullResidual,
                       FullResidualRecipe, LSGradient, LSGradientRecipe, CompressedResidual, CompressedResidualRecipe,

@@ -18,7 +18,8 @@ LIB_PATH = os.path.join(HERE, "librla_b200.so")
 RLA_OK, RLA_E_DIM, RLA_E_ARG, RLA_E_DOMAIN, RLA_E_OOM, RLA_E_CUDA, RLA_E_TIMEOUT, RLA_E_NUMERIC, RLA_E_UNSUPPORTED = range(9)
 RLA_F32, RLA_F64 = 0, 1
 RLA_LEFT, RLA_RIGHT = 0, 1
-RLA_SPARSE_SIGN, RLA_COUNT_SKETCH, RLA_SRHT, RLA_FJLT, RLA_GAUSSIAN = range(5)
+RLA_SPARSE_SIGN, RLA_COUNT_SKETCH, RLA_SRHT, RLA_FJLT, RLA_GAUSSIAN, RLA_SAMPLING = range(6)
+RLA_DIST_UNIFORM, RLA_DIST_L2NORM, RLA_DIST_AGMON = range(3)
 RLA_SIDE_LEFT, RLA_SIDE_RIGHT = 0, 1
 RLA_PREC_NATIVE, RLA_PREC_SPLIT_BF16 = 0, 1
 
@@ -100,6 +101,9 @@ SIGNATURES = {
     "rla_randsvd_batch_destroy": (ctypes.c_int, [vp]),
     "rla_randsvd_grouped": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(SvdProblem), ctypes.POINTER(RangeParams)]),
     "rla_sketch_solve": (ctypes.c_int, [vp, vp, i64, i64, vp, i64, vp, vp]),
+    "rla_sampling_create": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, i64, i64, ctypes.c_int, ctypes.c_int, i64,
+                                           ctypes.c_uint64, ctypes.POINTER(vp)]),
+    "rla_sampling_update": (ctypes.c_int, [vp, vp, i64, i64, vp, i64, vp, i64, vp, i64, vp]),
     "rla_ihs_create": (ctypes.c_int, [vp, vp, ctypes.c_int, i64, i64, ctypes.c_double, ctypes.POINTER(vp)]),
     "rla_ihs_start": (ctypes.c_int, [vp, vp, vp, i64, vp, vp, vp, vp]),
     "rla_ihs_step": (ctypes.c_int, [vp, vp, vp, i64, vp, vp, vp, vp]),

@@ -256,6 +256,10 @@ class CompressorRecipe:
             L.check(L.lib().rla_sketch_get_draws(ctx.handle, self.handle, idx.ctypes.data, vals.ctypes.data,
                                                  signs.ctypes.data, kptr.ctypes.data), ctx.handle)
             out = {"colptr": kptr, "rowval": idx[: i.k_nnz], "nzval": vals[: i.k_nnz], "signs": signs}
+        elif kind == L.RLA_SAMPLING:
+            idx = np.zeros(i.compression_dim, np.int64)
+            L.check(L.lib().rla_sketch_get_draws(ctx.handle, self.handle, idx.ctypes.data, None, None, None), ctx.handle)
+            out = {"idx": idx}
         elif kind == L.RLA_GAUSSIAN:
             vals = np.zeros(i.n_rows * i.n_cols, self.np_dtype)
             L.check(L.lib().rla_sketch_get_draws(ctx.handle, self.handle, None, vals.ctypes.data, None, None), ctx.handle)
@@ -445,6 +449,9 @@ def complete_compressor(compressor: Compressor, *args, seed: Optional[int] = Non
         A = args[0]
     else:
         raise ArgumentError("complete_compressor takes (A), (A, b) or (x, A, b).")
+    from . import sampling as _smp
+    if isinstance(compressor, _smp.Sampling):
+        return _smp.complete_sampling(compressor, args, seed, device)
     if type(compressor) not in _KIND:
         raise ArgumentError(f"No `complete_compressor` method exists for compressor of type "
                             f"{type(compressor).__name__} and matrix of type {type(A).__name__}.")
@@ -457,6 +464,9 @@ def update_compressor_(S, *args) -> None:
     """update_compressor!(S), (S, A), (S, A, b), (S, x, A, b): fresh draws in place."""
     if not isinstance(S, CompressorRecipe):
         raise ArgumentError(f"No method `update_compressor` exists for compressor recipe of type {type(S).__name__}.")
+    from . import sampling as _smp
+    if isinstance(S, _smp.SamplingRecipe):
+        return _smp.update_sampling_(S, args)
     ctx = L.Context.get(S._ctx.device)
     L.check(L.lib().rla_sketch_update(ctx.handle, S.handle), ctx.handle)
     S._cache = None

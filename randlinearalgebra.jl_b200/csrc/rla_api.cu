@@ -75,6 +75,9 @@ static int dispatch(rla_ctx *ctx, const rla_sketch *sk, int side, int trans_s, i
         case RLA_FJLT:
             return compress ? fjlt_compress<T>(ctx, sk, A, x_es, x_vs, nv, C, y_es, y_vs, alpha, beta)
                             : fjlt_expand<T>(ctx, sk, A, x_es, x_vs, nv, C, y_es, y_vs, alpha, beta);
+        case RLA_SAMPLING:
+            return compress ? sampling_compress<T>(ctx, sk, A, x_es, x_vs, nv, C, y_es, y_vs, alpha, beta)
+                            : sampling_expand<T>(ctx, sk, A, x_es, x_vs, nv, C, y_es, y_vs, alpha, beta);
     }
     return set_error(ctx, RLA_E_ARG, "unknown compressor kind");
 }

@@ -306,4 +306,13 @@ struct rla_sketch {
     int64_t k_nnz = 0;
     // Gaussian: op, column-major n_rows x n_cols
     void *dense = nullptr;
+    // Sampling (rla_sampling.cu)
+    int s_dist = 0;                // RLA_DIST_*
+    bool s_replace = false;
+    int64_t s_beta = 1;            // Agmon subset size
+    int64_t *sidx = nullptr;       // [s] sampled indices (0-based), the recipe's idx
+    int64_t *splan = nullptr;      // expand plan: [U] targets, [U+1] run offsets, [s] positions
+    int64_t s_uniq = 0;            // U: distinct sampled indices
+    double *sweights = nullptr;    // [L] L2Norm weights of the last update
+    bool s_has_weights = false;
 };

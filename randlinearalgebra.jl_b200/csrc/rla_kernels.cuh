@@ -13,6 +13,17 @@ int sketch_mul_impl(rla_ctx *ctx, const rla_sketch *sk, int side, int trans_s, i
 // update_compressor! ordered on ctx's stream, without waiting for it (rla_sketch.cu).
 int sketch_redraw_async(rla_ctx *ctx, rla_sketch *sk);
 
+// Sampling (rla_sampling.cu): draw for the current distribution, gather / scatter-add
+// applies, parity-mode indices.
+int sampling_draw(rla_ctx *ctx, rla_sketch *sk);
+int sampling_set_indices(rla_ctx *ctx, rla_sketch *sk, const int64_t *idx);
+template <class T>
+int sampling_compress(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_t x_es, int64_t x_vs, int64_t nv, T *Y,
+                      int64_t y_es, int64_t y_vs, double alpha, double beta);
+template <class T>
+int sampling_expand(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_t x_es, int64_t x_vs, int64_t nv, T *Y,
+                    int64_t y_es, int64_t y_vs, double alpha, double beta);
+
 // SparseSign / CountSketch (rla_sparse.cu).  Vectors of the input X: element (k, v) at
 // X[k*x_es + v*x_vs]; the output likewise.  Compress maps length-L vectors to length s,
 // expand maps length-s vectors to length L.

@@ -519,6 +519,7 @@ static Rng make_rng(const rla_sketch *sk) {
 static int draw(rla_ctx *ctx, rla_sketch *sk, bool sync = true) {
     Rng rng = make_rng(sk);
     const int kind = sk->p.kind;
+    if (kind == RLA_SAMPLING) return sampling_draw(ctx, sk);
     if (kind == RLA_SPARSE_SIGN || kind == RLA_COUNT_SKETCH) {
         draw_sparse_kernel<<<ceil_div_i(sk->L, 128), 128, 0, ctx->stream>>>(
             rng, kind == RLA_SPARSE_SIGN ? STREAM_SPARSE : STREAM_COUNT, sk->L, (int)sk->nnz, sk->s,
@@ -578,7 +579,8 @@ int sketch_redraw_async(rla_ctx *ctx, rla_sketch *sk) {
 
 static void free_sketch_buffers(rla_sketch *sk) {
     void *ptrs[] = {sk->bucket, sk->negative, sk->meta, sk->rows, sk->signbits, sk->sign_tl, sk->tile_flags, sk->extra, sk->p2_ptr, sk->p2_list,
-                    sk->k_ptr, sk->k_col, sk->k_val, sk->kt_ptr, sk->kt_row, sk->kt_val, sk->dense};
+                    sk->k_ptr, sk->k_col, sk->k_val, sk->kt_ptr, sk->kt_row, sk->kt_val, sk->dense,
+                    sk->sidx, sk->splan, sk->sweights};
     for (void *p : ptrs)
         if (p) cudaFree(p);
 }
@@ -593,6 +595,7 @@ int rla_sketch_create(rla_ctx *ctx, const rla_sketch_params *pp, rla_sketch **ou
     if (!ctx || !pp || !out) return RLA_E_ARG;
     *out = nullptr;
     const rla_sketch_params &p = *pp;
+    if (p.kind == RLA_SAMPLING) return set_error(ctx, RLA_E_ARG, "Sampling recipes are made by rla_sampling_create.");
     if (p.kind < RLA_SPARSE_SIGN || p.kind > RLA_GAUSSIAN) return set_error(ctx, RLA_E_ARG, "Unknown compressor kind %d.", p.kind);
     if (p.card != RLA_LEFT && p.card != RLA_RIGHT)
         return set_error(ctx, RLA_E_ARG, "`cardinality` must be specified as `Left()` or `Right()`.");
@@ -731,6 +734,10 @@ int rla_sketch_get_draws(rla_ctx *ctx, const rla_sketch *sk, int64_t *idx, void 
     RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     const int kind = sk->p.kind;
     const size_t es = dtype_size(sk->p.dtype);
+    if (kind == RLA_SAMPLING) {
+        if (idx) RLA_CUDA_TRY(ctx, cudaMemcpy(idx, sk->sidx, sizeof(int64_t) * sk->s, cudaMemcpyDeviceToHost));
+        return RLA_OK;
+    }
     if (kind == RLA_SPARSE_SIGN || kind == RLA_COUNT_SKETCH) {
         size_t ne = (size_t)(sk->L * sk->nnz);
         std::vector<int32_t> b(ne);
@@ -789,6 +796,10 @@ int rla_sketch_set_draws(rla_ctx *ctx, rla_sketch *sk, const int64_t *idx, const
     const int kind = sk->p.kind;
     const size_t es = dtype_size(sk->p.dtype);
     auto val_at = [&](size_t i) -> double { return es == 4 ? (double)((const float *)vals)[i] : ((const double *)vals)[i]; };
+    if (kind == RLA_SAMPLING) {
+        if (!idx) return set_error(ctx, RLA_E_ARG, "Sampling draws need the indices.");
+        return sampling_set_indices(ctx, sk, idx);
+    }
     if (kind == RLA_SPARSE_SIGN || kind == RLA_COUNT_SKETCH) {
         if (!idx || !vals) return set_error(ctx, RLA_E_ARG, "Sparse draws need indices and values.");
         size_t ne = (size_t)(sk->L * sk->nnz);

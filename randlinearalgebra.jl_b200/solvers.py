@@ -360,7 +360,8 @@ def complete_solver(ingredients: Solver, x, A, b, seed=None) -> SolverRecipe:
 def _device_matrix(A, dt, dev):
     """Column-major device copy (or the tensor itself when it already is one)."""
     import torch
-    if isinstance(A, torch.Tensor) and A.is_cuda and A.dtype == dt and A.stride(0) == 1 and A.stride(1) >= A.shape[0]:
+    if isinstance(A, torch.Tensor) and A.is_cuda and A.dtype == dt and A.stride(0) == 1 and (
+            A.shape[1] <= 1 or A.stride(1) >= A.shape[0]):
         return A
     t = A if isinstance(A, torch.Tensor) else torch.from_numpy(np.asfortranarray(A))
     return t.to(device=dev, dtype=dt).t().contiguous().t()
@@ -389,7 +390,8 @@ def rsolve_(solver: SolverRecipe, x, A, b) -> None:
     xd, copied = _device_vector(x, dt, dev)
     solver.solution_vec = xd
     lib, ctx = L.lib(), L.Context.get(dev.index)
-    args = (ctx.handle, solver._h, Ad.data_ptr(), Ad.stride(1), bd.data_ptr())
+    lda = max(Ad.shape[0], 1) if Ad.shape[1] <= 1 else Ad.stride(1)
+    args = (ctx.handle, solver._h, Ad.data_ptr(), lda, bd.data_ptr())
     vecs = (xd.data_ptr(), solver.residual_vec.data_ptr(), solver.gradient_vec.data_ptr())
     L.check(lib.rla_ihs_start(*args, *vecs), ctx.handle)
     solver._live = True

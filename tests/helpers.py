@@ -9,6 +9,8 @@ def oracle_recipe(orc, S, dtype=np.float64):
     i = S.info
     d = S.draws()
     card = "left" if i.card == 0 else "right"
+    if i.kind == 5:  # Sampling
+        return orc.Recipe("sampling", card, int(i.n_rows), int(i.n_cols), dtype, idx=d["idx"].astype(np.int64))
     if i.kind in (0, 1):
         kind = "sparse_sign" if i.kind == 0 else "count_sketch"
         nnz = int(i.nnz)

@@ -113,3 +113,50 @@ def test_ihs_oracle_max_it_zero(orc):
     res = orc.ihs_rsolve(A, b, np.ones(4), lambda i: None, max_it=0)
     assert res.iteration == 0 and np.array_equal(res.x, np.ones(4))
     assert np.allclose(res.residual_vec, b - A @ np.ones(4))
+
+
+# ---- Sampling (src/Compressors/sampling.jl) -------------------------------------------
+@pytest.mark.parametrize("card", ["left", "right"])
+@pytest.mark.parametrize("replace", [False, True])
+def test_oracle_sampling_matches_dense(orc, card, replace):
+    """The oracle's gather / in-order scatter-add equals the dense selection matrix
+    (P(i, idx(i)) = 1; S = P for Left, P' for Right) in all four orientations."""
+    rng = np.random.default_rng(4)
+    S = orc.draw_sampling(rng, card, 9, 25, replace=replace)
+    D = S.dense()
+    nr, nc = S.n_rows, S.n_cols
+    A = rng.standard_normal((nc, 3)); C = rng.standard_normal((nr, 3)); C0 = C.copy()
+    orc.mul_SA(C, S, A, 2.0, 0.5)
+    assert np.allclose(C, 2 * D @ A + 0.5 * C0)
+    A = rng.standard_normal((4, nr)); C = rng.standard_normal((4, nc)); C0 = C.copy()
+    orc.mul_AS(C, A, S, 2.0, 0.5)
+    assert np.allclose(C, 2 * A @ D + 0.5 * C0)
+    A = rng.standard_normal((nr, 2)); C = rng.standard_normal((nc, 2)); C0 = C.copy()
+    orc.mul_StA(C, S, A, 1.5, 0.0)
+    assert np.allclose(C, 1.5 * D.T @ A)
+    A = rng.standard_normal((2, nc)); C = rng.standard_normal((2, nr)); C0 = C.copy()
+    orc.mul_ASt(C, A, S, 1.5, 0.25)
+    assert np.allclose(C, 1.5 * A @ D.T + 0.25 * C0)
+
+
+def test_oracle_agmon_order(orc):
+    """agmon.jl: the k largest residuals, ties by candidate index."""
+    A = np.eye(5)
+    x = np.array([3.0, 1.0, 3.0, 2.0, 0.0])
+    b = np.zeros(5)
+    assert orc.agmon_select(A, x, b, "left", np.arange(5), 3).tolist() == [0, 2, 3]
+    assert orc.agmon_select(A, x, b, "left", np.array([4, 2, 0]), 2).tolist() == [0, 2]
+
+
+def test_sampling_constructors(rla):
+    s = rla.Sampling()
+    assert type(s.cardinality) is rla.Left and s.compression_dim == 2 and type(s.distribution) is rla.Uniform
+    with pytest.raises(rla.ArgumentError, match=r"^Field `compression_dim` must be positive\.$"):
+        rla.Sampling(compression_dim=-1)
+    with pytest.raises(rla.ArgumentError, match="`Undef\\(\\)` is not allowed in `Sampling` structure."):
+        rla.Sampling(cardinality=rla.Undef())
+    d = rla.Agmon()
+    assert type(d.cardinality) is rla.Undef and d.replace is False and d.beta == 1
+    with pytest.raises(rla.ArgumentError, match=r"^`Agmon` beta must be >= 1, got beta=0$"):
+        rla.Agmon(beta=0)
+    assert type(rla.L2Norm().cardinality) is rla.Undef and rla.Uniform(replace=True).replace
