@@ -704,6 +704,135 @@ def ihs_cpu_sample(m, n, s, iters=2):
 
 
 # --------------------------------------------------------------------------------------
+# Sampling workload
+# --------------------------------------------------------------------------------------
+SMP_METRIC = "sampling compressor step (update_compressor! with L2Norm weights + draw, then S*A), GB/s"
+
+
+def sampling_arm(args):
+    """Sampling(Left, compression_dim = 4096, L2Norm(replace = false)) on A 2^20 x 512 FP32 ~ N(0,1).
+    One step = update_compressor!(S, x, A, b) (squared row norms of A, Efraimidis-Spirakis keys,
+    radix select of the 4096 smallest, expand plan) followed by mul!(C, S, A) (row gather).
+    Algorithmic bytes per step: 4*m*n (A read by the weights pass) + 2*4*s*n (gather)."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    world, rank, local = dist_setup(args.gpus)
+    from __graft_entry__ import load_package
+    rla = load_package()
+    from randlinearalgebra_b200 import _lib as L
+    dev = torch.device("cuda", local if world > 1 else 0)
+    m, n, s = M, args.cols, S
+    g = torch.Generator(device=dev)
+    g.manual_seed(7 + rank)
+    A = torch.randn(n, m, device=dev, generator=g, dtype=torch.float32).t()
+    x = torch.zeros(n, device=dev)
+    b = torch.zeros(m, device=dev)
+    Sm = rla.complete_compressor(rla.Sampling(compression_dim=s, distribution=rla.L2Norm()), A, seed=8000 + rank)
+    C = torch.zeros(n, s, device=dev).t()
+    ctx = L.Context.get(dev.index)
+    lib = L.lib()
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        rla.update_compressor_(Sm, x, A, b)
+        rla.mul_(C, Sm, A)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    lib.rla_ctx_set_timing(ctx.handle, 1)
+    lib.rla_ctx_kernel_time(ctx.handle, 3, ctypes.byref(ctypes.c_double()), ctypes.byref(ctypes.c_int64()))
+    K = args.steps
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    props = torch.cuda.get_device_properties(dev)
+    clocks = ClockSampler(f"GPU-{props.uuid}" if getattr(props, "uuid", None) else dev.index)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    t0.record(stream)
+    for _ in range(K):
+        step()
+    t1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    barrier(world)
+    ms = allreduce_max(t0.elapsed_time(t1), world)
+    tot, cnt = ctypes.c_double(), ctypes.c_int64()
+    L.check(lib.rla_ctx_kernel_time(ctx.handle, 3, ctypes.byref(tot), ctypes.byref(cnt)), ctx.handle)
+    lib.rla_ctx_set_timing(ctx.handle, 0)
+    bytes_step = 4 * m * n + 2 * 4 * s * n
+    value = job_throughput(world, bytes_step * K, ms / 1e3)
+    # correctness guard: the gathered rows are the sampled rows of A
+    idx = torch.from_numpy(Sm.idx).to(dev)
+    assert torch.equal(C, A[idx, :]), "gather differs from A[idx, :]"
+
+    # ---- end to end: pinned host A in, C out, one step through the public API ------------
+    A_h = torch.empty(n, m, dtype=torch.float32, pin_memory=True).t()
+    A_h.copy_(A)
+    C_h = torch.zeros(n, s, dtype=torch.float32, pin_memory=True).t()
+    torch.cuda.synchronize()
+    barrier(world)
+    w0 = time.perf_counter()
+    Ad = A_h.to(dev, non_blocking=True)
+    rla.update_compressor_(Sm, x, Ad, b)
+    rla.mul_(C_h, Sm, Ad)
+    torch.cuda.synchronize()
+    e2e_s = allreduce_max(time.perf_counter() - w0, world)
+    e2e = {"value": round(job_throughput(world, bytes_step, e2e_s), 3), "unit": "GB/s",
+           "h2d_bytes_per_step": 4 * m * n, "d2h_bytes_per_step": 4 * s * n, "ms_per_step": round(e2e_s * 1e3, 3)}
+    del A_h, Ad
+    if rank != 0:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    peak, peak_kind = peaks()
+    w_ms = tot.value / max(cnt.value, 1)
+    w_gbs = 4 * m * n / (w_ms / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": "sq_norms_rows_kernel", "achieved": round(w_gbs, 2), "peak": peak,
+                "peak_source": peak_kind, "unit": "GB/s", "frac": round(w_gbs / peak, 4), "traffic": None,
+                "algorithmic_bytes_per_launch": 4 * m * n, "avg_launch_ms": round(w_ms, 4),
+                "launches_timed": cnt.value}
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        cpu = sampling_cpu_sample(m, s)
+    line = {"metric": SMP_METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": K,
+            "warmup": args.warmup, "ms_per_step": round(ms / K, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (weights f64)",
+            "data": "synthetic N(0,1) generated on device (seed 7+rank)",
+            "config": {"workload": f"sampling left L2Norm without replacement, A {m}x{n} f32 -> {s}x{n}",
+                       "m": m, "n": n, "s": s, "parallelism": f"replicas x{world}",
+                       "l2": "A is 2.15 GB (larger than L2), no flush needed"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def sampling_cpu_sample(m, s, ncol=64):
+    """The oracle's restatement on the host: squared row norms (numpy, all cores), weighted
+    sampling without replacement (numpy Generator.choice), the row gather, on `ncol` columns."""
+    import numpy as np
+
+    from __graft_entry__ import load_oracle
+    orc = load_oracle()
+    rng = np.random.default_rng(7)
+    A = np.asfortranarray(rng.standard_normal((m, ncol), dtype=np.float32))
+    t0 = time.perf_counter()
+    w = orc.l2norm_weights(A, "left")
+    R = orc.draw_sampling(rng, "left", s, m, replace=False, weights=w, dtype=np.float32)
+    C = np.zeros((s, ncol), np.float32, order="F")
+    orc.mul_SA(C, R, A)
+    dt = time.perf_counter() - t0
+    return {"value": round((4 * m * ncol + 8 * s * ncol) / dt / 1e9, 4), "unit": "GB/s", "cores": os.cpu_count(),
+            "kind": "port", "sample": f"one update + apply on {ncol} of the columns of the {m}-row A (numpy)"}
+
+
+# --------------------------------------------------------------------------------------
 # Batched RandSVD workload
 # --------------------------------------------------------------------------------------
 BT_COUNT = 512
@@ -1020,7 +1149,8 @@ def main():
     ap.add_argument("--cols", type=int, default=NCOL,
                     help="columns of A (default 512, the benchmark workload; smaller values make small "
                          "cases of the same kernels for profiler captures)")
-    ap.add_argument("--workload", choices=["sketch", "randsvd", "batched", "serve", "ihs"], default="sketch",
+    ap.add_argument("--workload", choices=["sketch", "randsvd", "batched", "serve", "ihs", "sampling"],
+                    default="sketch",
                     help="sketch: SRHT + CountSketch apply (default); randsvd: mixed-precision RandSVD; "
                          "batched: 512 uneven RandSVD instances")
     ap.add_argument("--batch-count", type=int, default=BT_COUNT, help="instances of the batched workload")
@@ -1054,6 +1184,13 @@ def main():
                               "for the sketch and randsvd workloads only"}), flush=True)
         else:
             batched_arm(args)
+    elif args.workload == "sampling":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "sampling workload: the reference arm is timed "
+                              "for the sketch and randsvd workloads only (the CPU restatement is in cpu_baseline)"}),
+                  flush=True)
+        else:
+            sampling_arm(args)
     elif args.workload == "ihs":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "ihs workload: the reference arm is timed "

@@ -364,7 +364,8 @@ int rla_server_stop(rla_server *srv);
 /* ---- kernel timing (tracing aid, no reference counterpart) ------------------------- */
 /* While enabled, the context records CUDA events around each launch of a timed kernel
  * class on its stream (class 0: the tensor-core GEMM kernel; 1: the IHS fused pass over A;
- * 2: the IHS compressor apply S*A).  rla_ctx_kernel_time
+ * 2: the IHS compressor apply S*A; 3: the L2Norm weights pass of rla_sampling_update).
+ * rla_ctx_kernel_time
  * synchronises the stream, returns the summed device time (ms) and launch count of the
  * class since the last call, and clears the record. */
 int rla_ctx_set_timing(rla_ctx *ctx, int enable);

@@ -179,7 +179,7 @@ int rla_ctx_set_timing(rla_ctx *ctx, int enable) {
 
 int rla_ctx_kernel_time(rla_ctx *ctx, int kernel_class, double *ms_total, int64_t *launches) {
     if (!ctx || !ms_total || !launches) return RLA_E_ARG;
-    if (kernel_class < 0 || kernel_class > 2) return set_error(ctx, RLA_E_ARG, "unknown kernel class %d", kernel_class);
+    if (kernel_class < 0 || kernel_class > 3) return set_error(ctx, RLA_E_ARG, "unknown kernel class %d", kernel_class);
     RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     double tot = 0.0;
     auto &v = ctx->timed[kernel_class];

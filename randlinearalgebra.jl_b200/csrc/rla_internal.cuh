@@ -45,8 +45,9 @@ struct rla_ctx {
     cudaMemPool_t pool = nullptr;  // context-owned stream-ordered pool, keeps freed memory mapped
     int *tc_status = nullptr;  // non-zero after a tensor-core kernel's bounded wait ran out
     bool timing = false;       // record CUDA events around timed kernel classes
-    // classes: 0 tensor-core GEMM, 1 IHS fused pass over A, 2 IHS compressor apply
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> timed[3];
+    // classes: 0 tensor-core GEMM, 1 IHS fused pass over A, 2 IHS compressor apply,
+    // 3 Sampling L2Norm weights pass over A
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> timed[4];
 };
 
 namespace rla {
@@ -311,8 +312,8 @@ struct rla_sketch {
     bool s_replace = false;
     int64_t s_beta = 1;            // Agmon subset size
     int64_t *sidx = nullptr;       // [s] sampled indices (0-based), the recipe's idx
-    int64_t *splan = nullptr;      // expand plan: [U] targets, [U+1] run offsets, [s] positions
-    int64_t s_uniq = 0;            // U: distinct sampled indices
+    int64_t *splan = nullptr;      // expand plan: [s] targets, [s+1] run offsets, [s] positions, U
+    int64_t *s_err = nullptr;      // precondition flags of the last draw (0: none)
     double *sweights = nullptr;    // [L] L2Norm weights of the last update
     bool s_has_weights = false;
 };

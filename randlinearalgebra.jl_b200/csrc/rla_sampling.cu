@@ -117,9 +117,25 @@ __global__ void es_keys_kernel(Rng rng, int64_t L, const double *w, uint64_t *ke
     key[j] = (uint64_t)__double_as_longlong(k);
 }
 
-__global__ void radix_hist_kernel(const uint64_t *key, int64_t n, uint64_t prefix, uint64_t mask, int shift,
-                                  unsigned *hist) {
+// Radix-select state in device memory: the known high bits of the threshold key, their
+// mask, and the rank of the threshold among the keys that share them.
+struct SelState {
+    uint64_t prefix, mask;
+    int64_t rem;
+};
+
+__global__ void sel_init_kernel(SelState *st, int64_t k, unsigned *hist) {
+    if (threadIdx.x == 0) {
+        st->prefix = 0;
+        st->mask = 0;
+        st->rem = k;
+    }
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
+}
+
+__global__ void radix_hist_kernel(const uint64_t *key, int64_t n, const SelState *st, int shift, unsigned *hist) {
     __shared__ unsigned h[256];
+    const uint64_t prefix = st->prefix, mask = st->mask;
     for (int i = threadIdx.x; i < 256; i += blockDim.x) h[i] = 0;
     __syncthreads();
     for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
@@ -131,10 +147,80 @@ __global__ void radix_hist_kernel(const uint64_t *key, int64_t n, uint64_t prefi
         if (h[i]) atomicAdd(&hist[i], h[i]);
 }
 
+// The digit at `shift` of the threshold: the first digit whose cumulative count reaches
+// the remaining rank.  One CTA of 256 threads; the histogram is cleared for the next pass.
+__global__ void radix_pick_kernel(SelState *st, unsigned *hist, int shift) {
+    if (threadIdx.x == 0) {
+        int64_t rem = st->rem;
+        int d = 0;
+        for (; d < 255 && rem > (int64_t)hist[d]; ++d) rem -= hist[d];
+        st->rem = rem;
+        st->prefix |= (uint64_t)d << shift;
+        st->mask |= (uint64_t)255 << shift;
+    }
+    __syncthreads();
+    hist[threadIdx.x] = 0;
+}
+
+// count(key < T) by atomics on a 64-bit counter (integer sums are order-independent).
+__global__ void count_below_kernel(const uint64_t *key, int64_t n, uint64_t T, unsigned long long *count) {
+    __shared__ unsigned c;
+    if (threadIdx.x == 0) c = 0;
+    __syncthreads();
+    unsigned mine = 0;
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x)
+        mine += key[j] < T;
+    atomicAdd(&c, mine);
+    __syncthreads();
+    if (threadIdx.x == 0 && c) atomicAdd(count, (unsigned long long)c);
+}
+
+// err = count + 1 when fewer than s keys are below +inf (positive weights), else unchanged.
+__global__ void check_positive_kernel(const unsigned long long *count, int64_t s, int64_t *err) {
+    if ((int64_t)*count < s) *err = (int64_t)*count + 1;
+}
+
+// err = -1 when the weights do not sum to a positive finite number.
+__global__ void check_sum_kernel(const double *cdf, int64_t L, int64_t *err) {
+    const double W = cdf[L - 1];
+    if (!(W > 0.0) || !isfinite(W)) *err = -1;
+}
+
+// Exclusive scans of the two block-count arrays (one CTA).
+__global__ void __launch_bounds__(1024) scan2_kernel(const int64_t *a, const int64_t *b, int64_t n, int64_t *oa,
+                                                     int64_t *ob) {
+    __shared__ int64_t pa[1024], pb[1024];
+    const int t = threadIdx.x, nt = blockDim.x;
+    const int64_t per = (n + nt - 1) / nt, lo = min(n, (int64_t)t * per), hi = min(n, lo + per);
+    int64_t sa = 0, sb = 0;
+    for (int64_t i = lo; i < hi; ++i) {
+        sa += a[i];
+        sb += b[i];
+    }
+    pa[t] = sa;
+    pb[t] = sb;
+    __syncthreads();
+    for (int off = 1; off < nt; off <<= 1) {
+        const int64_t va = t >= off ? pa[t - off] : 0, vb = t >= off ? pb[t - off] : 0;
+        __syncthreads();
+        pa[t] += va;
+        pb[t] += vb;
+        __syncthreads();
+    }
+    int64_t ra = pa[t] - sa, rb = pb[t] - sb;
+    for (int64_t i = lo; i < hi; ++i) {
+        oa[i] = ra;
+        ob[i] = rb;
+        ra += a[i];
+        rb += b[i];
+    }
+}
+
 // Per 1024-element block: how many keys are below T and how many equal it.
-__global__ void __launch_bounds__(1024) select_count_kernel(const uint64_t *key, int64_t n, uint64_t T,
+__global__ void __launch_bounds__(1024) select_count_kernel(const uint64_t *key, int64_t n, const SelState *st,
                                                             int64_t *blk_lt, int64_t *blk_eq) {
     __shared__ int wl[32], we[32];
+    const uint64_t T = st->prefix;
     const int64_t j = blockIdx.x * 1024ll + threadIdx.x;
     const uint64_t k = j < n ? key[j] : ~0ull;
     const unsigned bl = __ballot_sync(FULL, j < n && k < T), be = __ballot_sync(FULL, j < n && k == T);
@@ -158,10 +244,12 @@ __global__ void __launch_bounds__(1024) select_count_kernel(const uint64_t *key,
 // The selected set is {key < T} plus the first `need` keys equal to T (index order); a
 // selected j lands at lt_before(j) + min(eq_before(j), need), so the output is in index
 // order.  off_lt / off_eq: exclusive prefix sums of the block counts.
-__global__ void __launch_bounds__(1024) select_write_kernel(const uint64_t *key, int64_t n, uint64_t T, int64_t need,
+__global__ void __launch_bounds__(1024) select_write_kernel(const uint64_t *key, int64_t n, const SelState *st,
                                                             const int64_t *off_lt, const int64_t *off_eq,
                                                             const int64_t *cand, int64_t *out) {
     __shared__ int wl[32], we[32];
+    const uint64_t T = st->prefix;
+    const int64_t need = st->rem;
     const int64_t j = blockIdx.x * 1024ll + threadIdx.x;
     const uint64_t k = j < n ? key[j] : ~0ull;
     const bool lt = j < n && k < T, eq = j < n && k == T;
@@ -308,13 +396,15 @@ __global__ void sample_scale_kernel(T *Y, int64_t y_es, int64_t y_vs, int64_t L,
 
 // expand, step 2: for every distinct target u, Y(tgt(u), v) += alpha * X(p, v) for the
 // positions p of u in increasing order (the reference's accumulation order).
+// plan layout [tgt: s][run_ptr: s+1][run_pos: s][U]; threads u >= U exit.
 template <class T>
-__global__ void sample_scatter_kernel(const T *X, int64_t x_es, int64_t x_vs, int64_t nv, const int64_t *tgt,
-                                      const int64_t *run_ptr, const int64_t *run_pos, int64_t U, T *Y, int64_t y_es,
-                                      int64_t y_vs, T alpha, int v_fast) {
+__global__ void sample_scatter_kernel(const T *X, int64_t x_es, int64_t x_vs, int64_t nv, const int64_t *plan,
+                                      int64_t s, T *Y, int64_t y_es, int64_t y_vs, T alpha, int v_fast) {
     const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (t >= U * nv) return;
-    const int64_t u = v_fast ? t / nv : t % U, v = v_fast ? t % nv : t / U;
+    if (t >= s * nv) return;
+    const int64_t u = v_fast ? t / nv : t % s, v = v_fast ? t % nv : t / s;
+    if (u >= plan[3 * s + 1]) return;
+    const int64_t *tgt = plan, *run_ptr = plan + s, *run_pos = plan + 2 * s + 1;
     T *yp = Y + tgt[u] * y_es + v * y_vs;
     T acc = *yp;
     for (int64_t q = run_ptr[u]; q < run_ptr[u + 1]; ++q) acc += alpha * X[run_pos[q] * x_es + v * x_vs];
@@ -338,50 +428,61 @@ static Rng sampling_rng(const rla_sketch *sk) {
 static int sel_check(rla_ctx *ctx, const char *what) { return check_launch(ctx, what); }
 
 // The k smallest keys of key[0:n) (k <= n), written to out in index order (cand maps
-// positions to indices when given).
+// positions to indices when given).  Everything stays on the stream: 8 histogram/pick pairs
+// over the key bytes (MSB first), block counts, their scans, the ordered write.
 static int select_smallest(rla_ctx *ctx, const uint64_t *key, int64_t n, int64_t k, const int64_t *cand,
                            int64_t *out) {
-    unsigned *hist = nullptr;
-    RLA_TRY(scratch_get(ctx, 256 * sizeof(unsigned), (void **)&hist));
-    uint64_t prefix = 0, mask = 0;
-    int64_t rem = k;  // rank (1-based) of the threshold key among the remaining ones
-    unsigned hh[256];
-    const int gb = (int)std::min<int64_t>(ceil_div(n, 256), 4 * (int64_t)ctx->sm_count);
-    for (int shift = 56; shift >= 0; shift -= 8) {
-        RLA_CUDA_TRY(ctx, cudaMemsetAsync(hist, 0, 256 * sizeof(unsigned), ctx->stream));
-        radix_hist_kernel<<<gb, 256, 0, ctx->stream>>>(key, n, prefix, mask, shift, hist);
-        RLA_TRY(sel_check(ctx, "radix_hist"));
-        RLA_CUDA_TRY(ctx, cudaMemcpyAsync(hh, hist, sizeof(hh), cudaMemcpyDeviceToHost, ctx->stream));
-        RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-        int d = 0;
-        for (; d < 255 && rem > (int64_t)hh[d]; ++d) rem -= hh[d];
-        prefix |= (uint64_t)d << shift;
-        mask |= (uint64_t)255 << shift;
-    }
-    const uint64_t T = prefix;  // the k-th smallest key; `rem` of its copies are taken
     const int64_t nb = ceil_div(n, 1024);
-    int64_t *blk = nullptr;
     void *p = nullptr;
-    RLA_CUDA_TRY(ctx, pool_malloc_s(ctx, &p, sizeof(int64_t) * 4 * nb, ctx->stream));
-    blk = (int64_t *)p;
-    select_count_kernel<<<(unsigned)nb, 1024, 0, ctx->stream>>>(key, n, T, blk, blk + nb);
-    RLA_TRY(sel_check(ctx, "select_count"));
-    std::vector<int64_t> h(2 * nb), off(2 * nb);
-    RLA_CUDA_TRY(ctx, cudaMemcpyAsync(h.data(), blk, sizeof(int64_t) * 2 * nb, cudaMemcpyDeviceToHost, ctx->stream));
-    RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-    int64_t a = 0, b = 0;
-    for (int64_t i = 0; i < nb; ++i) {
-        off[i] = a;
-        off[nb + i] = b;
-        a += h[i];
-        b += h[nb + i];
+    const size_t st_bytes = 64, hist_bytes = 256 * sizeof(unsigned);
+    RLA_CUDA_TRY(ctx, pool_malloc_s(ctx, &p, st_bytes + hist_bytes + sizeof(int64_t) * 4 * nb, ctx->stream));
+    SelState *st = (SelState *)p;
+    unsigned *hist = (unsigned *)((char *)p + st_bytes);
+    int64_t *blk = (int64_t *)((char *)p + st_bytes + hist_bytes);
+    sel_init_kernel<<<1, 256, 0, ctx->stream>>>(st, k, hist);
+    const int gb = (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, 256), 4 * (int64_t)ctx->sm_count));
+    for (int shift = 56; shift >= 0; shift -= 8) {
+        radix_hist_kernel<<<gb, 256, 0, ctx->stream>>>(key, n, st, shift, hist);
+        radix_pick_kernel<<<1, 256, 0, ctx->stream>>>(st, hist, shift);
     }
-    RLA_CUDA_TRY(ctx, cudaMemcpyAsync(blk + 2 * nb, off.data(), sizeof(int64_t) * 2 * nb, cudaMemcpyHostToDevice,
-                                      ctx->stream));
-    select_write_kernel<<<(unsigned)nb, 1024, 0, ctx->stream>>>(key, n, T, rem, blk + 2 * nb, blk + 3 * nb, cand, out);
-    RLA_TRY(sel_check(ctx, "select_write"));
+    select_count_kernel<<<(unsigned)nb, 1024, 0, ctx->stream>>>(key, n, st, blk, blk + nb);
+    scan2_kernel<<<1, 1024, 0, ctx->stream>>>(blk, blk + nb, nb, blk + 2 * nb, blk + 3 * nb);
+    select_write_kernel<<<(unsigned)nb, 1024, 0, ctx->stream>>>(key, n, st, blk + 2 * nb, blk + 3 * nb, cand, out);
+    RLA_TRY(sel_check(ctx, "select_smallest"));
     RLA_CUDA_TRY(ctx, cudaFreeAsync(p, ctx->stream));
     return RLA_OK;
+}
+
+// Expand plan of sorted indices on the device: targets are the run heads, positions the
+// identity.  One CTA; plan layout [tgt: s][ptr: s+1][pos: s][U].
+__global__ void __launch_bounds__(1024) plan_sorted_kernel(const int64_t *idx, int64_t s, int64_t *plan) {
+    __shared__ int64_t part[1024];
+    int64_t *tgt = plan, *ptr = plan + s, *pos = plan + 2 * s + 1, *U = plan + 3 * s + 1;
+    const int t = threadIdx.x, nt = blockDim.x;
+    const int64_t per = (s + nt - 1) / nt, lo = min(s, (int64_t)t * per), hi = min(s, lo + per);
+    int64_t c = 0;
+    for (int64_t i = lo; i < hi; ++i) c += (i == 0 || idx[i] != idx[i - 1]);
+    part[t] = c;
+    __syncthreads();
+    for (int off = 1; off < nt; off <<= 1) {
+        const int64_t v = t >= off ? part[t - off] : 0;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    int64_t u = part[t] - c;
+    for (int64_t i = lo; i < hi; ++i) {
+        pos[i] = i;
+        if (i == 0 || idx[i] != idx[i - 1]) {
+            tgt[u] = idx[i];
+            ptr[u] = i;
+            ++u;
+        }
+    }
+    if (t == nt - 1) {
+        ptr[part[t]] = s;
+        *U = part[t];
+    }
 }
 
 // Expand plan from the current indices: distinct targets with their positions in order.
@@ -403,11 +504,11 @@ static int sampling_plan(rla_ctx *ctx, rla_sketch *sk) {
             ptr.push_back(q);
         }
     ptr.push_back(s);
-    sk->s_uniq = (int64_t)tgt.size();
-    std::vector<int64_t> plan(tgt.size() + ptr.size() + pos.size());
+    std::vector<int64_t> plan(3 * s + 2, 0);  // [tgt: s][ptr: s+1][pos: s][U]
     std::copy(tgt.begin(), tgt.end(), plan.begin());
-    std::copy(ptr.begin(), ptr.end(), plan.begin() + tgt.size());
-    std::copy(pos.begin(), pos.end(), plan.begin() + tgt.size() + ptr.size());
+    std::copy(ptr.begin(), ptr.end(), plan.begin() + s);
+    std::copy(pos.begin(), pos.end(), plan.begin() + 2 * s + 1);
+    plan[3 * s + 1] = (int64_t)tgt.size();
     RLA_CUDA_TRY(ctx, cudaMemcpyAsync(sk->splan, plan.data(), sizeof(int64_t) * plan.size(), cudaMemcpyHostToDevice,
                                       ctx->stream));
     RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
@@ -415,6 +516,7 @@ static int sampling_plan(rla_ctx *ctx, rla_sketch *sk) {
 }
 
 // sample_distribution! for Uniform / L2Norm: `w` holds the weights (nullptr: uniform).
+// Failed preconditions are flagged in sk->s_err (read by sampling_finish).
 static int sample_weighted(rla_ctx *ctx, rla_sketch *sk, const double *w) {
     const int64_t s = sk->s, L = sk->L;
     Rng rng = sampling_rng(sk);
@@ -425,13 +527,7 @@ static int sample_weighted(rla_ctx *ctx, rla_sketch *sk, const double *w) {
         scan_f64_kernel<<<1, 1024, 0, ctx->stream>>>(w, L, cdf);
         exp_draw_kernel<<<ceil_div_i(s + 1, 256), 256, 0, ctx->stream>>>(rng, s + 1, e);
         scan_f64_kernel<<<1, 1024, 0, ctx->stream>>>(e, s + 1, P);
-        double W = 0.0;
-        RLA_CUDA_TRY(ctx, cudaMemcpyAsync(&W, cdf + L - 1, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-        RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-        if (!(W > 0.0) || !isfinite(W)) {
-            cudaFreeAsync(p, ctx->stream);
-            return set_error(ctx, RLA_E_ARG, "The sampling weights must have a positive finite sum.");
-        }
+        check_sum_kernel<<<1, 1, 0, ctx->stream>>>(cdf, L, sk->s_err);
         cdf_search_kernel<<<ceil_div_i(s, 256), 256, 0, ctx->stream>>>(P, s, cdf, L, sk->sidx);
         RLA_TRY(check_launch(ctx, "sample_with_replacement"));
         RLA_CUDA_TRY(ctx, cudaFreeAsync(p, ctx->stream));
@@ -441,33 +537,33 @@ static int sample_weighted(rla_ctx *ctx, rla_sketch *sk, const double *w) {
         return set_error(ctx, RLA_E_ARG, "Cannot draw %lld samples from %lld samples without replacement.",
                          (long long)s, (long long)L);
     void *p = nullptr;
-    RLA_CUDA_TRY(ctx, pool_malloc_s(ctx, &p, sizeof(uint64_t) * L, ctx->stream));
+    RLA_CUDA_TRY(ctx, pool_malloc_s(ctx, &p, sizeof(uint64_t) * L + 64, ctx->stream));
     uint64_t *key = (uint64_t *)p;
+    unsigned long long *cnt = (unsigned long long *)(key + L);
     es_keys_kernel<<<ceil_div_i(L, 256), 256, 0, ctx->stream>>>(rng, L, w, key);
     RLA_TRY(check_launch(ctx, "es_keys"));
     if (w) {
         // at least s positive weights (keys below +inf)
-        const uint64_t inf_bits = 0x7ff0000000000000ull;
-        int64_t *cnt = nullptr;
-        RLA_TRY(scratch_get(ctx, sizeof(int64_t) * 2 * ceil_div(L, 1024), (void **)&cnt));
-        select_count_kernel<<<(unsigned)ceil_div(L, 1024), 1024, 0, ctx->stream>>>(key, L, inf_bits, cnt,
-                                                                                   cnt + ceil_div(L, 1024));
-        std::vector<int64_t> h(ceil_div(L, 1024));
-        RLA_CUDA_TRY(ctx, cudaMemcpyAsync(h.data(), cnt, sizeof(int64_t) * h.size(), cudaMemcpyDeviceToHost,
-                                          ctx->stream));
-        RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-        int64_t pos = 0;
-        for (int64_t v : h) pos += v;
-        if (pos < s) {
-            cudaFreeAsync(p, ctx->stream);
-            return set_error(ctx, RLA_E_ARG,
-                             "Cannot draw %lld samples without replacement from %lld indices of positive weight.",
-                             (long long)s, (long long)pos);
-        }
+        RLA_CUDA_TRY(ctx, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), ctx->stream));
+        count_below_kernel<<<(int)std::min<int64_t>(ceil_div(L, 256), 4 * (int64_t)ctx->sm_count), 256, 0,
+                             ctx->stream>>>(key, L, 0x7ff0000000000000ull, cnt);
+        check_positive_kernel<<<1, 1, 0, ctx->stream>>>(cnt, s, sk->s_err);
     }
     int rc = select_smallest(ctx, key, L, s, nullptr, sk->sidx);
     cudaFreeAsync(p, ctx->stream);
     return rc;
+}
+
+// Read the precondition flags of the last draw (synchronises the stream).
+static int sampling_finish(rla_ctx *ctx, rla_sketch *sk) {
+    int64_t err = 0;
+    RLA_CUDA_TRY(ctx, cudaMemcpyAsync(&err, sk->s_err, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+    RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (err == 0) return RLA_OK;
+    RLA_CUDA_TRY(ctx, cudaMemsetAsync(sk->s_err, 0, sizeof(int64_t), ctx->stream));
+    if (err < 0) return set_error(ctx, RLA_E_ARG, "The sampling weights must have a positive finite sum.");
+    return set_error(ctx, RLA_E_ARG, "Cannot draw %lld samples without replacement from %lld indices of positive weight.",
+                     (long long)sk->s, (long long)(err - 1));
 }
 
 template <class T>
@@ -538,7 +634,11 @@ int sampling_draw(rla_ctx *ctx, rla_sketch *sk) {
         rc = sample_weighted(ctx, sk, sk->sweights);
     } else
         return set_error(ctx, RLA_E_ARG, "`Agmon` sampling needs x, A and b: use rla_sampling_update.");
-    if (rc == RLA_OK) rc = sampling_plan(ctx, sk);
+    if (rc == RLA_OK) {
+        plan_sorted_kernel<<<1, 1024, 0, ctx->stream>>>(sk->sidx, sk->s, sk->splan);
+        rc = check_launch(ctx, "plan_sorted");
+    }
+    if (rc == RLA_OK) rc = sampling_finish(ctx, sk);
     return rc;
 }
 
@@ -546,20 +646,25 @@ template <class T>
 static int sampling_update_t(rla_ctx *ctx, rla_sketch *sk, int64_t a_rows, int64_t a_cols, const T *A, int64_t lda,
                              const T *x, const T *b, const T *r) {
     if (sk->s_dist == RLA_DIST_L2NORM) {
+        cudaEvent_t e0 = timing_begin(ctx);
         if (sk->p.card == RLA_LEFT)
             sq_norms_rows_kernel<T><<<ceil_div_i(a_rows, 256), 256, 0, ctx->stream>>>(A, lda, a_rows, a_cols, sk->sweights);
         else
             sq_norms_cols_kernel<T><<<ceil_div_i(a_cols * 32, 256), 256, 0, ctx->stream>>>(A, lda, a_rows, a_cols,
                                                                                          sk->sweights);
+        timing_end(ctx, 3, e0);
         RLA_TRY(check_launch(ctx, "l2norm_weights"));
         sk->s_has_weights = true;
         RLA_TRY(sample_weighted(ctx, sk, sk->sweights));
     } else if (sk->s_dist == RLA_DIST_UNIFORM) {
         RLA_TRY(sample_weighted(ctx, sk, nullptr));
     } else {
+        // Agmon's indices come in residual order: the plan is built on the host
         RLA_TRY(sample_agmon_t<T>(ctx, sk, a_rows, a_cols, A, lda, x, b, r));
+        return sampling_plan(ctx, sk);
     }
-    return sampling_plan(ctx, sk);
+    plan_sorted_kernel<<<1, 1024, 0, ctx->stream>>>(sk->sidx, sk->s, sk->splan);
+    return check_launch(ctx, "plan_sorted");
 }
 
 int sampling_update(rla_ctx *ctx, rla_sketch *sk, int64_t a_rows, int64_t a_cols, const void *A, int64_t lda,
@@ -590,11 +695,9 @@ int sampling_expand(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_t x_es
                                                                                     beta == 0.0, v_fast);
         RLA_TRY(check_launch(ctx, "sample_scale"));
     }
-    const int64_t U = sk->s_uniq;
-    if (U * nv == 0) return RLA_OK;
-    const int64_t *tgt = sk->splan, *ptr = tgt + U, *pos = ptr + U + 1;
-    sample_scatter_kernel<T><<<ceil_div_i(U * nv, 256), 256, 0, ctx->stream>>>(X, x_es, x_vs, nv, tgt, ptr, pos, U, Y,
-                                                                                y_es, y_vs, (T)alpha, v_fast);
+    if (sk->s * nv == 0) return RLA_OK;
+    sample_scatter_kernel<T><<<ceil_div_i(sk->s * nv, 256), 256, 0, ctx->stream>>>(X, x_es, x_vs, nv, sk->splan, sk->s,
+                                                                                    Y, y_es, y_vs, (T)alpha, v_fast);
     return check_launch(ctx, "sample_scatter");
 }
 
@@ -667,7 +770,9 @@ int rla_sampling_create(rla_ctx *ctx, int card, int dtype, int64_t compression_d
     sk->s_beta = beta;
     sk->scale = 1.0;
     cudaError_t e = cudaMalloc((void **)&sk->sidx, sizeof(int64_t) * sk->s);
-    if (e == cudaSuccess) e = cudaMalloc((void **)&sk->splan, sizeof(int64_t) * (3 * sk->s + 1));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&sk->splan, sizeof(int64_t) * (3 * sk->s + 2));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&sk->s_err, sizeof(int64_t));
+    if (e == cudaSuccess) e = cudaMemsetAsync(sk->s_err, 0, sizeof(int64_t), ctx->stream);
     if (e == cudaSuccess && distribution == RLA_DIST_L2NORM) e = cudaMalloc((void **)&sk->sweights, sizeof(double) * sk->L);
     if (e == cudaSuccess) e = cudaMemsetAsync(sk->sidx, 0, sizeof(int64_t) * sk->s, ctx->stream);
     int rc = e == cudaSuccess ? RLA_OK : set_error(ctx, RLA_E_OOM, "%s", cudaGetErrorString(e));
@@ -706,7 +811,7 @@ int rla_sampling_update(rla_ctx *ctx, rla_sketch *sk, int64_t a_rows, int64_t a_
     RLA_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
     const uint64_t saved = sk->draw_count;
     int rc = sampling_update(ctx, sk, a_rows, a_cols, A, lda, x, b, r);
-    if (rc == RLA_OK) RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (rc == RLA_OK) rc = sampling_finish(ctx, sk);
     if (rc == RLA_OK) sk->draw_count = saved + 1;
     return rc;
 }

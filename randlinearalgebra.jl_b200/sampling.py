@@ -149,11 +149,18 @@ class UniformRecipe(_RecipeBase):
         self.cardinality, self.replace = cardinality, replace
         self._set(A, seed)
 
+    @property
+    def state_space(self):
+        return np.arange(self._dim)
+
+    @property
+    def weights(self):
+        return np.ones(self._dim)
+
     def _set(self, A, seed=None):
         Ad = _device_matrix(A)
         dim = Ad.shape[0] if isinstance(self.cardinality, Left) else Ad.shape[1]
-        self.state_space = np.arange(dim)
-        self.weights = np.ones(dim)
+        self._dim = dim
         self._dist = L.RLA_DIST_UNIFORM
         if seed is not None or not hasattr(self, "_sampler") or self._sampler.args[2] != dim:
             self._sampler = _DeviceSampler(_card_code(self.cardinality), rla_dtype(Ad.dtype), dim, self._dist,
@@ -169,13 +176,23 @@ class L2NormRecipe(_RecipeBase):
         self._sampler = None
         self._set(A, seed)
 
-    def _set(self, A, seed=None):
+    @property
+    def state_space(self):
+        return np.arange(self._dim)
+
+    @property
+    def weights(self):
+        """Squared row (Left) / column (Right) norms of the A of the last update (computed on access)."""
         import torch
+        Ad = self._data[0]
+        left = isinstance(self.cardinality, Left)
+        return torch.linalg.vector_norm(Ad.double(), dim=1 if left else 0).pow(2).cpu().numpy()
+
+    def _set(self, A, seed=None):
         Ad = _device_matrix(A)
         left = isinstance(self.cardinality, Left)
         dim = Ad.shape[0] if left else Ad.shape[1]
-        self.state_space = np.arange(dim)
-        self.weights = torch.sum(Ad.double() ** 2, dim=1 if left else 0).cpu().numpy()
+        self._dim = dim
         self._dist = L.RLA_DIST_L2NORM
         if self._sampler is None or self._sampler.args[2] != dim:
             self._sampler = _DeviceSampler(_card_code(self.cardinality), rla_dtype(Ad.dtype), dim, self._dist,
@@ -204,7 +221,7 @@ class AgmonRecipe(_RecipeBase):
         if self.beta > dim:
             raise ArgumentError(f"`Agmon` beta must be <= number of {'rows' if left else 'columns'} ({dim}), "
                                 f"got beta={self.beta}")
-        self.state_space = np.arange(dim)
+        self._dim = dim
         self.sample_buffer = np.zeros(self.beta, np.int64)
         self.A, self.b, self.x, self.r = A, b, x, r
         self._dist = L.RLA_DIST_AGMON
@@ -213,6 +230,10 @@ class AgmonRecipe(_RecipeBase):
                                            self.replace, self.beta,
                                            _next_seed() if self._seed is None else self._seed)
         self._data = (Ad, _device_vector(x, Ad.dtype), _device_vector(b, Ad.dtype), _device_vector(r, Ad.dtype))
+
+    @property
+    def state_space(self):
+        return np.arange(self._dim)
 
     def _sample(self, k: int) -> np.ndarray:
         if k > self.beta:
