@@ -308,6 +308,40 @@ int rla_ihs_errors(rla_ctx *ctx, rla_ihs *h, double *full_residual, double *ls_g
 int rla_ihs_solve(rla_ctx *ctx, rla_ihs *h, const void *A, int64_t lda, const void *b, void *x, void *r,
                   void *g, int64_t max_it, int64_t collection_rate, double threshold, int error_kind,
                   double *hist, int64_t hist_len, int64_t *iterations, int *converged);
+/* ---- Kaczmarz and ColumnProjection ---------------------------------------------------------
+ * Kaczmarz (src/Solvers/kaczmarz.jl:63-368; Left compressor S, s x m) and ColumnProjection
+ * (src/Solvers/col_projection.jl:63-372; Right compressor S, n x s) on A (m x n, ld lda).
+ * One step is one iteration after the logger check: update_compressor!, the sketched block
+ * (S*A and S*b, or A*S), the sub-problem -- Kaczmarz: the minimum-norm correction of the
+ * sketched rows (LQSolver, lq.jl; the scalar kaczmarz_update! for s = 1; no update when the
+ * sketched rows are zero); ColumnProjection: the least-squares correction over the sketched
+ * columns (QRSolver, qr.jl) -- through the FP64 Cholesky factor of the equilibrated s x s
+ * Gram matrix, then x += alpha*u (and r -= alpha*A*S*u).  b, x, r are device vectors of the
+ * element type the caller owns; ColumnProjection keeps the residual r = b - Ax
+ * (rla_proj_start sets it).  rla_proj_error computes an error method's value for the current
+ * iterate (synchronises): RLA_ERR_FULL_RESIDUAL ||b - Ax|| (full_residual.jl),
+ * RLA_ERR_LS_GRADIENT ||A'r|| (ls_gradient.jl), RLA_ERR_COMPRESSED_RESIDUAL ||Sb - SAx|| of
+ * the last sketched rows (compressed_residual.jl; 0 before the first step); RLA_E_NUMERIC
+ * when the last sub-problem was singular.  Block sizes s <= 4096. */
+typedef struct rla_proj rla_proj;
+#define RLA_PROJ_KACZMARZ 0
+#define RLA_PROJ_COLUMN 1
+#define RLA_ERR_FULL_RESIDUAL 0
+#define RLA_ERR_LS_GRADIENT 1
+#define RLA_ERR_COMPRESSED_RESIDUAL 2
+int rla_proj_create(rla_ctx *ctx, rla_sketch *compressor, int kind, int dtype, int64_t m, int64_t n,
+                    double alpha, rla_proj **out);
+int rla_proj_start(rla_ctx *ctx, rla_proj *h, const void *A, int64_t lda, const void *b, const void *x,
+                   void *r);
+int rla_proj_step(rla_ctx *ctx, rla_proj *h, const void *A, int64_t lda, const void *b, void *x,
+                  void *r);
+int rla_proj_error(rla_ctx *ctx, rla_proj *h, int kind, const void *A, int64_t lda, const void *b,
+                   const void *x, const void *r, double *value);
+/* The last sketched block (owned by the solver): Kaczmarz (S*A)' (n x s, ld n) and S*b (s);
+ * ColumnProjection A*S (m x s, ld m). */
+int rla_proj_workspace(const rla_proj *h, void **compressed_mat, void **compressed_vec);
+int rla_proj_destroy(rla_proj *h);
+
 /* Device workspaces of the solver (owned by it): compressed_mat (s x n, ld s, the element
  * type; the last S*A), update (n; the last u), R_equilibrated (n x n FP64, upper triangle; the
  * Cholesky factor of D (SA)'(SA) D) and d (n FP64; D = diag(d)), so R = R_equilibrated D^-1. */

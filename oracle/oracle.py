@@ -633,3 +633,100 @@ def _solve_tri(T: np.ndarray, v: np.ndarray, lower: bool) -> np.ndarray:
         else:
             out[i] = (v[i] - T[i, i + 1:] @ out[i + 1:]) / T[i, i]
     return out
+
+
+@dataclass
+class ProjResult:
+    x: np.ndarray
+    residual_vec: Optional[np.ndarray]
+    hist: np.ndarray
+    iteration: int
+    converged: bool
+    errors: list
+
+
+def _logger_update(state, err, i, max_it, threshold, collection_rate, hist):
+    """update_logger! of BasicLogger (basic_logger.jl:84-101); state = [record_location]."""
+    conv = (err < threshold) if i < max_it else True
+    if conv:
+        hist[state[0]] = err
+    elif i % collection_rate == 0:
+        hist[state[0]] = err
+        state[0] += 1
+    return conv
+
+
+def kaczmarz_rsolve(A, b, x0, sketches, alpha=1.0, max_it=0, threshold=0.0, collection_rate=1,
+                    error="full") -> ProjResult:
+    """rsolve!(::KaczmarzRecipe, x, A, b) (kaczmarz.jl:323-368) in float64 with the LQ
+    sub-solver (lq.jl: ldiv! through qr!(A')'); ``sketches(i)`` is the Left compressor drawn
+    in iteration i.  error: "full" (FullResidual) or "compressed" (CompressedResidual on the
+    last sketched rows, zero before the first)."""
+    A = A.astype(np.float64)
+    b = b.astype(np.float64)
+    x = x0.astype(np.float64).copy()
+    hist = np.zeros(int(math.ceil(max_it / collection_rate)) + 1 if max_it > 0 else 1)
+    state, it, conv, errs = [0], 0, False, []
+    SA, Sb = None, None
+    for i in range(1, max_it + 1):
+        if error == "full":
+            err = float(np.linalg.norm(b - A @ x))
+        else:
+            err = 0.0 if SA is None else float(np.linalg.norm(Sb - SA @ x))
+        errs.append(err)
+        it = i
+        conv = _logger_update(state, err, i, max_it, threshold, collection_rate, hist)
+        if conv:
+            break
+        S = _as_f64(sketches(i))
+        SA = np.zeros((S.n_rows, A.shape[1]))
+        mul_SA(SA, S, A)
+        Sb = np.zeros(S.n_rows)
+        mul_SA(Sb, S, b)
+        if not np.any(SA):
+            continue
+        if SA.shape[0] == 1:  # kaczmarz_update! (kaczmarz.jl:280-290)
+            a = SA[0]
+            scaling = alpha * (a @ x - Sb[0]) / (a @ a)
+            x -= scaling * a
+        else:                 # kaczmarz_update_block! with the LQ solve (kaczmarz.jl:292-305)
+            r = Sb - SA @ x
+            Q, R = np.linalg.qr(SA.T)  # SA' = QR, SA = R'Q'
+            u = Q @ _solve_tri(R.T, r, lower=True)
+            x += alpha * u
+    return ProjResult(x, None, hist, it, conv, errs)
+
+
+def colproj_rsolve(A, b, x0, sketches, alpha=1.0, max_it=0, threshold=0.0, collection_rate=1) -> ProjResult:
+    """rsolve!(::ColumnProjectionRecipe, x, A, b) (col_projection.jl:328-372) in float64 with
+    LSGradient and the QR sub-solver (qr.jl); ``sketches(i)`` is the Right compressor drawn in
+    iteration i."""
+    A = A.astype(np.float64)
+    b = b.astype(np.float64)
+    x = x0.astype(np.float64).copy()
+    r = b - A @ x
+    hist = np.zeros(int(math.ceil(max_it / collection_rate)) + 1 if max_it > 0 else 1)
+    state, it, conv, errs = [0], 0, False, []
+    for i in range(1, max_it + 1):
+        err = float(np.linalg.norm(A.T @ r))
+        errs.append(err)
+        it = i - 1
+        conv = _logger_update(state, err, i - 1, max_it, threshold, collection_rate, hist)
+        if conv:
+            return ProjResult(x, r, hist, it, conv, errs)
+        S = _as_f64(sketches(i))
+        AS = np.zeros((A.shape[0], S.n_cols))
+        mul_AS(AS, A, S)
+        if AS.shape[1] == 1:  # colproj_update! (col_projection.jl:300-307)
+            u = np.array([AS[:, 0] @ r / (AS[:, 0] @ AS[:, 0])])
+        else:                 # colproj_update_block! with qr!(AS) \ r
+            Q, R = np.linalg.qr(AS)
+            u = _solve_tri(R, Q.T @ r, lower=False)
+        Su = np.zeros(A.shape[1])
+        mul_SA(Su, S, u)
+        x += alpha * Su
+        r -= alpha * (AS @ u)
+    err = float(np.linalg.norm(A.T @ r))
+    errs.append(err)
+    conv = _logger_update(state, err, max_it, max_it, threshold, collection_rate, hist)
+    return ProjResult(x, r, hist, max_it, conv, errs)

@@ -20,6 +20,8 @@ from .sampling import (Sampling, SamplingRecipe, Distribution, DistributionRecip
 from .solvers import (Solver, SolverRecipe, Logger, LoggerRecipe, SolverError, SolverErrorRecipe, BasicLogger,
                       BasicLoggerRecipe, threshold_stop, complete_logger, update_logger_, reset_logger_, FullResidual,
                       FullResidualRecipe, LSGradient, LSGradientRecipe, CompressedResidual, CompressedResidualRecipe,
-                      complete_error, compute_error, IHS, IHSRecipe, complete_solver, rsolve_)
+                      complete_error, compute_error, IHS, IHSRecipe, complete_solver, rsolve_, SubSolver,
+                      SubSolverRecipe, LQSolver, LQSolverRecipe, QRSolver, QRSolverRecipe, complete_sub_solver,
+                      update_sub_solver_, ldiv_, Kaczmarz, KaczmarzRecipe, ColumnProjection, ColumnProjectionRecipe)
 
 __version__ = "0.1.0"

@@ -20,6 +20,8 @@ RLA_F32, RLA_F64 = 0, 1
 RLA_LEFT, RLA_RIGHT = 0, 1
 RLA_SPARSE_SIGN, RLA_COUNT_SKETCH, RLA_SRHT, RLA_FJLT, RLA_GAUSSIAN, RLA_SAMPLING = range(6)
 RLA_DIST_UNIFORM, RLA_DIST_L2NORM, RLA_DIST_AGMON = range(3)
+RLA_PROJ_KACZMARZ, RLA_PROJ_COLUMN = 0, 1
+RLA_ERR_FULL_RESIDUAL, RLA_ERR_LS_GRADIENT, RLA_ERR_COMPRESSED_RESIDUAL = range(3)
 RLA_SIDE_LEFT, RLA_SIDE_RIGHT = 0, 1
 RLA_PREC_NATIVE, RLA_PREC_SPLIT_BF16 = 0, 1
 
@@ -104,6 +106,13 @@ SIGNATURES = {
     "rla_sampling_create": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, i64, i64, ctypes.c_int, ctypes.c_int, i64,
                                            ctypes.c_uint64, ctypes.POINTER(vp)]),
     "rla_sampling_update": (ctypes.c_int, [vp, vp, i64, i64, vp, i64, vp, i64, vp, i64, vp]),
+    "rla_proj_create": (ctypes.c_int, [vp, vp, ctypes.c_int, ctypes.c_int, i64, i64, ctypes.c_double,
+                                       ctypes.POINTER(vp)]),
+    "rla_proj_start": (ctypes.c_int, [vp, vp, vp, i64, vp, vp, vp]),
+    "rla_proj_step": (ctypes.c_int, [vp, vp, vp, i64, vp, vp, vp]),
+    "rla_proj_error": (ctypes.c_int, [vp, vp, ctypes.c_int, vp, i64, vp, vp, vp, ctypes.POINTER(ctypes.c_double)]),
+    "rla_proj_workspace": (ctypes.c_int, [vp, ctypes.POINTER(vp), ctypes.POINTER(vp)]),
+    "rla_proj_destroy": (ctypes.c_int, [vp]),
     "rla_ihs_create": (ctypes.c_int, [vp, vp, ctypes.c_int, i64, i64, ctypes.c_double, ctypes.POINTER(vp)]),
     "rla_ihs_start": (ctypes.c_int, [vp, vp, vp, i64, vp, vp, vp, vp]),
     "rla_ihs_step": (ctypes.c_int, [vp, vp, vp, i64, vp, vp, vp, vp]),

@@ -60,6 +60,12 @@ int gemm(rla_ctx *ctx, int64_t M, int64_t N, int64_t K, const TA *A, int64_t lda
 template <class T>
 int gram_fp64(rla_ctx *ctx, const T *Y, int64_t rows, int64_t l, int64_t ldy, double *G);
 
+// Least-squares pieces (rla_ls.cu): equilibration D G D (d = diag(G)^-1/2) and the
+// solve x = d .* R^-1 R^-T (d .* c) with the Cholesky factor R of the equilibrated G.
+int ls_equilibrate(rla_ctx *ctx, double *G, int64_t l, double *d);
+template <class TX>
+int ls_chol_solve(rla_ctx *ctx, const double *R, int64_t l, const double *d, const double *c, TX *x);
+
 // Small dense FP64 kernels (rla_linalg.cu)
 // In place: G (l x l, ld l) -> upper Cholesky factor R (lower part zeroed).  `shift` is
 // added to the diagonal first.  *breakdown (device int) is set to 1 when a pivot is not

@@ -152,6 +152,24 @@ __global__ void __launch_bounds__(TS_THREADS) ls_trisolve_kernel(const double *R
     for (int64_t i = tid; i < l; i += nt) x[i] = (TX)(d[i] * v[i]);
 }
 
+// D G D with d = diag(G)^-1/2 (so the Cholesky factor is of an equilibrated matrix).
+int ls_equilibrate(rla_ctx *ctx, double *G, int64_t l, double *d) {
+    ls_diag_kernel<<<ceil_div_i(l, 256), 256, 0, ctx->stream>>>(G, l, d);
+    ls_scale_kernel<<<(unsigned)l, 256, 0, ctx->stream>>>(G, l, d);
+    return check_launch(ctx, "ls_equilibrate");
+}
+
+// x = d .* R^-1 R^-T (d .* c) for the factor R of the equilibrated matrix.
+template <class TX>
+int ls_chol_solve(rla_ctx *ctx, const double *R, int64_t l, const double *d, const double *c, TX *x) {
+    const size_t smem = sizeof(double) * (size_t)l;
+    if (smem > 48 * 1024) RLA_CUDA_TRY(ctx, set_smem_max(ls_trisolve_kernel<TX>));
+    ls_trisolve_kernel<TX><<<1, TS_THREADS, smem, ctx->stream>>>(R, l, d, c, x);
+    return check_launch(ctx, "ls_trisolve");
+}
+template int ls_chol_solve<float>(rla_ctx *, const double *, int64_t, const double *, const double *, float *);
+template int ls_chol_solve<double>(rla_ctx *, const double *, int64_t, const double *, const double *, double *);
+
 size_t ls_work_bytes(int64_t s, int64_t n) {
     auto r = [](size_t b) { return (b + 255) & ~size_t(255); };
     return r(sizeof(float) * s * n) + r(sizeof(float) * s) + r(sizeof(double) * n * n) + r(sizeof(double) * 3 * n) +

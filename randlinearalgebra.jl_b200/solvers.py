@@ -24,7 +24,7 @@ import numpy as np
 from . import _lib as L
 from ._arrays import Operand, rla_dtype
 from .compressors import Compressor, CompressorRecipe, Left, SparseSign, complete_compressor
-from .errors import ArgumentError, RLAError
+from .errors import ArgumentError, DimensionMismatch, RLAError
 
 
 # ----------------------------------------------------------------------------------
@@ -318,6 +318,8 @@ def complete_solver(ingredients: Solver, x, A, b, seed=None) -> SolverRecipe:
     """complete_solver(::IHS, x, A, b) (ihs.jl:127-206).  `seed` seeds the compressor's draws
     (default: the next seed of the process-wide sequence, see compressors.seed_)."""
     import torch
+    if isinstance(ingredients, (Kaczmarz, ColumnProjection)):
+        return _complete_proj(ingredients, x, A, b, seed)
     if not isinstance(ingredients, IHS):
         raise ArgumentError(f"No method `complete_solver` exists for solver of type {type(ingredients).__name__}.")
     dt = _torch_dtype(A)
@@ -378,6 +380,8 @@ def _device_vector(v, dt, dev):
 def rsolve_(solver: SolverRecipe, x, A, b) -> None:
     """rsolve!(::IHSRecipe, x, A, b) (ihs.jl:214-254)."""
     import torch
+    if isinstance(solver, (KaczmarzRecipe, ColumnProjectionRecipe)):
+        return _rsolve_proj(solver, x, A, b)
     if not isinstance(solver, IHSRecipe):
         raise ArgumentError(f"No method `rsolve!` exists for solver recipe of type {type(solver).__name__}.")
     if A.shape[0] != solver._m or A.shape[1] != solver._n:
@@ -408,6 +412,290 @@ def rsolve_(solver: SolverRecipe, x, A, b) -> None:
         solver.compressor._refresh_info()
     if isinstance(solver.error, FullResidualRecipe) and solver.error.residual.shape[0] == solver._m:
         solver.error.residual.copy_(bd - Ad @ xd)
+    if copied:
+        if isinstance(x, torch.Tensor):
+            x.copy_(xd)
+        else:
+            x[...] = xd.cpu().numpy()
+        solver.solution_vec = x
+    return None
+
+
+# ----------------------------------------------------------------------------------
+# Sub-solvers (src/Solvers/SubSolvers.jl, SubSolvers/{lq,qr}.jl)
+# ----------------------------------------------------------------------------------
+class SubSolver:
+    """Abstract supertype of the solvers of a sketched block."""
+
+
+class SubSolverRecipe:
+    """Abstract supertype of completed sub-solvers."""
+
+
+class LQSolver(SubSolver):
+    """lq.jl: minimum-norm solution of a wide block (ldiv! through qr!(A')')."""
+
+
+class QRSolver(SubSolver):
+    """qr.jl: least-squares solution of a tall block (ldiv! through qr!(A))."""
+
+
+class LQSolverRecipe(SubSolverRecipe):
+    def __init__(self, A):
+        self.A = A
+
+
+class QRSolverRecipe(SubSolverRecipe):
+    def __init__(self, A):
+        self.A = A
+
+
+def complete_sub_solver(solver: SubSolver, A, *args) -> SubSolverRecipe:
+    if isinstance(solver, LQSolver):
+        return LQSolverRecipe(A)
+    if isinstance(solver, QRSolver):
+        return QRSolverRecipe(A)
+    raise ArgumentError(f"No method `complete_sub_solver` exists for sub-solver of type {type(solver).__name__}.")
+
+
+def update_sub_solver_(solver: SubSolverRecipe, A) -> None:
+    solver.A = A
+
+
+def ldiv_(x, solver: SubSolverRecipe, b) -> None:
+    """ldiv!(x, recipe, b): LQ -> minimum-norm solution, QR -> least-squares solution
+    (a host convenience of the sub-solver API; the device solvers solve their blocks
+    themselves)."""
+    import torch
+    A = solver.A if isinstance(solver.A, torch.Tensor) else torch.as_tensor(np.asarray(solver.A))
+    bb = b if isinstance(b, torch.Tensor) else torch.as_tensor(np.asarray(b))
+    A64, b64 = A.double().cpu(), bb.double().cpu()
+    if isinstance(solver, LQSolverRecipe):
+        sol = A64.T @ torch.linalg.solve(A64 @ A64.T, b64)
+    elif isinstance(solver, QRSolverRecipe):
+        sol = torch.linalg.lstsq(A64, b64.unsqueeze(1)).solution.squeeze(1)
+    else:
+        raise ArgumentError(f"No method `ldiv!` exists for sub-solver of type {type(solver).__name__}.")
+    if isinstance(x, torch.Tensor):
+        x.copy_(sol.to(x.dtype))
+    else:
+        x[...] = sol.numpy()
+
+
+# ----------------------------------------------------------------------------------
+# Kaczmarz (src/Solvers/kaczmarz.jl) and ColumnProjection (src/Solvers/col_projection.jl)
+# ----------------------------------------------------------------------------------
+class Kaczmarz(Solver):
+    """kaczmarz.jl:63-107: fields alpha, compressor, log, error, sub_solver."""
+
+    def __init__(self, compressor: Compressor = None, log: Logger = None, error: SolverError = None,
+                 sub_solver: SubSolver = None, alpha: float = 1.0):
+        compressor = SparseSign(cardinality=Left()) if compressor is None else compressor
+        if type(compressor.cardinality) is not Left:
+            warnings.warn("Compressor has cardinality `Right` but kaczmarzcompresses  from the  `Left`.")
+        self.alpha = float(alpha)
+        self.compressor = compressor
+        self.log = BasicLogger() if log is None else log
+        self.error = FullResidual() if error is None else error
+        self.sub_solver = LQSolver() if sub_solver is None else sub_solver
+
+
+class ColumnProjection(Solver):
+    """col_projection.jl:89-121: fields alpha, compressor, error, log, sub_solver."""
+
+    def __init__(self, alpha: float = 1.0, compressor: Compressor = None, error: SolverError = None,
+                 log: Logger = None, sub_solver: SubSolver = None):
+        from .compressors import Right
+        compressor = SparseSign(cardinality=Right()) if compressor is None else compressor
+        if type(compressor.cardinality) is not Right:
+            warnings.warn("Compressor has cardinality `Left` but ColumnProjectioncompresses from the `Right`. This "
+                          "may cause an inefficiency.")
+        self.alpha = float(alpha)
+        self.compressor = compressor
+        self.error = LSGradient() if error is None else error
+        self.log = BasicLogger() if log is None else log
+        self.sub_solver = QRSolver() if sub_solver is None else sub_solver
+
+
+class _ProjRecipe(SolverRecipe):
+    """Shared device state of KaczmarzRecipe / ColumnProjectionRecipe (rla_proj_*)."""
+
+    def _init_device(self, kind, A, dtype):
+        ctx = L.Context.get(self.compressor._ctx.device)
+        h = ctypes.c_void_p()
+        m, n = A.shape[0], A.shape[1]
+        L.check(L.lib().rla_proj_create(ctx.handle, self.compressor.handle, kind, rla_dtype(dtype), m, n,
+                                        float(self.alpha), ctypes.byref(h)), ctx.handle)
+        self._h, self._ctx, self._m, self._n, self._kind = h, ctx, m, n, kind
+        self._live = False
+
+    def _workspace(self):
+        mat, vec = ctypes.c_void_p(), ctypes.c_void_p()
+        L.check(L.lib().rla_proj_workspace(self._h, ctypes.byref(mat), ctypes.byref(vec)))
+        return mat.value, vec.value
+
+    def _view(self, ptr, shape, strides, dtype):
+        import torch
+        es = 4 if dtype == torch.float32 else 8
+        v = _DeviceView(ptr, shape, tuple(es * s for s in strides), "<f4" if es == 4 else "<f8", self)
+        return torch.as_tensor(v, device=f"cuda:{self._ctx.device}")
+
+    def _error(self, kind, A, b, x, r) -> float:
+        val = ctypes.c_double()
+        lda = max(A.shape[0], 1) if A.shape[1] <= 1 else A.stride(1)
+        L.check(L.lib().rla_proj_error(self._ctx.handle, self._h, kind, A.data_ptr(), lda,
+                                       None if b is None else b.data_ptr(), None if x is None else x.data_ptr(),
+                                       None if r is None else r.data_ptr(), ctypes.byref(val)), self._ctx.handle)
+        return val.value
+
+    def __del__(self):
+        try:
+            if getattr(self, "_h", None):
+                L.lib().rla_proj_destroy(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+
+class KaczmarzRecipe(_ProjRecipe):
+    """kaczmarz.jl:109-160: fields compressor, log, error, sub_solver, alpha, compressed_mat,
+    compressed_vec, solution_vec, update_vec, mat_view, vec_view (views of the solver's last
+    sketched block)."""
+
+    @property
+    def compressed_mat(self):
+        s = self.compressor.n_rows
+        return self._view(self._workspace()[0], (s, self._n), (self._n, 1), self._dtype)
+
+    @property
+    def compressed_vec(self):
+        return self._view(self._workspace()[1], (self.compressor.n_rows,), (1,), self._dtype)
+
+    @property
+    def mat_view(self):
+        return self.compressed_mat
+
+    @property
+    def vec_view(self):
+        return self.compressed_vec
+
+
+class ColumnProjectionRecipe(_ProjRecipe):
+    """col_projection.jl:159-200: fields compressor, log, error, sub_solver, alpha,
+    compressed_mat, solution_vec, update_vec, mat_view, residual_vec."""
+
+    @property
+    def compressed_mat(self):
+        s = self.compressor.n_cols
+        return self._view(self._workspace()[0], (self._m, s), (1, self._m), self._dtype)
+
+    @property
+    def mat_view(self):
+        return self.compressed_mat
+
+
+def _complete_proj(ingredients, x, A, b, seed):
+    import torch
+    kz = isinstance(ingredients, Kaczmarz)
+    dt = _torch_dtype(A)
+    np_dt = np.float32 if dt == torch.float32 else np.float64
+    comp = ingredients.compressor
+    if getattr(comp, "type", np_dt) != np_dt:
+        comp = copy.copy(comp)
+        object.__setattr__(comp, "type", np_dt)
+    compressor = complete_compressor(comp, x, A, b, seed=seed) if kz else complete_compressor(comp, A, b, seed=seed)
+    logger = complete_logger(ingredients.log)
+    error = complete_error(ingredients.error, ingredients, A, b)
+    name = "a kaczmarz solver" if kz else "a `ColumnProjection` solver"
+    if kz:
+        if not hasattr(error, "residual"):
+            raise ArgumentError(f"ErrorRecipe {type(error).__name__} does not contain the field 'residual' and is "
+                                f"not valid for {name}.")
+        if not hasattr(logger, "converged"):
+            raise ArgumentError(f"LoggerRecipe {type(logger).__name__} does not contain the field 'converged' and "
+                                f"is not valid for {name}.")
+        if not isinstance(ingredients.sub_solver, LQSolver):
+            raise ArgumentError("The device Kaczmarz solver takes the LQSolver sub-solver.")
+    else:
+        if not hasattr(error, "gradient"):
+            raise ArgumentError(f"ErrorRecipe {type(error).__name__} does not contain the field 'gradient' and is "
+                                f"not valid for {name}.")
+        if not hasattr(logger, "max_it"):
+            raise ArgumentError(f"LoggerRecipe {type(logger).__name__} does not contain the field `max_it` and is "
+                                f"not valid for {name}.")
+        if not hasattr(logger, "converged"):
+            raise ArgumentError(f"LoggerRecipe {type(logger).__name__} does not contain the field `converged` and "
+                                f"is not valid for {name}.")
+        if not isinstance(ingredients.sub_solver, QRSolver):
+            raise ArgumentError("The device ColumnProjection solver takes the QRSolver sub-solver.")
+    R = (KaczmarzRecipe if kz else ColumnProjectionRecipe)()
+    R.compressor, R.log, R.error, R.alpha = compressor, logger, error, ingredients.alpha
+    R.sub_solver = complete_sub_solver(ingredients.sub_solver, None)
+    R.solution_vec = x
+    R._dtype = dt
+    R._init_device(L.RLA_PROJ_KACZMARZ if kz else L.RLA_PROJ_COLUMN, A, dt)
+    dev = torch.device("cuda", R._ctx.device)
+    R.update_vec = torch.zeros(A.shape[1] if kz else compressor.n_cols, dtype=dt, device=dev)
+    if not kz:
+        R.residual_vec = torch.zeros(A.shape[0], dtype=dt, device=dev)
+    return R
+
+
+def _proj_error(solver, A, b, x):
+    """compute_error for the built-in error methods, on the device solver."""
+    e = solver.error
+    if isinstance(e, FullResidualRecipe):
+        return solver._error(L.RLA_ERR_FULL_RESIDUAL, A, b, x, None)
+    if isinstance(e, LSGradientRecipe):
+        if not isinstance(solver, ColumnProjectionRecipe):
+            raise ArgumentError(f"type {type(solver).__name__} has no field residual_vec")
+        return solver._error(L.RLA_ERR_LS_GRADIENT, A, None, None, solver.residual_vec)
+    if isinstance(e, CompressedResidualRecipe):
+        if not isinstance(solver, KaczmarzRecipe):
+            raise ArgumentError(f"type {type(solver).__name__} has no field vec_view")
+        return solver._error(L.RLA_ERR_COMPRESSED_RESIDUAL, A, None, x, None)
+    return compute_error(e, solver, A, b)
+
+
+def _rsolve_proj(solver, x, A, b):
+    import torch
+    kz = isinstance(solver, KaczmarzRecipe)
+    reset_logger_(solver.log)
+    if kz:
+        if x.shape[0] != A.shape[1]:
+            raise DimensionMismatch(f"Dimension of `x`, {x.shape[0]} is different from number of columns in `A`,"
+                                    f"{A.shape[1]}.")
+        if b.shape[0] != A.shape[0]:
+            raise DimensionMismatch(f"Dimension of `b`, {b.shape[0]} is different from number of rows in `A`,"
+                                    f"{A.shape[0]}.")
+    dt = solver._dtype
+    dev = torch.device("cuda", solver._ctx.device)
+    Ad = _device_matrix(A, dt, dev)
+    bd, _ = _device_vector(b, dt, dev)
+    xd, copied = _device_vector(x, dt, dev)
+    solver.solution_vec = xd
+    lib, ctx = L.lib(), solver._ctx
+    lda = max(Ad.shape[0], 1) if Ad.shape[1] <= 1 else Ad.stride(1)
+    rp = None if kz else solver.residual_vec.data_ptr()
+    L.check(lib.rla_proj_start(ctx.handle, solver._h, Ad.data_ptr(), lda, bd.data_ptr(), xd.data_ptr(), rp),
+            ctx.handle)
+    off = 0 if kz else 1  # ColumnProjection logs iteration i-1 (col_projection.jl:334)
+    for i in range(1, solver.log.max_it + 1):
+        err = _proj_error(solver, Ad, bd, xd)
+        update_logger_(solver.log, err, i - off)
+        if solver.log.converged:
+            break
+        L.check(lib.rla_proj_step(ctx.handle, solver._h, Ad.data_ptr(), lda, bd.data_ptr(), xd.data_ptr(), rp),
+                ctx.handle)
+        solver.compressor._cache = None
+    else:
+        if not kz:  # col_projection.jl:368-369: the error after the last iteration
+            update_logger_(solver.log, _proj_error(solver, Ad, bd, xd), solver.log.max_it)
+    solver.compressor._refresh_info()
+    if isinstance(solver.error, FullResidualRecipe) and solver.error.residual.shape[0] == Ad.shape[0]:
+        solver.error.residual.copy_(bd - Ad @ xd)
+    if isinstance(solver.error, LSGradientRecipe) and not kz:
+        solver.error.gradient.copy_(-(Ad.T @ solver.residual_vec))
     if copied:
         if isinstance(x, torch.Tensor):
             x.copy_(xd)
