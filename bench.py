@@ -833,6 +833,126 @@ def sampling_cpu_sample(m, s, ncol=64):
 
 
 # --------------------------------------------------------------------------------------
+# Kaczmarz workload
+# --------------------------------------------------------------------------------------
+KZ_METRIC = "block Kaczmarz iterations/s (sampled rows, LQ block solve)"
+# kernel launches of one step: redraw (Sampling: keys, 8 radix hist/pick pairs, count, scan,
+# write, plan), S*A and S*b gathers, residual (2), Gram (2), zero check, equilibration (2),
+# Cholesky (1 CTA for s < 128), triangular solve, mask, update
+KZ_LAUNCHES_PER_STEP = 35
+
+
+def kaczmarz_arm(args):
+    """rsolve!(Kaczmarz) on A 2^18 x 512 FP32 ~ N(0,1), b = A x*, with a Sampling(Left,
+    compression_dim = 64, Uniform(replace = false)) compressor: one step = one iteration
+    (update_compressor!, the 64 sampled rows and entries of b, the LQ block solve through the
+    FP64 Cholesky factor of their Gram matrix, x += u)."""
+    import numpy as np
+    import torch
+
+    world, rank, local = dist_setup(args.gpus)
+    from __graft_entry__ import load_package
+    rla = load_package()
+    from randlinearalgebra_b200 import _lib as L
+    dev = torch.device("cuda", local if world > 1 else 0)
+    m, n, s = args.ihs_m, args.ihs_n, 64
+    g = torch.Generator(device=dev)
+    g.manual_seed(9 + rank)
+    A = torch.randn(n, m, device=dev, generator=g, dtype=torch.float32).t()
+    b = A @ torch.randn(n, device=dev, generator=g, dtype=torch.float32)
+    x = torch.zeros(n, device=dev, dtype=torch.float32)
+    solver = rla.complete_solver(rla.Kaczmarz(compressor=rla.Sampling(compression_dim=s,
+                                                                      distribution=rla.Uniform()),
+                                              log=rla.BasicLogger(max_it=10)), x, A, b, seed=9000 + rank)
+    ctx = solver._ctx
+    lib = L.lib()
+    stream = torch.cuda.current_stream(dev)
+    cargs = (ctx.handle, solver._h, A.data_ptr(), A.stride(1), b.data_ptr(), x.data_ptr(), None)
+    L.check(lib.rla_proj_start(*cargs), ctx.handle)
+    for _ in range(args.warmup):
+        L.check(lib.rla_proj_step(*cargs), ctx.handle)
+    K = args.steps
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    props = torch.cuda.get_device_properties(dev)
+    clocks = ClockSampler(f"GPU-{props.uuid}" if getattr(props, "uuid", None) else dev.index)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    h0 = time.perf_counter()
+    t0.record(stream)
+    for _ in range(K):
+        L.check(lib.rla_proj_step(*cargs), ctx.handle)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    host_s = time.perf_counter() - h0
+    clk = clocks.stop()
+    barrier(world)
+    ms = allreduce_max(t0.elapsed_time(t1), world)
+    value = world * K / (ms / 1e3)
+    res = float(torch.linalg.vector_norm(b - A @ x) / torch.linalg.vector_norm(b))
+    # end to end: rsolve_ with pinned host A, b, x (A copied once per solve)
+    A_h = torch.empty(n, m, dtype=torch.float32, pin_memory=True).t()
+    A_h.copy_(A)
+    b_h = b.cpu().pin_memory()
+    x_h = torch.zeros(n, dtype=torch.float32, pin_memory=True)
+    e2e_it = 50
+    sol_h = rla.complete_solver(rla.Kaczmarz(compressor=rla.Sampling(compression_dim=s, distribution=rla.Uniform()),
+                                             log=rla.BasicLogger(max_it=e2e_it)), x_h, A_h, b_h, seed=9500 + rank)
+    torch.cuda.synchronize()
+    w0 = time.perf_counter()
+    rla.rsolve_(sol_h, x_h, A_h, b_h)
+    torch.cuda.synchronize()
+    e2e_s = allreduce_max(time.perf_counter() - w0, world)
+    e2e = {"value": round(world * e2e_it / e2e_s, 3), "unit": "iterations/s",
+           "h2d_bytes_per_step": round(4 * (m * n + m + n) / e2e_it), "d2h_bytes_per_step": round(4 * n / e2e_it + 8),
+           "ms_per_step": round(e2e_s * 1e3 / e2e_it, 3),
+           "note": f"one rsolve_ of {e2e_it} iterations (FullResidual checked every iteration: a pass over A)"}
+    del A_h
+    if rank != 0:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        cpu = kaczmarz_cpu_sample(m, n, s)
+    line = {"metric": KZ_METRIC, "value": round(value, 2), "unit": "iterations/s", "n_gpus": world, "steps": K,
+            "warmup": args.warmup, "ms_per_step": round(ms / K, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (Gram, Cholesky and solves f64)",
+            "data": "synthetic A ~ N(0,1), b = A x* generated on device (seed 9+rank)",
+            "config": {"workload": f"kaczmarz: A {m}x{n} f32, sampling left s={s} uniform without replacement",
+                       "m": m, "n": n, "s": s, "parallelism": f"replicas x{world}",
+                       "host_ms_per_step": round(host_s * 1e3 / K, 4)},
+            "roofline": {"bound": "latency", "note": "each step moves ~4*s*n bytes; the step is a chain of ~35 "
+                         "small launches", "achieved": None, "peak": None, "frac": None, "traffic": None},
+            "solution": {"rel_residual_after_warmup_and_steps": res},
+            "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": KZ_LAUNCHES_PER_STEP * K}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def kaczmarz_cpu_sample(m, n, s, iters=200):
+    """The oracle's rsolve! (numpy float64, LAPACK QR for the LQ block) on the same shape."""
+    import numpy as np
+
+    from __graft_entry__ import load_oracle
+    orc = load_oracle()
+    rng = np.random.default_rng(9)
+    A = np.asfortranarray(rng.standard_normal((m, n), dtype=np.float32))
+    b = A @ rng.standard_normal(n).astype(np.float32)
+    sk = [orc.draw_sampling(rng, "left", s, m, replace=False, dtype=np.float32) for _ in range(iters)]
+    t0 = time.perf_counter()
+    orc.kaczmarz_rsolve(A, b, np.zeros(n, np.float32), lambda i: sk[i - 1], max_it=iters + 1, threshold=-1.0,
+                        error="compressed")
+    dt = time.perf_counter() - t0
+    return {"value": round(iters / dt, 3), "unit": "iterations/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"{iters} iterations of the oracle's Kaczmarz rsolve! (CompressedResidual, so no full pass "
+                      f"over A per iteration) on the same {m}x{n} shape"}
+
+
+# --------------------------------------------------------------------------------------
 # Batched RandSVD workload
 # --------------------------------------------------------------------------------------
 BT_COUNT = 512
@@ -1149,7 +1269,7 @@ def main():
     ap.add_argument("--cols", type=int, default=NCOL,
                     help="columns of A (default 512, the benchmark workload; smaller values make small "
                          "cases of the same kernels for profiler captures)")
-    ap.add_argument("--workload", choices=["sketch", "randsvd", "batched", "serve", "ihs", "sampling"],
+    ap.add_argument("--workload", choices=["sketch", "randsvd", "batched", "serve", "ihs", "sampling", "kaczmarz"],
                     default="sketch",
                     help="sketch: SRHT + CountSketch apply (default); randsvd: mixed-precision RandSVD; "
                          "batched: 512 uneven RandSVD instances")
@@ -1184,6 +1304,13 @@ def main():
                               "for the sketch and randsvd workloads only"}), flush=True)
         else:
             batched_arm(args)
+    elif args.workload == "kaczmarz":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "kaczmarz workload: the reference arm is timed "
+                              "for the sketch and randsvd workloads only (the CPU restatement is in cpu_baseline)"}),
+                  flush=True)
+        else:
+            kaczmarz_arm(args)
     elif args.workload == "sampling":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "sampling workload: the reference arm is timed "

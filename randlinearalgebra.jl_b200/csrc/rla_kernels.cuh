@@ -15,7 +15,9 @@ int sketch_redraw_async(rla_ctx *ctx, rla_sketch *sk);
 
 // Sampling (rla_sampling.cu): draw for the current distribution, gather / scatter-add
 // applies, parity-mode indices.
-int sampling_draw(rla_ctx *ctx, rla_sketch *sk);
+// `sync`: read the draw's precondition flags (and wait); without it they stay on the device
+// for the next synchronous call to report.
+int sampling_draw(rla_ctx *ctx, rla_sketch *sk, bool sync);
 int sampling_set_indices(rla_ctx *ctx, rla_sketch *sk, const int64_t *idx);
 template <class T>
 int sampling_compress(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_t x_es, int64_t x_vs, int64_t nv, T *Y,

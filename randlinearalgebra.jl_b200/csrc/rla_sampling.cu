@@ -625,7 +625,7 @@ static int sample_agmon_t(rla_ctx *ctx, rla_sketch *sk, int64_t a_rows, int64_t 
 
 // Draw for the current distribution.  Uniform needs no data; L2Norm uses the weights of the
 // last rla_sampling_update (or those passed in); Agmon needs x, A, b every time.
-int sampling_draw(rla_ctx *ctx, rla_sketch *sk) {
+int sampling_draw(rla_ctx *ctx, rla_sketch *sk, bool sync) {
     int rc = RLA_OK;
     if (sk->s_dist == RLA_DIST_UNIFORM) rc = sample_weighted(ctx, sk, nullptr);
     else if (sk->s_dist == RLA_DIST_L2NORM) {
@@ -638,7 +638,7 @@ int sampling_draw(rla_ctx *ctx, rla_sketch *sk) {
         plan_sorted_kernel<<<1, 1024, 0, ctx->stream>>>(sk->sidx, sk->s, sk->splan);
         rc = check_launch(ctx, "plan_sorted");
     }
-    if (rc == RLA_OK) rc = sampling_finish(ctx, sk);
+    if (rc == RLA_OK && sync) rc = sampling_finish(ctx, sk);
     return rc;
 }
 
@@ -777,7 +777,7 @@ int rla_sampling_create(rla_ctx *ctx, int card, int dtype, int64_t compression_d
     if (e == cudaSuccess) e = cudaMemsetAsync(sk->sidx, 0, sizeof(int64_t) * sk->s, ctx->stream);
     int rc = e == cudaSuccess ? RLA_OK : set_error(ctx, RLA_E_OOM, "%s", cudaGetErrorString(e));
     // Uniform draws at once; L2Norm and Agmon draw in rla_sampling_update (they need A)
-    if (rc == RLA_OK) rc = distribution == RLA_DIST_UNIFORM ? sampling_draw(ctx, sk) : sampling_plan(ctx, sk);
+    if (rc == RLA_OK) rc = distribution == RLA_DIST_UNIFORM ? sampling_draw(ctx, sk, true) : sampling_plan(ctx, sk);
     if (rc == RLA_OK) RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     if (rc != RLA_OK) {
         rla_sketch_destroy(sk);

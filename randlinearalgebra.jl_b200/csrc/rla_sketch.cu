@@ -519,7 +519,7 @@ static Rng make_rng(const rla_sketch *sk) {
 static int draw(rla_ctx *ctx, rla_sketch *sk, bool sync = true) {
     Rng rng = make_rng(sk);
     const int kind = sk->p.kind;
-    if (kind == RLA_SAMPLING) return sampling_draw(ctx, sk);
+    if (kind == RLA_SAMPLING) return sampling_draw(ctx, sk, sync);
     if (kind == RLA_SPARSE_SIGN || kind == RLA_COUNT_SKETCH) {
         draw_sparse_kernel<<<ceil_div_i(sk->L, 128), 128, 0, ctx->stream>>>(
             rng, kind == RLA_SPARSE_SIGN ? STREAM_SPARSE : STREAM_COUNT, sk->L, (int)sk->nnz, sk->s,
