@@ -512,13 +512,13 @@ int householder_q(rla_ctx *ctx, T *Y, int64_t m, int64_t l, int64_t ldy, double 
 template int householder_q<float>(rla_ctx *, float *, int64_t, int64_t, int64_t, double *);
 template int householder_q<double>(rla_ctx *, double *, int64_t, int64_t, int64_t, double *);
 
-// ---- multi-CTA blocked right-looking Cholesky (l >= MC_MIN) ------------------------------
+// ---- blocked right-looking Cholesky over several CTAs (l >= MC_MIN) ------------------------
 // Panel step p (MB columns): chol_panel_kernel factors the diagonal block in every CTA
 // (redundantly; CTA 0 writes it back) and solves R_pp' X = G(p:p+pb, cols) for the CTA's
 // 256 columns of the panel rows (one thread per column), zeroing the mirrored lower entries
 // G(cols, p:p+pb); chol_syrk_kernel then updates the trailing upper triangle,
 // G(I, J) -= R(p, I)' R(p, J), in 64 x 64 tiles (I <= J) spread over the GPU.
-constexpr int MB = 64, MC_MIN = 128, MP_THREADS = 256;
+constexpr int MB = 64, MC_MIN = 33, MP_THREADS = 256;
 
 // Upper Cholesky of the diagonal block G(p:p+pb, p:p+pb) (+ shift on its diagonal) into R
 // (shared, ld MB+2, rows t < pb, zero below the diagonal) and rinv[t] = 1/R(t,t).  The 256
@@ -552,7 +552,7 @@ __device__ void chol_diag_block(const double *G, int64_t l, int64_t p, int pb, d
             if (tid == 0) *bad = 1;
             v = 1.0;
         }
-        const double piv = sqrt(v), rp = 1.0 / piv, rp2 = rp * rp;
+        const double rp = rsqrt(v), piv = v * rp, rp2 = rp * rp;
         if (tid < MB) {
             const int c = tid;
             if (c >= t && c < pb) R[t][c] = c == t ? piv : buf[c] * rp;

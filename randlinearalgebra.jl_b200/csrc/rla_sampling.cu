@@ -150,16 +150,25 @@ __global__ void radix_hist_kernel(const uint64_t *key, int64_t n, const SelState
 // The digit at `shift` of the threshold: the first digit whose cumulative count reaches
 // the remaining rank.  One CTA of 256 threads; the histogram is cleared for the next pass.
 __global__ void radix_pick_kernel(SelState *st, unsigned *hist, int shift) {
-    if (threadIdx.x == 0) {
-        int64_t rem = st->rem;
-        int d = 0;
-        for (; d < 255 && rem > (int64_t)hist[d]; ++d) rem -= hist[d];
-        st->rem = rem;
-        st->prefix |= (uint64_t)d << shift;
+    __shared__ int64_t inc[256];
+    const int t = threadIdx.x;
+    const int64_t h = hist[t];
+    inc[t] = h;
+    __syncthreads();
+    for (int off = 1; off < 256; off <<= 1) {  // inclusive prefix sums of the counts
+        const int64_t v = t >= off ? inc[t - off] : 0;
+        __syncthreads();
+        inc[t] += v;
+        __syncthreads();
+    }
+    const int64_t rem = st->rem, before = inc[t] - h;
+    // the digit whose bucket holds the rem-th key (the last one if rounding ever overshoots)
+    if ((before < rem && rem <= inc[t]) || (t == 255 && rem > inc[255])) {
+        st->rem = rem - before;
+        st->prefix |= (uint64_t)t << shift;
         st->mask |= (uint64_t)255 << shift;
     }
-    __syncthreads();
-    hist[threadIdx.x] = 0;
+    hist[t] = 0;
 }
 
 // count(key < T) by atomics on a 64-bit counter (integer sums are order-independent).
