@@ -50,13 +50,17 @@ __global__ void draw_sparse_kernel(Rng rng, uint32_t stream, int64_t L, int nnz,
 // with every lane adding one value to its bucket.  Here, per tile (one warp per tile):
 //  * in every sub-round, lanes whose bucket repeats an earlier lane's are marked deferred
 //    (bit 30 of their main word), so the main sub-rounds touch distinct bins;
-//  * deferred items are packed greedily, in (sub-round, lane) order, into extra rounds in
-//    which each lane holds at most one item and all buckets differ;
-//  * tiles with more than MAX_DEFER deferred items or MAX_XROUNDS extra rounds are marked
-//    SLOW and resolved at run time instead (only for tiny compression dimensions).
+//  * deferred items are packed first-fit, in (sub-round, lane) order, into extra rounds in
+//    which each lane holds at most one item and all shared-memory banks (bucket mod 32),
+//    hence all buckets, differ: an extra round costs one wavefront per access;
+//  * tiles with more than SS_MAX_DEFER deferred items or SS_MAX_XROUNDS extra rounds are
+//    marked SLOW and resolved at run time instead (only for tiny compression dimensions).
+// The packing runs on all lanes at once: lane r keeps the lane and bank masks of extra
+// round r, and a ballot picks the first round that takes an item.
 // Pass 0 writes the main words and counts extra rounds; pass 1 (after an exclusive scan of
 // the counts) writes the extra words and the tile flags.  Both passes schedule identically.
-constexpr int SCHED_WARPS = 8, MAX_DEFER = 64, MAX_XROUNDS = 16;
+constexpr int SCHED_WARPS = 8, SS_MAX_DEFER = 512, SS_MAX_XROUNDS = 32;
+constexpr int MAX_DEFER = 64;  // CountSketch schedule: deferred entries per batch
 constexpr uint32_t TILE_SLOW = 0x80000000u;
 
 template <int PASS>
@@ -64,11 +68,8 @@ __global__ void __launch_bounds__(SCHED_WARPS * 32) sparse_sched_kernel(const in
                                                                          int64_t L, int nnz, uint32_t *meta,
                                                                          int32_t *nrounds, const int64_t *round_base,
                                                                          uint32_t *tile_flags, uint32_t *extra) {
-    __shared__ uint32_t list[SCHED_WARPS][MAX_DEFER];
-    __shared__ uint32_t rlanes[SCHED_WARPS][MAX_XROUNDS];
-    __shared__ uint32_t rbkt[SCHED_WARPS][MAX_XROUNDS][32];
-    __shared__ uint8_t place[SCHED_WARPS][MAX_DEFER];
-    __shared__ int nround_s[SCHED_WARPS];
+    __shared__ uint32_t list[SCHED_WARPS][SS_MAX_DEFER];
+    __shared__ uint8_t place[SCHED_WARPS][SS_MAX_DEFER];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int64_t tile = (int64_t)blockIdx.x * SCHED_WARPS + w;
     const int64_t ntile = (L + 127) / 128;
@@ -87,44 +88,34 @@ __global__ void __launch_bounds__(SCHED_WARPS * 32) sparse_sched_kernel(const in
             const unsigned bal = __ballot_sync(FULL, defer);
             if (defer) {
                 const int pos = cnt + __popc(bal & lt);
-                if (pos < MAX_DEFER) list[w][pos] = b | ((uint32_t)t << 22) | ((uint32_t)lane << 24) | (neg << 31);
+                if (pos < SS_MAX_DEFER) list[w][pos] = b | ((uint32_t)t << 22) | ((uint32_t)lane << 24) | (neg << 31);
             }
             cnt += __popc(bal);
         }
     __syncwarp();
     int R = 0;
-    bool slow = cnt > MAX_DEFER;
-    if (!slow && lane == 0) {
-        for (int k = 0; k < cnt && !slow; ++k) {
-            const uint32_t it = list[w][k];
-            const uint32_t bk = it & 0x3fffffu, ln = (it >> 24) & 31u;
-            int r = 0;
-            for (; r < R; ++r) {
-                if (rlanes[w][r] & (1u << ln)) continue;
-                bool clash = false;
-                for (int q = 0; q < 32 && !clash; ++q)
-                    if ((rlanes[w][r] >> q) & 1u) clash = rbkt[w][r][q] == bk;
-                if (!clash) break;
-            }
-            if (r == R) {
-                if (R == MAX_XROUNDS) {
-                    slow = true;
-                    break;
-                }
-                rlanes[w][R++] = 0u;
-            }
-            rlanes[w][r] |= 1u << ln;
-            rbkt[w][r][ln] = bk;
-            place[w][k] = (uint8_t)r;
+    bool slow = cnt > SS_MAX_DEFER;
+    uint32_t rl = 0u, rb = 0u;  // lane r: lanes and banks taken in extra round r
+    for (int k = 0; k < cnt && !slow; ++k) {  // warp-uniform trip count
+        const uint32_t it = list[w][k];
+        const uint32_t lbit = 1u << ((it >> 24) & 31u), bbit = 1u << (it & 31u);
+        const unsigned fits = __ballot_sync(FULL, lane < R && !((rl & lbit) | (rb & bbit)));
+        int r;
+        if (fits) {
+            r = __ffs(fits) - 1;
+        } else if (R < SS_MAX_XROUNDS) {
+            r = R++;
+        } else {
+            slow = true;
+            break;
         }
-        nround_s[w] = slow ? -1 : R;
+        if (lane == r) {
+            rl |= lbit;
+            rb |= bbit;
+        }
+        if (lane == 0) place[w][k] = (uint8_t)r;
     }
-    __syncwarp();
-    if (!slow) R = nround_s[w];
-    if (R < 0) {
-        slow = true;
-        R = 0;
-    }
+    if (slow) R = 0;
     if (PASS == 0) {
         if (lane == 0) nrounds[tile] = slow ? 0 : R;
         return;
@@ -462,10 +453,10 @@ static int build_meta(rla_ctx *ctx, rla_sketch *sk) {
     sparse_sched_kernel<0><<<blocks, SCHED_WARPS * 32, 0, ctx->stream>>>(sk->bucket, sk->negative, sk->L, (int)sk->nnz,
                                                                          sk->meta, nr, nullptr, nullptr, nullptr);
     RLA_TRY(check_launch(ctx, "sparse_sched(0)"));
-    if (ntile * MAX_XROUNDS < (int64_t(1) << 23)) {
-        // the schedule never needs more than MAX_XROUNDS rounds per tile: size `extra` for
+    if (ntile * SS_MAX_XROUNDS < (int64_t(1) << 23)) {
+        // the schedule never needs more than SS_MAX_XROUNDS rounds per tile: size `extra` for
         // that once and scan the counts on the device, so a redraw waits on nothing
-        const int64_t cap = std::max<int64_t>(ntile * MAX_XROUNDS, 1);
+        const int64_t cap = std::max<int64_t>(ntile * SS_MAX_XROUNDS, 1);
         if (sk->extra_rounds_cap < cap) {
             if (sk->extra) RLA_CUDA_TRY(ctx, cudaFree(sk->extra));
             sk->extra = nullptr;
@@ -491,7 +482,8 @@ static int build_meta(rla_ctx *ctx, rla_sketch *sk) {
         hb[i] = tot;
         tot += hn[i];
     }
-    if (tot >= (int64_t(1) << 24)) return set_error(ctx, RLA_E_UNSUPPORTED, "too many deferred rounds");
+    // a tile flag holds the tile's first extra round in bits 8..30
+    if (tot >= (int64_t(1) << 23)) return set_error(ctx, RLA_E_UNSUPPORTED, "too many deferred rounds");
     if (tot > sk->extra_rounds_cap) {
         if (sk->extra) RLA_CUDA_TRY(ctx, cudaFree(sk->extra));
         sk->extra = nullptr;

@@ -217,6 +217,36 @@ __device__ __forceinline__ T pick4(const T (&v)[4], uint32_t t) {
     return (t & 2u) ? hi : lo;
 }
 
+constexpr int XPF = 4;  // extra-round words a lane keeps in flight
+
+// First XPF extra words of a non-SLOW tile (0 past its round count), loaded before the
+// tile's main sub-rounds so that their latency hides behind them.
+__device__ __forceinline__ void extra_prefetch(const uint32_t *extra, uint32_t flag, int lane, uint32_t (&pf)[XPF]) {
+    const int R = (int)(flag & 0xffu);
+    const uint32_t *xp = extra + (int64_t)(flag >> 8) * 32 + lane;
+#pragma unroll
+    for (int i = 0; i < XPF; ++i) pf[i] = (i < R) ? __ldg(xp + i * 32) : 0u;
+}
+
+// Extra rounds of a non-SLOW tile; word r + XPF is loaded while round r runs.
+template <class T, bool WIN>
+__device__ __forceinline__ void extra_rounds(const CompressContigParams<T> &p, T *bins, const T (&val)[4],
+                                             uint32_t flag, int lane, uint32_t (&pf)[XPF]) {
+    const int R = (int)(flag & 0xffu);
+    const uint32_t *xp = p.extra + (int64_t)(flag >> 8) * 32 + lane;
+    for (int r = 0; r < R; r += XPF) {
+#pragma unroll
+        for (int i = 0; i < XPF; ++i) {
+            if (r + i < R) {
+                const uint32_t w = pf[i];
+                pf[i] = (r + i + XPF < R) ? __ldg(xp + (r + i + XPF) * 32) : 0u;
+                rmw<T, WIN>(bins, pick4(val, (w >> 22) & 3u), w, (w & BIT_VALID) != 0u, p.bin_lo, p.bin_cnt);
+                __syncwarp();
+            }
+        }
+    }
+}
+
 // One 128-element tile kk of vector xv whose values are already in registers: lane holds
 // elements 4*lane .. 4*lane+3; metadata of nonzero slot e is meta[(kk*nnz + e)*128 ...].
 template <class T, bool WIN, bool CHECK>
@@ -232,6 +262,8 @@ __device__ __forceinline__ void tile_rounds(const CompressContigParams<T> &p, T 
             }
         return;
     }
+    uint32_t pf[XPF];
+    extra_prefetch(p.extra, flag, lane, pf);
     for (int e = 0; e < p.nnz; ++e) {
         const uint32_t *mp = p.meta + (kk * p.nnz + e) * 128 + lane * 4;
         uint32_t mw[4];
@@ -249,15 +281,7 @@ __device__ __forceinline__ void tile_rounds(const CompressContigParams<T> &p, T 
             __syncwarp();
         }
     }
-    if (flag) {  // extra rounds for the deferred items (warp-uniform)
-        const int R = (int)(flag & 0xffu);
-        const uint32_t *xp = p.extra + (int64_t)(flag >> 8) * 32 + lane;
-        for (int r = 0; r < R; ++r) {
-            const uint32_t w = __ldg(xp + r * 32);
-            rmw<T, WIN>(bins, pick4(val, (w >> 22) & 3u), w, (w & BIT_VALID) != 0u, p.bin_lo, p.bin_cnt);
-            __syncwarp();
-        }
-    }
+    extra_rounds<T, WIN>(p, bins, val, flag, lane, pf);  // deferred items (warp-uniform count)
 }
 
 // U full CountSketch tiles held in registers.
@@ -289,20 +313,14 @@ struct Batch {
                 tile_rounds<T, WIN, false>(p, bins, val[b], k + b, (k + b) * 128 + lane * 4, fl[b], lane);
                 continue;
             }
+            uint32_t pf[XPF];
+            extra_prefetch(p.extra, fl[b], lane, pf);
 #pragma unroll
             for (int t = 0; t < 4; ++t) {
                 rmw<T, WIN>(bins, val[b][t], mw[b][t], !(mw[b][t] & BIT_DEFER), p.bin_lo, p.bin_cnt);
                 __syncwarp();
             }
-            if (fl[b]) {
-                const int R = (int)(fl[b] & 0xffu);
-                const uint32_t *xp = p.extra + (int64_t)(fl[b] >> 8) * 32 + lane;
-                for (int r = 0; r < R; ++r) {
-                    const uint32_t w = __ldg(xp + r * 32);
-                    rmw<T, WIN>(bins, pick4(val[b], (w >> 22) & 3u), w, (w & BIT_VALID) != 0u, p.bin_lo, p.bin_cnt);
-                    __syncwarp();
-                }
-            }
+            extra_rounds<T, WIN>(p, bins, val[b], fl[b], lane, pf);
         }
     }
 };

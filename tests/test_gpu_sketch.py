@@ -86,6 +86,17 @@ def test_left_compress_fused_path(rla, orc, dev, kind, dtype):
         assert err < TOL[dtype], (kind, L, s, k, err)
 
 
+@pytest.mark.parametrize("s", [24, 40, 96, 128, 256, 2048])
+def test_sparse_sign_deferral_regimes(rla, orc, dev, s):
+    """nnz = 8 over compression dimensions from ones whose tiles overflow the deferral
+    schedule (run-time resolution) through many extra rounds per tile to almost none."""
+    rng = np.random.default_rng(s)
+    for dtype in (np.float32, np.float64):
+        S = make(rla, "sparse_sign", "left", s, 30011, dtype, seed=3 * s)
+        err = run_orient(rla, orc, S, "SA", 9, dtype, dev, rng, alpha=1.0, beta=0.0)
+        assert err < TOL[dtype], (s, dtype, err)
+
+
 @pytest.mark.parametrize("dtype,L,s,k", [(np.float64, 70001, 40000, 3), (np.float32, 100003, 60000, 2)])
 def test_count_sketch_windowed_bins(rla, orc, dev, dtype, L, s, k):
     """Compression dimensions whose bins exceed one CTA's shared memory (several bin windows)."""
