@@ -295,7 +295,7 @@ struct rla_sketch {
     // SRHT
     int32_t *rows = nullptr;       // [s] sampled padded rows (op)
     uint32_t *signbits = nullptr;  // [ceil(N/32)] bit r = 1 means +1
-    uint4 *sign_tl = nullptr;      // fused compress kernel: per (chunk, thread) 128 sign bits in register order
+    uint4 *sign_tl = nullptr;      // fused compress kernel: per (chunk, thread) sign bits in register order (FP32: 64 as uint2, FP64: 128)
     int32_t *p2_ptr = nullptr;     // expand tables: per low-bit position, samples sorted
     int32_t *p2_list = nullptr;
     int64_t chunk = 0;             // WHT chunk length used by the expand tables

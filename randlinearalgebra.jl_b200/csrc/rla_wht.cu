@@ -5,17 +5,16 @@
 // rows (srht.jl:220-286, fwht.jl:21-70).  Here the left compress (S*A on column-major A)
 // is one pass over A:
 //
-//   N = N1 * CH with CH = 2^14 (FP32) / 2^12 (FP64).  For a padded column x,
-//   y[r] = sum_c (-1)^popc(r1 & c) * Z_c[r2],  r = r1*CH + r2,
-//   where Z_c = H_CH (D x)[c*CH : (c+1)*CH] is the natural-order WHT of chunk c.
+//   N = N1 * 2^CH with CH = 14 (FP32) / 13 (FP64).  For a padded column x,
+//   y[r] = sum_c (-1)^popc(r1 & c) * Z_c[r2],  r = r1*2^CH + r2,
+//   where Z_c = H_{2^CH} (D x)[c*2^CH : (c+1)*2^CH] is the natural-order WHT of chunk c.
 //
-// A CTA of 2^TB threads holds one chunk in registers (2^TB values per thread): pass A
-// covers the chunk bits held in registers after a 16-byte coalesced load (sign flip fused
-// into the load), the chunk goes through a bank-conflict-free swizzled shared buffer,
-// pass B covers the remaining bits, and each sampled row accumulates +-Z_c[r2] into a
-// shared accumulator.  Columns are split over the persistent grid (stream-K); a column
-// shared by several CTAs is finished by the last CTA to arrive, which adds the partial
-// accumulators in CTA order, so results are reproducible bit for bit.
+// A CTA of 256 threads holds one chunk in registers (16 16-byte vectors per thread) and
+// transforms its bits in three register passes, moving between them through a
+// bank-conflict-free swizzled 64 KB shared buffer (sign flip fused into the first pass);
+// each sampled row then accumulates +-Z_c[r2].  Columns are split over the persistent grid
+// (stream-K); a column shared by several CTAs is finished by the last CTA to arrive, which
+// adds the partial accumulators in CTA order, so results are reproducible bit for bit.
 #include <mutex>
 
 #include "rla_internal.cuh"
@@ -24,16 +23,20 @@ namespace rla {
 
 template <class T>
 struct WhtCfg;
-// CH = chunk bits, NT = threads of a fused-kernel CTA.  FP64: 2^TB threads with 2^TB values
-// each, two passes of TB bits.  FP32: 256 threads with 64 values each, three passes (6 + 6 + 2
-// bits), which keeps two CTAs of 8 warps on an SM.
+// The fused compress kernel's CTA: NT = 256 threads; a 16-byte vector holds 2^VB elements;
+// a chunk has CH = VB + 12 bits (2^14 FP32 or 2^13 FP64 elements, 64 KB either way), and each
+// thread holds 16 vectors of it.
 template <>
 struct WhtCfg<float> {
-    static constexpr int CH = 14, NT = 256;
+    static constexpr int VB = 2, CH = 14, NT = 256;
+    using V = float4;
+    using SignW = uint2;  // 64 sign bits per thread and chunk
 };
 template <>
 struct WhtCfg<double> {
-    static constexpr int TB = 6, VB = 1, CH = 2 * TB, NT = 1 << TB;
+    static constexpr int VB = 1, CH = 13, NT = 256;
+    using V = double2;
+    using SignW = uint32_t;  // 32 sign bits per thread and chunk
 };
 
 // Register storage of one thread's 2^TB chunk elements.  FP32 values live in float2
@@ -108,15 +111,6 @@ struct SrhtParams {
     Split split;
 };
 
-// Position of chunk element e in the swizzled shared buffer: the low 3 bits of the
-// 16-byte vector index are XOR-ed with bits [VB+TB, VB+TB+3) of e.
-template <int TB, int VB>
-__device__ __forceinline__ int swz(int e) {
-    int f = e >> VB;
-    f ^= (e >> (VB + TB)) & 7;
-    return (f << VB) | (e & ((1 << VB) - 1));
-}
-
 template <class T>
 __device__ __forceinline__ T flip(T x, uint32_t keep) {
     if constexpr (sizeof(T) == 4) {
@@ -126,24 +120,81 @@ __device__ __forceinline__ T flip(T x, uint32_t keep) {
     }
 }
 
-// Pass-A loads of chunk c of column xv: thread t holds elements (t << VB) + (k << (VB+TB)) + i.
-template <class T, bool VEC, int TB, int VB>
-__device__ __forceinline__ void load_chunk(const T *__restrict__ xv, int64_t cbase, int64_t L, int t,
-                                           Regs<T, TB> &r) {
-    constexpr int VW = 1 << VB, KV = 1 << (TB - VB);
+// Element address of chunk element e in the shared buffer: the 16-byte slot bits
+// [VB, VB+3) XOR bits [VB+4, VB+7).  Every 16-byte access of the kernel below then puts the
+// 8 lanes of each quarter warp on 8 different slots of a 128-byte row: no bank conflicts.
+template <int VB>
+__device__ __forceinline__ int swzv(int e) { return e ^ (((e >> (VB + 4)) & 7) << VB); }
+
+// Vector m (elements 2^VB*m ...) of a thread's registers.
+__device__ __forceinline__ void set_vec(Regs<float, 6> &r, int m, float4 q) {
+    r.d[2 * m] = make_float2(q.x, q.y);
+    r.d[2 * m + 1] = make_float2(q.z, q.w);
+}
+__device__ __forceinline__ void set_vec(Regs<double, 5> &r, int m, double2 q) {
+    r.d[2 * m] = q.x;
+    r.d[2 * m + 1] = q.y;
+}
+__device__ __forceinline__ float4 get_vec(const Regs<float, 6> &r, int m) {
+    return make_float4(r.d[2 * m].x, r.d[2 * m].y, r.d[2 * m + 1].x, r.d[2 * m + 1].y);
+}
+__device__ __forceinline__ double2 get_vec(const Regs<double, 5> &r, int m) {
+    return make_double2(r.d[2 * m], r.d[2 * m + 1]);
+}
+
+__device__ __forceinline__ uint32_t sign_word(uint2 sg, int q) { return q < 32 ? sg.x : sg.y; }
+__device__ __forceinline__ uint32_t sign_word(uint32_t sg, int) { return sg; }
+
+// Radix-2 butterflies over bits 0..3 of the index of a thread's 16 vectors (the elements of
+// a vector are carried through): packed FP32x2 adds and subtracts, or FP64 scalar ones.
+__device__ __forceinline__ void wht_vec16(Regs<float, 6> &r) {
+    const float2 m1 = make_float2(-1.f, -1.f);
 #pragma unroll
-    for (int k = 0; k < KV; ++k) {
-        const int64_t e0 = cbase + ((int64_t)t << VB) + ((int64_t)k << (VB + TB));
-        if (VEC && e0 + VW <= L) {
-            if constexpr (sizeof(T) == 4) {
-                const float4 q = __ldg(reinterpret_cast<const float4 *>(xv + e0));
-                r.d[2 * k] = make_float2(q.x, q.y);
-                r.d[2 * k + 1] = make_float2(q.z, q.w);
-            } else {
-                const double2 q = __ldg(reinterpret_cast<const double2 *>(xv + e0));
-                r.d[2 * k] = q.x;
-                r.d[2 * k + 1] = q.y;
+    for (int h = 0; h < 4; ++h)
+#pragma unroll
+        for (int m = 0; m < 16; ++m)
+            if (!(m & (1 << h))) {
+#pragma unroll
+                for (int o = 0; o < 2; ++o) {
+                    const float2 a = r.d[2 * m + o], b = r.d[2 * (m | (1 << h)) + o];
+                    r.d[2 * m + o] = __fadd2_rn(a, b);
+                    r.d[2 * (m | (1 << h)) + o] = __ffma2_rn(b, m1, a);
+                }
             }
+}
+__device__ __forceinline__ void wht_vec16(Regs<double, 5> &r) {
+#pragma unroll
+    for (int h = 0; h < 4; ++h)
+#pragma unroll
+        for (int m = 0; m < 16; ++m)
+            if (!(m & (1 << h))) {
+#pragma unroll
+                for (int o = 0; o < 2; ++o) {
+                    const double a = r.d[2 * m + o], b = r.d[2 * (m | (1 << h)) + o];
+                    r.d[2 * m + o] = a + b;
+                    r.d[2 * (m | (1 << h)) + o] = a - b;
+                }
+            }
+}
+
+// Pass-A loads of the chunk at cbase of column xv: register q = i | k<<VB (i < 2^VB, k < 16)
+// holds element i | t<<VB | k<<(VB+8).
+template <class T, bool VEC>
+__device__ __forceinline__ void load_chunk(const T *__restrict__ xv, int64_t cbase, int64_t L, int t,
+                                           Regs<T, WhtCfg<T>::VB + 4> &r) {
+    constexpr int VB = WhtCfg<T>::VB, CH = WhtCfg<T>::CH, VW = 1 << VB;
+    using V = typename WhtCfg<T>::V;
+    if (VEC && cbase + (1 << CH) <= L) {  // whole chunk inside the column: no per-vector checks
+        const V *src = reinterpret_cast<const V *>(xv + cbase) + t;
+#pragma unroll
+        for (int k = 0; k < 16; ++k) set_vec(r, k, __ldg(src + (k << 8)));
+        return;
+    }
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        const int64_t e0 = cbase + ((int64_t)t << VB) + ((int64_t)k << (VB + 8));
+        if (VEC && e0 + VW <= L) {
+            set_vec(r, k, __ldg(reinterpret_cast<const V *>(xv + e0)));
         } else {
 #pragma unroll
             for (int i = 0; i < VW; ++i) r.set(k * VW + i, (e0 + i < L) ? __ldg(xv + e0 + i) : T(0));
@@ -151,68 +202,85 @@ __device__ __forceinline__ void load_chunk(const T *__restrict__ xv, int64_t cba
     }
 }
 
-// SPT = sampled rows per thread: thread t owns samples t + k*NT (k < SPT) of the window,
-// keeping their packed (r1, swizzled r2) and their accumulators in registers.
+// Fused compress, one CTA of 256 threads per chunk at a time.  Chunk element bits
+// (e = 0..2^CH-1) by pass, lane l, warp w:
+//   pass A (after the coalesced load): register q = i | k<<VB holds e = i | t<<VB | k<<(VB+8);
+//          butterflies over e bits [0, VB) and [VB+8, VB+12);
+//   pass B: vectors m hold e = m<<VB | t<<(VB+4); butterflies over e bits [VB, VB+4);
+//   pass C: vectors m hold e = (l&15)<<VB | m<<(VB+4) | (l>>4)<<(VB+8) | w<<(VB+9);
+//          butterflies over e bits [VB+4, VB+8).
+// The chunk then holds H_c (D x) in natural order, and each thread's SPT sampled rows
+// r = r1*2^CH + r2 add (-1)^popc(r1 & c) * Z_c[r2]:
+//   y[r] = sum_c (-1)^popc(r1 & c) * Z_c[r2],  Z_c = H_{2^CH} (D x)[c*2^CH : (c+1)*2^CH].
+// Columns are split over the persistent grid (stream-K); a column shared by several CTAs is
+// finished by the last CTA to arrive, which adds the partial accumulators in CTA order, so
+// results are reproducible bit for bit.
 template <class T, bool VEC, int SPT>
-__global__ void __launch_bounds__(1 << WhtCfg<T>::TB, 2) srht_fused_kernel(SrhtParams<T> p) {
-    constexpr int TB = WhtCfg<T>::TB, VB = WhtCfg<T>::VB;
-    constexpr int CH = 2 * TB, NT = 1 << TB, VW = 1 << VB, KV = 1 << (TB - VB);
+__global__ void __launch_bounds__(256, 2) srht_fused_kernel(SrhtParams<T> p) {
+    constexpr int VB = WhtCfg<T>::VB, CH = WhtCfg<T>::CH, NT = 256;
+    using V = typename WhtCfg<T>::V;
+    using SignW = typename WhtCfg<T>::SignW;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *Z = reinterpret_cast<T *>(smem_raw);
     __shared__ int last_flag;
-    const int t = threadIdx.x;
+    const int t = threadIdx.x, lane = t & 31, wp = t >> 5;
     const int g = blockIdx.x;
     const int64_t u0 = p.split.start(g), u1 = p.split.start(g + 1);
     if (u0 >= u1) return;
+    // With 16 samples per thread their packed rows live in shared memory (after the chunk),
+    // which keeps the kernel within 128 registers; each thread reads only its own entries.
+    constexpr bool SR_SMEM = SPT > 8;
+    uint32_t *sr_s = reinterpret_cast<uint32_t *>(Z + (1 << CH));
     T acc[SPT];
-    uint32_t sr[SPT];
+    uint32_t sr[SR_SMEM ? 1 : SPT];
 #pragma unroll
     for (int k = 0; k < SPT; ++k) {
         const int i = t + k * NT;
         acc[k] = T(0);
         const uint32_t row = i < p.s_cnt ? (uint32_t)__ldg(p.rows + p.s_lo + i) : 0u;
-        sr[k] = ((row >> CH) << CH) | (uint32_t)swz<TB, VB>((int)(row & ((1u << CH) - 1)));
+        const uint32_t packed = ((row >> CH) << CH) | (uint32_t)swzv<VB>((int)(row & ((1u << CH) - 1)));
+        if constexpr (SR_SMEM) sr_s[k * NT + t] = packed;
+        else sr[k] = packed;
     }
-    const int t_lo = t & (VW - 1), t_hi = t >> VB;
-    // The swizzle only permutes the low 3 bits of a vector index, so every address this
-    // thread touches is one of 8 per-thread bases plus a compile-time offset.
-    int offA[8], offB[8];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-        offA[j] = (t ^ j) << VB;
-        offB[j] = ((j ^ (t_hi & 7)) << VB) + (t_hi << (TB + VB)) + t_lo;
-    }
-    Regs<T, TB> r;
-    uint4 sg;
+    // Per-thread bases.  The swizzle flips the slot bits only, so every address below is a
+    // base (XOR a compile-time pattern) plus a compile-time offset:
+    //   pass A, vector k: baseA + k<<(VB+8)
+    //   pass B, vector m: baseB ^ (m&7)<<VB, + (m>>3)<<(VB+3)
+    //   pass C, vector m: baseC ^ (m&7)<<VB, + m<<(VB+4)
+    const int baseA = swzv<VB>(t << VB);
+    const int baseB = (t << (VB + 4)) | ((t & 7) << VB);
+    const int baseC = ((lane & 15) << VB) | ((lane >> 4) << (VB + 8)) | (wp << (VB + 9));
+    Regs<T, VB + 4> r;
+    SignW sg;
+    const SignW *sign_tl = reinterpret_cast<const SignW *>(p.sign_tl);
     int64_t v = u0 / p.cpv, c = u0 - v * p.cpv;
-    load_chunk<T, VEC, TB, VB>(p.X + v * p.x_ld, c << CH, p.L, t, r);
-    sg = __ldg(p.sign_tl + c * NT + t);
+    load_chunk<T, VEC>(p.X + v * p.x_ld, c << CH, p.L, t, r);
+    sg = __ldg(sign_tl + c * NT + t);
     for (int64_t u = u0; u < u1; ++u) {
-        // ---- pass A: sign flip, butterflies over the register bits, swizzled store ----
+        // ---- pass A: sign flip, butterflies over the register bits, vector stores ----
 #pragma unroll
-        for (int q = 0; q < (1 << TB); ++q) {
-            const uint32_t w = q < 32 ? sg.x : q < 64 ? sg.y : q < 96 ? sg.z : sg.w;
-            r.set(q, flip<T>(r.get(q), w >> (q & 31)));
-        }
+        for (int q = 0; q < (16 << VB); ++q) r.set(q, flip<T>(r.get(q), sign_word(sg, q) >> (q & 31)));
         r.wht();
 #pragma unroll
-        for (int k = 0; k < KV; ++k) {
-            T *dst = Z + offA[k & 7] + (k << (TB + VB));
-            if constexpr (sizeof(T) == 4) {
-                *reinterpret_cast<float4 *>(dst) =
-                    make_float4(r.d[2 * k].x, r.d[2 * k].y, r.d[2 * k + 1].x, r.d[2 * k + 1].y);
-            } else {
-                *reinterpret_cast<double2 *>(dst) = make_double2(r.d[2 * k], r.d[2 * k + 1]);
+        for (int k = 0; k < 16; ++k) *reinterpret_cast<V *>(Z + baseA + (k << (VB + 8))) = get_vec(r, k);
+        __syncthreads();
+        // ---- passes B and C (each vector is read and written by one thread) ----
+#pragma unroll
+        for (int pass = 0; pass < 2; ++pass) {
+            const int base = pass == 0 ? baseB : baseC;
+#pragma unroll
+            for (int m = 0; m < 16; ++m) {
+                const int off = pass == 0 ? ((m >> 3) << (VB + 3)) : (m << (VB + 4));
+                set_vec(r, m, *reinterpret_cast<const V *>(Z + (base ^ ((m & 7) << VB)) + off));
             }
+            wht_vec16(r);
+#pragma unroll
+            for (int m = 0; m < 16; ++m) {
+                const int off = pass == 0 ? ((m >> 3) << (VB + 3)) : (m << (VB + 4));
+                *reinterpret_cast<V *>(Z + (base ^ ((m & 7) << VB)) + off) = get_vec(r, m);
+            }
+            if (pass == 0) __syncthreads();
         }
-        __syncthreads();
-        // ---- pass B: the remaining TB bits ----
-#pragma unroll
-        for (int q = 0; q < (1 << TB); ++q) r.set(q, Z[offB[q & 7] + ((q & ~7) << VB)]);
-        r.wht();
-#pragma unroll
-        for (int q = 0; q < (1 << TB); ++q) Z[offB[q & 7] + ((q & ~7) << VB)] = r.get(q);
-        __syncthreads();
         // ---- prefetch the next chunk while the sampled rows are accumulated ----
         const int64_t vcur = v, ccur = c;
         if (u + 1 < u1) {
@@ -220,14 +288,16 @@ __global__ void __launch_bounds__(1 << WhtCfg<T>::TB, 2) srht_fused_kernel(SrhtP
                 c = 0;
                 ++v;
             }
-            load_chunk<T, VEC, TB, VB>(p.X + v * p.x_ld, c << CH, p.L, t, r);
-            sg = __ldg(p.sign_tl + c * NT + t);
+            load_chunk<T, VEC>(p.X + v * p.x_ld, c << CH, p.L, t, r);
+            sg = __ldg(sign_tl + c * NT + t);
         }
+        __syncthreads();
         const uint32_t cc = (uint32_t)ccur;
 #pragma unroll
         for (int k = 0; k < SPT; ++k) {
-            const T z = Z[sr[k] & ((1u << CH) - 1)];
-            acc[k] += (__popc((sr[k] >> CH) & cc) & 1) ? -z : z;
+            const uint32_t srk = SR_SMEM ? sr_s[k * NT + t] : sr[k % (SR_SMEM ? 1 : SPT)];
+            const T z = Z[srk & ((1u << CH) - 1)];
+            acc[k] += (__popc((srk >> CH) & cc) & 1) ? -z : z;
         }
         __syncthreads();
         const bool col_done = (u + 1 == u1) || (ccur + 1 == p.cpv);
@@ -278,263 +348,47 @@ __global__ void __launch_bounds__(1 << WhtCfg<T>::TB, 2) srht_fused_kernel(SrhtP
     }
 }
 
-// Word address of FP32 chunk element e in the shared buffer: bits 2..4 XOR bits 6..8.
-// Every 16-byte access of the FP32 kernel below then puts the 8 lanes of each quarter warp
-// on 8 different 16-byte slots of a 128-byte row, so none has a bank conflict.
-__device__ __forceinline__ int swz32(int e) { return e ^ (((e >> 6) & 7) << 2); }
-
-// Radix-2 butterflies over bits 0..3 of the index of 16 four-float vectors (all lanes of a
-// vector are carried through), as packed FP32x2 adds and subtracts.
-__device__ __forceinline__ void wht_vec16(Regs<float, 6> &r) {
-    const float2 m1 = make_float2(-1.f, -1.f);
-#pragma unroll
-    for (int h = 0; h < 4; ++h)
-#pragma unroll
-        for (int m = 0; m < 16; ++m)
-            if (!(m & (1 << h))) {
-#pragma unroll
-                for (int o = 0; o < 2; ++o) {
-                    const float2 a = r.d[2 * m + o], b = r.d[2 * (m | (1 << h)) + o];
-                    r.d[2 * m + o] = __fadd2_rn(a, b);
-                    r.d[2 * (m | (1 << h)) + o] = __ffma2_rn(b, m1, a);
-                }
-            }
-}
-
-// Pass-A loads of FP32 chunk c of column xv: register q = i | k<<2 holds element i | t<<2 | k<<10.
-template <bool VEC>
-__device__ __forceinline__ void load_chunk32(const float *__restrict__ xv, int64_t cbase, int64_t L, int t,
-                                             Regs<float, 6> &r) {
-    if (VEC && cbase + (1 << 14) <= L) {  // whole chunk inside the column: no per-vector checks
-        const float4 *src = reinterpret_cast<const float4 *>(xv + cbase) + t;
-#pragma unroll
-        for (int k = 0; k < 16; ++k) {
-            const float4 q = __ldg(src + (k << 8));
-            r.d[2 * k] = make_float2(q.x, q.y);
-            r.d[2 * k + 1] = make_float2(q.z, q.w);
-        }
-        return;
-    }
-#pragma unroll
-    for (int k = 0; k < 16; ++k) {
-        const int64_t e0 = cbase + ((int64_t)t << 2) + ((int64_t)k << 10);
-        if (VEC && e0 + 4 <= L) {
-            const float4 q = __ldg(reinterpret_cast<const float4 *>(xv + e0));
-            r.d[2 * k] = make_float2(q.x, q.y);
-            r.d[2 * k + 1] = make_float2(q.z, q.w);
-        } else {
-#pragma unroll
-            for (int i = 0; i < 4; ++i) r.set(4 * k + i, (e0 + i < L) ? __ldg(xv + e0 + i) : 0.f);
-        }
-    }
-}
-
-// FP32 fused compress.  Chunk element bits (e = 0..2^14-1) by pass, lane l, warp w:
-//   pass A (after the coalesced load): registers q = i | k<<2 hold e = i | t<<2 | k<<10
-//          (i < 4, k < 16); butterflies over e bits {0, 1, 10..13};
-//   pass B: 16-byte vectors m hold e = m<<2 | t<<6; butterflies over e bits 2..5;
-//   pass C: 16-byte vectors m hold e = (l&15)<<2 | m<<6 | (l>>4)<<10 | w<<11; butterflies
-//          over e bits 6..9.
-// The chunk then holds H (D x) in natural order, and each thread's SPT sampled rows add
-// +-Z_c[r2] as in the FP64 kernel.
-template <bool VEC, int SPT>
-__global__ void __launch_bounds__(256, 2) srht_fused32_kernel(SrhtParams<float> p) {
-    constexpr int CH = 14, NT = 256;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    float *Z = reinterpret_cast<float *>(smem_raw);
-    __shared__ int last_flag;
-    const int t = threadIdx.x, lane = t & 31, wp = t >> 5;
-    const int g = blockIdx.x;
-    const int64_t u0 = p.split.start(g), u1 = p.split.start(g + 1);
-    if (u0 >= u1) return;
-    // With 16 samples per thread their packed rows live in shared memory (after the chunk),
-    // which keeps the kernel within 128 registers; each thread reads only its own entries.
-    constexpr bool SR_SMEM = SPT > 8;
-    uint32_t *sr_s = reinterpret_cast<uint32_t *>(Z + (1 << CH));
-    float acc[SPT];
-    uint32_t sr[SR_SMEM ? 1 : SPT];
-#pragma unroll
-    for (int k = 0; k < SPT; ++k) {
-        const int i = t + k * NT;
-        acc[k] = 0.f;
-        const uint32_t row = i < p.s_cnt ? (uint32_t)__ldg(p.rows + p.s_lo + i) : 0u;
-        const uint32_t packed = ((row >> CH) << CH) | (uint32_t)swz32((int)(row & ((1u << CH) - 1)));
-        if constexpr (SR_SMEM) sr_s[k * NT + t] = packed;
-        else sr[k] = packed;
-    }
-    // Per-thread bases.  The swizzle flips bits 2..4 only, so every address below is a base
-    // (XOR a compile-time pattern) plus a compile-time offset.
-    const int baseA = swz32(t << 2);                                   // + k<<10
-    const int baseB = (t << 6) | ((t & 7) << 2);                       // ^ (m&7)<<2, + (m>>3)<<5
-    const int baseC = ((lane & 15) << 2) | ((lane >> 4) << 10) | (wp << 11);  // ^ (m&7)<<2, + m<<6
-    Regs<float, 6> r;
-    uint2 sg;
-    const uint2 *sign_tl = reinterpret_cast<const uint2 *>(p.sign_tl);
-    int64_t v = u0 / p.cpv, c = u0 - v * p.cpv;
-    load_chunk32<VEC>(p.X + v * p.x_ld, c << CH, p.L, t, r);
-    sg = __ldg(sign_tl + c * NT + t);
-    for (int64_t u = u0; u < u1; ++u) {
-        // ---- pass A: sign flip, butterflies over the register bits, vector stores ----
-#pragma unroll
-        for (int q = 0; q < 64; ++q) r.set(q, flip<float>(r.get(q), (q < 32 ? sg.x : sg.y) >> (q & 31)));
-        r.wht();
-#pragma unroll
-        for (int k = 0; k < 16; ++k)
-            *reinterpret_cast<float4 *>(Z + baseA + (k << 10)) =
-                make_float4(r.d[2 * k].x, r.d[2 * k].y, r.d[2 * k + 1].x, r.d[2 * k + 1].y);
-        __syncthreads();
-        // ---- passes B and C (each vector is read and written by one thread) ----
-#pragma unroll
-        for (int pass = 0; pass < 2; ++pass) {
-            const int base = pass == 0 ? baseB : baseC;
-#pragma unroll
-            for (int m = 0; m < 16; ++m) {
-                const int off = pass == 0 ? ((m >> 3) << 5) : (m << 6);
-                const float4 q = *reinterpret_cast<const float4 *>(Z + (base ^ ((m & 7) << 2)) + off);
-                r.d[2 * m] = make_float2(q.x, q.y);
-                r.d[2 * m + 1] = make_float2(q.z, q.w);
-            }
-            wht_vec16(r);
-#pragma unroll
-            for (int m = 0; m < 16; ++m) {
-                const int off = pass == 0 ? ((m >> 3) << 5) : (m << 6);
-                *reinterpret_cast<float4 *>(Z + (base ^ ((m & 7) << 2)) + off) =
-                    make_float4(r.d[2 * m].x, r.d[2 * m].y, r.d[2 * m + 1].x, r.d[2 * m + 1].y);
-            }
-            if (pass == 0) __syncthreads();
-        }
-        // ---- prefetch the next chunk while the sampled rows are accumulated ----
-        const int64_t vcur = v, ccur = c;
-        if (u + 1 < u1) {
-            if (++c == p.cpv) {
-                c = 0;
-                ++v;
-            }
-            load_chunk32<VEC>(p.X + v * p.x_ld, c << CH, p.L, t, r);
-            sg = __ldg(sign_tl + c * NT + t);
-        }
-        __syncthreads();
-        const uint32_t cc = (uint32_t)ccur;
-#pragma unroll
-        for (int k = 0; k < SPT; ++k) {
-            const uint32_t srk = SR_SMEM ? sr_s[k * NT + t] : sr[k % (SR_SMEM ? 1 : SPT)];
-            const float z = Z[srk & ((1u << CH) - 1)];
-            acc[k] += (__popc((srk >> CH) & cc) & 1) ? -z : z;
-        }
-        __syncthreads();
-        const bool col_done = (u + 1 == u1) || (ccur + 1 == p.cpv);
-        if (!col_done) continue;
-        // ---- column finished in this CTA's range ----
-        const int64_t vbeg = vcur * p.cpv;
-        const bool exclusive = (u0 <= vbeg) && (vbeg + p.cpv <= u1);
-        if (exclusive) {
-#pragma unroll
-            for (int k = 0; k < SPT; ++k) {
-                const int i = t + k * NT;
-                if (i < p.s_cnt) {
-                    float *yp = p.Y + (p.s_lo + i) * p.y_es + vcur * p.y_vs;
-                    float res = p.alpha * acc[k];
-                    if (!p.beta_zero) res += p.beta * *yp;
-                    *yp = res;
-                }
-                acc[k] = 0.f;
-            }
-        } else {
-            float *part = p.partials + (int64_t)p.split.slot(g, vbeg) * p.s_cnt;
-#pragma unroll
-            for (int k = 0; k < SPT; ++k) {
-                const int i = t + k * NT;
-                if (i < p.s_cnt) part[i] = acc[k];
-                acc[k] = 0.f;
-            }
-            __threadfence();
-            __syncthreads();
-            const int gf = p.split.owner(vbeg), gl = p.split.owner(vbeg + p.cpv - 1);
-            if (t == 0) last_flag = (atomicAdd(&p.counters[vcur], 1) == gl - gf);
-            __syncthreads();
-            if (last_flag) {
-                __threadfence();
-                for (int i = t; i < p.s_cnt; i += NT) {
-                    float a = __ldcg(p.partials + (int64_t)p.split.slot(gf, vbeg) * p.s_cnt + i);
-#pragma unroll 4
-                    for (int gg = gf + 1; gg <= gl; ++gg) a += __ldcg(p.partials + (int64_t)(2 * gg) * p.s_cnt + i);
-                    float *yp = p.Y + (p.s_lo + i) * p.y_es + vcur * p.y_vs;
-                    float res = p.alpha * a;
-                    if (!p.beta_zero) res += p.beta * *yp;
-                    *yp = res;
-                }
-                if (t == 0) p.counters[vcur] = 0;
-            }
-        }
-        __syncthreads();
-    }
-}
-
 // Launch the fused kernel with the smallest samples-per-thread that holds s_cnt samples.
 template <class T, bool VEC>
 static void launch_srht_fused(const SrhtParams<T> &p, int grid, size_t smem, cudaStream_t st) {
-    // smem: the chunk buffer; the FP32 kernel adds room for its sample rows when it needs it
+    // smem: the chunk buffer; room for the packed sample rows is added here when needed
     constexpr int NT = WhtCfg<T>::NT;
     auto go = [&](auto kern) {
         set_smem_max(kern);
         kern<<<grid, NT, smem, st>>>(p);
     };
     const int spt = (p.s_cnt + NT - 1) / NT;
-    if constexpr (sizeof(T) == 4) {
-        if (spt > 8) smem += (size_t)NT * 16 * sizeof(uint32_t);  // packed sample rows
-        if (spt <= 1) go(srht_fused32_kernel<VEC, 1>);
-        else if (spt <= 2) go(srht_fused32_kernel<VEC, 2>);
-        else if (spt <= 4) go(srht_fused32_kernel<VEC, 4>);
-        else if (spt <= 8) go(srht_fused32_kernel<VEC, 8>);
-        else go(srht_fused32_kernel<VEC, 16>);
-    } else {
-        if (spt <= 1) go(srht_fused_kernel<T, VEC, 1>);
-        else if (spt <= 2) go(srht_fused_kernel<T, VEC, 2>);
-        else if (spt <= 4) go(srht_fused_kernel<T, VEC, 4>);
-        else if (spt <= 8) go(srht_fused_kernel<T, VEC, 8>);
-        else go(srht_fused_kernel<T, VEC, 16>);
-    }
+    if (spt > 8) smem += (size_t)NT * 16 * sizeof(uint32_t);
+    if (spt <= 1) go(srht_fused_kernel<T, VEC, 1>);
+    else if (spt <= 2) go(srht_fused_kernel<T, VEC, 2>);
+    else if (spt <= 4) go(srht_fused_kernel<T, VEC, 4>);
+    else if (spt <= 8) go(srht_fused_kernel<T, VEC, 8>);
+    else go(srht_fused_kernel<T, VEC, 16>);
 }
 
-// Largest samples window of one fused launch: 16 samples per thread (4096 FP32, 1024 FP64).
+// Largest samples window of one fused launch: 16 samples per thread (4096).
 template <class T>
 constexpr int srht_window() {
     return WhtCfg<T>::NT * 16;
 }
 
-// Per (chunk, thread) sign masks in pass-A register order (bit q = element
-// (t << VB) + ((q >> VB) << (VB+TB)) + (q & (VW-1)) of the chunk), so a thread reads its
-// 2^TB signs with one 16-byte load.
-// FP32 kernel: per (chunk, thread) 64 bits, bit q = element (q & 3) | t<<2 | (q>>2)<<10.
-__global__ void sign_table32_kernel(const uint32_t *signbits, int64_t nchunks, uint2 *out) {
-    constexpr int CH = 14, NT = 256;
+// Per (chunk, thread) sign masks in pass-A register order: bit q is the sign of element
+// (q & (2^VB-1)) | t<<VB | (q>>VB)<<(VB+8) of the chunk, so a thread reads its signs with one
+// 8-byte (FP32) or 4-byte (FP64) load.
+template <class T>
+__global__ void sign_table_kernel(const uint32_t *signbits, int64_t nchunks, typename WhtCfg<T>::SignW *out) {
+    constexpr int VB = WhtCfg<T>::VB, CH = WhtCfg<T>::CH, NT = WhtCfg<T>::NT;
     const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (idx >= nchunks * NT) return;
     const int64_t c = idx / NT;
     const int t = (int)(idx % NT);
     uint32_t w[2] = {0u, 0u};
-    for (int q = 0; q < 64; ++q) {
-        const int64_t e = (c << CH) + (q & 3) + ((int64_t)t << 2) + ((int64_t)(q >> 2) << 10);
+    for (int q = 0; q < (16 << VB); ++q) {
+        const int64_t e = (c << CH) + (q & ((1 << VB) - 1)) + ((int64_t)t << VB) + ((int64_t)(q >> VB) << (VB + 8));
         w[q >> 5] |= ((signbits[e >> 5] >> (e & 31)) & 1u) << (q & 31);
     }
-    out[idx] = make_uint2(w[0], w[1]);
-}
-
-template <class T>
-__global__ void sign_table_kernel(const uint32_t *signbits, int64_t nchunks, uint4 *out) {
-    constexpr int TB = WhtCfg<T>::TB, VB = WhtCfg<T>::VB, CH = 2 * TB, NT = 1 << TB, VW = 1 << VB;
-    const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (idx >= nchunks * NT) return;
-    const int64_t c = idx / NT;
-    const int t = (int)(idx % NT);
-    uint32_t w[4] = {0u, 0u, 0u, 0u};
-    for (int q = 0; q < (1 << TB); ++q) {
-        const int k = q / VW, i = q % VW;
-        const int64_t e = (c << CH) + ((int64_t)t << VB) + ((int64_t)k << (VB + TB)) + i;
-        const uint32_t b = (signbits[e >> 5] >> (e & 31)) & 1u;
-        w[q >> 5] |= b << (q & 31);
-    }
-    out[idx] = make_uint4(w[0], w[1], w[2], w[3]);
+    if constexpr (sizeof(T) == 4) out[idx] = make_uint2(w[0], w[1]);
+    else out[idx] = w[0];
 }
 
 int build_srht_sign_table(rla_ctx *ctx, rla_sketch *sk) {
@@ -543,15 +397,15 @@ int build_srht_sign_table(rla_ctx *ctx, rla_sketch *sk) {
     const int NT = f32 ? WhtCfg<float>::NT : WhtCfg<double>::NT;
     if (sk->N < ((int64_t)1 << CH)) return RLA_OK;
     const int64_t nchunks = sk->N >> CH;
-    // FP32: 8 bytes per (chunk, thread); FP64: 16
-    const size_t bytes = (f32 ? sizeof(uint2) : sizeof(uint4)) * nchunks * NT;
+    const size_t bytes = (f32 ? sizeof(WhtCfg<float>::SignW) : sizeof(WhtCfg<double>::SignW)) * nchunks * NT;
     if (!sk->sign_tl) RLA_CUDA_TRY(ctx, cudaMalloc(&sk->sign_tl, bytes));
     const int64_t n = nchunks * NT;
     if (f32)
-        sign_table32_kernel<<<ceil_div_i(n, 256), 256, 0, ctx->stream>>>(sk->signbits, nchunks,
-                                                                         reinterpret_cast<uint2 *>(sk->sign_tl));
+        sign_table_kernel<float><<<ceil_div_i(n, 256), 256, 0, ctx->stream>>>(
+            sk->signbits, nchunks, reinterpret_cast<WhtCfg<float>::SignW *>(sk->sign_tl));
     else
-        sign_table_kernel<double><<<ceil_div_i(n, 256), 256, 0, ctx->stream>>>(sk->signbits, nchunks, sk->sign_tl);
+        sign_table_kernel<double><<<ceil_div_i(n, 256), 256, 0, ctx->stream>>>(
+            sk->signbits, nchunks, reinterpret_cast<WhtCfg<double>::SignW *>(sk->sign_tl));
     return check_launch(ctx, "sign_table");
 }
 
@@ -761,7 +615,7 @@ template <class T>
 int srht_compress(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_t x_es, int64_t x_vs, int64_t nv, T *Y,
                   int64_t y_es, int64_t y_vs, double alpha, double beta) {
     if (nv == 0) return RLA_OK;
-    constexpr int CH = WhtCfg<T>::CH, VB = sizeof(T) == 4 ? 2 : 1;  // VB: log2 of a 16-byte vector
+    constexpr int CH = WhtCfg<T>::CH, VB = WhtCfg<T>::VB;
     const size_t es = sizeof(T);
     const int64_t L = sk->L, N = sk->N, s = sk->s;
     const T a = (T)(alpha * sk->scale);
@@ -925,7 +779,7 @@ static int noalloc_setup(rla_ctx *ctx, NoallocDevice **out) {
 template <class T>
 static int srht_noalloc_t(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_t ldx, int64_t nv, T *Y,
                           int64_t ldy, double alpha, double beta, const NoallocDevice &nd) {
-    constexpr int CH = WhtCfg<T>::CH, VB = sizeof(T) == 4 ? 2 : 1;  // VB: log2 of a 16-byte vector
+    constexpr int CH = WhtCfg<T>::CH, VB = WhtCfg<T>::VB;
     const size_t es = sizeof(T);
     const int64_t L = sk->L, N = sk->N, s = sk->s;
     const T a = (T)(alpha * sk->scale);
