@@ -49,7 +49,7 @@ WORKLOAD = "srht+countsketch left apply, fp32, A 2^20x512 -> 4096x512"
 METRIC = "sketch apply throughput (SRHT + CountSketch, HBM GB/s of algorithmic bytes)"
 # DRAM bytes (read + write) per full-size launch: ncu capture of the 2^20x128 case
 # (profiles/*_2p20x128_f32.md) scaled by 512/128 columns; the work splits evenly by column.
-TRAFFIC_PER_LAUNCH = {"srht_fused32_kernel": 2186983424, "cs_compress_kernel": 2250834944}
+TRAFFIC_PER_LAUNCH = {"srht_fused_kernel": 2186983424, "cs_compress_kernel": 2250834944}
 
 
 def peaks():
@@ -328,7 +328,7 @@ def b200_arm(args):
         return
 
     peak, peak_kind = peaks()
-    dom_name, dom_ms = ("srht_fused32_kernel", srht_ms) if srht_ms >= cs_ms else ("cs_compress_kernel", cs_ms)
+    dom_name, dom_ms = ("srht_fused_kernel", srht_ms) if srht_ms >= cs_ms else ("cs_compress_kernel", cs_ms)
     achieved = BYTES_PER_APPLY / (dom_ms / 1e3) / 1e9
     traffic = TRAFFIC_PER_LAUNCH.get(dom_name) if (M, NCOL) == (2**20, 512) else None
     roofline = {"bound": "hbm", "kernel": dom_name, "achieved": round(achieved, 2), "peak": peak,
