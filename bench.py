@@ -838,7 +838,7 @@ KZ_METRIC = "block Kaczmarz iterations/s (sampled rows, LQ block solve)"
 # kernel launches of one step: redraw (Sampling: keys, 8 radix hist/pick pairs, count, scan,
 # write, plan), S*A and S*b gathers, residual (2), Gram (2), zero check, equilibration (2),
 # Cholesky (1 CTA for s < 128), triangular solve, mask, update
-KZ_LAUNCHES_PER_STEP = 35
+KZ_LAUNCHES_PER_STEP = 15
 
 
 def kaczmarz_arm(args):
@@ -922,7 +922,7 @@ def kaczmarz_arm(args):
             "config": {"workload": f"kaczmarz: A {m}x{n} f32, sampling left s={s} uniform without replacement",
                        "m": m, "n": n, "s": s, "parallelism": f"replicas x{world}",
                        "host_ms_per_step": round(host_s * 1e3 / K, 4)},
-            "roofline": {"bound": "latency", "note": "each step moves ~4*s*n bytes; the step is a chain of ~35 "
+            "roofline": {"bound": "latency", "note": "each step moves ~4*s*n bytes; the step is a chain of 15 "
                          "small launches", "achieved": None, "peak": None, "frac": None, "traffic": None},
             "solution": {"rel_residual_after_warmup_and_steps": res},
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": KZ_LAUNCHES_PER_STEP * K}

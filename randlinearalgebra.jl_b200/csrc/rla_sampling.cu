@@ -31,7 +31,7 @@
 
 namespace rla {
 
-enum : uint32_t { STREAM_SAMPLE_EXP = 9, STREAM_SAMPLE_KEYS = 10, STREAM_SAMPLE_CAND = 11 };
+enum : uint32_t { STREAM_SAMPLE_EXP = 9, STREAM_SAMPLE_KEYS = 10, STREAM_SAMPLE_CAND = 11, STREAM_SAMPLE_FLOYD = 12 };
 
 // ---- weights ----------------------------------------------------------------------
 template <class T>
@@ -115,6 +115,50 @@ __global__ void es_keys_kernel(Rng rng, int64_t L, const double *w, uint64_t *ke
     const double wj = w ? w[j] : 1.0;
     const double k = wj > 0.0 ? e / wj : INFINITY;
     key[j] = (uint64_t)__double_as_longlong(k);
+}
+
+// Uniform sampling without replacement for small s: Floyd's algorithm (Bentley and Floyd,
+// "A sample of brilliance", CACM 30(9), 1987).  For j = L-s .. L-1 take t uniform in [0, j],
+// or j when t was taken already; every s-subset of [0, L) is equally likely.  One warp: lane
+// 0 draws, the warp tests membership in the shared-memory list, then sorts the list
+// (bitonic) so the indices come out in increasing order like the selection path's.
+constexpr int FLOYD_MAX = 256;
+
+__global__ void __launch_bounds__(32) floyd_sample_kernel(Rng rng, int64_t L, int s, int64_t *idx) {
+    __shared__ uint32_t set[FLOYD_MAX];
+    const int lane = threadIdx.x;
+    WordStream ws{rng, STREAM_SAMPLE_FLOYD, 0};
+    for (int i = 0; i < s; ++i) {
+        const uint32_t j = (uint32_t)(L - s + i);
+        uint32_t t = 0;
+        if (lane == 0) t = uniform_below(j + 1u, ws);
+        t = __shfl_sync(FULL, t, 0);
+        bool hit = false;
+        for (int q = lane; q < i; q += 32) hit |= set[q] == t;
+        hit = __any_sync(FULL, hit);
+        if (lane == 0) set[i] = hit ? j : t;
+        __syncwarp();
+    }
+    int P = 1;
+    while (P < s) P <<= 1;
+    for (int q = s + lane; q < P; q += 32) set[q] = 0xffffffffu;
+    __syncwarp();
+    for (int k = 2; k <= P; k <<= 1)
+        for (int h = k >> 1; h > 0; h >>= 1) {
+            for (int q = lane; q < P; q += 32) {
+                const int o = q ^ h;
+                if (o > q) {
+                    const uint32_t a = set[q], b = set[o];
+                    const bool up = (q & k) == 0;
+                    if ((a > b) == up) {
+                        set[q] = b;
+                        set[o] = a;
+                    }
+                }
+            }
+            __syncwarp();
+        }
+    for (int q = lane; q < s; q += 32) idx[q] = (int64_t)set[q];
 }
 
 // Radix-select state in device memory: the known high bits of the threshold key, their
@@ -545,6 +589,10 @@ static int sample_weighted(rla_ctx *ctx, rla_sketch *sk, const double *w) {
     if (s > L)
         return set_error(ctx, RLA_E_ARG, "Cannot draw %lld samples from %lld samples without replacement.",
                          (long long)s, (long long)L);
+    if (!w && s <= FLOYD_MAX) {  // uniform, few samples: one warp instead of a selection over L keys
+        floyd_sample_kernel<<<1, 32, 0, ctx->stream>>>(rng, L, (int)s, sk->sidx);
+        return check_launch(ctx, "floyd_sample");
+    }
     void *p = nullptr;
     RLA_CUDA_TRY(ctx, pool_malloc_s(ctx, &p, sizeof(uint64_t) * L + 64, ctx->stream));
     uint64_t *key = (uint64_t *)p;

@@ -68,8 +68,26 @@ def test_uniform_draws(rla, dev, card):
 
 
 def test_uniform_without_replacement_takes_all(rla, dev):
-    S, _ = sampler(rla, dev, "left", 300, 300, np.float32, False)
-    assert np.array_equal(S.idx, np.arange(300))
+    # 300 samples go through the key selection, 200 through Floyd's algorithm (s <= 256)
+    for s in (300, 200):
+        S, _ = sampler(rla, dev, "left", s, s, np.float32, False)
+        assert np.array_equal(S.idx, np.arange(s))
+
+
+def test_uniform_without_replacement_inclusion_law(rla, dev):
+    """Small s (Floyd's algorithm): distinct increasing indices, each index drawn with
+    probability s/L (1500 draws of 8 from 32: standard deviation 0.011 around 0.25)."""
+    S, A = sampler(rla, dev, "left", 8, 32, np.float64, False, seed=11)
+    A_d = to_dev(A, dev)
+    x0, b0 = np.zeros(A.shape[1]), np.zeros(A.shape[0])
+    counts = np.zeros(32)
+    for _ in range(1500):
+        rla.update_compressor_(S, x0, A_d, b0)
+        idx = np.asarray(S.idx)
+        assert len(idx) == 8 and (np.diff(idx) > 0).all() and idx[0] >= 0 and idx[-1] < 32
+        counts[idx] += 1
+    freq = counts / 1500
+    assert np.abs(freq - 0.25).max() < 0.06, freq
 
 
 def test_l2norm_weights_and_frequencies(rla, dev):
