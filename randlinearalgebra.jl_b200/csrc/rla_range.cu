@@ -183,7 +183,7 @@ int gram_fp64(rla_ctx *ctx, const T *Y, int64_t rows, int64_t l, int64_t ldy, do
     const int ntiles = nt * (nt + 1) / 2;
     int64_t nchunks = std::max<int64_t>(1, ceil_div(2 * (int64_t)ctx->sm_count * 2, ntiles));
     int64_t rpc = ceil_div(ceil_div(rows, nchunks), GRAM_KR) * GRAM_KR;
-    rpc = std::max<int64_t>(rpc, 256);
+    rpc = std::max<int64_t>(rpc, 2 * GRAM_KR);  // short Y (a Kaczmarz block): still several CTAs
     nchunks = std::max<int64_t>(1, ceil_div(rows, rpc));
     if (nchunks > 65535) {
         nchunks = 65535;
