@@ -47,8 +47,8 @@ def bytes_per_apply(ncol: int = NCOL) -> int:
 BYTES_PER_APPLY = bytes_per_apply()
 WORKLOAD = "srht+countsketch left apply, fp32, A 2^20x512 -> 4096x512"
 METRIC = "sketch apply throughput (SRHT + CountSketch, HBM GB/s of algorithmic bytes)"
-# DRAM bytes (read + write) per full-size launch: ncu capture of the 2^20x128 case
-# (profiles/*_2p20x128_f32.md) scaled by 512/128 columns; the work splits evenly by column.
+# DRAM bytes (read + write) per full-size launch: ncu capture of each kernel on the
+# 2^20x128 case, scaled by 512/128 columns; the work splits evenly by column.
 TRAFFIC_PER_LAUNCH = {"srht_fused_kernel": 2186983424, "cs_compress_kernel": 2250834944}
 
 
@@ -209,6 +209,14 @@ def cpu_sample(threads: int, budget_s: float, srht_draws=None, cs_draws=None):
     return gbs, desc, ts + tc
 
 
+def sketch_config(m: int, ncol: int, world: int) -> dict:
+    """The `config` of a sketch-apply line; both arms print the same one."""
+    wl = WORKLOAD if (ncol, m) == (512, 2**20) else \
+        WORKLOAD.replace("2^20x512", f"{m}x{ncol}").replace("512 ->", f"{ncol} ->").replace("4096x512", f"4096x{ncol}")
+    return {"workload": wl, "m": m, "n": ncol, "s": S, "parallelism": f"replicas x{world}",
+            "l2": f"inputs larger than L2 ({4 * m * ncol / 1e9:.2f} GB per A), no flush needed"}
+
+
 def reference_arm(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -227,7 +235,7 @@ def reference_arm(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * tot / args.steps, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic N(0,1), seed 2",
-            "config": {"workload": WORKLOAD, "m": M, "n": NCOL, "s": S},
+            "config": sketch_config(M, args.cols, args.gpus),
             "cpu_baseline": {"value": round(v, 3), "unit": "GB/s", "cores": threads, "kind": "port",
                              "sample": desc + "; CPU restatement in oracle/ (Julia is not installed)"},
             "e2e": {"value": round(v, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -351,11 +359,7 @@ def b200_arm(args):
     line = {"metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": K,
             "warmup": args.warmup, "ms_per_step": round(ms / K, 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic N(0,1) generated on device (torch.randn, seed 2+rank)",
-            "config": {"workload": WORKLOAD if (NCOL, M) == (512, 2**20) else
-                       WORKLOAD.replace("2^20x512", f"{M}x{NCOL}").replace("512 ->", f"{NCOL} ->").replace("4096x512", f"4096x{NCOL}"),
-                       "m": M, "n": NCOL,
-                       "s": S, "parallelism": f"replicas x{world}",
-                       "l2": "inputs larger than L2 (2.15 GB per A), no flush needed"},
+            "config": sketch_config(M, NCOL, world),
             "roofline": roofline, "kernels": kernels, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
             "gpu_launches": 2 * K}
     print(json.dumps(line), flush=True)

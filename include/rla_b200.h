@@ -184,6 +184,20 @@ int rla_sketch_mul_async(rla_ctx *ctx, const rla_sketch *sk, int side, int trans
                          int64_t a_rows, int64_t a_cols, const void *A, int64_t lda, int trans_a,
                          double alpha, double beta);
 
+/* mul!(C, S, transpose(B), alpha, beta) for a Left SparseSign or CountSketch recipe S and
+ * a sparse B (sparse_sign.jl:364-442, count_sketch.jl:215-262): C (c_rows x c_cols,
+ * column-major, ld ldc) = alpha*S*A + beta*C with A = transpose(B) (a_rows x a_cols), B an
+ * a_cols x a_rows SparseMatrixCSC.  A is passed by rows, which is B's compressed-column
+ * storage: a_rowptr[a_rows+1] = B.colptr - 1, a_colidx[a_nnz] = B.rowval - 1 (distinct
+ * within a row), a_vals[a_nnz] = B.nzval in S's element type; all device pointers.  Each
+ * C(i, c) is summed over the long indices j in increasing order, as the reference's loops
+ * do; no atomics.  The first call after a draw builds a per-recipe plan (a stable sort of
+ * the draws by row of S).  Synchronous.  Other recipes or cardinalities: RLA_E_ARG. */
+int rla_sketch_mul_sparse_t(rla_ctx *ctx, rla_sketch *sk, int64_t c_rows, int64_t c_cols,
+                            void *C, int64_t ldc, int64_t a_rows, int64_t a_cols, int64_t a_nnz,
+                            const int64_t *a_rowptr, const int64_t *a_colidx, const void *a_vals,
+                            double alpha, double beta);
+
 /* ---- range approximators --------------------------------------------------------- */
 typedef struct rla_range_params {
     int64_t power_its;       /* q (randsvd.jl:339, rangefinder.jl) */
@@ -405,6 +419,14 @@ int rla_server_stop(rla_server *srv);
 int rla_ctx_set_timing(rla_ctx *ctx, int enable);
 int rla_ctx_kernel_time(rla_ctx *ctx, int kernel_class, double *ms_total, int64_t *launches);
 
+/* ---- bounded device-side waits (failure detection, no reference counterpart) ---------- */
+/* Limit, in seconds (0 to 60, default 2), of one pipeline wait of the tensor-core GEMM
+ * kernel on an mbarrier.  A wait that runs out makes every CTA of the launch stop issuing
+ * work, wait (for at most 2 s more) for the copies and MMAs it already issued, release its
+ * tensor memory and exit; the call then returns RLA_E_TIMEOUT and the context stays usable.
+ * A limit of 0 makes any wait that is not already satisfied run out (used by the tests). */
+int rla_ctx_set_wait_limit(rla_ctx *ctx, double seconds);
+
 /* ---- split-BF16 tensor-core GEMM ------------------------------------------------ */
 /* No counterpart in the reference (its products go to BLAS gemm): the product kernel used
  * by RLA_PREC_SPLIT_BF16, exposed for callers and tests.  C = alpha*op(A)*B + beta*C with
@@ -431,7 +453,9 @@ int rla_gemm_bf16x3(rla_ctx *ctx, int trans_a, int64_t m, int64_t n, int64_t k,
  * The first call on a device looks up the arrays' device addresses; make that first call
  * before any stream capture.  All calls share the arrays, which keep the last call's
  * contents: calls whose GPU work overlaps (other streams or threads without ordering)
- * race.  Returns once the work is queued; synchronize the stream before reading C. */
+ * race.  The call runs on the context's device and leaves the calling thread's current
+ * device as it found it.  Negative dimensions are rejected with RLA_E_ARG.  Returns once
+ * the work is queued; synchronize the stream before reading C. */
 #define RLA_NOALLOC_SCRATCH_BYTES (8u << 20)
 #define RLA_NOALLOC_MAX_COLS 65536
 int rla_srht_mul_noalloc(rla_ctx *ctx, const rla_sketch *sk,

@@ -129,6 +129,9 @@ SIGNATURES = {
     "rla_server_last_error": (ctypes.c_char_p, [vp]),
     "rla_server_stop": (ctypes.c_int, [vp]),
     "rla_ctx_set_timing": (ctypes.c_int, [vp, ctypes.c_int]),
+    "rla_ctx_set_wait_limit": (ctypes.c_int, [vp, ctypes.c_double]),
+    "rla_sketch_mul_sparse_t": (ctypes.c_int, [vp, vp, i64, i64, vp, i64, i64, i64, i64, vp, vp, vp,
+                                               ctypes.c_double, ctypes.c_double]),
     "rla_ctx_kernel_time": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(i64)]),
     "rla_gemm_bf16x3": (ctypes.c_int, [vp, ctypes.c_int, i64, i64, i64, vp, i64, vp, i64, vp, i64,
                                        ctypes.c_double, ctypes.c_double]),

@@ -489,10 +489,65 @@ def _sketch_mul(C, S: CompressorRecipe, A, side: int, trans_s: int, alpha: float
     Cop.finish()
 
 
+def _is_sparse(x) -> bool:
+    """A torch sparse-CSR tensor or a scipy.sparse matrix."""
+    try:
+        import torch
+        if isinstance(x, torch.Tensor):
+            return x.layout == torch.sparse_csr
+    except ImportError:
+        pass
+    return hasattr(x, "tocsr") and hasattr(x, "nnz")
+
+
+def _sketch_mul_sparse(C, S: CompressorRecipe, A, alpha: float, beta: float) -> None:
+    """mul!(C, S, transpose(B), alpha, beta) (sparse_sign.jl:364-442, count_sketch.jl:215-262).
+
+    A sparse m x n matrix given by rows -- a torch sparse-CSR tensor or a scipy.sparse
+    matrix -- is Julia's transpose(B) of the n x m SparseMatrixCSC B: the same three arrays.
+    Host operands are copied to the device."""
+    import torch
+    if S.info.kind not in (L.RLA_SPARSE_SIGN, L.RLA_COUNT_SKETCH) or not isinstance(S.cardinality, Left):
+        raise ArgumentError(f"No method `mul!` defined for ({type(C).__name__}, {type(S).__name__}, "
+                            f"{type(A).__name__}, {type(alpha).__name__}, {type(beta).__name__}).")
+    dev = torch.device("cuda", S._ctx.device)
+    tdt = torch.float32 if S._dtype == 0 else torch.float64
+    if isinstance(A, torch.Tensor):
+        rows, cols = A.shape
+        rowptr = A.crow_indices().to(dev, torch.int64).contiguous()
+        colidx = A.col_indices().to(dev, torch.int64).contiguous()
+        vals = A.values().to(dev).contiguous()
+    else:
+        csr = A.tocsr(copy=True)
+        csr.sum_duplicates()
+        rows, cols = csr.shape
+        rowptr = torch.from_numpy(np.asarray(csr.indptr, np.int64)).to(dev)
+        colidx = torch.from_numpy(np.asarray(csr.indices, np.int64)).to(dev)
+        vals = torch.from_numpy(np.ascontiguousarray(csr.data)).to(dev)
+    if vals.dtype != tdt:
+        raise ArgumentError("The compressor, A and C must share one element type (Float32 or Float64).")
+    Cop = Operand(C, "col", writable=True)
+    if Cop.dtype != S._dtype:
+        raise ArgumentError("The compressor, A and C must share one element type (Float32 or Float64).")
+    if Cop.trans:
+        raise ArgumentError("C must be stored column-major (a dense matrix, not a transpose).")
+    ctx = L.Context.get(S._ctx.device)
+    st = L.lib().rla_sketch_mul_sparse_t(ctx.handle, S.handle, Cop.rows, Cop.cols, Cop.ptr, Cop.ld, rows, cols,
+                                         int(vals.numel()), rowptr.data_ptr(), colidx.data_ptr(), vals.data_ptr(),
+                                         float(alpha), float(beta))
+    L.check(st, ctx.handle)
+    Cop.finish()
+
+
 def mul_(C, X, Y, alpha: float = 1.0, beta: float = 0.0):
     """mul!(C, S, A, alpha, beta) / mul!(C, A, S, alpha, beta) and the adjoint forms;
     also dispatches to the approximator methods."""
     from . import approximators as _ap
+    if _is_sparse(Y) and isinstance(X, CompressorRecipe):
+        return _sketch_mul_sparse(C, X, Y, alpha, beta)
+    if _is_sparse(X) or _is_sparse(Y):
+        raise ArgumentError(f"No method `mul!` defined for ({type(C).__name__}, {type(X).__name__}, "
+                            f"{type(Y).__name__}, {type(alpha).__name__}, {type(beta).__name__}).")
     if isinstance(X, CompressorRecipe):
         return _sketch_mul(C, X, Y, L.RLA_SIDE_LEFT, 0, alpha, beta)
     if isinstance(X, CompressorAdjoint):

@@ -177,6 +177,14 @@ int rla_ctx_set_timing(rla_ctx *ctx, int enable) {
     return RLA_OK;
 }
 
+int rla_ctx_set_wait_limit(rla_ctx *ctx, double seconds) {
+    if (!ctx) return RLA_E_ARG;
+    if (!(seconds >= 0.0) || seconds > 60.0)
+        return set_error(ctx, RLA_E_ARG, "wait limit must lie in [0, 60] seconds");
+    ctx->wait_ns = (uint64_t)(seconds * 1e9);
+    return RLA_OK;
+}
+
 int rla_ctx_kernel_time(rla_ctx *ctx, int kernel_class, double *ms_total, int64_t *launches) {
     if (!ctx || !ms_total || !launches) return RLA_E_ARG;
     if (kernel_class < 0 || kernel_class > 3) return set_error(ctx, RLA_E_ARG, "unknown kernel class %d", kernel_class);

@@ -44,6 +44,7 @@ struct rla_ctx {
     int64_t scratch_high_water = 0;
     cudaMemPool_t pool = nullptr;  // context-owned stream-ordered pool, keeps freed memory mapped
     int *tc_status = nullptr;  // non-zero after a tensor-core kernel's bounded wait ran out
+    uint64_t wait_ns = 2000000000ull;  // limit of a device-side pipeline wait (rla_ctx_set_wait_limit)
     bool timing = false;       // record CUDA events around timed kernel classes
     // classes: 0 tensor-core GEMM, 1 IHS fused pass over A, 2 IHS compressor apply,
     // 3 Sampling L2Norm weights pass over A
@@ -292,6 +293,9 @@ struct rla_sketch {
     uint32_t *extra = nullptr;     // deferred items: 32 words (one per lane) per extra round
     int64_t extra_rounds_cap = 0;
     int batch_mode = 0;            // 1: CountSketch schedule over 512-element batches (see rla_sketch.cu)
+    int64_t *tp_ptr = nullptr;     // sparse-operand plan (rla_sparse_op.cu): [s+1] offsets per bucket
+    int32_t *tp_idx = nullptr;     // [L*nnz] entries j*nnz+slot by bucket, j increasing
+    uint64_t tp_version = 0;       // draw_count the plan was built for
     // SRHT
     int32_t *rows = nullptr;       // [s] sampled padded rows (op)
     uint32_t *signbits = nullptr;  // [ceil(N/32)] bit r = 1 means +1

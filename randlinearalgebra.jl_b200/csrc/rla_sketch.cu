@@ -572,7 +572,7 @@ int sketch_redraw_async(rla_ctx *ctx, rla_sketch *sk) {
 static void free_sketch_buffers(rla_sketch *sk) {
     void *ptrs[] = {sk->bucket, sk->negative, sk->meta, sk->rows, sk->signbits, sk->sign_tl, sk->tile_flags, sk->extra, sk->p2_ptr, sk->p2_list,
                     sk->k_ptr, sk->k_col, sk->k_val, sk->kt_ptr, sk->kt_row, sk->kt_val, sk->dense,
-                    sk->sidx, sk->splan, sk->sweights, sk->s_err};
+                    sk->sidx, sk->splan, sk->sweights, sk->s_err, sk->tp_ptr, sk->tp_idx};
     for (void *p : ptrs)
         if (p) cudaFree(p);
 }

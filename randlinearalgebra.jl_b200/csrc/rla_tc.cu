@@ -99,16 +99,30 @@ __device__ __forceinline__ uint64_t global_ns() {
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
 }
-// Wait for the phase of parity `parity` to complete; gives up after ~2 s (and 2^26 polls),
-// records the failure in *status and returns false.
-__device__ __noinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int *status) {
+// Wait for the phase of parity `parity` to complete; gives up after limit_ns (and 2^26
+// polls) or once another CTA has recorded a failure, records the failure in *status and
+// returns false.
+__device__ __noinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int *status, uint64_t limit_ns) {
     if (mbar_try(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    for (uint32_t it = 0; it < (1u << 26) && limit_ns > 0; ++it) {
+        if (mbar_try(bar, parity)) return true;
+        if ((it & 63u) == 0u && (global_ns() - t0 > limit_ns || *(volatile int *)status != 0)) break;
+    }
+    atomicExch(status, 1);
+    return false;
+}
+
+// Drain wait before a CTA releases its shared memory or tensor memory: waits for copies or
+// MMAs already issued, whatever the pipeline limit, for at most 2 s (and 2^26 polls).
+constexpr uint64_t TC_DRAIN_NS = 2000000000ull;
+__device__ __noinline__ bool mbar_drain(uint32_t bar, uint32_t parity, int *status) {
     const uint64_t t0 = global_ns();
     for (uint32_t it = 0; it < (1u << 26); ++it) {
         if (mbar_try(bar, parity)) return true;
-        if ((it & 63u) == 0u && (global_ns() - t0 > 2000000000ull || *(volatile int *)status != 0)) break;
+        if ((it & 63u) == 0u && global_ns() - t0 > TC_DRAIN_NS) break;
     }
-    atomicExch(status, 1);
+    atomicExch(status, 2);
     return false;
 }
 
@@ -178,6 +192,7 @@ struct TcParams {
     float *out;       // FP32 tile output: out + split*split_stride + row + col*ldo
     int64_t ldo, split_stride;
     int *status;
+    uint64_t wait_ns;  // limit of one pipeline wait
 };
 
 __global__ void __launch_bounds__(TC_THREADS, 1)
@@ -230,10 +245,12 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap map_ahi, const __grid_constan
         if (lane == 0) {
             // ---- TMA producer ----
             const uint32_t tx = stage_bytes;
+            int issued = 0;
             for (int kb = 0; kb < nkb; ++kb) {
                 const int s = kb % p.stages;
                 const uint32_t ph = (uint32_t)(kb / p.stages) & 1u;
-                if (!mbar_wait(empty_bar(s), ph ^ 1u, p.status)) break;
+                if (!mbar_wait(empty_bar(s), ph ^ 1u, p.status, p.wait_ns)) break;
+                issued = kb + 1;
                 const uint32_t st = base + (uint32_t)s * stage_bytes;
                 const uint32_t a_hi = st, a_lo = st + TC_A_BYTES, b_hi = st + 2 * TC_A_BYTES, b_lo = b_hi + b_bytes;
                 const int k0 = (kb0 + kb) * TC_BK;
@@ -254,6 +271,11 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap map_ahi, const __grid_constan
                     tma_load_2d(b_lo + off, &map_blo, full_bar(s), k0, c * (int)chunk_cols);
                 }
             }
+            // No copy into this CTA's shared memory may be outstanding when it exits: wait for
+            // the last phase issued on every stage (earlier phases of a stage completed before
+            // its slot was reissued).  Immediate on the normal path.
+            for (int kb = max(0, issued - p.stages); kb < issued; ++kb)
+                mbar_drain(full_bar(kb % p.stages), (uint32_t)(kb / p.stages) & 1u, p.status);
         }
         __syncwarp();
     } else if (warp == 1) {
@@ -263,7 +285,7 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap map_ahi, const __grid_constan
             for (int kb = 0; kb < nkb; ++kb) {
                 const int s = kb % p.stages;
                 const uint32_t ph = (uint32_t)(kb / p.stages) & 1u;
-                if (!mbar_wait(full_bar(s), ph, p.status)) break;
+                if (!mbar_wait(full_bar(s), ph, p.status, p.wait_ns)) break;
                 tc_fence_after();
                 const uint32_t st = base + (uint32_t)s * stage_bytes;
                 const uint32_t a_hi = st, a_lo = st + TC_A_BYTES, b_hi = st + 2 * TC_A_BYTES, b_lo = b_hi + b_bytes;
@@ -294,7 +316,10 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap map_ahi, const __grid_constan
         __syncwarp();
     }
     // ---- epilogue: all four warps; warp w owns TMEM lanes 32w .. 32w+31 ----
-    const bool ok = nkb > 0 && mbar_wait(done_bar, 0u, p.status);
+    bool ok = nkb > 0 && mbar_wait(done_bar, 0u, p.status, p.wait_ns);
+    // the MMAs issued before a failed wait still write tensor memory: drain them before the
+    // accumulator is read and released (done_bar is committed on every path)
+    if (!ok) mbar_drain(done_bar, 0u, p.status);
     __syncwarp();
     tc_fence_after();
     const int row = m0 + warp * 32 + lane;
@@ -463,7 +488,7 @@ int tc_gemm_bf16x3(rla_ctx *ctx, int64_t M, int64_t N, int64_t K, const bf16 *Ah
             out = (float *)ws;
         }
         TcParams p{(int)M, (int)nb, (int)K, pl.BN, pl.nch, a_kmajor, pl.nkb, pl.kbps, pl.stages, pl.tmem_cols,
-                   out, ldo, sstride, status};
+                   out, ldo, sstride, status, ctx->wait_ns};
         RLA_CUDA_TRY(ctx, set_smem_max(tc_gemm_kernel));
         cudaEvent_t e0 = nullptr, e1 = nullptr;
         if (ctx->timing) {

@@ -766,8 +766,7 @@ static int noalloc_setup(rla_ctx *ctx, NoallocDevice **out) {
     NoallocDevice &d = dev[ctx->device];
     if (!d.ready) {
         // In host code the array names are host-side stand-ins; the device addresses come
-        // from the runtime, per device, with that device current.
-        RLA_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+        // from the runtime, per device, with that device current (the caller made it so).
         RLA_CUDA_TRY(ctx, cudaGetSymbolAddress(&d.partials, g_noalloc_partials));
         RLA_CUDA_TRY(ctx, cudaGetSymbolAddress((void **)&d.counters, g_noalloc_counters));
         d.ready = true;
@@ -836,6 +835,7 @@ extern "C" int rla_srht_mul_noalloc(rla_ctx *ctx, const rla_sketch *sk, int64_t 
     if (!ctx) return RLA_E_ARG;
     if (!sk || sk->p.kind != RLA_SRHT || sk->p.card != RLA_LEFT)
         return set_error(ctx, RLA_E_ARG, "rla_srht_mul_noalloc needs a Left-cardinality SRHT recipe.");
+    if (c_rows < 0 || c_cols < 0 || a_rows < 0 || a_cols < 0) return set_error(ctx, RLA_E_ARG, "Negative dimension.");
     if (sk->device != ctx->device) return set_error(ctx, RLA_E_ARG, "Compressor lives on another device.");
     // left_mul_dimcheck (src/helpers/mul_dim_checks.jl:41-64)
     if (a_rows != sk->n_cols)
@@ -850,9 +850,23 @@ extern "C" int rla_srht_mul_noalloc(rla_ctx *ctx, const rla_sketch *sk, int64_t 
     if (a_cols == 0) return RLA_OK;
     if (!A || !C || lda < std::max<int64_t>(1, a_rows) || ldc < std::max<int64_t>(1, c_rows))
         return set_error(ctx, RLA_E_ARG, "NULL pointer or leading dimension smaller than the row count.");
+    // Every call runs on the context's device and hands the calling thread its own current
+    // device back, whichever it was.
+    int caller_dev = 0;
+    RLA_CUDA_TRY(ctx, cudaGetDevice(&caller_dev));
+    RLA_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
     NoallocDevice *nd = nullptr;
-    RLA_TRY(noalloc_setup(ctx, &nd));
-    if (sk->p.dtype == RLA_F32)
-        return srht_noalloc_t<float>(ctx, sk, (const float *)A, lda, a_cols, (float *)C, ldc, alpha, beta, *nd);
-    return srht_noalloc_t<double>(ctx, sk, (const double *)A, lda, a_cols, (double *)C, ldc, alpha, beta, *nd);
+    int st = noalloc_setup(ctx, &nd);
+    if (st == RLA_OK) {
+        if (sk->p.dtype == RLA_F32)
+            st = srht_noalloc_t<float>(ctx, sk, (const float *)A, lda, a_cols, (float *)C, ldc, alpha, beta, *nd);
+        else
+            st = srht_noalloc_t<double>(ctx, sk, (const double *)A, lda, a_cols, (double *)C, ldc, alpha, beta, *nd);
+    }
+    if (caller_dev != ctx->device) {
+        const cudaError_t e = cudaSetDevice(caller_dev);
+        if (st == RLA_OK && e != cudaSuccess)
+            return set_error(ctx, RLA_E_CUDA, "restoring the caller's device %d: %s", caller_dev, cudaGetErrorString(e));
+    }
+    return st;
 }

@@ -245,3 +245,46 @@ def test_split_bf16_rejects_float64(rla, dev):
     A = np.random.default_rng(1).standard_normal((20, 10))
     with pytest.raises(rla.ArgumentError, match="Split-BF16 products take Float32 data."):
         rla.rapproximate(rla.RandSVD(compressor=comp, precision=rla.RLA_PREC_SPLIT_BF16), to_dev(A, dev), seed=1)
+
+
+def test_randsvd_split_bf16_full_size_vs_oracle(rla, orc, dev):
+    """The mixed-precision RandSVD workload at its full size: A 65536x8192 Float32 =
+    U diag(i^-1.5) V' (rank 512, U and V orthonormal) + 1e-6 N(0,1), k = 256, p = 16 (l = 272),
+    q = 2, orthogonalized, split-BF16 products (randsvd.jl:174-189, power_its.jl:53-80).
+
+    The oracle runs the same algorithm in numpy FP64 on the host with the library's Gaussian
+    draws.  Singular values and the projection error ||A - UU'A|| / ||A|| of the library's
+    factors agree with the oracle's within 1e-4; both projection errors are evaluated by
+    the same FP64 products."""
+    import torch
+    m, n, k, p, q, r = 65536, 8192, 256, 16, 2, 512
+    l = k + p
+    g = torch.Generator(device=dev)
+    g.manual_seed(3)
+    Uo = torch.linalg.qr(torch.randn(m, r, device=dev, generator=g))[0]
+    Vo = torch.linalg.qr(torch.randn(n, r, device=dev, generator=g))[0]
+    sig = torch.arange(1, r + 1, device=dev, dtype=torch.float32) ** -1.5
+    At = (Vo * sig) @ Uo.t()
+    At.add_(torch.randn(n, m, device=dev, generator=g), alpha=1e-6)
+    del Uo, Vo
+    A = At.t()  # column-major m x n
+    comp = rla.Gaussian(cardinality=rla.Right(), compression_dim=l, type=np.float32)
+    rec = rla.rapproximate(rla.RandSVD(compressor=comp, power_its=q, orthogonalize=True,
+                                       precision=rla.RLA_PREC_SPLIT_BF16), A, seed=3000)
+    U = rec.U.double()
+    S = rec.S.cpu().numpy().astype(np.float64)
+    A64h = np.asfortranarray(At.t().double().cpu().numpy())
+    ref = orc.randsvd(A64h, oracle_recipe(orc, rec.compressor), q=q, orthogonalize=True)
+    assert rel_err(S, ref.S) < 1e-4, rel_err(S, ref.S)
+    del A64h
+    A64 = A.double()
+    nA = torch.linalg.norm(A64)
+
+    def proj_err(Q):
+        return float(torch.linalg.norm(A64 - Q @ (Q.t() @ A64)) / nA)
+
+    e_gpu = proj_err(U)
+    e_ref = proj_err(torch.from_numpy(np.ascontiguousarray(ref.U)).to(dev))
+    assert abs(e_gpu - e_ref) < 1e-4, (e_gpu, e_ref)
+    I = torch.eye(l, device=dev, dtype=torch.float64)
+    assert float(torch.max(torch.abs(U.t() @ U - I))) < 1e-5

@@ -254,3 +254,42 @@ def test_load_draws_parity_mode(rla, orc, dev, kind):
     ref = np.zeros((s, 5))
     orc.mul_SA(ref, R, A)
     assert rel_err(Cd.cpu().numpy(), ref) < 1e-12
+
+
+def test_sparse_sign_left_fp64_4096x256(rla, orc, dev):
+    """The plain SparseSign workload exactly: A 4096x256 Float64 ~ N(0,1), compression
+    dimension 512, 8 nonzeros per column, Left (test/Compressors/sparse_sign.jl:299-459).
+
+    The draws exported into the oracle recipe satisfy the reference's invariants (8 sorted,
+    distinct rows per column; values +-1/sqrt(8) exactly), S*I materialises exactly the
+    dense operator built from those draws (every entry is one signed term), and S*A agrees
+    with the oracle's CSC loop to 1e-12 relative, alone and in 5-argument form."""
+    m, n, s, nnz = 4096, 256, 512, 8
+    rng = np.random.default_rng(1)
+    S = rla.complete_compressor(rla.SparseSign(cardinality=rla.Left(), compression_dim=s, nnz=nnz, type=np.float64),
+                                np.zeros((m, 1)), seed=1)
+    colptr, rowval, nzval = S.op
+    assert np.array_equal(colptr, np.arange(0, m * nnz + 1, nnz))
+    rv = rowval.reshape(m, nnz)
+    assert np.all(np.diff(rv, axis=1) > 0) and rv.min() >= 0 and rv.max() < s
+    sc = 1 / np.sqrt(np.float64(nnz))
+    assert set(np.unique(nzval)) <= {sc, -sc}
+    dense = np.zeros((s, m))
+    dense[rowval, np.repeat(np.arange(m), nnz)] = nzval
+    mat = to_dev(np.zeros((s, m)), dev)
+    rla.mul_(mat, S, to_dev(np.eye(m), dev))
+    assert np.array_equal(mat.cpu().numpy(), dense)
+    R = oracle_recipe(orc, S)
+    A = rng.standard_normal((m, n))
+    Cd = to_dev(np.zeros((s, n)), dev)
+    rla.mul_(Cd, S, to_dev(A, dev))
+    ref = np.zeros((s, n))
+    orc.mul_SA(ref, R, A)
+    assert rel_err(Cd.cpu().numpy(), ref) < 1e-12
+    assert rel_err(Cd.cpu().numpy(), dense @ A) < 1e-12
+    C0 = rng.standard_normal((s, n))
+    Cd = to_dev(C0, dev)
+    rla.mul_(Cd, S, to_dev(A, dev), 2.0, 2.0)
+    ref = C0.copy(order="F")
+    orc.mul_SA(ref, R, A, 2.0, 2.0)
+    assert rel_err(Cd.cpu().numpy(), ref) < 1e-12

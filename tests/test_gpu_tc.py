@@ -81,3 +81,26 @@ def test_gemm_deterministic(rla, dev):
                                           C.stride(1), 1.0, 0.0), ctx.handle)
         outs.append(C.cpu().numpy())
     assert np.array_equal(outs[0], outs[1])
+
+
+@pytest.mark.gpu
+def test_wait_limit_runs_out_and_context_recovers(rla, dev):
+    """Failure detection without a GPU fault.  With a wait limit of zero every mbarrier wait
+    of the GEMM kernel that is not already satisfied runs out: the kernel records the
+    failure in its status word, stops issuing copies and MMAs, waits (bounded) for the ones
+    already issued, releases its tensor memory and exits, and the call reports
+    RLA_E_TIMEOUT.  The same context then computes the product correctly."""
+    import torch
+    L = rla._lib.lib()
+    ctx = rla._lib.Context.get(dev.index or 0)
+    rla._lib.check(L.rla_ctx_set_wait_limit(ctx.handle, 0.0), ctx.handle)
+    try:
+        with pytest.raises(rla.RLAError, match="timed out"):
+            run_gemm(rla, torch, dev, 0, 4096, 256, 2048)
+    finally:
+        rla._lib.check(L.rla_ctx_set_wait_limit(ctx.handle, 2.0), ctx.handle)
+    for trans_a in (0, 1):
+        err = run_gemm(rla, torch, dev, trans_a, 4096, 256, 2048)
+        assert err < TOL, (trans_a, err)
+    with pytest.raises(rla.ArgumentError, match="wait limit"):
+        rla._lib.check(L.rla_ctx_set_wait_limit(ctx.handle, -1.0), ctx.handle)
