@@ -45,6 +45,7 @@ extern "C" {
 #define RLA_E_TIMEOUT 6      /* a bounded device-side wait ran out */
 #define RLA_E_NUMERIC 7      /* Cholesky breakdown not repaired by the shifted fallback */
 #define RLA_E_UNSUPPORTED 8  /* combination not provided by this build */
+#define RLA_E_CANCELLED 9    /* serving: the request was cancelled before it started */
 
 /* ---- enumerations ---------------------------------------------------------------- */
 #define RLA_F32 0
@@ -394,6 +395,8 @@ typedef struct rla_server_config {
     int max_group;            /* RandSVD requests (k <= 128) run as one grouped batch */
     int mode;                 /* RLA_SERVE_BATCHED or RLA_SERVE_PLAIN */
     uint64_t memory_budget;   /* bytes of workspace admitted at once (0: 150 GB) */
+    uint64_t sketch_cache_bytes; /* cap on resident sketches (0: memory_budget / 8); counted
+                                    in the budget, least recently used evicted first */
 } rla_server_config;
 
 typedef struct rla_server rla_server;
@@ -406,6 +409,20 @@ int rla_server_poll(rla_server *srv, uint64_t *tags, double *latency_s, int *sta
 const char *rla_server_last_error(rla_server *srv);
 /* Block until the queue is empty and nothing runs. */
 int rla_server_wait_idle(rla_server *srv);
+/* Remove a request that is still queued; rla_server_poll then reports it with status
+ * RLA_E_CANCELLED.  RLA_E_ARG when no queued request has that tag (it already started). */
+int rla_server_cancel(rla_server *srv, uint64_t tag);
+/* Fault injection on the host (failure-detection tests): when the request with this tag is
+ * taken by a worker, its workspace allocation fails as if the device were out of memory;
+ * that request alone completes with RLA_E_OOM and nothing of it reaches the GPU. */
+int rla_server_inject_alloc_failure(rla_server *srv, uint64_t tag);
+typedef struct rla_server_stats {
+    int64_t queued, running;     /* requests waiting / being worked on */
+    uint64_t workspace_bytes;    /* estimated workspace of the running requests */
+    uint64_t cache_bytes;        /* resident sketches (estimated device bytes) */
+    int64_t cache_entries, evictions;
+} rla_server_stats;
+int rla_server_get_stats(rla_server *srv, rla_server_stats *out);
 /* Finish queued work and shut the workers down. */
 int rla_server_stop(rla_server *srv);
 

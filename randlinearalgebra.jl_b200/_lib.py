@@ -59,9 +59,15 @@ class Request(ctypes.Structure):
 
 class ServerConfig(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("slots", ctypes.c_int), ("max_group", ctypes.c_int), ("mode", ctypes.c_int),
-                ("memory_budget", ctypes.c_uint64)]
+                ("memory_budget", ctypes.c_uint64), ("sketch_cache_bytes", ctypes.c_uint64)]
 
 
+class ServerStats(ctypes.Structure):
+    _fields_ = [("queued", ctypes.c_int64), ("running", ctypes.c_int64), ("workspace_bytes", ctypes.c_uint64),
+                ("cache_bytes", ctypes.c_uint64), ("cache_entries", ctypes.c_int64), ("evictions", ctypes.c_int64)]
+
+
+RLA_E_CANCELLED = 9
 RLA_REQ_LS, RLA_REQ_SVD = 0, 1
 RLA_SERVE_BATCHED, RLA_SERVE_PLAIN = 0, 1
 RLA_BATCH_AUTOTUNE = 1
@@ -128,6 +134,9 @@ SIGNATURES = {
     "rla_server_wait_idle": (ctypes.c_int, [vp]),
     "rla_server_last_error": (ctypes.c_char_p, [vp]),
     "rla_server_stop": (ctypes.c_int, [vp]),
+    "rla_server_cancel": (ctypes.c_int, [vp, ctypes.c_uint64]),
+    "rla_server_inject_alloc_failure": (ctypes.c_int, [vp, ctypes.c_uint64]),
+    "rla_server_get_stats": (ctypes.c_int, [vp, ctypes.POINTER(ServerStats)]),
     "rla_ctx_set_timing": (ctypes.c_int, [vp, ctypes.c_int]),
     "rla_ctx_set_wait_limit": (ctypes.c_int, [vp, ctypes.c_double]),
     "rla_sketch_mul_sparse_t": (ctypes.c_int, [vp, vp, i64, i64, vp, i64, i64, i64, i64, vp, vp, vp,

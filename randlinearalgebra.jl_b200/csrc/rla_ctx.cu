@@ -78,6 +78,7 @@ const char *rla_status_string(int status) {
         case RLA_E_TIMEOUT: return "device wait timed out";
         case RLA_E_NUMERIC: return "numerical breakdown";
         case RLA_E_UNSUPPORTED: return "unsupported";
+        case RLA_E_CANCELLED: return "cancelled";
         default: return "unknown status";
     }
 }

@@ -27,9 +27,9 @@ def sketch_solve(S, A, b, x) -> None:
 
 class Server:
     def __init__(self, device: int = 0, slots: int = 4, max_group: int = 64, plain: bool = False,
-                 memory_budget: int = 0):
+                 memory_budget: int = 0, sketch_cache_bytes: int = 0):
         cfg = L.ServerConfig(device, slots, max_group, L.RLA_SERVE_PLAIN if plain else L.RLA_SERVE_BATCHED,
-                             memory_budget)
+                             memory_budget, sketch_cache_bytes)
         h = ctypes.c_void_p()
         st = L.lib().rla_server_start(ctypes.byref(cfg), ctypes.byref(h))
         if st != L.RLA_OK:
@@ -73,6 +73,20 @@ class Server:
 
     def wait_idle(self) -> None:
         L.lib().rla_server_wait_idle(self.handle)
+
+    def cancel(self, tag: int) -> None:
+        """Remove a queued request; poll then reports it with status RLA_E_CANCELLED."""
+        if L.lib().rla_server_cancel(self.handle, tag) != L.RLA_OK:
+            raise ArgumentError(f"no queued request with tag {tag}")
+
+    def inject_alloc_failure(self, tag: int) -> None:
+        """Fault injection: the request with this tag fails its workspace allocation."""
+        L.check(L.lib().rla_server_inject_alloc_failure(self.handle, tag))
+
+    def stats(self) -> dict:
+        st = L.ServerStats()
+        L.check(L.lib().rla_server_get_stats(self.handle, ctypes.byref(st)))
+        return {f: getattr(st, f) for f, _ in L.ServerStats._fields_}
 
     def stop(self) -> None:
         if self.handle:
