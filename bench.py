@@ -329,6 +329,24 @@ def b200_arm(args):
            "ms_per_step": round(e2e_s * 1e3, 3)}
     del A_h
 
+    # ---- the metric's second half on the same GPU: config-3 RandSVD and the served mix ----
+    extras = {}
+    if world == 1 and not args.no_extras and (M, NCOL) == (2**20, 512):
+        del A, C1, C2
+        torch.cuda.empty_cache()
+        r = rs_measure(rla, torch, dev, RS_M, RS_N, 3, 3, with_e2e=False)
+        extras["randsvd"] = {"workload": RS_WORKLOAD, "ms_per_rapproximate": round(r["ms"], 3),
+                             "tflops": round(r["flops"] / (r["ms"] / 1e3) / 1e12, 2),
+                             "roofline": rs_roofline(RS_M, RS_N, r), "error": r["error"], "clocks": r["clocks"]}
+        ls, svd, servers = serve_setup(rla, torch, dev, 4)
+        curve = sv_curve(rla, torch, dev, ls, svd, servers, SV_SLO_RATES, 200, 1, seed0=20)
+        for srv in servers.values():
+            srv.stop()
+        del ls, svd
+        torch.cuda.empty_cache()
+        extras["serve"] = {"workload": SV_WORKLOAD + "; offered rates below saturation, 200 requests per rate",
+                           "curve": curve, "at_slo": sv_at_slo(curve, SV_SLO_RATES)}
+
     if rank != 0:
         if world > 1:
             import torch.distributed as dist
@@ -361,7 +379,7 @@ def b200_arm(args):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic N(0,1) generated on device (torch.randn, seed 2+rank)",
             "config": sketch_config(M, NCOL, world),
             "roofline": roofline, "kernels": kernels, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
-            "gpu_launches": 2 * K}
+            "gpu_launches": 2 * K, **extras}
     print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
@@ -441,18 +459,15 @@ def randsvd_reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
-def randsvd_arm(args):
+def rs_measure(rla, torch, dev, m, n, steps, warmup, rank=0, world=1, with_e2e=True):
+    """Config-3 RandSVD on this GPU: timed rapproximate! calls, tensor-core GEMM kernel time,
+    error against the FP64 run of the same algorithm on the same draws, and (optionally) the
+    end-to-end rate with A in pinned host memory."""
     import ctypes
 
     import numpy as np
-    import torch
-
-    world, rank, local = dist_setup(args.gpus)
-    from __graft_entry__ import load_package
-    rla = load_package()
     from randlinearalgebra_b200 import _lib as L
-    dev = torch.device("cuda", local if world > 1 else 0)
-    m, n, l, q = args.rs_m, args.rs_n, RS_K + RS_P, RS_Q
+    l, q = RS_K + RS_P, RS_Q
     A = rs_problem(torch, dev, m, n, min(RS_R, n), 3 + rank)
     comp = rla.Gaussian(cardinality=rla.Right(), compression_dim=l, type=np.float32)
     rec = rla.complete_approximator(rla.RandSVD(compressor=comp, power_its=q, orthogonalize=True,
@@ -461,12 +476,11 @@ def randsvd_arm(args):
     ctx = L.Context.get(dev.index)
     lib = L.lib()
     stream = torch.cuda.current_stream(dev)
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         rla.rapproximate_(rec, A)
     lib.rla_ctx_set_timing(ctx.handle, 1)
     ms_tc, n_tc = ctypes.c_double(), ctypes.c_int64()
     L.check(lib.rla_ctx_kernel_time(ctx.handle, 0, ctypes.byref(ms_tc), ctypes.byref(n_tc)), ctx.handle)
-    K = args.steps
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     props = torch.cuda.get_device_properties(dev)
     clocks = ClockSampler(f"GPU-{props.uuid}" if getattr(props, "uuid", None) else dev.index)
@@ -474,7 +488,7 @@ def randsvd_arm(args):
     torch.cuda.synchronize()
     clocks.start()
     t0.record(stream)
-    for _ in range(K):
+    for _ in range(steps):
         rla.rapproximate_(rec, A)
     t1.record(stream)
     torch.cuda.synchronize()
@@ -484,7 +498,6 @@ def randsvd_arm(args):
     L.check(lib.rla_ctx_kernel_time(ctx.handle, 0, ctypes.byref(ms_tc), ctypes.byref(n_tc)), ctx.handle)
     lib.rla_ctx_set_timing(ctx.handle, 0)
     fl = rs_flops(m, n, l, q)
-    value = world * fl * K / (ms / 1e3) / 1e9
 
     # ---- error against the FP64 run of the same algorithm on the same draws --------------
     U32, S32 = rec.U.double(), rec.S.double()
@@ -502,56 +515,77 @@ def randsvd_arm(args):
     s_err = float(torch.linalg.norm(S32 - rec64.S) / torch.linalg.norm(rec64.S))
     del A64, rec64
     torch.cuda.empty_cache()
-
-    # ---- end to end: host A (pinned) in, factors out, through the public API --------------
-    A_h = torch.empty(n, m, dtype=torch.float32, pin_memory=True).t()
-    A_h.copy_(A)
-    e2e_steps = 2
-    rla.rapproximate_(rec, A_h)
-    torch.cuda.synchronize()
-    barrier(world)
-    w0 = time.perf_counter()
-    for _ in range(e2e_steps):
+    out = {"ms": ms / steps, "flops": fl, "tc_ms": ms_tc.value, "tc_launches": n_tc.value, "clocks": clk,
+           "error": {"proj_err_split": e32, "proj_err_fp64": e64, "proj_err_diff": abs(e32 - e64),
+                     "sigma_rel_err": s_err, "tolerance": 1e-4}}
+    if with_e2e:
+        # ---- end to end: host A (pinned) in, factors out, through the public API ----------
+        A_h = torch.empty(n, m, dtype=torch.float32, pin_memory=True).t()
+        A_h.copy_(A)
+        e2e_steps = 2
         rla.rapproximate_(rec, A_h)
-        Uh, Sh, Vh = rec.U.cpu(), rec.S.cpu(), rec.V.cpu()
-    e2e_s = allreduce_max((time.perf_counter() - w0) / e2e_steps, world)
-    e2e = {"value": round(world * fl / e2e_s / 1e9, 3), "unit": "GFLOP/s", "h2d_bytes_per_step": 4 * m * n,
-           "d2h_bytes_per_step": 4 * (m + n) * l + 8 * l, "ms_per_step": round(e2e_s * 1e3, 3)}
-    del A_h
-    if rank != 0:
-        if world > 1:
-            import torch.distributed as dist
-            dist.destroy_process_group()
-        return
+        torch.cuda.synchronize()
+        barrier(world)
+        w0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            rla.rapproximate_(rec, A_h)
+            rec.U.cpu(), rec.S.cpu(), rec.V.cpu()
+        e2e_s = allreduce_max((time.perf_counter() - w0) / e2e_steps, world)
+        out["e2e"] = {"value": round(world * fl / e2e_s / 1e9, 3), "unit": "GFLOP/s", "h2d_bytes_per_step": 4 * m * n,
+                      "d2h_bytes_per_step": 4 * (m + n) * l + 8 * l, "ms_per_step": round(e2e_s * 1e3, 3)}
+        del A_h
+    del A, rec
+    torch.cuda.empty_cache()
+    return out
+
+
+def rs_roofline(m, n, r):
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
             pk = json.load(f)
         peak_bf16, peak_kind = float(pk["bf16_tflops"]), "measured"
     except Exception:
         peak_bf16, peak_kind = 1590.0, "fallback"
-    tc_avg_ms = ms_tc.value / max(n_tc.value, 1)
+    l = RS_K + RS_P
+    tc_avg_ms = r["tc_ms"] / max(r["tc_launches"], 1)
     tc_flops = 2.0 * m * n * l  # each of the 2q+2 products with A
     achieved = tc_flops / (tc_avg_ms / 1e3) / 1e12
-    roofline = {"bound": "tensor", "kernel": "tc_gemm_kernel", "achieved": round(achieved, 2),
-                "peak": round(peak_bf16 / 3, 2), "peak_source": f"{peak_kind} bf16 dense / 3 (three BF16 products per split product)",
-                "unit": "TFLOP/s", "frac": round(achieved / (peak_bf16 / 3), 4), "traffic": None,
-                "launches_timed": n_tc.value, "avg_launch_ms": round(tc_avg_ms, 4),
-                "tensor_flops_per_launch": 3 * tc_flops}
+    return {"bound": "tensor", "kernel": "tc_gemm_kernel", "achieved": round(achieved, 2),
+            "peak": round(peak_bf16 / 3, 2), "peak_source": f"{peak_kind} bf16 dense / 3 (three BF16 products per split product)",
+            "unit": "TFLOP/s", "frac": round(achieved / (peak_bf16 / 3), 4), "traffic": None,
+            "launches_timed": r["tc_launches"], "avg_launch_ms": round(tc_avg_ms, 4),
+            "tensor_flops_per_launch": 3 * tc_flops}
+
+
+def randsvd_arm(args):
+    import torch
+
+    world, rank, local = dist_setup(args.gpus)
+    from __graft_entry__ import load_package
+    rla = load_package()
+    dev = torch.device("cuda", local if world > 1 else 0)
+    m, n, l, q = args.rs_m, args.rs_n, RS_K + RS_P, RS_Q
+    K = args.steps
+    r = rs_measure(rla, torch, dev, m, n, K, args.warmup, rank, world)
+    value = world * r["flops"] / (r["ms"] / 1e3) / 1e9
+    if rank != 0:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         g, desc, _ = rs_cpu_sample(f"{os.cpu_count()} host threads")
         cpu = {"value": round(g, 3), "unit": "GFLOP/s", "cores": os.cpu_count(), "kind": "port", "sample": desc}
     line = {"metric": RS_METRIC, "value": round(value, 2), "unit": "GFLOP/s", "n_gpus": world, "steps": K,
-            "warmup": args.warmup, "ms_per_step": round(ms / K, 4), "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": round(r["ms"], 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 data, bf16x3 products, f64 small factorizations",
             "data": "synthetic U diag(i^-1.5) V' + 1e-6 N(0,1) generated on device (seed 3+rank)",
             "config": {"workload": RS_WORKLOAD if (m, n) == (RS_M, RS_N) else
                        RS_WORKLOAD.replace("65536x8192", f"{m}x{n}"), "m": m, "n": n, "k": RS_K, "p": RS_P, "q": q,
                        "parallelism": f"replicas x{world}", "l2": "A is 2.15 GB (larger than L2), no flush needed"},
-            "roofline": roofline,
-            "error": {"proj_err_split": e32, "proj_err_fp64": e64, "proj_err_diff": abs(e32 - e64),
-                      "sigma_rel_err": s_err, "tolerance": 1e-4},
-            "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches_tensor_core": n_tc.value}
+            "roofline": rs_roofline(m, n, r), "error": r["error"],
+            "cpu_baseline": cpu, "e2e": r["e2e"], "clocks": r["clocks"], "gpu_launches_tensor_core": r["tc_launches"]}
     print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
@@ -1218,6 +1252,50 @@ def sv_run(rla, torch, dev, ls, svd, lam, nreq, srv, seed, ls_frac=0.6):
     return thr, float(np.percentile(ls_lat, 50)), float(np.percentile(ls_lat, 99))
 
 
+SV_SLO_RATES = [100, 200, 400, 700, 1000, 1500]  # offered rates of the latency-throughput curve
+
+
+def sv_curve(rla, torch, dev, ls, svd, servers, rates, nreq, reps, seed0=10):
+    """Latency-throughput curve of both modes: per offered rate, the median (by throughput) of
+    `reps` runs of nreq requests.  Returns {"batched": {rate: ...}, "plain": {rate: ...}}."""
+    res = {"batched": {}, "plain": {}}
+    for lam in rates:
+        for mode, plain in (("batched", False), ("plain", True)):
+            runs = sorted((sv_run(rla, torch, dev, ls, svd, lam, nreq, servers[plain], seed0 + lam + 1000 * r)
+                           for r in range(reps)), key=lambda x: x[0])
+            thr, p50, p99 = runs[len(runs) // 2]
+            res[mode][lam] = {"req_per_s": round(thr, 1), "p50_ms": round(1e3 * p50, 3), "p99_ms": round(1e3 * p99, 3),
+                              "runs_req_per_s": [round(x[0], 1) for x in runs]}
+    return res
+
+
+def sv_at_slo(curve, rates):
+    """Throughput at a fixed p99 SLO.  The SLO is twice the plain path's p99 at the lowest
+    offered rate (its service latency when nothing queues); each mode's figure is the highest
+    measured throughput among the rates whose p99 stays within the SLO."""
+    slo = 2.0 * curve["plain"][rates[0]]["p99_ms"]
+    out = {"p99_slo_ms": round(slo, 3)}
+    for mode in ("batched", "plain"):
+        ok = [curve[mode][r]["req_per_s"] for r in rates if curve[mode][r]["p99_ms"] <= slo]
+        out[f"{mode}_req_per_s"] = max(ok) if ok else None
+    b, pl = out["batched_req_per_s"], out["plain_req_per_s"]
+    out["ratio"] = None if (b is None or not pl) else round(b / pl, 2)
+    return out
+
+
+def serve_setup(rla, torch, dev, slots, rank=0):
+    """Pool of device-resident problems and one warmed, long-running server per mode."""
+    ls, svd = sv_pool(torch, dev, 24, 16, seed=5 + rank)
+    torch.cuda.synchronize()
+    servers = {False: rla.Server(slots=slots, max_group=32, plain=False),
+               True: rla.Server(slots=1, max_group=32, plain=True)}
+    for srv in servers.values():
+        sv_warm(torch, dev, ls, svd, srv)
+    sv_run(rla, torch, dev, ls, svd, 5000, 60, servers[False], 1)
+    sv_run(rla, torch, dev, ls, svd, 5000, 30, servers[True], 2)
+    return ls, svd, servers
+
+
 def serve_arm(args):
     import numpy as np
     import torch
@@ -1226,15 +1304,10 @@ def serve_arm(args):
     from __graft_entry__ import load_package
     rla = load_package()
     dev = torch.device("cuda", local if world > 1 else 0)
-    ls, svd = sv_pool(torch, dev, 24, 16, seed=5 + rank)
-    torch.cuda.synchronize()
     lams = [int(x) for x in args.serve_rates.split(",")]
     # one long-running server per mode, as a deployment keeps it: its contexts, sketch cache
-    # and memory pools are built once, during the warm-up below
-    servers = {False: rla.Server(slots=args.slots, max_group=32, plain=False),
-               True: rla.Server(slots=1, max_group=32, plain=True)}
-    for srv in servers.values():
-        sv_warm(torch, dev, ls, svd, srv)
+    # and memory pools are built once, during the warm-up
+    ls, svd, servers = serve_setup(rla, torch, dev, args.slots, rank)
     if args.serve_mix is not None:  # capacity of one request type (diagnostics)
         for plain in (False, True):
             thr, p50, p99 = sv_run(rla, torch, dev, ls, svd, max(lams), args.serve_requests, servers[plain], 3,
@@ -1244,22 +1317,14 @@ def serve_arm(args):
         for srv in servers.values():
             srv.stop()
         return
-    # and a short run per mode at a moderate rate (pools, grouped-batch paths)
-    sv_run(rla, torch, dev, ls, svd, 5000, 60, servers[False], 1)
-    sv_run(rla, torch, dev, ls, svd, 5000, 30, servers[True], 2)
-    res = {"batched": {}, "plain": {}}
     props = torch.cuda.get_device_properties(dev)
     clocks = ClockSampler(f"GPU-{props.uuid}" if getattr(props, "uuid", None) else dev.index)
     clocks.start()
-    for lam in lams:
-        for mode, plain in (("batched", False), ("plain", True)):
-            # SV_REPS runs per rate and mode; the median run (by throughput) is reported, so one
-            # run disturbed by other work on the shared host does not decide the line
-            runs = sorted((sv_run(rla, torch, dev, ls, svd, lam, args.serve_requests, servers[plain],
-                                  10 + lam + 1000 * r) for r in range(SV_REPS)), key=lambda x: x[0])
-            thr, p50, p99 = runs[len(runs) // 2]
-            res[mode][lam] = {"req_per_s": round(thr, 1), "p50_ms": round(1e3 * p50, 3), "p99_ms": round(1e3 * p99, 3),
-                              "runs_req_per_s": [round(x[0], 1) for x in runs]}
+    # SV_REPS runs per rate and mode; the median run (by throughput) is reported, so one run
+    # disturbed by other work on the shared host does not decide the line
+    res = sv_curve(rla, torch, dev, ls, svd, servers, lams, args.serve_requests, SV_REPS)
+    # below saturation: the latency-throughput curve and the throughput at a fixed p99 SLO
+    slo_curve = sv_curve(rla, torch, dev, ls, svd, servers, SV_SLO_RATES, args.serve_requests // 2, 1, seed0=20)
     clk = clocks.stop()
     for srv in servers.values():
         srv.stop()
@@ -1287,6 +1352,7 @@ def serve_arm(args):
                        "slots": args.slots, "max_group": 32, "memory_budget_gb": 150,
                        "parallelism": f"replicas x{world}"},
             "serving": res,
+            "below_saturation": {"curve": slo_curve, "at_slo": sv_at_slo(slo_curve, SV_SLO_RATES)},
             "equal_p99": {"plain_req_per_s": res["plain"][pl_best]["req_per_s"], "p99_budget_ms": p99_budget,
                           "batched_req_per_s": b_at,
                           "ratio": None if b_at is None else round(b_at / res["plain"][pl_best]["req_per_s"], 2)},
@@ -1307,6 +1373,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="sketch workload: skip the RandSVD and serving keys of the line (profiling runs)")
     ap.add_argument("--rows", type=int, default=M,
                     help="rows of A (default 2^20; 4194304 with --cols 128 is the tall-skinny variant)")
     ap.add_argument("--cols", type=int, default=NCOL,
