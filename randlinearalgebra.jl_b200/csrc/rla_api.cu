@@ -9,6 +9,7 @@
 // (columns of a column-major matrix) and "strided" otherwise.
 #include "rla_internal.cuh"
 #include "rla_kernels.cuh"
+#include "rla_tc.cuh"
 
 namespace rla {
 
@@ -40,6 +41,17 @@ static int dimcheck(rla_ctx *ctx, const rla_sketch *sk, int side, int trans_s, i
     return trans_s ? left(c_cols, c_rows, nr, nc, a_cols, a_rows) : right(c_rows, c_cols, a_rows, a_cols, nr, nc);
 }
 
+// Dense products of the Gaussian sketch: Float32 on the tensor cores (three BF16 terms per
+// operand, an FP32-accurate product), Float64 on the FP64 pipes.
+template <class T>
+static int dense_gemm(rla_ctx *ctx, int64_t M, int64_t N, int64_t K, const T *A, int64_t lda, int ta, const T *B,
+                      int64_t ldb, int tb, T *C, int64_t ldc, double alpha, double beta) {
+    if constexpr (std::is_same<T, float>::value)
+        return gemm_f32_tc<float>(ctx, M, N, K, A, lda, ta, B, ldb, tb, C, ldc, alpha, beta);
+    else
+        return gemm<T, T, T, double>(ctx, M, N, K, A, lda, ta, B, ldb, tb, C, ldc, alpha, beta);
+}
+
 template <class T>
 static int dispatch(rla_ctx *ctx, const rla_sketch *sk, int side, int trans_s, int64_t c_rows, int64_t c_cols, T *C,
                     int64_t ldc, int trans_c, int64_t a_rows, int64_t a_cols, const T *A, int64_t lda, int trans_a,
@@ -50,12 +62,12 @@ static int dispatch(rla_ctx *ctx, const rla_sketch *sk, int side, int trans_s, i
         const int64_t lds = sk->n_rows;
         if (side == RLA_SIDE_LEFT) {
             const int64_t K = trans_s ? sk->n_rows : sk->n_cols;
-            if (!trans_c) return gemm<T, T, T, double>(ctx, c_rows, c_cols, K, S, lds, trans_s, A, lda, trans_a, C, ldc, alpha, beta);
-            return gemm<T, T, T, double>(ctx, c_cols, c_rows, K, A, lda, !trans_a, S, lds, !trans_s, C, ldc, alpha, beta);
+            if (!trans_c) return dense_gemm<T>(ctx, c_rows, c_cols, K, S, lds, trans_s, A, lda, trans_a, C, ldc, alpha, beta);
+            return dense_gemm<T>(ctx, c_cols, c_rows, K, A, lda, !trans_a, S, lds, !trans_s, C, ldc, alpha, beta);
         }
         const int64_t K = a_cols;
-        if (!trans_c) return gemm<T, T, T, double>(ctx, c_rows, c_cols, K, A, lda, trans_a, S, lds, trans_s, C, ldc, alpha, beta);
-        return gemm<T, T, T, double>(ctx, c_cols, c_rows, K, S, lds, !trans_s, A, lda, !trans_a, C, ldc, alpha, beta);
+        if (!trans_c) return dense_gemm<T>(ctx, c_rows, c_cols, K, A, lda, trans_a, S, lds, trans_s, C, ldc, alpha, beta);
+        return dense_gemm<T>(ctx, c_cols, c_rows, K, S, lds, !trans_s, A, lda, !trans_a, C, ldc, alpha, beta);
     }
     const bool compress = side == RLA_SIDE_LEFT ? ((sk->p.card == RLA_LEFT) != (trans_s != 0))
                                                 : ((sk->p.card == RLA_RIGHT) != (trans_s != 0));

@@ -282,27 +282,31 @@ struct Owned {
     }
 };
 
-// Operands of the split-BF16 tensor-core path (RLA_PREC_SPLIT_BF16, FP32 data): A split
-// once into hi/lo BF16 copies; one hi/lo buffer pair reused for the thin factor of each
+// Operands of the tensor-core products with A (Float32 data): A split once into NT BF16
+// terms (NT = 2 for RLA_PREC_SPLIT_BF16, about 16 bits; NT = 3 for RLA_PREC_NATIVE, an
+// FP32-accurate product); one buffer set reused for the terms of the thin factor of each
 // product (Omega, Q or Z).
 struct TcOps {
-    bf16 *a_hi = nullptr, *a_lo = nullptr;
+    int nt = 2;
+    bf16 *a[3] = {nullptr, nullptr, nullptr};
     int64_t lda = 0;
-    bf16 *x_hi = nullptr, *x_lo = nullptr;
+    bf16 *x[3] = {nullptr, nullptr, nullptr};
 };
 
-static int tc_ops_make(rla_ctx *ctx, const float *A, int64_t m, int64_t n, int64_t lda, int64_t l, TcOps &ops,
+static int tc_ops_make(rla_ctx *ctx, const float *A, int64_t m, int64_t n, int64_t lda, int64_t l, int nt, TcOps &ops,
                        Owned &own) {
+    ops.nt = nt;
     ops.lda = ceil_div(m, 8) * 8;
     const size_t na = (size_t)ops.lda * n, nx = (size_t)ceil_div(std::max(m, n), 8) * 8 * l;
     bf16 *buf = nullptr;
-    RLA_CUDA_TRY(ctx, pool_malloc_s(ctx, (void **)&buf, sizeof(bf16) * 2 * (na + nx), ctx->stream));
+    RLA_CUDA_TRY(ctx, pool_malloc_s(ctx, (void **)&buf, sizeof(bf16) * nt * (na + nx), ctx->stream));
     own.ptrs.push_back(buf);
-    ops.a_hi = buf;
-    ops.a_lo = buf + na;
-    ops.x_hi = buf + 2 * na;
-    ops.x_lo = buf + 2 * na + nx;
-    return split_bf16(ctx, A, m, n, lda, ops.a_hi, ops.a_lo, ops.lda);
+    for (int t = 0; t < nt; ++t) {
+        ops.a[t] = buf + t * na;
+        ops.x[t] = buf + nt * na + t * nx;
+    }
+    return nt == 2 ? split_terms_launch<2>(ctx, A, m, n, lda, 0, ops.a, ops.lda)
+                   : split_terms_launch<3>(ctx, A, m, n, lda, 0, ops.a, ops.lda);
 }
 
 // out (rows_out x l) = op(A) * X with X (k x l, ld ldx) FP32; op(A) = A' when at.
@@ -311,9 +315,13 @@ static int tc_apply(rla_ctx *ctx, const TcOps &ops, int at, int64_t m, int64_t n
                     int64_t l, TO *out, int64_t ldo) {
     const int64_t k = at ? m : n, rows_out = at ? n : m;
     const int64_t ldxs = ceil_div(k, 8) * 8;
-    RLA_TRY(split_bf16(ctx, X, k, l, ldx, ops.x_hi, ops.x_lo, ldxs));
-    return tc_gemm_bf16x3<TO>(ctx, rows_out, l, k, ops.a_hi, ops.a_lo, ops.lda, at, ops.x_hi, ops.x_lo, ldxs, out, ldo,
-                              1.0, 0.0, 0);
+    const bf16 *a[3] = {ops.a[0], ops.a[1], ops.a[2]}, *x[3] = {ops.x[0], ops.x[1], ops.x[2]};
+    if (ops.nt == 2) {
+        RLA_TRY(split_terms_launch<2>(ctx, X, k, l, ldx, 0, ops.x, ldxs));
+        return tc_gemm_split<2, TO>(ctx, rows_out, l, k, a, ops.lda, at, x, ldxs, out, ldo, 1.0, 0.0, 0);
+    }
+    RLA_TRY(split_terms_launch<3>(ctx, X, k, l, ldx, 0, ops.x, ldxs));
+    return tc_gemm_split<3, TO>(ctx, rows_out, l, k, a, ops.lda, at, x, ldxs, out, ldo, 1.0, 0.0, 0);
 }
 
 // Q (m x l, ld ldq) <- range of A*Omega after the power iterations.  With `tc` (FP32 data
@@ -392,9 +400,11 @@ static int randsvd_t(rla_ctx *ctx, const rla_sketch *om, int64_t m, int64_t n, c
     RLA_CUDA_TRY(ctx, pool_malloc_s(ctx, (void **)&Q, sizeof(T) * m * l, ctx->stream));
     own.ptrs.push_back(Q);
     TcOps tc;
-    const bool use_tc = pr->precision == RLA_PREC_SPLIT_BF16;
+    // Float32 products with A run on the tensor cores: split BF16 (2 terms) when asked,
+    // otherwise three terms (FP32 accuracy)
+    const bool use_tc = std::is_same<T, float>::value;
     if constexpr (std::is_same<T, float>::value)
-        if (use_tc) RLA_TRY(tc_ops_make(ctx, A, m, n, lda, l, tc, own));
+        RLA_TRY(tc_ops_make(ctx, A, m, n, lda, l, pr->precision == RLA_PREC_SPLIT_BF16 ? 2 : 3, tc, own));
     RLA_TRY(range_core<T>(ctx, om, m, n, A, lda, pr, Q, m, own, use_tc ? &tc : nullptr, false));
     // Bt = A'Q (n x l) in FP64 (randsvd.jl:183-185 forms QA in Float64)
     double *Bt, *X, *J, *sig, *jw;
@@ -449,12 +459,12 @@ int rla_rangefinder(rla_ctx *ctx, const rla_sketch *om, int dtype, int64_t m, in
     int rc;
     if (dtype == RLA_F32) {
         TcOps tc;
-        const bool use_tc = pr->precision == RLA_PREC_SPLIT_BF16;
-        if (use_tc) RLA_TRY(tc_ops_make(ctx, (const float *)A, m, n, lda, om->n_cols, tc, own));
-        rc = range_core<float>(ctx, om, m, n, (const float *)A, lda, pr, (float *)Q, ldq, own, use_tc ? &tc : nullptr);
+        RLA_TRY(tc_ops_make(ctx, (const float *)A, m, n, lda, om->n_cols, pr->precision == RLA_PREC_SPLIT_BF16 ? 2 : 3,
+                            tc, own));
+        rc = range_core<float>(ctx, om, m, n, (const float *)A, lda, pr, (float *)Q, ldq, own, &tc);
         RLA_TRY(rc);
         RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-        return use_tc ? tc_status_check(ctx) : RLA_OK;
+        return tc_status_check(ctx);
     }
     rc = range_core<double>(ctx, om, m, n, (const double *)A, lda, pr, (double *)Q, ldq, own);
     RLA_TRY(rc);

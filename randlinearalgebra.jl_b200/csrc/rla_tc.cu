@@ -1,13 +1,17 @@
 // rla_tc.cu -- split-BF16 GEMM on the 5th-generation tensor cores (tcgen05 + TMEM + TMA).
 //
-// C = alpha * op(A) * B + beta * C for FP32 data whose products must keep about 16
-// mantissa bits: every FP32 operand x is split into hi = bf16(x) and lo = bf16(x - hi) and
-// the product is hi*hi + hi*lo + lo*hi, three tcgen05.mma.kind::f16 per k-step into one
-// FP32 accumulator in tensor memory (lo*lo is below FP32 rounding of the result).
+// C = alpha * op(A) * B + beta * C for FP32 data on BF16 tensor cores.  Every FP32 operand
+// x is split into NT BF16 terms t0 = bf16(x), t1 = bf16(x - t0), t2 = bf16(x - t0 - t1) and
+// the product keeps the term pairs of order below NT, all into one FP32 accumulator in
+// tensor memory (tcgen05.mma.kind::f16):
+//   NT = 2: t0*t0 + t0*t1 + t1*t0 (3 MMAs per k-step, about 16 mantissa bits; the
+//           split-BF16 precision mode of RandSVD);
+//   NT = 3: t0*t0 + t0*t1 + t1*t0 + t0*t2 + t1*t1 + t2*t0 (6 MMAs, about 24 bits: an FP32
+//           product, used for the Gaussian sketch and native-precision Float32 products).
 //
-//   * tile: 128 rows of op(A) x BN <= 288 columns of B per CTA, so a tall A is read from
-//     HBM once per output tile; BK = 32 (64-byte rows, 64-byte swizzle) so that 4 stages
-//     of {A_hi, A_lo, B_hi, B_lo} fit in shared memory;
+//   * tile: 128 rows of op(A) x BN columns of B per CTA (BN <= 288 for NT = 2, <= 160 for
+//     NT = 3), so a tall A is read from HBM once per output tile; BK = 32 (64-byte rows,
+//     64-byte swizzle) so that 4 stages of the NT terms of both operands fit in shared memory;
 //   * op(A) is K-major (A' * X: A column-major, K = rows of A) or MN-major (A * X), both
 //     loaded by TMA and described to the MMA by shared-memory descriptors; B is K-major;
 //   * warp 0 lane 0 issues TMA loads, warp 1 lane 0 issues the MMAs and commits them to
@@ -28,10 +32,23 @@
 namespace rla {
 
 // ------------------------------------------------------------------------------------
-// FP32 -> (hi, lo) BF16 split; element (r, c) of X at X[r + c*ldx], outputs at [r + c*ldo]
+// FP32 -> NT BF16 terms; element (r, c) of X at X[r + c*ldx], outputs at [r + c*ldo]
+// (or, transposed, at [c + r*ldo])
 // ------------------------------------------------------------------------------------
-__global__ void split_bf16_kernel(const float *__restrict__ X, int64_t rows, int64_t cols, int64_t ldx,
-                                  bf16 *__restrict__ hi, bf16 *__restrict__ lo, int64_t ldo, int vec) {
+template <int NT>
+__device__ __forceinline__ void split_terms(float v, bf16 (&t)[NT]) {
+    float rem = v;
+#pragma unroll
+    for (int q = 0; q < NT; ++q) {
+        t[q] = __float2bfloat16_rn(rem);
+        rem -= __bfloat162float(t[q]);
+    }
+}
+
+template <int NT>
+__global__ void split_terms_kernel(const float *__restrict__ X, int64_t rows, int64_t cols, int64_t ldx, bf16 *o0,
+                                   bf16 *o1, bf16 *o2, int64_t ldo, int vec) {
+    bf16 *outs[3] = {o0, o1, o2};
     const int64_t groups = (rows + 7) / 8;
     for (int64_t c = blockIdx.y; c < cols; c += gridDim.y) {
         const float *xc = X + c * ldx;
@@ -47,29 +64,83 @@ __global__ void split_bf16_kernel(const float *__restrict__ X, int64_t rows, int
 #pragma unroll
                 for (int i = 0; i < 8; ++i) v[i] = (r0 + i < rows) ? __ldg(xc + r0 + i) : 0.f;
             }
-            __align__(16) bf16 h[8], l[8];
+            __align__(16) bf16 t[NT][8];
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
-                h[i] = __float2bfloat16_rn(v[i]);
-                l[i] = __float2bfloat16_rn(v[i] - __bfloat162float(h[i]));
+                bf16 ti[NT];
+                split_terms<NT>(v[i], ti);
+#pragma unroll
+                for (int q = 0; q < NT; ++q) t[q][i] = ti[q];
             }
             // ldo is a multiple of 8 and r0 + 8 <= ldo, so whole 16-byte groups are written
-            *reinterpret_cast<uint4 *>(hi + r0 + c * ldo) = *reinterpret_cast<const uint4 *>(h);
-            *reinterpret_cast<uint4 *>(lo + r0 + c * ldo) = *reinterpret_cast<const uint4 *>(l);
+#pragma unroll
+            for (int q = 0; q < NT; ++q)
+                *reinterpret_cast<uint4 *>(outs[q] + r0 + c * ldo) = *reinterpret_cast<const uint4 *>(t[q]);
         }
     }
 }
 
-int split_bf16(rla_ctx *ctx, const float *X, int64_t rows, int64_t cols, int64_t ldx, bf16 *hi, bf16 *lo, int64_t ldo) {
+// Transposed split: output element (c, r) at [c + r*ldo] (rows x cols in, cols x rows out),
+// through 32 x 32 shared-memory tiles so reads and writes are both coalesced.  Output rows
+// cols .. ldo-1 of a 32-row block that reaches them are written as zeros.
+template <int NT>
+__global__ void split_terms_t_kernel(const float *__restrict__ X, int64_t rows, int64_t cols, int64_t ldx, bf16 *o0,
+                                     bf16 *o1, bf16 *o2, int64_t ldo) {
+    __shared__ float tile[32][33];
+    bf16 *outs[3] = {o0, o1, o2};
+    const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+    for (int64_t cb = blockIdx.y; cb * 32 < cols; cb += gridDim.y) {
+        for (int64_t rb = blockIdx.x; rb * 32 < rows; rb += gridDim.x) {
+            const int64_t r0 = rb * 32, c0 = cb * 32;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int64_t r = r0 + tx, c = c0 + ty + 8 * k;
+                tile[ty + 8 * k][tx] = (r < rows && c < cols) ? __ldg(X + r + c * ldx) : 0.f;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                // output column r = r0 + ty + 8k, output row c = c0 + tx
+                const int64_t r = r0 + ty + 8 * k, c = c0 + tx;
+                if (r < rows && c < ldo) {
+                    bf16 t[NT];
+                    split_terms<NT>(c < cols ? tile[tx][ty + 8 * k] : 0.f, t);
+#pragma unroll
+                    for (int q = 0; q < NT; ++q) outs[q][c + r * ldo] = t[q];
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+template <int NT>
+int split_terms_launch(rla_ctx *ctx, const float *X, int64_t rows, int64_t cols, int64_t ldx, int transpose,
+                       bf16 *const *out, int64_t ldo) {
     if (rows <= 0 || cols <= 0) return RLA_OK;
-    if (ldo % 8 != 0 || ldo < rows || ((uintptr_t)hi | (uintptr_t)lo) % 16 != 0)
-        return set_error(ctx, RLA_E_ARG, "split_bf16: output leading dimension must be a multiple of 8");
-    const int vec = (ldx % 4 == 0) && ((uintptr_t)X % 16 == 0);
-    const int64_t groups = (rows + 7) / 8;
-    const unsigned gx = (unsigned)std::min<int64_t>(ceil_div(groups, 256), 4096);
-    const unsigned gy = (unsigned)std::min<int64_t>(cols, 65535);
-    split_bf16_kernel<<<dim3(gx, gy), 256, 0, ctx->stream>>>(X, rows, cols, ldx, hi, lo, ldo, vec);
-    return check_launch(ctx, "split_bf16");
+    const int64_t out_rows = transpose ? cols : rows;
+    uintptr_t al = 0;
+    for (int q = 0; q < NT; ++q) al |= (uintptr_t)out[q];
+    if (ldo % 8 != 0 || ldo < out_rows || al % 16 != 0)
+        return set_error(ctx, RLA_E_ARG, "split: output leading dimension must be a multiple of 8");
+    bf16 *o0 = out[0], *o1 = out[1], *o2 = NT > 2 ? out[2] : nullptr;
+    if (!transpose) {
+        const int vec = (ldx % 4 == 0) && ((uintptr_t)X % 16 == 0);
+        const int64_t groups = (rows + 7) / 8;
+        const unsigned gx = (unsigned)std::min<int64_t>(ceil_div(groups, 256), 4096);
+        const unsigned gy = (unsigned)std::min<int64_t>(cols, 65535);
+        split_terms_kernel<NT><<<dim3(gx, gy), 256, 0, ctx->stream>>>(X, rows, cols, ldx, o0, o1, o2, ldo, vec);
+    } else {
+        const unsigned gx = (unsigned)std::min<int64_t>(ceil_div(rows, 32), 65535);
+        const unsigned gy = (unsigned)std::min<int64_t>(ceil_div(cols, 32), 65535);
+        split_terms_t_kernel<NT><<<dim3(gx, gy), dim3(32, 8), 0, ctx->stream>>>(X, rows, cols, ldx, o0, o1, o2, ldo);
+    }
+    return check_launch(ctx, "split_terms");
+}
+
+int split_bf16(rla_ctx *ctx, const float *X, int64_t rows, int64_t cols, int64_t ldx, bf16 *hi, bf16 *lo, int64_t ldo) {
+    bf16 *out[2] = {hi, lo};
+    return split_terms_launch<2>(ctx, X, rows, cols, ldx, 0, out, ldo);
 }
 
 // ------------------------------------------------------------------------------------
@@ -178,7 +249,21 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int M, int N, int a_mn_major, 
 // GEMM kernel
 // ------------------------------------------------------------------------------------
 constexpr int TC_BM = 128, TC_BK = 32, TC_THREADS = 128;
-constexpr uint32_t TC_A_BYTES = TC_BM * TC_BK * 2;  // 8 KB per operand half
+constexpr uint32_t TC_A_BYTES = TC_BM * TC_BK * 2;  // 8 KB per operand term
+
+// Tensor maps of the NT BF16 terms of both operands.
+template <int NT>
+struct TcMaps {
+    CUtensorMap a[NT], b[NT];
+};
+
+// Term pairs (A term, B term) of the product, largest first.
+__host__ __device__ constexpr int tc_pairs(int NT) { return NT == 2 ? 3 : 6; }
+__device__ __forceinline__ void tc_pair(int i, int &ta, int &tb) {
+    constexpr int PA[6] = {0, 0, 1, 0, 1, 2}, PB[6] = {0, 1, 0, 2, 1, 0};
+    ta = PA[i];
+    tb = PB[i];
+}
 
 struct TcParams {
     int M, N, K;      // op(A) is M x K, B is K x N
@@ -195,15 +280,14 @@ struct TcParams {
     uint64_t wait_ns;  // limit of one pipeline wait
 };
 
-__global__ void __launch_bounds__(TC_THREADS, 1)
-tc_gemm_kernel(const __grid_constant__ CUtensorMap map_ahi, const __grid_constant__ CUtensorMap map_alo,
-               const __grid_constant__ CUtensorMap map_bhi, const __grid_constant__ CUtensorMap map_blo, TcParams p) {
+template <int NT>
+__global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_constant__ TcMaps<NT> maps, TcParams p) {
     extern __shared__ unsigned char smem_raw[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t raw = smem_u32(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;
     const uint32_t b_bytes = (uint32_t)p.BN * TC_BK * 2;
-    const uint32_t stage_bytes = 2 * TC_A_BYTES + 2 * b_bytes;
+    const uint32_t stage_bytes = NT * TC_A_BYTES + NT * b_bytes;
     const uint32_t bar_base = base + (uint32_t)p.stages * stage_bytes;  // full[s], empty[s], done
     auto full_bar = [&](int s) { return bar_base + 8u * (uint32_t)s; };
     auto empty_bar = [&](int s) { return bar_base + 8u * (uint32_t)(p.stages + s); };
@@ -224,10 +308,11 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap map_ahi, const __grid_constan
         }
         mbar_init(done_bar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&map_ahi)) : "memory");
-        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&map_alo)) : "memory");
-        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&map_bhi)) : "memory");
-        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&map_blo)) : "memory");
+#pragma unroll
+        for (int q = 0; q < NT; ++q) {
+            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&maps.a[q])) : "memory");
+            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&maps.b[q])) : "memory");
+        }
     }
     if (warp == 2) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tmem_slot),
@@ -252,23 +337,22 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap map_ahi, const __grid_constan
                 if (!mbar_wait(empty_bar(s), ph ^ 1u, p.status, p.wait_ns)) break;
                 issued = kb + 1;
                 const uint32_t st = base + (uint32_t)s * stage_bytes;
-                const uint32_t a_hi = st, a_lo = st + TC_A_BYTES, b_hi = st + 2 * TC_A_BYTES, b_lo = b_hi + b_bytes;
                 const int k0 = (kb0 + kb) * TC_BK;
                 mbar_arrive_expect_tx(full_bar(s), tx);
-                if (p.a_kmajor) {
-                    tma_load_2d(a_hi, &map_ahi, full_bar(s), k0, m0);
-                    tma_load_2d(a_lo, &map_alo, full_bar(s), k0, m0);
-                } else {
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        tma_load_2d(a_hi + q * 2048u, &map_ahi, full_bar(s), m0 + 32 * q, k0);
-                        tma_load_2d(a_lo + q * 2048u, &map_alo, full_bar(s), m0 + 32 * q, k0);
+                for (int t = 0; t < NT; ++t) {
+                    const uint32_t a_t = st + (uint32_t)t * TC_A_BYTES;
+                    const uint32_t b_t = st + NT * TC_A_BYTES + (uint32_t)t * b_bytes;
+                    if (p.a_kmajor) {
+                        tma_load_2d(a_t, &maps.a[t], full_bar(s), k0, m0);
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) tma_load_2d(a_t + q * 2048u, &maps.a[t], full_bar(s), m0 + 32 * q, k0);
                     }
-                }
-                for (int c = 0; c < p.nch; ++c) {
-                    const uint32_t off = (uint32_t)c * chunk_cols * TC_BK * 2;
-                    tma_load_2d(b_hi + off, &map_bhi, full_bar(s), k0, c * (int)chunk_cols);
-                    tma_load_2d(b_lo + off, &map_blo, full_bar(s), k0, c * (int)chunk_cols);
+                    for (int c = 0; c < p.nch; ++c) {
+                        const uint32_t off = (uint32_t)c * chunk_cols * TC_BK * 2;
+                        tma_load_2d(b_t + off, &maps.b[t], full_bar(s), k0, c * (int)chunk_cols);
+                    }
                 }
             }
             // No copy into this CTA's shared memory may be outstanding when it exits: wait for
@@ -288,25 +372,28 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap map_ahi, const __grid_constan
                 if (!mbar_wait(full_bar(s), ph, p.status, p.wait_ns)) break;
                 tc_fence_after();
                 const uint32_t st = base + (uint32_t)s * stage_bytes;
-                const uint32_t a_hi = st, a_lo = st + TC_A_BYTES, b_hi = st + 2 * TC_A_BYTES, b_lo = b_hi + b_bytes;
 #pragma unroll
                 for (int kk = 0; kk < TC_BK / 16; ++kk) {
-                    uint64_t dah, dal;
-                    if (p.a_kmajor) {  // 128 rows of 64 B, 8-row groups 512 B apart; k-step = 32 B
-                        dah = sdesc_sw64(a_hi + kk * 32u, 16u, 512u);
-                        dal = sdesc_sw64(a_lo + kk * 32u, 16u, 512u);
-                    } else {           // 32-row blocks of 2 KB; k rows 64 B apart; k-step = 16 rows
-                        dah = sdesc_sw64(a_hi + kk * 1024u, 2048u, 512u);
-                        dal = sdesc_sw64(a_lo + kk * 1024u, 2048u, 512u);
+                    uint64_t da[NT];
+#pragma unroll
+                    for (int t = 0; t < NT; ++t) {
+                        const uint32_t a_t = st + (uint32_t)t * TC_A_BYTES;
+                        // K-major: 128 rows of 64 B, 8-row groups 512 B apart; k-step = 32 B.
+                        // MN-major: 32-row blocks of 2 KB; k rows 64 B apart; k-step = 16 rows.
+                        da[t] = p.a_kmajor ? sdesc_sw64(a_t + kk * 32u, 16u, 512u) : sdesc_sw64(a_t + kk * 1024u, 2048u, 512u);
                     }
                     for (int c = 0; c < p.nch; ++c) {
                         const uint32_t off = (uint32_t)c * chunk_cols * TC_BK * 2 + kk * 32u;
-                        const uint64_t dbh = sdesc_sw64(b_hi + off, 16u, 512u);
-                        const uint64_t dbl = sdesc_sw64(b_lo + off, 16u, 512u);
+                        uint64_t db[NT];
+#pragma unroll
+                        for (int t = 0; t < NT; ++t) db[t] = sdesc_sw64(st + NT * TC_A_BYTES + (uint32_t)t * b_bytes + off, 16u, 512u);
                         const uint32_t d = tmem + (uint32_t)c * chunk_cols;
-                        mma_bf16(d, dah, dbh, idesc, (kb | kk) != 0 ? 1u : 0u);
-                        mma_bf16(d, dah, dbl, idesc, 1u);
-                        mma_bf16(d, dal, dbh, idesc, 1u);
+#pragma unroll
+                        for (int i = 0; i < tc_pairs(NT); ++i) {
+                            int ta, tb;
+                            tc_pair(i, ta, tb);
+                            mma_bf16(d, da[ta], db[tb], idesc, (i > 0 || (kb | kk) != 0) ? 1u : 0u);
+                        }
                     }
                 }
                 mma_commit(empty_bar(s));
@@ -414,13 +501,13 @@ int tc_status_check(rla_ctx *ctx) {
     return RLA_OK;
 }
 
-TcPlan tc_plan(const rla_ctx *ctx, int64_t M, int64_t N, int64_t K, int splits) {
+TcPlan tc_plan(const rla_ctx *ctx, int64_t M, int64_t N, int64_t K, int splits, int NT) {
     TcPlan pl;
-    const int64_t nb = std::min<int64_t>(N, 288);
+    const int64_t nb = std::min<int64_t>(N, tc_max_bn(NT));
     pl.BN = (int)(nb <= 256 ? ceil_div(nb, 16) * 16 : ceil_div(nb, 32) * 32);
     pl.nch = pl.BN > 256 ? 2 : 1;
     const int64_t b_bytes = (int64_t)pl.BN * TC_BK * 2;
-    const int64_t stage = 2 * TC_A_BYTES + 2 * b_bytes;
+    const int64_t stage = NT * TC_A_BYTES + NT * b_bytes;
     const int64_t budget = ctx->smem_optin - 1024 - 256;
     pl.stages = (int)std::max<int64_t>(2, std::min<int64_t>(8, budget / stage));
     pl.smem = (size_t)(pl.stages * stage + 1024 + 256);
@@ -431,7 +518,7 @@ TcPlan tc_plan(const rla_ctx *ctx, int64_t M, int64_t N, int64_t K, int splits) 
     pl.nkb = (int)nkb;
     if (splits <= 0) {
         // model: waves x k-blocks per split x MMA time per k-block, plus partial-tile traffic
-        const double t_kb = 0.45e-6 * (double)pl.BN / 288.0, bw = 6.0e12;
+        const double t_kb = 0.15e-6 * tc_pairs(NT) * (double)pl.BN / 288.0, bw = 6.0e12;
         double best = 1e30;
         splits = 1;
         for (int s = 1; s <= std::min<int64_t>(nkb, 64); ++s) {
@@ -450,28 +537,24 @@ TcPlan tc_plan(const rla_ctx *ctx, int64_t M, int64_t N, int64_t K, int splits) 
     return pl;
 }
 
-template <class TC>
-int tc_gemm_bf16x3(rla_ctx *ctx, int64_t M, int64_t N, int64_t K, const bf16 *Ahi, const bf16 *Alo, int64_t lda,
-                   int a_kmajor, const bf16 *Bhi, const bf16 *Blo, int64_t ldb, TC *C, int64_t ldc, double alpha,
-                   double beta, int splits) {
+template <int NT, class TC>
+int tc_gemm_split(rla_ctx *ctx, int64_t M, int64_t N, int64_t K, const bf16 *const *A, int64_t lda, int a_kmajor,
+                  const bf16 *const *B, int64_t ldb, TC *C, int64_t ldc, double alpha, double beta, int splits) {
     if (M <= 0 || N <= 0) return RLA_OK;
     if (M >= (1ll << 31) || K >= (1ll << 31)) return set_error(ctx, RLA_E_UNSUPPORTED, "tensor-core GEMM: dimension above 2^31");
     int *status = nullptr;
     RLA_TRY(tc_status_get(ctx, &status));
-    for (int64_t n0 = 0; n0 < N; n0 += 288) {
-        const int64_t nb = std::min<int64_t>(288, N - n0);
-        TcPlan pl = tc_plan(ctx, M, nb, K, splits);
-        CUtensorMap mah, mal, mbh, mbl;
-        if (a_kmajor) {
-            RLA_TRY(make_map(ctx, &mah, Ahi, K, M, lda, TC_BK, TC_BM));
-            RLA_TRY(make_map(ctx, &mal, Alo, K, M, lda, TC_BK, TC_BM));
-        } else {
-            RLA_TRY(make_map(ctx, &mah, Ahi, M, K, lda, 32, TC_BK));
-            RLA_TRY(make_map(ctx, &mal, Alo, M, K, lda, 32, TC_BK));
-        }
+    const int max_bn = tc_max_bn(NT);
+    for (int64_t n0 = 0; n0 < N; n0 += max_bn) {
+        const int64_t nb = std::min<int64_t>(max_bn, N - n0);
+        TcPlan pl = tc_plan(ctx, M, nb, K, splits, NT);
+        TcMaps<NT> maps;
         const uint32_t box_n = (uint32_t)(pl.BN / pl.nch);
-        RLA_TRY(make_map(ctx, &mbh, Bhi + n0 * ldb, K, nb, ldb, TC_BK, box_n));
-        RLA_TRY(make_map(ctx, &mbl, Blo + n0 * ldb, K, nb, ldb, TC_BK, box_n));
+        for (int t = 0; t < NT; ++t) {
+            if (a_kmajor) RLA_TRY(make_map(ctx, &maps.a[t], A[t], K, M, lda, TC_BK, TC_BM));
+            else RLA_TRY(make_map(ctx, &maps.a[t], A[t], M, K, lda, 32, TC_BK));
+            RLA_TRY(make_map(ctx, &maps.b[t], B[t] + n0 * ldb, K, nb, ldb, TC_BK, box_n));
+        }
         TC *Cn = C + n0 * ldc;
         const bool direct = pl.splits == 1 && std::is_same<TC, float>::value && alpha == 1.0 && beta == 0.0;
         float *out;
@@ -489,14 +572,14 @@ int tc_gemm_bf16x3(rla_ctx *ctx, int64_t M, int64_t N, int64_t K, const bf16 *Ah
         }
         TcParams p{(int)M, (int)nb, (int)K, pl.BN, pl.nch, a_kmajor, pl.nkb, pl.kbps, pl.stages, pl.tmem_cols,
                    out, ldo, sstride, status, ctx->wait_ns};
-        RLA_CUDA_TRY(ctx, set_smem_max(tc_gemm_kernel));
+        RLA_CUDA_TRY(ctx, set_smem_max(tc_gemm_kernel<NT>));
         cudaEvent_t e0 = nullptr, e1 = nullptr;
         if (ctx->timing) {
             RLA_CUDA_TRY(ctx, cudaEventCreate(&e0));
             RLA_CUDA_TRY(ctx, cudaEventCreate(&e1));
             RLA_CUDA_TRY(ctx, cudaEventRecord(e0, ctx->stream));
         }
-        tc_gemm_kernel<<<dim3(pl.mt, pl.splits), TC_THREADS, pl.smem, ctx->stream>>>(mah, mal, mbh, mbl, p);
+        tc_gemm_kernel<NT><<<dim3(pl.mt, pl.splits), TC_THREADS, pl.smem, ctx->stream>>>(maps, p);
         RLA_TRY(check_launch(ctx, "tc_gemm"));
         if (ctx->timing) {
             RLA_CUDA_TRY(ctx, cudaEventRecord(e1, ctx->stream));
@@ -513,10 +596,61 @@ int tc_gemm_bf16x3(rla_ctx *ctx, int64_t M, int64_t N, int64_t K, const bf16 *Ah
     return RLA_OK;
 }
 
+template int split_terms_launch<2>(rla_ctx *, const float *, int64_t, int64_t, int64_t, int, bf16 *const *, int64_t);
+template int split_terms_launch<3>(rla_ctx *, const float *, int64_t, int64_t, int64_t, int, bf16 *const *, int64_t);
+#define RLA_INST_TC(NT, TC)                                                                                          \
+    template int tc_gemm_split<NT, TC>(rla_ctx *, int64_t, int64_t, int64_t, const bf16 *const *, int64_t, int,     \
+                                       const bf16 *const *, int64_t, TC *, int64_t, double, double, int);
+RLA_INST_TC(2, float)
+RLA_INST_TC(2, double)
+RLA_INST_TC(3, float)
+RLA_INST_TC(3, double)
+#undef RLA_INST_TC
+
+template <class TC>
+int tc_gemm_bf16x3(rla_ctx *ctx, int64_t M, int64_t N, int64_t K, const bf16 *Ahi, const bf16 *Alo, int64_t lda,
+                   int a_kmajor, const bf16 *Bhi, const bf16 *Blo, int64_t ldb, TC *C, int64_t ldc, double alpha,
+                   double beta, int splits) {
+    const bf16 *a[2] = {Ahi, Alo}, *b[2] = {Bhi, Blo};
+    return tc_gemm_split<2, TC>(ctx, M, N, K, a, lda, a_kmajor, b, ldb, C, ldc, alpha, beta, splits);
+}
+
 template int tc_gemm_bf16x3<float>(rla_ctx *, int64_t, int64_t, int64_t, const bf16 *, const bf16 *, int64_t, int,
                                    const bf16 *, const bf16 *, int64_t, float *, int64_t, double, double, int);
 template int tc_gemm_bf16x3<double>(rla_ctx *, int64_t, int64_t, int64_t, const bf16 *, const bf16 *, int64_t, int,
                                     const bf16 *, const bf16 *, int64_t, double *, int64_t, double, double, int);
+
+// C (M x N, ld ldc, TC) = alpha * op(A) * op(B) + beta * C for Float32 A and B on the
+// tensor cores with three BF16 terms per operand (an FP32-accurate product).  op(A) may be
+// A or A' (both layouts are read by TMA); op(B) must be K-major for the MMA, so B' (tb = 1)
+// is transposed while it is split.  The split copies come from the context's memory pool.
+template <class TC>
+int gemm_f32_tc(rla_ctx *ctx, int64_t M, int64_t N, int64_t K, const float *A, int64_t lda, int ta, const float *B,
+                int64_t ldb, int tb, TC *C, int64_t ldc, double alpha, double beta) {
+    if (M <= 0 || N <= 0) return RLA_OK;
+    if (K <= 0) return gemm<float, float, TC, double>(ctx, M, N, K, A, lda, ta, B, ldb, tb, C, ldc, alpha, beta);
+    const int64_t a_rows = ta ? K : M, a_cols = ta ? M : K;
+    const int64_t lda2 = ceil_div(a_rows, 8) * 8, ldb2 = ceil_div(K, 8) * 8;
+    const size_t na = (size_t)lda2 * a_cols, nb = (size_t)ldb2 * N;
+    bf16 *buf = nullptr;
+    RLA_CUDA_TRY(ctx, pool_malloc_s(ctx, (void **)&buf, sizeof(bf16) * 3 * (na + nb) + 256, ctx->stream));
+    bf16 *a3[3] = {buf, buf + na, buf + 2 * na};
+    bf16 *b3[3] = {buf + 3 * na, buf + 3 * na + nb, buf + 3 * na + 2 * nb};
+    int rc = split_terms_launch<3>(ctx, A, a_rows, a_cols, lda, 0, a3, lda2);
+    if (rc == RLA_OK) rc = tb ? split_terms_launch<3>(ctx, B, N, K, ldb, 1, b3, ldb2)
+                              : split_terms_launch<3>(ctx, B, K, N, ldb, 0, b3, ldb2);
+    if (rc == RLA_OK) {
+        const bf16 *ac[3] = {a3[0], a3[1], a3[2]}, *bc[3] = {b3[0], b3[1], b3[2]};
+        rc = tc_gemm_split<3, TC>(ctx, M, N, K, ac, lda2, ta, bc, ldb2, C, ldc, alpha, beta, 0);
+    }
+    cudaFreeAsync(buf, ctx->stream);
+    return rc;
+}
+
+template int gemm_f32_tc<float>(rla_ctx *, int64_t, int64_t, int64_t, const float *, int64_t, int, const float *,
+                                int64_t, int, float *, int64_t, double, double);
+template int gemm_f32_tc<double>(rla_ctx *, int64_t, int64_t, int64_t, const float *, int64_t, int, const float *,
+                                 int64_t, int, double *, int64_t, double, double);
 
 }  // namespace rla
 
