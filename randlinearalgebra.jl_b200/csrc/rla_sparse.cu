@@ -561,16 +561,17 @@ __global__ void __launch_bounds__(32) cs_compress_kernel(CompressContigParams<T>
     }
 }
 
-// ---- CountSketch, column groups: G = 16 / sizeof(T) columns per warp ------------------
-// The bucket of row j is the same for every column, so a warp takes G columns (4 Float32
-// or 2 Float64) at once and keeps its bins as 16-byte slots [slot][G]: one random
-// shared-memory read-modify-write then adds G values.  A random 16-byte warp access costs
-// about 10.4 wavefronts for 128 values where a random 4-byte one costs 3.5 for 32, and the
-// schedule word of a row is read once for G columns.  The schedule words are those of the
-// one-column kernel (cs_sched_kernel): their byte offsets are in units of sizeof(T) and are
-// scaled by G here.  Batches are 512 rows; lane holds rows tb*128 + 4*lane + t (t < 4) of
-// tile tb in element tb*4 + t.  The batch after next is prefetched into L2 with a bulk
-// prefetch while the next one is loaded into registers.
+// ---- CountSketch, column groups: G columns per warp ---------------------------------------
+// The bucket of row j is the same for every column, so a warp takes G columns at once
+// (G * sizeof(T) = 8 or 16 bytes) and keeps its bins as slots [slot][G]: one random
+// shared-memory read-modify-write then adds G values, and the schedule word of a row is
+// read once for G columns.  A random 16-byte warp access costs about 10.4 wavefronts for
+// 128 values and a random 8-byte one about 6.2 for 64, where a random 4-byte one costs 3.5
+// for 32; wider slots also mean larger bins and fewer warps per SM.  The schedule words are
+// those of the one-column kernel (cs_sched_kernel): their byte offsets are in units of
+// sizeof(T) and are scaled by G here.  Batches are 512 rows; lane holds rows tb*128 +
+// 4*lane + t (t < 4) of tile tb in element tb*4 + t.  The batch after next is prefetched
+// into L2 with a bulk prefetch while the next half batch is loaded into registers.
 template <class T>
 struct CsGroupParams {
     const T *X;
@@ -590,11 +591,19 @@ struct CsGroupParams {
     Split split;
 };
 
-template <class T>
-struct alignas(16) Vec16 {
-    static constexpr int G = 16 / (int)sizeof(T);
+template <class T, int G>
+struct alignas(G * sizeof(T)) VecG {
     T v[G];
 };
+
+// Bypass-L1 load of one slot (8 or 16 bytes) written by another warp.
+template <class V>
+__device__ __forceinline__ V ldcg_slot(const V *p) {
+    V x;
+    if constexpr (sizeof(V) == 16) *reinterpret_cast<float4 *>(&x) = __ldcg(reinterpret_cast<const float4 *>(p));
+    else *reinterpret_cast<float2 *>(&x) = __ldcg(reinterpret_cast<const float2 *>(p));
+    return x;
+}
 
 template <class T>
 __device__ __forceinline__ T sign_one(uint32_t w) {
@@ -606,12 +615,10 @@ __device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes) {
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
 
-constexpr int CS_GROUP_RMW = 4;  // read-modify-writes of a half batch issued back to back
-
-// Half H of a 512-row batch (tiles 2H and 2H+1): 8 rows per lane, G columns each.
-template <class T, bool CHECK>
+// Half H of a 512-row batch (tiles 2H and 2H+1): 8 rows per lane, G columns each.  RMW of
+// its read-modify-writes are issued back to back (reads first).
+template <class T, int G, int RMW, bool CHECK>
 struct CsGroupHalf {
-    static constexpr int G = 16 / (int)sizeof(T);
     T val[8][G];
     uint32_t mw[8];
     __device__ __forceinline__ void load(const CsGroupParams<T> &p, const T *xg, int64_t bt, int H, int lane,
@@ -649,18 +656,18 @@ struct CsGroupHalf {
     // Main sub-rounds of a batch that is not SLOW: every non-deferred target of a batch is
     // distinct (deferred rows own list entries), so reads and writes are issued in groups.
     __device__ __forceinline__ void run(unsigned char *sm) {
-        using V = Vec16<T>;
+        using V = VecG<T, G>;
 #pragma unroll
-        for (int h = 0; h < 8; h += CS_GROUP_RMW) {
-            V old[CS_GROUP_RMW];
-            uint32_t o[CS_GROUP_RMW];
+        for (int h = 0; h < 8; h += RMW) {
+            V old[RMW];
+            uint32_t o[RMW];
 #pragma unroll
-            for (int i = 0; i < CS_GROUP_RMW; ++i) {
+            for (int i = 0; i < RMW; ++i) {
                 o[i] = (mw[h + i] & CS_OFF_MASK) * G;
                 old[i] = *reinterpret_cast<const V *>(sm + o[i]);
             }
 #pragma unroll
-            for (int i = 0; i < CS_GROUP_RMW; ++i) {
+            for (int i = 0; i < RMW; ++i) {
                 const T sg = sign_one<T>(mw[h + i]);
 #pragma unroll
                 for (int c = 0; c < G; ++c) old[i].v[c] = fma(sg, val[h + i][c], old[i].v[c]);
@@ -687,16 +694,15 @@ struct CsGroupExtra {
         xb0 = __ldg(extra + bt * 64 + lane);
         xb1 = __ldg(extra + bt * 64 + 32 + lane);
     }
-    template <class T>
+    template <class T, int G>
     __device__ __forceinline__ void run(unsigned char *sm, uint32_t list_off, int lane) const {
-        using V = Vec16<T>;
-        constexpr int G = V::G;
+        using V = VecG<T, G>;
         __syncwarp();
         if (fl == 0u || (fl & TILE_SLOW)) return;
 #pragma unroll
         for (int r = 0; r < 2; ++r) {
             if (r == 1 && fl < 2u) break;
-            V *e = reinterpret_cast<V *>(sm + list_off + (r * 32 + lane) * 16);
+            V *e = reinterpret_cast<V *>(sm + list_off + (r * 32 + lane) * sizeof(V));
             V *t = reinterpret_cast<V *>(sm + ((r ? xb1 : xb0) & CS_OFF_MASK) * G);
             V a = *t;
             const V x = *e;
@@ -712,10 +718,9 @@ struct CsGroupExtra {
 // Finish this warp's share of column group v (bins [s][G]): write it when the warp covered
 // the whole group, else store the partial bins; the last warp to arrive adds all partials
 // in warp order (deterministic).
-template <class T>
+template <class T, int G>
 __device__ void flush_group(const CsGroupParams<T> &p, unsigned char *sm, int g, int64_t v, bool exclusive, int lane) {
-    using V = Vec16<T>;
-    constexpr int G = V::G;
+    using V = VecG<T, G>;
     __syncwarp();
     V *bv = reinterpret_cast<V *>(sm);
     const int64_t s = p.s;
@@ -754,13 +759,10 @@ __device__ void flush_group(const CsGroupParams<T> &p, unsigned char *sm, int g,
         __threadfence();
         const V *p0 = reinterpret_cast<const V *>(p.partials) + (int64_t)p.split.slot(gf, vbeg) * s;
         for (int64_t i = lane; i < s; i += 32) {
-            V acc;
-            *reinterpret_cast<float4 *>(&acc) = __ldcg(reinterpret_cast<const float4 *>(p0 + i));
+            V acc = ldcg_slot(p0 + i);
 #pragma unroll 4
             for (int gg = gf + 1; gg <= gl; ++gg) {
-                V x;
-                *reinterpret_cast<float4 *>(&x) =
-                    __ldcg(reinterpret_cast<const float4 *>(reinterpret_cast<const V *>(p.partials) + (int64_t)(2 * gg) * s + i));
+                const V x = ldcg_slot(reinterpret_cast<const V *>(p.partials) + (int64_t)(2 * gg) * s + i);
 #pragma unroll
                 for (int c = 0; c < G; ++c) acc.v[c] += x.v[c];
             }
@@ -771,21 +773,21 @@ __device__ void flush_group(const CsGroupParams<T> &p, unsigned char *sm, int g,
     __syncwarp();
 }
 
-template <class T>
+template <class T, int G, int RMW>
 __global__ void __launch_bounds__(32) cs_group_kernel(CsGroupParams<T> p) {
-    constexpr int G = 16 / (int)sizeof(T);
+    using V = VecG<T, G>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x;
     const int g = blockIdx.x;
     {
-        float4 *z = reinterpret_cast<float4 *>(smem_raw);
-        for (int64_t i = lane; i < p.s + 96; i += 32) z[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        V *z = reinterpret_cast<V *>(smem_raw);
+        for (int64_t i = lane; i < p.s + 96; i += 32) z[i] = V{};
     }
     __syncwarp();
     if (g >= p.split.W) return;
     const int64_t u0 = p.split.start(g), u1 = p.split.start(g + 1);
     if (u0 >= u1) return;
-    const uint32_t list_off = (uint32_t)(p.s * 16);
+    const uint32_t list_off = (uint32_t)(p.s * sizeof(V));
     // a padding row's word: the lane's dummy slot (offsets in units of sizeof(T))
     const uint32_t pad = (uint32_t)((p.s + 64 + lane) * (int64_t)sizeof(T));
     const int64_t full = p.L / 512;
@@ -808,7 +810,7 @@ __global__ void __launch_bounds__(32) cs_group_kernel(CsGroupParams<T> p) {
         pf(k + 1);
         if (k < kfull) {
             // software pipeline over half batches: one half is loaded while the other runs
-            CsGroupHalf<T, false> h0, h1;
+            CsGroupHalf<T, G, RMW, false> h0, h1;
             CsGroupExtra ex, exn;
             h0.load(p, xg, k, 0, lane, pad);
             ex.load(p.tile_flags, p.extra, k, lane);
@@ -825,7 +827,7 @@ __global__ void __launch_bounds__(32) cs_group_kernel(CsGroupParams<T> p) {
                 }
                 if (slow) h1.resolve(smem_raw, lane);
                 else h1.run(smem_raw);
-                ex.template run<T>(smem_raw, list_off, lane);
+                ex.template run<T, G>(smem_raw, list_off, lane);
                 ++k;
                 if (!more) break;
                 ex = exn;
@@ -836,19 +838,26 @@ __global__ void __launch_bounds__(32) cs_group_kernel(CsGroupParams<T> p) {
             ec.load(p.tile_flags, p.extra, k, lane);
 #pragma unroll 1
             for (int H = 0; H < 2; ++H) {
-                CsGroupHalf<T, true> hc;
+                CsGroupHalf<T, G, RMW, true> hc;
                 hc.load(p, xg, k, H, lane, pad);
                 if (ec.fl & TILE_SLOW) hc.resolve(smem_raw, lane);
                 else hc.run(smem_raw);
             }
-            ec.template run<T>(smem_raw, list_off, lane);
+            ec.template run<T, G>(smem_raw, list_off, lane);
         }
         const bool exclusive = (u0 <= vbeg) && (vbeg + p.tpv <= u1);
-        flush_group(p, smem_raw, g, v, exclusive, lane);
+        flush_group<T, G>(p, smem_raw, g, v, exclusive, lane);
         u = vbeg + kend;
         ++v;
     }
 }
+
+// Columns per warp and read-modify-writes in flight of the column-group kernel.
+template <class T>
+struct CsGroupCfg {
+    static constexpr int G = sizeof(T) == 4 ? 4 : 2;
+    static constexpr int RMW = 8;
+};
 
 // ---- strided-vector compress: element (k, v) at X[v + k*x_ld]; lane = vector ----------
 template <class T>
@@ -993,25 +1002,27 @@ int sparse_compress(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_t x_es
         const int64_t total = tpv * nv;
         const bool vec = (x_vs % (16 / es) == 0) && ((uintptr_t)X % 16 == 0);
         if (bm) {
-            // column groups of 16 bytes (4 Float32 / 2 Float64 columns per warp) when the
-            // vectors are 16-byte aligned and the [s + 96][G] bins fit one CTA
-            constexpr int G = 16 / (int)sizeof(T);
+            // column groups (G columns per warp) when the vectors are 16-byte aligned and the
+            // [s + 96][G] bins fit one CTA
+            constexpr int G = CsGroupCfg<T>::G, RMW = CsGroupCfg<T>::RMW;
             const int64_t ng = nv / G;
-            if (vec && ng > 0 && (s + 96) * 16 <= (int64_t)cap) {
-                const size_t smem = (size_t)(s + 96) * 16;
-                RLA_CUDA_TRY(ctx, set_smem_max(cs_group_kernel<T>));
+            const int64_t slot = G * (int64_t)sizeof(T);
+            if (vec && ng > 0 && (s + 96) * slot <= (int64_t)cap) {
+                const size_t smem = (size_t)((s + 96) * slot);
+                auto kern = cs_group_kernel<T, G, RMW>;
+                RLA_CUDA_TRY(ctx, set_smem_max(kern));
                 int per_sm = 1;
-                RLA_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cs_group_kernel<T>, 32, smem));
+                RLA_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32, smem));
                 const int64_t tpg = ceil_div(L, 512), tot = tpg * ng;
                 int64_t W = (int64_t)ctx->sm_count * std::max(per_sm, 1);
                 W = std::max<int64_t>(1, std::min<int64_t>(W, ceil_div(tot, 8)));
                 void *part = nullptr;
                 int *cnt = nullptr;
-                RLA_TRY(scratch_get(ctx, (size_t)(2 * W) * (size_t)s * 16, &part));
+                RLA_TRY(scratch_get(ctx, (size_t)(2 * W) * (size_t)(s * slot), &part));
                 RLA_TRY(counters_get(ctx, (size_t)ng, &cnt));
                 CsGroupParams<T> gp{X, x_vs, L, ng, sk->meta, sk->tile_flags, sk->extra, s, Y, y_es, y_vs, a, (T)beta,
                                     beta_zero, (T *)part, cnt, tpg, Split::make(tot, (int)W)};
-                cs_group_kernel<T><<<(int)W, 32, smem, ctx->stream>>>(gp);
+                kern<<<(int)W, 32, smem, ctx->stream>>>(gp);
                 RLA_TRY(check_launch(ctx, "cs_group"));
                 if (ng * G == nv) return RLA_OK;
                 // the remaining nv % G vectors go through the one-column kernel below
