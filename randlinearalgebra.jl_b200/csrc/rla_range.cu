@@ -283,9 +283,8 @@ struct Owned {
 };
 
 // Operands of the tensor-core products with A (Float32 data): A split once into NT BF16
-// terms (NT = 2 for RLA_PREC_SPLIT_BF16, about 16 bits; NT = 3 for RLA_PREC_NATIVE, an
-// FP32-accurate product); one buffer set reused for the terms of the thin factor of each
-// product (Omega, Q or Z).
+// terms (NT = 2 for RLA_PREC_SPLIT_BF16, about 16 bits); one buffer set reused for the terms
+// of the thin factor of each product (Omega, Q or Z).
 struct TcOps {
     int nt = 2;
     bf16 *a[3] = {nullptr, nullptr, nullptr};
@@ -400,11 +399,9 @@ static int randsvd_t(rla_ctx *ctx, const rla_sketch *om, int64_t m, int64_t n, c
     RLA_CUDA_TRY(ctx, pool_malloc_s(ctx, (void **)&Q, sizeof(T) * m * l, ctx->stream));
     own.ptrs.push_back(Q);
     TcOps tc;
-    // Float32 products with A run on the tensor cores: split BF16 (2 terms) when asked,
-    // otherwise three terms (FP32 accuracy)
-    const bool use_tc = std::is_same<T, float>::value;
+    const bool use_tc = pr->precision == RLA_PREC_SPLIT_BF16;
     if constexpr (std::is_same<T, float>::value)
-        RLA_TRY(tc_ops_make(ctx, A, m, n, lda, l, pr->precision == RLA_PREC_SPLIT_BF16 ? 2 : 3, tc, own));
+        if (use_tc) RLA_TRY(tc_ops_make(ctx, A, m, n, lda, l, 2, tc, own));
     RLA_TRY(range_core<T>(ctx, om, m, n, A, lda, pr, Q, m, own, use_tc ? &tc : nullptr, false));
     // Bt = A'Q (n x l) in FP64 (randsvd.jl:183-185 forms QA in Float64)
     double *Bt, *X, *J, *sig, *jw;
@@ -459,12 +456,12 @@ int rla_rangefinder(rla_ctx *ctx, const rla_sketch *om, int dtype, int64_t m, in
     int rc;
     if (dtype == RLA_F32) {
         TcOps tc;
-        RLA_TRY(tc_ops_make(ctx, (const float *)A, m, n, lda, om->n_cols, pr->precision == RLA_PREC_SPLIT_BF16 ? 2 : 3,
-                            tc, own));
-        rc = range_core<float>(ctx, om, m, n, (const float *)A, lda, pr, (float *)Q, ldq, own, &tc);
+        const bool use_tc = pr->precision == RLA_PREC_SPLIT_BF16;
+        if (use_tc) RLA_TRY(tc_ops_make(ctx, (const float *)A, m, n, lda, om->n_cols, 2, tc, own));
+        rc = range_core<float>(ctx, om, m, n, (const float *)A, lda, pr, (float *)Q, ldq, own, use_tc ? &tc : nullptr);
         RLA_TRY(rc);
         RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-        return tc_status_check(ctx);
+        return use_tc ? tc_status_check(ctx) : RLA_OK;
     }
     rc = range_core<double>(ctx, om, m, n, (const double *)A, lda, pr, (double *)Q, ldq, own);
     RLA_TRY(rc);

@@ -561,304 +561,6 @@ __global__ void __launch_bounds__(32) cs_compress_kernel(CompressContigParams<T>
     }
 }
 
-// ---- CountSketch, column groups: G columns per warp ---------------------------------------
-// The bucket of row j is the same for every column, so a warp takes G columns at once
-// (G * sizeof(T) = 8 or 16 bytes) and keeps its bins as slots [slot][G]: one random
-// shared-memory read-modify-write then adds G values, and the schedule word of a row is
-// read once for G columns.  A random 16-byte warp access costs about 10.4 wavefronts for
-// 128 values and a random 8-byte one about 6.2 for 64, where a random 4-byte one costs 3.5
-// for 32; wider slots also mean larger bins and fewer warps per SM.  The schedule words are
-// those of the one-column kernel (cs_sched_kernel): their byte offsets are in units of
-// sizeof(T) and are scaled by G here.  Batches are 512 rows; lane holds rows tb*128 +
-// 4*lane + t (t < 4) of tile tb in element tb*4 + t.  The batch after next is prefetched
-// into L2 with a bulk prefetch while the next half batch is loaded into registers.
-template <class T>
-struct CsGroupParams {
-    const T *X;
-    int64_t x_ld;
-    int64_t L, ngroups;
-    const uint32_t *meta;
-    const uint32_t *tile_flags;
-    const uint32_t *extra;
-    int64_t s;
-    T *Y;
-    int64_t y_es, y_vs;
-    T alpha, beta;
-    int beta_zero;
-    T *partials;
-    int *counters;
-    int64_t tpv;  // 512-row batches per column group
-    Split split;
-};
-
-template <class T, int G>
-struct alignas(G * sizeof(T)) VecG {
-    T v[G];
-};
-
-// Bypass-L1 load of one slot (8 or 16 bytes) written by another warp.
-template <class V>
-__device__ __forceinline__ V ldcg_slot(const V *p) {
-    V x;
-    if constexpr (sizeof(V) == 16) *reinterpret_cast<float4 *>(&x) = __ldcg(reinterpret_cast<const float4 *>(p));
-    else *reinterpret_cast<float2 *>(&x) = __ldcg(reinterpret_cast<const float2 *>(p));
-    return x;
-}
-
-template <class T>
-__device__ __forceinline__ T sign_one(uint32_t w) {
-    if constexpr (sizeof(T) == 4) return __uint_as_float((w & 0x80000000u) | 0x3f800000u);
-    else return __longlong_as_double((long long)(((uint64_t)(w & 0x80000000u) << 32) | 0x3ff0000000000000ull));
-}
-
-__device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes) {
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
-}
-
-// Half H of a 512-row batch (tiles 2H and 2H+1): 8 rows per lane, G columns each.  RMW of
-// its read-modify-writes are issued back to back (reads first).
-template <class T, int G, int RMW, bool CHECK>
-struct CsGroupHalf {
-    T val[8][G];
-    uint32_t mw[8];
-    __device__ __forceinline__ void load(const CsGroupParams<T> &p, const T *xg, int64_t bt, int H, int lane,
-                                         uint32_t pad) {
-        if constexpr (!CHECK) {
-#pragma unroll
-            for (int tt = 0; tt < 2; ++tt) {
-                const int64_t r0 = bt * 512 + (2 * H + tt) * 128 + lane * 4;
-#pragma unroll
-                for (int c = 0; c < G; ++c) {
-                    const T *xb = xg + c * p.x_ld + r0;
-                    if constexpr (sizeof(T) == 4) {
-                        const float4 q = __ldg(reinterpret_cast<const float4 *>(xb));
-                        val[tt * 4][c] = q.x; val[tt * 4 + 1][c] = q.y; val[tt * 4 + 2][c] = q.z; val[tt * 4 + 3][c] = q.w;
-                    } else {
-                        const double2 a = __ldg(reinterpret_cast<const double2 *>(xb));
-                        const double2 b = __ldg(reinterpret_cast<const double2 *>(xb + 2));
-                        val[tt * 4][c] = a.x; val[tt * 4 + 1][c] = a.y; val[tt * 4 + 2][c] = b.x; val[tt * 4 + 3][c] = b.y;
-                    }
-                }
-                const uint4 m = __ldg(reinterpret_cast<const uint4 *>(p.meta + r0));
-                mw[tt * 4] = m.x; mw[tt * 4 + 1] = m.y; mw[tt * 4 + 2] = m.z; mw[tt * 4 + 3] = m.w;
-            }
-        } else {
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                const int64_t j = bt * 512 + (2 * H + (i >> 2)) * 128 + lane * 4 + (i & 3);
-                const bool ok = j < p.L;
-#pragma unroll
-                for (int c = 0; c < G; ++c) val[i][c] = ok ? __ldg(xg + c * p.x_ld + j) : T(0);
-                mw[i] = ok ? __ldg(p.meta + j) : pad;
-            }
-        }
-    }
-    // Main sub-rounds of a batch that is not SLOW: every non-deferred target of a batch is
-    // distinct (deferred rows own list entries), so reads and writes are issued in groups.
-    __device__ __forceinline__ void run(unsigned char *sm) {
-        using V = VecG<T, G>;
-#pragma unroll
-        for (int h = 0; h < 8; h += RMW) {
-            V old[RMW];
-            uint32_t o[RMW];
-#pragma unroll
-            for (int i = 0; i < RMW; ++i) {
-                o[i] = (mw[h + i] & CS_OFF_MASK) * G;
-                old[i] = *reinterpret_cast<const V *>(sm + o[i]);
-            }
-#pragma unroll
-            for (int i = 0; i < RMW; ++i) {
-                const T sg = sign_one<T>(mw[h + i]);
-#pragma unroll
-                for (int c = 0; c < G; ++c) old[i].v[c] = fma(sg, val[h + i][c], old[i].v[c]);
-                *reinterpret_cast<V *>(sm + o[i]) = old[i];
-            }
-        }
-    }
-    // A SLOW batch: lanes sharing a target are summed in lane order at run time.
-    __device__ __forceinline__ void resolve(unsigned char *sm, int lane) {
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const uint32_t o = (mw[i] & CS_OFF_MASK) * G;
-#pragma unroll
-            for (int c = 0; c < G; ++c) cs_resolve<T>(sm, apply_sign(val[i][c], mw[i]), o + c * sizeof(T), lane);
-        }
-    }
-};
-
-// Extra-round words of a batch: flag (round count or TILE_SLOW) and two list targets.
-struct CsGroupExtra {
-    uint32_t fl, xb0, xb1;
-    __device__ __forceinline__ void load(const uint32_t *flags, const uint32_t *extra, int64_t bt, int lane) {
-        fl = __ldg(flags + bt);
-        xb0 = __ldg(extra + bt * 64 + lane);
-        xb1 = __ldg(extra + bt * 64 + 32 + lane);
-    }
-    template <class T, int G>
-    __device__ __forceinline__ void run(unsigned char *sm, uint32_t list_off, int lane) const {
-        using V = VecG<T, G>;
-        __syncwarp();
-        if (fl == 0u || (fl & TILE_SLOW)) return;
-#pragma unroll
-        for (int r = 0; r < 2; ++r) {
-            if (r == 1 && fl < 2u) break;
-            V *e = reinterpret_cast<V *>(sm + list_off + (r * 32 + lane) * sizeof(V));
-            V *t = reinterpret_cast<V *>(sm + ((r ? xb1 : xb0) & CS_OFF_MASK) * G);
-            V a = *t;
-            const V x = *e;
-#pragma unroll
-            for (int c = 0; c < G; ++c) a.v[c] += x.v[c];
-            *t = a;
-            *e = V{};
-            __syncwarp();
-        }
-    }
-};
-
-// Finish this warp's share of column group v (bins [s][G]): write it when the warp covered
-// the whole group, else store the partial bins; the last warp to arrive adds all partials
-// in warp order (deterministic).
-template <class T, int G>
-__device__ void flush_group(const CsGroupParams<T> &p, unsigned char *sm, int g, int64_t v, bool exclusive, int lane) {
-    using V = VecG<T, G>;
-    __syncwarp();
-    V *bv = reinterpret_cast<V *>(sm);
-    const int64_t s = p.s;
-    T *y0 = p.Y + v * G * p.y_vs;
-    auto out = [&](int64_t i, const V &acc) {
-#pragma unroll
-        for (int c = 0; c < G; ++c) {
-            T *yp = y0 + i * p.y_es + c * p.y_vs;
-            T r = p.alpha * acc.v[c];
-            if (!p.beta_zero) r += p.beta * *yp;
-            *yp = r;
-        }
-    };
-    if (exclusive) {
-        for (int64_t i = lane; i < s; i += 32) {
-            const V b = bv[i];
-            bv[i] = V{};
-            out(i, b);
-        }
-        __syncwarp();
-        return;
-    }
-    const int64_t vbeg = v * p.tpv;
-    V *part = reinterpret_cast<V *>(p.partials) + (int64_t)p.split.slot(g, vbeg) * s;
-    for (int64_t i = lane; i < s; i += 32) {
-        part[i] = bv[i];
-        bv[i] = V{};
-    }
-    __threadfence();
-    __syncwarp();
-    const int gf = p.split.owner(vbeg), gl = p.split.owner(vbeg + p.tpv - 1);
-    int old = 0;
-    if (lane == 0) old = atomicAdd(&p.counters[v], 1);
-    old = __shfl_sync(FULL, old, 0);
-    if (old == gl - gf) {
-        __threadfence();
-        const V *p0 = reinterpret_cast<const V *>(p.partials) + (int64_t)p.split.slot(gf, vbeg) * s;
-        for (int64_t i = lane; i < s; i += 32) {
-            V acc = ldcg_slot(p0 + i);
-#pragma unroll 4
-            for (int gg = gf + 1; gg <= gl; ++gg) {
-                const V x = ldcg_slot(reinterpret_cast<const V *>(p.partials) + (int64_t)(2 * gg) * s + i);
-#pragma unroll
-                for (int c = 0; c < G; ++c) acc.v[c] += x.v[c];
-            }
-            out(i, acc);
-        }
-        if (lane == 0) p.counters[v] = 0;
-    }
-    __syncwarp();
-}
-
-template <class T, int G, int RMW>
-__global__ void __launch_bounds__(32) cs_group_kernel(CsGroupParams<T> p) {
-    using V = VecG<T, G>;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int lane = threadIdx.x;
-    const int g = blockIdx.x;
-    {
-        V *z = reinterpret_cast<V *>(smem_raw);
-        for (int64_t i = lane; i < p.s + 96; i += 32) z[i] = V{};
-    }
-    __syncwarp();
-    if (g >= p.split.W) return;
-    const int64_t u0 = p.split.start(g), u1 = p.split.start(g + 1);
-    if (u0 >= u1) return;
-    const uint32_t list_off = (uint32_t)(p.s * sizeof(V));
-    // a padding row's word: the lane's dummy slot (offsets in units of sizeof(T))
-    const uint32_t pad = (uint32_t)((p.s + 64 + lane) * (int64_t)sizeof(T));
-    const int64_t full = p.L / 512;
-    int64_t v = u0 / p.tpv;
-    int64_t u = u0;
-    while (u < u1) {
-        const int64_t vbeg = v * p.tpv;
-        const int64_t kend = min(u1, vbeg + p.tpv) - vbeg;
-        const T *xg = p.X + v * G * p.x_ld;
-        int64_t k = u - vbeg;
-        const int64_t kfull = min(kend, full);
-        // L2 prefetch two batches ahead: lane c < G takes column c, lane G the words
-        auto pf = [&](int64_t kb) {
-            if (kb < kfull) {
-                if (lane < G) prefetch_l2(xg + lane * p.x_ld + kb * 512, 512 * sizeof(T));
-                else if (lane == G) prefetch_l2(p.meta + kb * 512, 2048);
-            }
-        };
-        pf(k);
-        pf(k + 1);
-        if (k < kfull) {
-            // software pipeline over half batches: one half is loaded while the other runs
-            CsGroupHalf<T, G, RMW, false> h0, h1;
-            CsGroupExtra ex, exn;
-            h0.load(p, xg, k, 0, lane, pad);
-            ex.load(p.tile_flags, p.extra, k, lane);
-            while (true) {
-                pf(k + 2);
-                h1.load(p, xg, k, 1, lane, pad);
-                const bool slow = (ex.fl & TILE_SLOW) != 0u;
-                if (slow) h0.resolve(smem_raw, lane);
-                else h0.run(smem_raw);
-                const bool more = k + 1 < kfull;
-                if (more) {
-                    h0.load(p, xg, k + 1, 0, lane, pad);
-                    exn.load(p.tile_flags, p.extra, k + 1, lane);
-                }
-                if (slow) h1.resolve(smem_raw, lane);
-                else h1.run(smem_raw);
-                ex.template run<T, G>(smem_raw, list_off, lane);
-                ++k;
-                if (!more) break;
-                ex = exn;
-            }
-        }
-        for (; k < kend; ++k) {
-            CsGroupExtra ec;
-            ec.load(p.tile_flags, p.extra, k, lane);
-#pragma unroll 1
-            for (int H = 0; H < 2; ++H) {
-                CsGroupHalf<T, G, RMW, true> hc;
-                hc.load(p, xg, k, H, lane, pad);
-                if (ec.fl & TILE_SLOW) hc.resolve(smem_raw, lane);
-                else hc.run(smem_raw);
-            }
-            ec.template run<T, G>(smem_raw, list_off, lane);
-        }
-        const bool exclusive = (u0 <= vbeg) && (vbeg + p.tpv <= u1);
-        flush_group<T, G>(p, smem_raw, g, v, exclusive, lane);
-        u = vbeg + kend;
-        ++v;
-    }
-}
-
-// Columns per warp and read-modify-writes in flight of the column-group kernel.
-template <class T>
-struct CsGroupCfg {
-    static constexpr int G = sizeof(T) == 4 ? 4 : 2;
-    static constexpr int RMW = 8;
-};
-
 // ---- strided-vector compress: element (k, v) at X[v + k*x_ld]; lane = vector ----------
 template <class T>
 struct CompressStridedParams {
@@ -1002,34 +704,6 @@ int sparse_compress(rla_ctx *ctx, const rla_sketch *sk, const T *X, int64_t x_es
         const int64_t total = tpv * nv;
         const bool vec = (x_vs % (16 / es) == 0) && ((uintptr_t)X % 16 == 0);
         if (bm) {
-            // column groups (G columns per warp) when the vectors are 16-byte aligned and the
-            // [s + 96][G] bins fit one CTA
-            constexpr int G = CsGroupCfg<T>::G, RMW = CsGroupCfg<T>::RMW;
-            const int64_t ng = nv / G;
-            const int64_t slot = G * (int64_t)sizeof(T);
-            if (vec && ng > 0 && (s + 96) * slot <= (int64_t)cap) {
-                const size_t smem = (size_t)((s + 96) * slot);
-                auto kern = cs_group_kernel<T, G, RMW>;
-                RLA_CUDA_TRY(ctx, set_smem_max(kern));
-                int per_sm = 1;
-                RLA_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32, smem));
-                const int64_t tpg = ceil_div(L, 512), tot = tpg * ng;
-                int64_t W = (int64_t)ctx->sm_count * std::max(per_sm, 1);
-                W = std::max<int64_t>(1, std::min<int64_t>(W, ceil_div(tot, 8)));
-                void *part = nullptr;
-                int *cnt = nullptr;
-                RLA_TRY(scratch_get(ctx, (size_t)(2 * W) * (size_t)(s * slot), &part));
-                RLA_TRY(counters_get(ctx, (size_t)ng, &cnt));
-                CsGroupParams<T> gp{X, x_vs, L, ng, sk->meta, sk->tile_flags, sk->extra, s, Y, y_es, y_vs, a, (T)beta,
-                                    beta_zero, (T *)part, cnt, tpg, Split::make(tot, (int)W)};
-                kern<<<(int)W, 32, smem, ctx->stream>>>(gp);
-                RLA_TRY(check_launch(ctx, "cs_group"));
-                if (ng * G == nv) return RLA_OK;
-                // the remaining nv % G vectors go through the one-column kernel below
-                X += ng * G * x_vs;
-                Y += ng * G * y_vs;
-                nv -= ng * G;
-            }
             // one warp per CTA: bins + 64 list entries + 32 dummy slots
             int bins_cs = (int)s;
             if ((int64_t)(s + 96) * (int64_t)es > cap) bins_cs = (int)(cap / (4 * es)) - 96;
