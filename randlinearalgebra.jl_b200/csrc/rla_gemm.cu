@@ -1,9 +1,9 @@
-// rla_gemm.cu -- CUDA-core GEMM for the native-precision path.
+// rla_gemm.cu -- GEMM entry for the native-precision path.
 //
 // C(M x N) = alpha * op(A)(M x K) * op(B)(K x N) + beta * C, all column-major.
 // Operand types may differ (FP32 data with an FP64 Gram accumulator, FP64 factors
-// applied to FP32 data) so one kernel covers the Gaussian sketch, the power iterations
-// and the FP64 pieces of CholeskyQR2 / RandSVD.
+// applied to FP32 data).  FP64 accumulation goes to the FP64 tensor-core kernel
+// (rla_dgemm.cu); the CUDA-core kernel below serves FP32 accumulation.
 #include "rla_internal.cuh"
 #include "rla_kernels.cuh"
 
@@ -82,6 +82,9 @@ template <class TA, class TB, class TC, class TAcc>
 int gemm(rla_ctx *ctx, int64_t M, int64_t N, int64_t K, const TA *A, int64_t lda, int ta, const TB *B, int64_t ldb,
          int tb, TC *C, int64_t ldc, double alpha, double beta, int b_upper) {
     if (M <= 0 || N <= 0) return RLA_OK;
+    // FP64 accumulation runs on the FP64 tensor cores
+    if constexpr (std::is_same<TAcc, double>::value)
+        return dgemm<TA, TB, TC>(ctx, M, N, K, A, lda, ta, B, ldb, tb, C, ldc, alpha, beta, b_upper, 0);
     constexpr int BM = 64, BN = 64, BK = 16, TM = 4, TN = 4;
     const int64_t gx = ceil_div(M, BM), gy = ceil_div(N, BN);
     if (gy > 65535) return set_error(ctx, RLA_E_UNSUPPORTED, "GEMM grid too large (N=%lld)", (long long)N);

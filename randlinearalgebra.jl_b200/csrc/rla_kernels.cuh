@@ -58,6 +58,13 @@ template <class TA, class TB, class TC, class TAcc>
 int gemm(rla_ctx *ctx, int64_t M, int64_t N, int64_t K, const TA *A, int64_t lda, int ta, const TB *B, int64_t ldb,
          int tb, TC *C, int64_t ldc, double alpha, double beta, int b_upper = 0);
 
+// FP64-accumulating GEMM on the FP64 tensor cores (rla_dgemm.cu): C = alpha*op(A)*op(B) +
+// beta*C, column-major, Float32 or Float64 operands.  b_upper as for gemm; sym: the product
+// is symmetric (M == N), only its upper tiles are computed and mirrored.
+template <class TA, class TB, class TC>
+int dgemm(rla_ctx *ctx, int64_t M, int64_t N, int64_t K, const TA *A, int64_t lda, int ta, const TB *B, int64_t ldb,
+          int tb, TC *C, int64_t ldc, double alpha, double beta, int b_upper = 0, int sym = 0);
+
 // G (l x l, ld l, FP64) = Y'Y for Y (rows x l, ld ldy), split over row chunks (rla_range.cu).
 template <class T>
 int gram_fp64(rla_ctx *ctx, const T *Y, int64_t rows, int64_t l, int64_t ldy, double *G);

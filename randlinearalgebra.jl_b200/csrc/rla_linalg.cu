@@ -181,22 +181,59 @@ __global__ void __launch_bounds__(CB_THREADS) chol_blocked_kernel(double *G, int
 
 // Rinv = R^-1 for upper-triangular R: one warp per column j solves R x = e_j by back
 // substitution, x staged in shared memory (wpc warps per CTA).
+// Column j of R^-1 (R upper triangular, l x l, ld l) by back substitution in column form:
+// x = e_j; for i = j .. 0: x_i /= R_ii, then x_r -= x_i R_ri for r < i.  Each step reads
+// column i of R (contiguous), one warp per column of the inverse, x in shared memory.  With
+// MT > 0 (l <= 32*MT) the next column of R is loaded into registers while the current one
+// is applied, so each step waits on shared memory only.
+template <int MT>
 __global__ void __launch_bounds__(256) tri_inv_upper_kernel(const double *R, int64_t l, double *Ri, int wpc) {
     extern __shared__ double xs_all[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int64_t j = (int64_t)blockIdx.x * wpc + wib;
     if (j >= l) return;
     double *x = xs_all + (int64_t)wib * l;
-    for (int64_t i = lane; i <= j; i += 32) x[i] = 0.0;
+    for (int64_t i = lane; i <= j; i += 32) x[i] = i == j ? 1.0 : 0.0;
     __syncwarp();
-    if (lane == 0) x[j] = 1.0 / R[j + j * l];
-    __syncwarp();
-    for (int64_t i = j - 1; i >= 0; --i) {
-        double d = 0.0;
-        for (int64_t k = i + 1 + lane; k <= j; k += 32) d += R[i + k * l] * x[k];
-        d = warp_sum(d);
-        if (lane == 0) x[i] = -d / R[i + i * l];
-        __syncwarp();
+    if constexpr (MT > 0) {
+        double rc[MT], rn[MT];
+        double dc = R[j + j * l], dn = 0.0;
+#pragma unroll
+        for (int t = 0; t < MT; ++t) {
+            const int64_t r = lane + 32 * t;
+            rc[t] = r < j ? R[r + j * l] : 0.0;
+        }
+        for (int64_t i = j; i >= 0; --i) {
+            if (i > 0) {
+                dn = R[(i - 1) + (i - 1) * l];
+#pragma unroll
+                for (int t = 0; t < MT; ++t) {
+                    const int64_t r = lane + 32 * t;
+                    rn[t] = r < i - 1 ? R[r + (i - 1) * l] : 0.0;
+                }
+            }
+            const double xi = x[i] / dc;
+            __syncwarp();
+            if (lane == 0) x[i] = xi;
+#pragma unroll
+            for (int t = 0; t < MT; ++t) {
+                const int64_t r = lane + 32 * t;
+                if (r < i) x[r] = fma(-xi, rc[t], x[r]);
+            }
+            __syncwarp();
+#pragma unroll
+            for (int t = 0; t < MT; ++t) rc[t] = rn[t];
+            dc = dn;
+        }
+    } else {
+        for (int64_t i = j; i >= 0; --i) {
+            const double xi = x[i] / R[i + i * l];
+            __syncwarp();
+            if (lane == 0) x[i] = xi;
+            const double *ri = R + i * l;
+            for (int64_t r = lane; r < i; r += 32) x[r] = fma(-xi, ri[r], x[r]);
+            __syncwarp();
+        }
     }
     double *out = Ri + j * l;
     for (int64_t i = lane; i < l; i += 32) out[i] = i <= j ? x[i] : 0.0;
@@ -709,8 +746,9 @@ int tri_inv_upper(rla_ctx *ctx, const double *R, int64_t l, double *Rinv) {
     if (per > ctx->smem_optin - 1024)
         return set_error(ctx, RLA_E_UNSUPPORTED, "triangular inverse of order %lld exceeds shared memory", (long long)l);
     const size_t smem = (size_t)per * wpc;
-    RLA_CUDA_TRY(ctx, set_smem_max(tri_inv_upper_kernel));
-    tri_inv_upper_kernel<<<ceil_div_i(l, wpc), 32 * wpc, smem, ctx->stream>>>(R, l, Rinv, wpc);
+    auto kern = l <= 128 ? tri_inv_upper_kernel<4> : (l <= 512 ? tri_inv_upper_kernel<16> : tri_inv_upper_kernel<0>);
+    RLA_CUDA_TRY(ctx, set_smem_max(kern));
+    kern<<<ceil_div_i(l, wpc), 32 * wpc, smem, ctx->stream>>>(R, l, Rinv, wpc);
     return check_launch(ctx, "tri_inv_upper");
 }
 

@@ -103,99 +103,10 @@ __global__ void convert_kernel(const TI *X, int64_t rows, int64_t cols, int64_t 
 }
 
 // ---- tall-skinny Gram matrix G = Y'Y (l x l, FP64 accumulation) ------------------------
-// Upper-triangle 64x64 tiles of G times row chunks of Y: each CTA accumulates one tile over
-// one chunk in FP64 registers (4x4 per thread) and writes it to part[chunk][tile]; the
-// reduction adds the chunks in order (deterministic) and mirrors the lower triangle.
-constexpr int GRAM_T = 64, GRAM_KR = 32;
-
-template <class T>
-__global__ void __launch_bounds__(256) gram_tile_kernel(const T *__restrict__ Y, int64_t rows, int64_t l, int64_t ldy,
-                                                        int64_t rows_per_chunk, int ntiles, double *__restrict__ part) {
-    __shared__ __align__(16) double As[GRAM_KR][GRAM_T];
-    __shared__ __align__(16) double Bs[GRAM_KR][GRAM_T];
-    // tile index -> (ti, tj) with ti <= tj, row-major over the upper triangle
-    const int nt = (int)((l + GRAM_T - 1) / GRAM_T);
-    int t = blockIdx.x, ti = 0;
-    while (t >= nt - ti) {
-        t -= nt - ti;
-        ++ti;
-    }
-    const int tj = ti + t;
-    const int64_t chunk = blockIdx.y;
-    const int64_t r0 = chunk * rows_per_chunk, r1 = min(rows, r0 + rows_per_chunk);
-    const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
-    const int64_t ci = (int64_t)ti * GRAM_T, cj = (int64_t)tj * GRAM_T;
-    double acc[4][4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
-    for (int64_t k0 = r0; k0 < r1; k0 += GRAM_KR) {
-#pragma unroll
-        for (int e = 0; e < (GRAM_KR * GRAM_T) / 256; ++e) {
-            const int idx = tid + 256 * e;
-            const int r = idx % GRAM_KR, c = idx / GRAM_KR;
-            const int64_t gr = k0 + r;
-            const bool rin = gr < r1;
-            As[r][c] = (rin && ci + c < l) ? (double)Y[gr + (ci + c) * ldy] : 0.0;
-            Bs[r][c] = (rin && cj + c < l) ? (double)Y[gr + (cj + c) * ldy] : 0.0;
-        }
-        __syncthreads();
-#pragma unroll 8
-        for (int kk = 0; kk < GRAM_KR; ++kk) {
-            const double2 a01 = *reinterpret_cast<const double2 *>(&As[kk][ty * 4]);
-            const double2 a23 = *reinterpret_cast<const double2 *>(&As[kk][ty * 4 + 2]);
-            const double2 b01 = *reinterpret_cast<const double2 *>(&Bs[kk][tx * 4]);
-            const double2 b23 = *reinterpret_cast<const double2 *>(&Bs[kk][tx * 4 + 2]);
-            const double a[4] = {a01.x, a01.y, a23.x, a23.y}, b[4] = {b01.x, b01.y, b23.x, b23.y};
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
-        }
-        __syncthreads();
-    }
-    double *out = part + (chunk * ntiles + blockIdx.x) * (GRAM_T * GRAM_T);
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) out[(ty * 4 + i) * GRAM_T + tx * 4 + j] = acc[i][j];
-}
-
-__global__ void gram_reduce_kernel(const double *__restrict__ part, int64_t nchunks, int ntiles, int64_t l, double *G) {
-    const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (idx >= l * l) return;
-    const int64_t i = idx % l, j = idx / l;
-    if (i > j) return;
-    const int nt = (int)((l + GRAM_T - 1) / GRAM_T);
-    const int ti = (int)(i / GRAM_T), tj = (int)(j / GRAM_T);
-    const int tile = ti * nt - ti * (ti - 1) / 2 + (tj - ti);
-    const int64_t off = (int64_t)tile * GRAM_T * GRAM_T + (i % GRAM_T) * GRAM_T + (j % GRAM_T);
-    double acc = 0.0;
-    for (int64_t c = 0; c < nchunks; ++c) acc += part[c * ntiles * GRAM_T * GRAM_T + off];
-    G[i + j * l] = acc;
-    G[j + i * l] = acc;
-}
-
 template <class T>
 int gram_fp64(rla_ctx *ctx, const T *Y, int64_t rows, int64_t l, int64_t ldy, double *G) {
-    const int nt = (int)ceil_div(l, GRAM_T);
-    const int ntiles = nt * (nt + 1) / 2;
-    int64_t nchunks = std::max<int64_t>(1, ceil_div(2 * (int64_t)ctx->sm_count * 2, ntiles));
-    int64_t rpc = ceil_div(ceil_div(rows, nchunks), GRAM_KR) * GRAM_KR;
-    rpc = std::max<int64_t>(rpc, 2 * GRAM_KR);  // short Y (a Kaczmarz block): still several CTAs
-    nchunks = std::max<int64_t>(1, ceil_div(rows, rpc));
-    if (nchunks > 65535) {
-        nchunks = 65535;
-        rpc = ceil_div(ceil_div(rows, nchunks), GRAM_KR) * GRAM_KR;
-        nchunks = ceil_div(rows, rpc);
-    }
-    void *ws = nullptr;
-    RLA_TRY(scratch_get(ctx, sizeof(double) * (size_t)nchunks * ntiles * GRAM_T * GRAM_T, &ws));
-    gram_tile_kernel<T><<<dim3(ntiles, (unsigned)nchunks), 256, 0, ctx->stream>>>(Y, rows, l, ldy, rpc, ntiles, (double *)ws);
-    RLA_TRY(check_launch(ctx, "gram_tile"));
-    gram_reduce_kernel<<<ceil_div_i(l * l, 256), 256, 0, ctx->stream>>>((const double *)ws, nchunks, ntiles, l, G);
-    return check_launch(ctx, "gram_reduce");
+    // symmetric FP64 product on the FP64 tensor cores: upper tiles, split over row chunks
+    return dgemm<T, T, double>(ctx, l, l, rows, Y, ldy, 1, Y, ldy, 0, G, l, 1.0, 0.0, 0, 1);
 }
 
 template int gram_fp64<float>(rla_ctx *, const float *, int64_t, int64_t, int64_t, double *);
@@ -210,13 +121,17 @@ struct OrthWork {
 // In-place orthonormalisation of Y (rows x l, ld ldy).  With `signs` the columns of Q get
 // the signs LAPACK's Householder QR of Y gives them (needed only where Q itself is
 // returned: column signs of intermediate bases cancel out of the final factors).
+// `passes` CholeskyQR passes: 2 (CholeskyQR2) for a basis that must be orthonormal to
+// working precision; 1 for an intermediate basis of the power iterations, which only has
+// to span range(Y) and be well conditioned (one pass with the FP64 Gram matrix leaves
+// ||Q'Q - I|| ~ u * cond(Y) for Float32 Y, ~ u * cond(Y)^2 for Float64).
 template <class T>
-static int orth(rla_ctx *ctx, T *Y, int64_t rows, int64_t l, int64_t ldy, OrthWork &w, bool signs = true) {
+static int orth(rla_ctx *ctx, T *Y, int64_t rows, int64_t l, int64_t ldy, OrthWork &w, bool signs = true,
+                int passes = 2) {
     if (l > rows)
         return set_error(ctx, RLA_E_UNSUPPORTED, "compression dimension %lld exceeds the %lld rows being orthogonalised",
                          (long long)l, (long long)rows);
     T *tmp = (T *)w.tmp;
-    int passes = 2;
     bool shifted_done = false;
     for (int pass = 0; pass < passes; ++pass) {
         RLA_TRY(gram_fp64<T>(ctx, Y, rows, l, ldy, w.G));
@@ -359,12 +274,14 @@ static int range_core(rla_ctx *ctx, const rla_sketch *om, int64_t m, int64_t n, 
     }
     if (!done) RLA_TRY(sketch_mul_impl(ctx, om, RLA_SIDE_RIGHT, 0, m, l, Q, ldq, 0, m, n, A, lda, 0, 1.0, 0.0));
     if (pr->orthogonalize) {
-        RLA_TRY(orth<T>(ctx, Q, m, l, ldq, wq, q_signs && pr->power_its == 0));
+        // intermediate bases (every one but the last Q) take one CholeskyQR pass
+        RLA_TRY(orth<T>(ctx, Q, m, l, ldq, wq, q_signs && pr->power_its == 0, pr->power_its == 0 ? 2 : 1));
         for (int64_t it = 0; it < pr->power_its; ++it) {
+            const bool last = it + 1 == pr->power_its;
             RLA_TRY(at_q(Q, Z));
-            RLA_TRY(orth<T>(ctx, Z, n, l, n, wz, false));
+            RLA_TRY(orth<T>(ctx, Z, n, l, n, wz, false, 1));
             RLA_TRY(a_z(Z, Q));
-            RLA_TRY(orth<T>(ctx, Q, m, l, ldq, wq, q_signs && it + 1 == pr->power_its));
+            RLA_TRY(orth<T>(ctx, Q, m, l, ldq, wq, q_signs && last, last ? 2 : 1));
         }
     } else {
         for (int64_t it = 0; it < pr->power_its; ++it) {
