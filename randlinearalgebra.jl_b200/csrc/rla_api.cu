@@ -41,11 +41,16 @@ static int dimcheck(rla_ctx *ctx, const rla_sketch *sk, int side, int trans_s, i
     return trans_s ? left(c_cols, c_rows, nr, nc, a_cols, a_rows) : right(c_rows, c_cols, a_rows, a_cols, nr, nc);
 }
 
-// Dense products of the Gaussian sketch.
+// Dense products of the Gaussian sketch: Float32 on the 5th-generation tensor cores (three
+// BF16 terms per operand, FP64 accumulation across k-chunks: an FP32-accurate product),
+// Float64 on the FP64 tensor cores.
 template <class T>
 static int dense_gemm(rla_ctx *ctx, int64_t M, int64_t N, int64_t K, const T *A, int64_t lda, int ta, const T *B,
                       int64_t ldb, int tb, T *C, int64_t ldc, double alpha, double beta) {
-    return gemm<T, T, T, double>(ctx, M, N, K, A, lda, ta, B, ldb, tb, C, ldc, alpha, beta);
+    if constexpr (std::is_same<T, float>::value)
+        return gemm_f32_tc<float>(ctx, M, N, K, A, lda, ta, B, ldb, tb, C, ldc, alpha, beta);
+    else
+        return gemm<T, T, T, double>(ctx, M, N, K, A, lda, ta, B, ldb, tb, C, ldc, alpha, beta);
 }
 
 template <class T>

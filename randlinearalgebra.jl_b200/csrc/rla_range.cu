@@ -198,8 +198,9 @@ struct Owned {
 };
 
 // Operands of the tensor-core products with A (Float32 data): A split once into NT BF16
-// terms (NT = 2 for RLA_PREC_SPLIT_BF16, about 16 bits); one buffer set reused for the terms
-// of the thin factor of each product (Omega, Q or Z).
+// terms (NT = 2 for RLA_PREC_SPLIT_BF16, about 16 bits; NT = 3 with FP64 accumulation across
+// k-chunks for RLA_PREC_NATIVE, an FP32-accurate product); one buffer set reused for the
+// terms of the thin factor of each product (Omega, Q or Z).
 struct TcOps {
     int nt = 2;
     bf16 *a[3] = {nullptr, nullptr, nullptr};
@@ -235,7 +236,7 @@ static int tc_apply(rla_ctx *ctx, const TcOps &ops, int at, int64_t m, int64_t n
         return tc_gemm_split<2, TO>(ctx, rows_out, l, k, a, ops.lda, at, x, ldxs, out, ldo, 1.0, 0.0, 0);
     }
     RLA_TRY(split_terms_launch<3>(ctx, X, k, l, ldx, 0, ops.x, ldxs));
-    return tc_gemm_split<3, TO>(ctx, rows_out, l, k, a, ops.lda, at, x, ldxs, out, ldo, 1.0, 0.0, 0);
+    return tc_gemm_f64acc<TO>(ctx, rows_out, l, k, a, ops.lda, at, x, ldxs, out, ldo, 1.0, 0.0);
 }
 
 // Q (m x l, ld ldq) <- range of A*Omega after the power iterations.  With `tc` (FP32 data
@@ -316,9 +317,11 @@ static int randsvd_t(rla_ctx *ctx, const rla_sketch *om, int64_t m, int64_t n, c
     RLA_CUDA_TRY(ctx, pool_malloc_s(ctx, (void **)&Q, sizeof(T) * m * l, ctx->stream));
     own.ptrs.push_back(Q);
     TcOps tc;
-    const bool use_tc = pr->precision == RLA_PREC_SPLIT_BF16;
+    // Float32 products with A run on the tensor cores: split BF16 (2 terms) when asked,
+    // otherwise three terms with FP64 accumulation (FP32 accuracy)
+    const bool use_tc = std::is_same<T, float>::value;
     if constexpr (std::is_same<T, float>::value)
-        if (use_tc) RLA_TRY(tc_ops_make(ctx, A, m, n, lda, l, 2, tc, own));
+        RLA_TRY(tc_ops_make(ctx, A, m, n, lda, l, pr->precision == RLA_PREC_SPLIT_BF16 ? 2 : 3, tc, own));
     RLA_TRY(range_core<T>(ctx, om, m, n, A, lda, pr, Q, m, own, use_tc ? &tc : nullptr, false));
     // Bt = A'Q (n x l) in FP64 (randsvd.jl:183-185 forms QA in Float64)
     double *Bt, *X, *J, *sig, *jw;
@@ -373,12 +376,12 @@ int rla_rangefinder(rla_ctx *ctx, const rla_sketch *om, int dtype, int64_t m, in
     int rc;
     if (dtype == RLA_F32) {
         TcOps tc;
-        const bool use_tc = pr->precision == RLA_PREC_SPLIT_BF16;
-        if (use_tc) RLA_TRY(tc_ops_make(ctx, (const float *)A, m, n, lda, om->n_cols, 2, tc, own));
-        rc = range_core<float>(ctx, om, m, n, (const float *)A, lda, pr, (float *)Q, ldq, own, use_tc ? &tc : nullptr);
+        RLA_TRY(tc_ops_make(ctx, (const float *)A, m, n, lda, om->n_cols, pr->precision == RLA_PREC_SPLIT_BF16 ? 2 : 3,
+                            tc, own));
+        rc = range_core<float>(ctx, om, m, n, (const float *)A, lda, pr, (float *)Q, ldq, own, &tc);
         RLA_TRY(rc);
         RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-        return use_tc ? tc_status_check(ctx) : RLA_OK;
+        return tc_status_check(ctx);
     }
     rc = range_core<double>(ctx, om, m, n, (const double *)A, lda, pr, (double *)Q, ldq, own);
     RLA_TRY(rc);

@@ -429,9 +429,186 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
     }
 }
 
+// ------------------------------------------------------------------------------------
+// FP32-accurate products: NT = 3 terms with FP64 accumulation across k-chunks.
+// The tensor cores accumulate in FP32, and over a long K that running sum drifts well above
+// the FP32 rounding of the result.  Here the MMAs of every TC_CHUNK k-blocks go into one of
+// two TMEM accumulators (ping-pong); four epilogue warps add each finished chunk into FP64
+// registers while the MMAs fill the other one.  Warps: 0 TMA producer (lane 0), 1 MMA
+// issuer (lane 0), 2 TMEM allocator, 4..7 chunk drain / epilogue (warp 4+q reads TMEM
+// lanes 32q .. 32q+31, the tile rows of its quarter).  Tiles are 128 x 64; the grid is
+// (N tiles, M tiles, splits), N fastest, so the CTAs that share an A tile run together and
+// A comes from HBM about once.  Output: FP64 partial tiles, one per split.
+constexpr int TC64_THREADS = 256, TC64_BN = 64, TC_CHUNK = 4;
+
+template <int NT>
+__global__ void __launch_bounds__(TC64_THREADS, 1)
+tc_gemm_f64acc_kernel(const __grid_constant__ TcMaps<NT> maps, TcParams p, double *out64) {
+    extern __shared__ unsigned char smem_raw[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t raw = smem_u32(smem_raw);
+    const uint32_t base = (raw + 1023u) & ~1023u;
+    const uint32_t b_bytes = (uint32_t)TC64_BN * TC_BK * 2;
+    const uint32_t stage_bytes = NT * TC_A_BYTES + NT * b_bytes;
+    const uint32_t bar_base = base + (uint32_t)p.stages * stage_bytes;
+    auto full_bar = [&](int s) { return bar_base + 8u * (uint32_t)s; };
+    auto empty_bar = [&](int s) { return bar_base + 8u * (uint32_t)(p.stages + s); };
+    auto accf_bar = [&](int x) { return bar_base + 16u * (uint32_t)p.stages + 8u * (uint32_t)x; };
+    auto acce_bar = [&](int x) { return bar_base + 16u * (uint32_t)p.stages + 16u + 8u * (uint32_t)x; };
+    const uint32_t done_bar = bar_base + 16u * (uint32_t)p.stages + 32u;
+    const uint32_t tmem_slot = done_bar + 8u;
+    unsigned char *gen_base = smem_raw + (base - raw);
+    volatile uint32_t *tmem_slot_ptr = reinterpret_cast<volatile uint32_t *>(gen_base + (tmem_slot - base));
+
+    const int n0 = blockIdx.x * TC64_BN;
+    const int m0 = blockIdx.y * TC_BM;
+    const int split = blockIdx.z;
+    const int kb0 = split * p.kbps;
+    const int nkb = max(0, min(p.nkb - kb0, p.kbps));
+    const int nchunks = (nkb + TC_CHUNK - 1) / TC_CHUNK;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < p.stages; ++s) {
+            mbar_init(full_bar(s), 1);
+            mbar_init(empty_bar(s), 1);
+        }
+        for (int x = 0; x < 2; ++x) {
+            mbar_init(accf_bar(x), 1);
+            mbar_init(acce_bar(x), 4);
+        }
+        mbar_init(done_bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+#pragma unroll
+        for (int q = 0; q < NT; ++q) {
+            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&maps.a[q])) : "memory");
+            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&maps.b[q])) : "memory");
+        }
+    }
+    if (warp == 2) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tmem_slot),
+                     "r"(p.tmem_cols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot_ptr;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---- TMA producer ----
+            int issued = 0;
+            for (int kb = 0; kb < nkb; ++kb) {
+                const int s = kb % p.stages;
+                const uint32_t ph = (uint32_t)(kb / p.stages) & 1u;
+                if (!mbar_wait(empty_bar(s), ph ^ 1u, p.status, p.wait_ns)) break;
+                issued = kb + 1;
+                const uint32_t st = base + (uint32_t)s * stage_bytes;
+                const int k0 = (kb0 + kb) * TC_BK;
+                mbar_arrive_expect_tx(full_bar(s), stage_bytes);
+#pragma unroll
+                for (int t = 0; t < NT; ++t) {
+                    const uint32_t a_t = st + (uint32_t)t * TC_A_BYTES;
+                    const uint32_t b_t = st + NT * TC_A_BYTES + (uint32_t)t * b_bytes;
+                    if (p.a_kmajor) {
+                        tma_load_2d(a_t, &maps.a[t], full_bar(s), k0, m0);
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) tma_load_2d(a_t + q * 2048u, &maps.a[t], full_bar(s), m0 + 32 * q, k0);
+                    }
+                    tma_load_2d(b_t, &maps.b[t], full_bar(s), k0, n0);
+                }
+            }
+            for (int kb = max(0, issued - p.stages); kb < issued; ++kb)
+                mbar_drain(full_bar(kb % p.stages), (uint32_t)(kb / p.stages) & 1u, p.status);
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // ---- MMA issuer: chunk c accumulates into TMEM columns (c & 1) * 64 ----
+            const uint32_t idesc = idesc_bf16(TC_BM, TC64_BN, p.a_kmajor ? 0 : 1, 0);
+            for (int kb = 0; kb < nkb; ++kb) {
+                const int c = kb / TC_CHUNK, x = c & 1;
+                const bool first = kb % TC_CHUNK == 0;
+                if (first) {
+                    // the epilogue has drained this buffer's previous chunk (c - 2)
+                    if (!mbar_wait(acce_bar(x), ((uint32_t)(c >> 1) & 1u) ^ 1u, p.status, p.wait_ns)) break;
+                    tc_fence_after();
+                }
+                const int s = kb % p.stages;
+                const uint32_t ph = (uint32_t)(kb / p.stages) & 1u;
+                if (!mbar_wait(full_bar(s), ph, p.status, p.wait_ns)) break;
+                tc_fence_after();
+                const uint32_t st = base + (uint32_t)s * stage_bytes;
+                const uint32_t d = tmem + (uint32_t)x * TC64_BN;
+#pragma unroll
+                for (int kk = 0; kk < TC_BK / 16; ++kk) {
+                    uint64_t da[NT], db[NT];
+#pragma unroll
+                    for (int t = 0; t < NT; ++t) {
+                        const uint32_t a_t = st + (uint32_t)t * TC_A_BYTES;
+                        da[t] = p.a_kmajor ? sdesc_sw64(a_t + kk * 32u, 16u, 512u) : sdesc_sw64(a_t + kk * 1024u, 2048u, 512u);
+                        db[t] = sdesc_sw64(st + NT * TC_A_BYTES + (uint32_t)t * b_bytes + kk * 32u, 16u, 512u);
+                    }
+#pragma unroll
+                    for (int i = 0; i < tc_pairs(NT); ++i) {
+                        int ta, tb;
+                        tc_pair(i, ta, tb);
+                        mma_bf16(d, da[ta], db[tb], idesc, (first && kk == 0 && i == 0) ? 0u : 1u);
+                    }
+                }
+                mma_commit(empty_bar(s));
+                if (kb % TC_CHUNK == TC_CHUNK - 1 || kb == nkb - 1) mma_commit(accf_bar(x));
+            }
+            mma_commit(done_bar);
+        }
+        __syncwarp();
+    } else if (warp >= 4) {
+        // ---- chunk drain: FP64 sums of the rows of this warp's TMEM lane quarter ----
+        const int q = warp - 4;
+        double acc[TC64_BN];
+#pragma unroll
+        for (int j = 0; j < TC64_BN; ++j) acc[j] = 0.0;
+        bool ok = true;
+        for (int c = 0; c < nchunks && ok; ++c) {
+            const int x = c & 1;
+            ok = mbar_wait(accf_bar(x), (uint32_t)(c >> 1) & 1u, p.status, p.wait_ns);
+            __syncwarp();
+            if (!ok) break;
+            tc_fence_after();
+#pragma unroll
+            for (int c0 = 0; c0 < TC64_BN; c0 += 16) {
+                uint32_t r[16];
+                tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(x * TC64_BN + c0), r);
+#pragma unroll
+                for (int j = 0; j < 16; ++j) acc[c0 + j] += (double)__uint_as_float(r[j]);
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(acce_bar(x)) : "memory");
+        }
+        const int row = m0 + q * 32 + lane;
+        if (row < p.M) {
+            double *o = out64 + (int64_t)split * p.split_stride + row;
+#pragma unroll
+            for (int j = 0; j < TC64_BN; ++j)
+                if (n0 + j < p.N) o[(int64_t)(n0 + j) * p.ldo] = ok ? acc[j] : 0.0;
+        }
+    }
+    // every MMA issued (done_bar is committed on every path) has finished before the
+    // accumulators are released
+    if (threadIdx.x == 64) mbar_drain(done_bar, 0u, p.status);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 2) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(p.tmem_cols) : "memory");
+    }
+}
+
 // C(i, j) = alpha * sum_s P[s](i, j) + beta * C(i, j), splits added in order.
-template <class TC>
-__global__ void splitk_reduce_kernel(const float *__restrict__ P, int splits, int64_t split_stride, int64_t ldp,
+template <class TC, class TP = float>
+__global__ void splitk_reduce_kernel(const TP *__restrict__ P, int splits, int64_t split_stride, int64_t ldp,
                                      int64_t M, int64_t N, TC *C, int64_t ldc, double alpha, double beta,
                                      int beta_zero) {
     for (int64_t j = blockIdx.y; j < N; j += gridDim.y) {
@@ -620,8 +797,56 @@ template int tc_gemm_bf16x3<float>(rla_ctx *, int64_t, int64_t, int64_t, const b
 template int tc_gemm_bf16x3<double>(rla_ctx *, int64_t, int64_t, int64_t, const bf16 *, const bf16 *, int64_t, int,
                                     const bf16 *, const bf16 *, int64_t, double *, int64_t, double, double, int);
 
+// C (M x N, ld ldc) = alpha * op(A) * B + beta * C from three BF16 terms of each operand,
+// FP64 accumulation across k-chunks (tc_gemm_f64acc_kernel); split-K partials in FP64.
+template <class TC>
+int tc_gemm_f64acc(rla_ctx *ctx, int64_t M, int64_t N, int64_t K, const bf16 *const *A, int64_t lda, int a_kmajor,
+                   const bf16 *const *B, int64_t ldb, TC *C, int64_t ldc, double alpha, double beta) {
+    constexpr int NT = 3;
+    if (M <= 0 || N <= 0) return RLA_OK;
+    if (M >= (1ll << 31) || K >= (1ll << 31) || N >= (1ll << 31))
+        return set_error(ctx, RLA_E_UNSUPPORTED, "tensor-core GEMM: dimension above 2^31");
+    int *status = nullptr;
+    RLA_TRY(tc_status_get(ctx, &status));
+    const int64_t mt = ceil_div(M, TC_BM), ntl = ceil_div(N, TC64_BN), nkb = ceil_div(K, TC_BK);
+    if (mt > 65535 || ntl > 65535) return set_error(ctx, RLA_E_UNSUPPORTED, "tensor-core GEMM: grid too large");
+    const int64_t stage = NT * TC_A_BYTES + NT * (int64_t)TC64_BN * TC_BK * 2;
+    const int64_t budget = ctx->smem_optin - 1024 - 256;
+    const int stages = (int)std::max<int64_t>(2, std::min<int64_t>(8, budget / stage));
+    const size_t smem = (size_t)(stages * stage + 1024 + 256);
+    // split K until the grid covers the GPU, keeping whole chunks per split
+    int64_t splits = 1;
+    const int64_t tiles = mt * ntl;
+    if (tiles < ctx->sm_count) splits = std::min<int64_t>(ceil_div(ctx->sm_count, tiles), std::max<int64_t>(1, nkb / (2 * TC_CHUNK)));
+    const int64_t kbps = ceil_div(ceil_div(nkb, splits), TC_CHUNK) * TC_CHUNK;
+    splits = ceil_div(nkb, kbps);
+    TcMaps<NT> maps;
+    for (int t = 0; t < NT; ++t) {
+        if (a_kmajor) RLA_TRY(make_map(ctx, &maps.a[t], A[t], K, M, lda, TC_BK, TC_BM));
+        else RLA_TRY(make_map(ctx, &maps.a[t], A[t], M, K, lda, 32, TC_BK));
+        RLA_TRY(make_map(ctx, &maps.b[t], B[t], K, N, ldb, TC_BK, TC64_BN));
+    }
+    const int64_t ldo = M, sstride = M * N;
+    void *ws = nullptr;
+    RLA_TRY(scratch_get(ctx, sizeof(double) * (size_t)sstride * splits, &ws));
+    TcParams p{(int)M, (int)N, (int)K, TC64_BN, 1, a_kmajor, (int)nkb, (int)kbps, stages, 2u * TC64_BN,
+               nullptr, ldo, sstride, status, ctx->wait_ns};
+    RLA_CUDA_TRY(ctx, set_smem_max(tc_gemm_f64acc_kernel<NT>));
+    cudaEvent_t e0 = timing_begin(ctx);
+    tc_gemm_f64acc_kernel<NT><<<dim3((unsigned)ntl, (unsigned)mt, (unsigned)splits), TC64_THREADS, smem, ctx->stream>>>(
+        maps, p, (double *)ws);
+    RLA_TRY(check_launch(ctx, "tc_gemm_f64acc"));
+    timing_end(ctx, 0, e0);
+    const unsigned gx = (unsigned)std::min<int64_t>(ceil_div(M, 256), 1024);
+    const unsigned gy = (unsigned)std::min<int64_t>(N, 65535);
+    splitk_reduce_kernel<TC, double><<<dim3(gx, gy), 256, 0, ctx->stream>>>((const double *)ws, (int)splits, sstride,
+                                                                              ldo, M, N, C, ldc, alpha, beta, beta == 0.0);
+    return check_launch(ctx, "splitk_reduce");
+}
+
 // C (M x N, ld ldc, TC) = alpha * op(A) * op(B) + beta * C for Float32 A and B on the
-// tensor cores with three BF16 terms per operand (an FP32-accurate product).  op(A) may be
+// tensor cores with three BF16 terms per operand and FP64 accumulation across k-chunks (an
+// FP32-accurate product).  op(A) may be
 // A or A' (both layouts are read by TMA); op(B) must be K-major for the MMA, so B' (tb = 1)
 // is transposed while it is split.  The split copies come from the context's memory pool.
 template <class TC>
@@ -641,7 +866,7 @@ int gemm_f32_tc(rla_ctx *ctx, int64_t M, int64_t N, int64_t K, const float *A, i
                               : split_terms_launch<3>(ctx, B, K, N, ldb, 0, b3, ldb2);
     if (rc == RLA_OK) {
         const bf16 *ac[3] = {a3[0], a3[1], a3[2]}, *bc[3] = {b3[0], b3[1], b3[2]};
-        rc = tc_gemm_split<3, TC>(ctx, M, N, K, ac, lda2, ta, bc, ldb2, C, ldc, alpha, beta, 0);
+        rc = tc_gemm_f64acc<TC>(ctx, M, N, K, ac, lda2, ta, bc, ldb2, C, ldc, alpha, beta);
     }
     cudaFreeAsync(buf, ctx->stream);
     return rc;

@@ -48,10 +48,16 @@ int tc_gemm_bf16x3(rla_ctx *ctx, int64_t M, int64_t N, int64_t K, const bf16 *Ah
 
 // C (M x N, ld ldc) = alpha * op(A) * op(B) + beta * C for Float32 column-major A, B with an
 // FP32-accurate product on the tensor cores (three BF16 terms per operand, six MMAs per
-// k-step, FP32 accumulation; split-K partial tiles added in FP64).  Asynchronous.
+// k-step, FP64 accumulation across k-chunks).  Asynchronous.
 template <class TC>
 int gemm_f32_tc(rla_ctx *ctx, int64_t M, int64_t N, int64_t K, const float *A, int64_t lda, int ta, const float *B,
                 int64_t ldb, int tb, TC *C, int64_t ldc, double alpha, double beta);
+
+// C = alpha * op(A) * B + beta * C from three BF16 terms per operand (K-major B), FP64
+// accumulation across chunks of four k-blocks.  Asynchronous.
+template <class TC>
+int tc_gemm_f64acc(rla_ctx *ctx, int64_t M, int64_t N, int64_t K, const bf16 *const *A, int64_t lda, int a_kmajor,
+                   const bf16 *const *B, int64_t ldb, TC *C, int64_t ldc, double alpha, double beta);
 
 // Device status word of the tensor-core kernels (non-zero after a timed-out wait).
 int tc_status_get(rla_ctx *ctx, int **out);

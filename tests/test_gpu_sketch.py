@@ -298,9 +298,11 @@ def test_sparse_sign_left_fp64_4096x256(rla, orc, dev):
 @pytest.mark.parametrize("orient", ["SA", "AS", "StA", "ASt"])
 @pytest.mark.parametrize("card", ["left", "right"])
 def test_gaussian_float32_tensor_core_sizes(rla, orc, dev, card, orient):
-    """Float32 Gaussian applies at long dimension 20000 (long accumulation chains, ragged
-    tiles): every orientation stays within the Float32 tolerance of the FP64 oracle
-    (gaussian.jl:154,168)."""
+    """Float32 Gaussian applies run on the tensor cores: three BF16 terms per operand, six
+    MMAs per k-step, FP32 accumulation in tensor memory for four k-blocks at a time and FP64
+    accumulation across those chunks.  At long dimension 20000 (long accumulation chains,
+    split-K, ragged tiles) every orientation stays within the Float32 tolerance of the FP64
+    oracle (gaussian.jl:154,168)."""
     rng = np.random.default_rng(hash((card, orient)) % 2**32)
     S = make(rla, "gaussian", card, 300, 20000, np.float32, seed=5)
     err = run_orient(rla, orc, S, orient, 70, np.float32, dev, rng, alpha=1.5, beta=0.5)
