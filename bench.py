@@ -593,6 +593,113 @@ def randsvd_arm(args):
 
 
 # --------------------------------------------------------------------------------------
+# Plain SparseSign workload (left apply, Float64)
+# --------------------------------------------------------------------------------------
+SS_M, SS_N, SS_S, SS_NNZ = 4096, 256, 512, 8
+SS_WORKLOAD = "sparse_sign left apply, fp64, A 4096x256 -> 512x256, nnz=8"
+
+
+def sparse_sign_arm(args):
+    """SparseSign Left, Float64, A 4096x256 ~ N(0,1) compressed to 512x256 with 8 nonzeros
+    per column.  One step = one S*A through the C ABI on device-resident A.  A and C (9.4 MB)
+    stay in L2 between steps, so the rate is an L2 rate; the line says so."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    world, rank, local = dist_setup(args.gpus)
+    from __graft_entry__ import load_package
+    rla = load_package()
+    from randlinearalgebra_b200 import _lib as L
+    dev = torch.device("cuda", local if world > 1 else 0)
+    g = torch.Generator(device=dev)
+    g.manual_seed(1 + rank)
+    A = torch.randn(SS_N, SS_M, device=dev, generator=g, dtype=torch.float64).t()
+    S = rla.complete_compressor(rla.SparseSign(cardinality=rla.Left(), compression_dim=SS_S, nnz=SS_NNZ,
+                                               type=np.float64), A, seed=1 + rank)
+    C = torch.zeros(SS_N, SS_S, device=dev, dtype=torch.float64).t()
+    ctx = L.Context.get(dev.index)
+    lib = L.lib()
+    stream = torch.cuda.current_stream(dev)
+
+    def apply():
+        L.check(lib.rla_sketch_mul_async(ctx.handle, S.handle, 0, 0, SS_S, SS_N, C.data_ptr(), SS_S, 0, SS_M, SS_N,
+                                         A.data_ptr(), SS_M, 0, 1.0, 0.0), ctx.handle)
+
+    for _ in range(args.warmup):
+        apply()
+    K = args.steps
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    props = torch.cuda.get_device_properties(dev)
+    clocks = ClockSampler(f"GPU-{props.uuid}" if getattr(props, "uuid", None) else dev.index)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    t0.record(stream)
+    for _ in range(K):
+        apply()
+    t1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    barrier(world)
+    ms = allreduce_max(t0.elapsed_time(t1), world) / K
+    nbytes = 8 * (SS_M * SS_N + SS_S * SS_N)
+    value = world * nbytes / (ms / 1e3) / 1e9
+    # end to end: host A in, host C out
+    A_h = torch.empty(SS_N, SS_M, dtype=torch.float64, pin_memory=True).t()
+    A_h.copy_(A)
+    C_h = torch.zeros(SS_N, SS_S, dtype=torch.float64, pin_memory=True).t()
+    rla.mul_(C_h, S, A_h)
+    w0 = time.perf_counter()
+    for _ in range(10):
+        rla.mul_(C_h, S, A_h)
+    e2e_s = allreduce_max((time.perf_counter() - w0) / 10, world)
+    if rank != 0:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    peak, peak_kind = peaks()
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        from __graft_entry__ import load_oracle
+        orc = load_oracle()
+        d = S.draws()
+        R = orc.Recipe("sparse_sign", "left", SS_S, SS_M, np.float64, nnz=SS_NNZ,
+                       csc=orc.CSC(SS_S, SS_M, np.arange(0, SS_M * SS_NNZ + 1, SS_NNZ), d["rowval"], d["nzval"]))
+        Ah = A.cpu().numpy()
+        Ch = np.zeros((SS_S, SS_N), order="F")
+        reps, w0 = 0, time.perf_counter()
+        while time.perf_counter() - w0 < 3.0:
+            orc.mul_SA(Ch, R, Ah)
+            reps += 1
+        dt = (time.perf_counter() - w0) / reps
+        cpu = {"value": round(nbytes / dt / 1e9, 4), "unit": "GB/s", "cores": 1, "kind": "port",
+               "sample": f"the whole workload, {reps} applies; C restatement of SparseArrays' CSC loop (oracle/)"}
+    line = {"metric": "SparseSign apply throughput (GB/s of algorithmic bytes 8*(m*n + s*n))", "value": round(value, 2),
+            "unit": "GB/s", "n_gpus": world, "steps": K, "warmup": args.warmup, "ms_per_step": round(ms, 5),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic N(0,1) generated on device (seed 1+rank)",
+            "config": {"workload": SS_WORKLOAD, "m": SS_M, "n": SS_N, "s": SS_S, "nnz": SS_NNZ,
+                       "parallelism": f"replicas x{world}",
+                       "l2": "A and C (9.4 MB) stay in L2 between steps: an L2 rate, not an HBM rate"},
+            "roofline": {"bound": "hbm", "kernel": "compress_contig_kernel", "achieved": round(value / world, 2),
+                         "peak": peak, "peak_source": peak_kind, "unit": "GB/s",
+                         "frac": round(value / world / peak, 4), "traffic": None,
+                         "note": "L2-resident workload; the fraction is of HBM peak for scale only"},
+            "cpu_baseline": cpu,
+            "e2e": {"value": round(world * nbytes / e2e_s / 1e9, 3), "unit": "GB/s",
+                    "h2d_bytes_per_step": 8 * SS_M * SS_N, "d2h_bytes_per_step": 8 * SS_S * SS_N,
+                    "ms_per_step": round(e2e_s * 1e3, 4)},
+            "clocks": clk, "gpu_launches": K}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+# --------------------------------------------------------------------------------------
 # IHS workload
 # --------------------------------------------------------------------------------------
 IHS_M, IHS_N = 2**18, 512
@@ -1380,7 +1487,8 @@ def main():
     ap.add_argument("--cols", type=int, default=NCOL,
                     help="columns of A (default 512, the benchmark workload; smaller values make small "
                          "cases of the same kernels for profiler captures)")
-    ap.add_argument("--workload", choices=["sketch", "randsvd", "batched", "serve", "ihs", "sampling", "kaczmarz"],
+    ap.add_argument("--workload", choices=["sketch", "randsvd", "batched", "serve", "ihs", "sampling", "kaczmarz",
+                                           "sparse_sign"],
                     default="sketch",
                     help="sketch: SRHT + CountSketch apply (default); randsvd: mixed-precision RandSVD; "
                          "batched: 512 uneven RandSVD instances")
@@ -1436,6 +1544,13 @@ def main():
                   flush=True)
         else:
             ihs_arm(args)
+    elif args.workload == "sparse_sign":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "sparse_sign workload: the reference arm is timed "
+                              "for the sketch and randsvd workloads only (the CPU restatement is in cpu_baseline)"}),
+                  flush=True)
+        else:
+            sparse_sign_arm(args)
     elif args.workload == "randsvd":
         if args.impl == "reference":
             randsvd_reference_arm(args)
