@@ -182,52 +182,54 @@ __global__ void __launch_bounds__(CB_THREADS) chol_blocked_kernel(double *G, int
 // Rinv = R^-1 for upper-triangular R: one warp per column j solves R x = e_j by back
 // substitution, x staged in shared memory (wpc warps per CTA).
 // Column j of R^-1 (R upper triangular, l x l, ld l) by back substitution in column form:
-// x = e_j; for i = j .. 0: x_i /= R_ii, then x_r -= x_i R_ri for r < i.  Each step reads
-// column i of R (contiguous), one warp per column of the inverse, x in shared memory.  With
-// MT > 0 (l <= 32*MT) the next column of R is loaded into registers while the current one
-// is applied, so each step waits on shared memory only.
+// x = e_j; for i = j .. 0: x_i *= 1/R_ii, then x_r -= x_i R_ri for r < i.  Each step reads
+// column i of R (contiguous), one warp per column of the inverse, x and the reciprocal
+// diagonal in shared memory.  With MT > 0 (l <= 32*MT) the columns two steps ahead are
+// loaded into registers while the current one is applied.
 template <int MT>
 __global__ void __launch_bounds__(256) tri_inv_upper_kernel(const double *R, int64_t l, double *Ri, int wpc) {
     extern __shared__ double xs_all[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    double *dinv = xs_all + (int64_t)wpc * l;
+    for (int64_t i = threadIdx.x; i < l; i += blockDim.x) dinv[i] = 1.0 / R[i + i * l];
+    __syncthreads();
     const int64_t j = (int64_t)blockIdx.x * wpc + wib;
     if (j >= l) return;
     double *x = xs_all + (int64_t)wib * l;
     for (int64_t i = lane; i <= j; i += 32) x[i] = i == j ? 1.0 : 0.0;
     __syncwarp();
     if constexpr (MT > 0) {
-        double rc[MT], rn[MT];
-        double dc = R[j + j * l], dn = 0.0;
+        // ring of three columns: r0 = column i, r1 = column i-1, r2 = column i-2
+        double r0[MT], r1[MT], r2[MT];
+        auto load = [&](int64_t col, double (&dst)[MT]) {
 #pragma unroll
-        for (int t = 0; t < MT; ++t) {
-            const int64_t r = lane + 32 * t;
-            rc[t] = r < j ? R[r + j * l] : 0.0;
-        }
-        for (int64_t i = j; i >= 0; --i) {
-            if (i > 0) {
-                dn = R[(i - 1) + (i - 1) * l];
-#pragma unroll
-                for (int t = 0; t < MT; ++t) {
-                    const int64_t r = lane + 32 * t;
-                    rn[t] = r < i - 1 ? R[r + (i - 1) * l] : 0.0;
-                }
+            for (int t = 0; t < MT; ++t) {
+                const int64_t r = lane + 32 * t;
+                dst[t] = (col >= 0 && r < col) ? R[r + col * l] : 0.0;
             }
-            const double xi = x[i] / dc;
+        };
+        load(j, r0);
+        load(j - 1, r1);
+        for (int64_t i = j; i >= 0; --i) {
+            load(i - 2, r2);
+            const double xi = x[i] * dinv[i];
             __syncwarp();
             if (lane == 0) x[i] = xi;
 #pragma unroll
             for (int t = 0; t < MT; ++t) {
                 const int64_t r = lane + 32 * t;
-                if (r < i) x[r] = fma(-xi, rc[t], x[r]);
+                if (r < i) x[r] = fma(-xi, r0[t], x[r]);
             }
             __syncwarp();
 #pragma unroll
-            for (int t = 0; t < MT; ++t) rc[t] = rn[t];
-            dc = dn;
+            for (int t = 0; t < MT; ++t) {
+                r0[t] = r1[t];
+                r1[t] = r2[t];
+            }
         }
     } else {
         for (int64_t i = j; i >= 0; --i) {
-            const double xi = x[i] / R[i + i * l];
+            const double xi = x[i] * dinv[i];
             __syncwarp();
             if (lane == 0) x[i] = xi;
             const double *ri = R + i * l;
@@ -363,12 +365,15 @@ __global__ void __launch_bounds__(1024) jacobi_finish_kernel(double *X, double *
 
 // ---- block one-sided Jacobi -------------------------------------------------------------
 // Columns in blocks of BJ_B; an outer round pairs blocks (circle method) and each CTA takes
-// one pair: it stages the pair's columns of X and J in shared memory, runs inner one-sided
-// (Hestenes) sweeps over them (one warp per column pair, circle-method rounds) until they
-// are mutually orthogonal to `tol` or BJ_INNER sweeps, and writes them back.  The largest
-// relative off-diagonal seen in a CTA's first inner sweep goes to *off (max over the outer
-// sweep), which the host reads to stop.
-constexpr int BJ_B = 16, BJ_INNER = 1, BJ_THREADS = 512;
+// one pair: it stages the pair's columns of X and J in shared memory (row stride rounded up
+// to an even count, zero padded, so the column loops run on 16-byte vectors), runs inner
+// one-sided (Hestenes) sweeps over them (one warp per column pair, circle-method rounds)
+// until they are mutually orthogonal to `tol` or BJ_INNER sweeps, and writes them back.
+// Small blocks spread each outer round over many SMs: the rotations of a sweep are the same
+// work whatever the blocking, and a pair's inner rounds are bound by the latency of one
+// warp's rotation.  The largest relative off-diagonal seen in a CTA's first inner sweep goes
+// to *off (max over the outer sweep), which the host reads to stop.
+constexpr int BJ_B = 8, BJ_INNER = 1, BJ_THREADS = 32 * BJ_B;
 
 __global__ void jacobi_identity_kernel(double *J, int64_t l) {
     const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -378,18 +383,19 @@ __global__ void jacobi_identity_kernel(double *J, int64_t l) {
 __global__ void __launch_bounds__(BJ_THREADS) block_jacobi_round_kernel(double *X, double *J, int64_t l, int nbp,
                                                                         int round, double tol,
                                                                         unsigned long long *off) {
-    extern __shared__ double bj_smem[];
+    extern __shared__ __align__(16) double bj_smem[];
     __shared__ unsigned long long inner_off;
     __shared__ int cols[2 * BJ_B];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = BJ_THREADS / 32;
-    const int nb = (int)((l + BJ_B - 1) / BJ_B);
+    const int li = (int)l, ls = (li + 1) & ~1;  // padded column stride
+    const int nb = (li + BJ_B - 1) / BJ_B;
     int bi, bj;
     tourney_pair(round, blockIdx.x, nbp, &bi, &bj);
     int c = 0;
     for (int q = 0; q < 2; ++q) {
         const int blk = q == 0 ? bi : bj;
         if (blk >= nb) continue;
-        const int c0 = blk * BJ_B, c1 = (int)(l < (int64_t)c0 + BJ_B ? l : (int64_t)c0 + BJ_B);
+        const int c0 = blk * BJ_B, c1 = min(li, c0 + BJ_B);
         for (int cc = c0; cc < c1; ++cc) {
             if (tid == 0) cols[c] = cc;
             ++c;
@@ -397,12 +403,12 @@ __global__ void __launch_bounds__(BJ_THREADS) block_jacobi_round_kernel(double *
     }
     __syncthreads();
     if (c < 2) return;
-    double *Xs = bj_smem, *Js = bj_smem + (int64_t)2 * BJ_B * l;
-    for (int64_t idx = tid; idx < (int64_t)c * l; idx += BJ_THREADS) {
-        const int q = (int)(idx / l);
-        const int64_t r = idx % l;
-        Xs[idx] = X[r + (int64_t)cols[q] * l];
-        Js[idx] = J[r + (int64_t)cols[q] * l];
+    double *Xs = bj_smem, *Js = bj_smem + 2 * BJ_B * ls;
+    for (int idx = tid; idx < c * ls; idx += BJ_THREADS) {
+        const int q = idx / ls, r = idx - q * ls;
+        const int64_t g = r + (int64_t)cols[q] * l;
+        Xs[idx] = r < li ? X[g] : 0.0;
+        Js[idx] = r < li ? J[g] : 0.0;
     }
     __syncthreads();
     const int cp = c + (c & 1);
@@ -419,13 +425,13 @@ __global__ void __launch_bounds__(BJ_THREADS) block_jacobi_round_kernel(double *
                     i = j;
                     j = t;
                 }
-                double *xi = Xs + (int64_t)i * l, *xj = Xs + (int64_t)j * l;
+                double2 *xi = reinterpret_cast<double2 *>(Xs + i * ls), *xj = reinterpret_cast<double2 *>(Xs + j * ls);
                 double a = 0, b = 0, g = 0;
-                for (int64_t k = lane; k < l; k += 32) {
-                    const double u = xi[k], w = xj[k];
-                    a = fma(u, u, a);
-                    b = fma(w, w, b);
-                    g = fma(u, w, g);
+                for (int k = lane; k < ls / 2; k += 32) {
+                    const double2 u = xi[k], w = xj[k];
+                    a = fma(u.x, u.x, fma(u.y, u.y, a));
+                    b = fma(w.x, w.x, fma(w.y, w.y, b));
+                    g = fma(u.x, w.x, fma(u.y, w.y, g));
                 }
                 a = warp_sum(a);
                 b = warp_sum(b);
@@ -436,14 +442,14 @@ __global__ void __launch_bounds__(BJ_THREADS) block_jacobi_round_kernel(double *
                     const double zeta = (b - a) / (2.0 * g);
                     const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
                     const double cs = 1.0 / sqrt(1.0 + t * t), sn = cs * t;
-                    double *ji = Js + (int64_t)i * l, *jj = Js + (int64_t)j * l;
-                    for (int64_t k = lane; k < l; k += 32) {
-                        const double u = xi[k], w = xj[k];
-                        xi[k] = cs * u - sn * w;
-                        xj[k] = sn * u + cs * w;
-                        const double uj = ji[k], wj = jj[k];
-                        ji[k] = cs * uj - sn * wj;
-                        jj[k] = sn * uj + cs * wj;
+                    double2 *ji = reinterpret_cast<double2 *>(Js + i * ls), *jj = reinterpret_cast<double2 *>(Js + j * ls);
+                    for (int k = lane; k < ls / 2; k += 32) {
+                        const double2 u = xi[k], w = xj[k];
+                        xi[k] = make_double2(cs * u.x - sn * w.x, cs * u.y - sn * w.y);
+                        xj[k] = make_double2(sn * u.x + cs * w.x, sn * u.y + cs * w.y);
+                        const double2 uj = ji[k], wj = jj[k];
+                        ji[k] = make_double2(cs * uj.x - sn * wj.x, cs * uj.y - sn * wj.y);
+                        jj[k] = make_double2(sn * uj.x + cs * wj.x, sn * uj.y + cs * wj.y);
                     }
                 }
             }
@@ -454,11 +460,12 @@ __global__ void __launch_bounds__(BJ_THREADS) block_jacobi_round_kernel(double *
         __syncthreads();
         if (done) break;
     }
-    for (int64_t idx = tid; idx < (int64_t)c * l; idx += BJ_THREADS) {
-        const int q = (int)(idx / l);
-        const int64_t r = idx % l;
-        X[r + (int64_t)cols[q] * l] = Xs[idx];
-        J[r + (int64_t)cols[q] * l] = Js[idx];
+    for (int idx = tid; idx < c * ls; idx += BJ_THREADS) {
+        const int q = idx / ls, r = idx - q * ls;
+        if (r >= li) continue;
+        const int64_t g = r + (int64_t)cols[q] * l;
+        X[g] = Xs[idx];
+        J[g] = Js[idx];
     }
 }
 
@@ -742,10 +749,11 @@ int cholesky_upper(rla_ctx *ctx, double *G, int64_t l, double shift, int *breakd
 
 int tri_inv_upper(rla_ctx *ctx, const double *R, int64_t l, double *Rinv) {
     const int64_t per = sizeof(double) * std::max<int64_t>(l, 1);
-    const int wpc = (int)std::max<int64_t>(1, std::min<int64_t>(8, (ctx->smem_optin - 1024) / per));
-    if (per > ctx->smem_optin - 1024)
+    // per warp one column of x, plus the reciprocal diagonal shared by the CTA
+    const int wpc = (int)std::max<int64_t>(1, std::min<int64_t>(8, (ctx->smem_optin - 1024) / per - 1));
+    if (2 * per > ctx->smem_optin - 1024)
         return set_error(ctx, RLA_E_UNSUPPORTED, "triangular inverse of order %lld exceeds shared memory", (long long)l);
-    const size_t smem = (size_t)per * wpc;
+    const size_t smem = (size_t)per * (wpc + 1);
     auto kern = l <= 128 ? tri_inv_upper_kernel<4> : (l <= 512 ? tri_inv_upper_kernel<16> : tri_inv_upper_kernel<0>);
     RLA_CUDA_TRY(ctx, set_smem_max(kern));
     kern<<<ceil_div_i(l, wpc), 32 * wpc, smem, ctx->stream>>>(R, l, Rinv, wpc);
@@ -754,7 +762,7 @@ int tri_inv_upper(rla_ctx *ctx, const double *R, int64_t l, double *Rinv) {
 
 int jacobi_svd(rla_ctx *ctx, double *X, double *J, double *sigma, int64_t l, double *work) {
     const double tol = 1e-15;
-    const size_t smem = sizeof(double) * 4 * BJ_B * (size_t)l;
+    const size_t smem = sizeof(double) * 4 * BJ_B * (size_t)((l + 1) & ~1);
     if (l <= 2 * BJ_B || smem > (size_t)ctx->smem_optin - 2048) {
         jacobi_kernel<<<1, 1024, 0, ctx->stream>>>(X, J, sigma, l, work, 60, tol);
         RLA_TRY(check_launch(ctx, "jacobi_svd"));
