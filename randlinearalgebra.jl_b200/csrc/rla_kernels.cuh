@@ -90,6 +90,7 @@ int tri_inv_upper(rla_ctx *ctx, const double *R, int64_t l, double *Rinv);
 // on return the columns of X are orthogonal, sigma[i] = ||X(:, i)||, columns sorted by
 // descending sigma, X(:, i) normalised, J permuted alongside.  `work` holds at least
 // 2*l*l + 2*l doubles.
-int jacobi_svd(rla_ctx *ctx, double *X, double *J, double *sigma, int64_t l, double *work);
+// Sweeps stop once no pair's relative off-diagonal |x_i'x_j| / (||x_i|| ||x_j||) exceeds tol.
+int jacobi_svd(rla_ctx *ctx, double *X, double *J, double *sigma, int64_t l, double *work, double tol = 1e-15);
 
 }  // namespace rla

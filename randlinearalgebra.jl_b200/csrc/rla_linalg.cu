@@ -760,8 +760,7 @@ int tri_inv_upper(rla_ctx *ctx, const double *R, int64_t l, double *Rinv) {
     return check_launch(ctx, "tri_inv_upper");
 }
 
-int jacobi_svd(rla_ctx *ctx, double *X, double *J, double *sigma, int64_t l, double *work) {
-    const double tol = 1e-15;
+int jacobi_svd(rla_ctx *ctx, double *X, double *J, double *sigma, int64_t l, double *work, double tol) {
     const size_t smem = sizeof(double) * 4 * BJ_B * (size_t)((l + 1) & ~1);
     if (l <= 2 * BJ_B || smem > (size_t)ctx->smem_optin - 2048) {
         jacobi_kernel<<<1, 1024, 0, ctx->stream>>>(X, J, sigma, l, work, 60, tol);
