@@ -392,7 +392,7 @@ typedef struct rla_request {
 typedef struct rla_server_config {
     int device;
     int slots;                /* concurrent workers (each with its own stream) */
-    int max_group;            /* RandSVD requests (k <= 128) run as one grouped batch */
+    int max_group;            /* RandSVD requests (k <= 128, m*n <= 2^22) run as one grouped batch */
     int mode;                 /* RLA_SERVE_BATCHED or RLA_SERVE_PLAIN */
     uint64_t memory_budget;   /* bytes of workspace admitted at once (0: 150 GB) */
     uint64_t sketch_cache_bytes; /* cap on resident sketches (0: memory_budget / 8); counted

@@ -4,11 +4,11 @@
 // requests from one FIFO queue.  A request is admitted when its estimated device workspace
 // fits the memory budget next to the work already running (a request is always admitted
 // when nothing runs, so none starves).  In RLA_SERVE_BATCHED mode a worker that takes a
-// RandSVD request with k <= 128 also takes the other pending ones that fit (up to
-// max_group) and runs them as one grouped batch (rla_batch.cu, eager launches); the other
-// workers keep taking requests meanwhile, so work that arrives while the GPU is busy
-// overlaps on the device.  Least-squares requests (sketch-and-solve, rla_ls.cu) and
-// RandSVD requests with k > 128 run one per worker; sketches stay resident (shared by the
+// RandSVD request with k <= 128 and at most 2^22 elements also takes the other pending such
+// requests that fit (up to max_group) and runs them as one grouped batch (rla_batch.cu,
+// eager launches); the other workers keep taking requests meanwhile, so work that arrives
+// while the GPU is busy overlaps on the device.  Least-squares requests (sketch-and-solve,
+// rla_ls.cu) and the other RandSVD requests run one per worker; sketches stay resident (shared by the
 // workers), keyed by shape and seed, in a cache whose estimated bytes count against the
 // memory budget: past its cap the least recently used sketch that no running request holds
 // is destroyed.  RLA_SERVE_PLAIN is the baseline: one worker, one request at a
@@ -59,6 +59,12 @@ size_t req_bytes(const rla_request &r) {
         return (size_t)(4 * m * k + 4 * n * k + 16 * n * k + 32 * k * k + 4 * ((m + 2047) / 2048) * n * k) + 4096;
     return (size_t)(12 * m * k + 40 * n * k + 64 * k * k) + 4096;
 }
+
+// RandSVD requests that run in grouped batches: rank k <= 128 and at most 2^22 elements of A.
+// Larger instances fill the GPU on their own, where the single-instance path (tensor-core
+// products, FP64 tensor-core factorizations) is faster than the grouped kernels.  The rule
+// depends on the request alone, so a request's result is the same alone and in any mix.
+bool groupable(const rla_request &r) { return r.kind == RLA_REQ_SVD && r.k <= 128 && r.m * r.n <= ((int64_t)1 << 22); }
 
 // Estimated device bytes of a resident sketch: SparseSign draws (bucket, sign, schedule
 // word per entry) and their per-tile schedule, or a dense Gaussian operator.
@@ -239,10 +245,10 @@ void worker_main(rla_server *S, int w) {
             job.push_back(f);
             bytes += f.bytes;
             S->in_use += f.bytes;
-            const bool group = batched && f.req.kind == RLA_REQ_SVD && f.req.k <= 128;
+            const bool group = batched && groupable(f.req);
             if (group) {
                 for (auto it = S->queue.begin(); it != S->queue.end() && (int)job.size() < S->cfg.max_group;) {
-                    if (it->req.kind == RLA_REQ_SVD && it->req.k <= 128 &&
+                    if (groupable(it->req) &&
                         S->in_use + it->bytes <= S->cfg.memory_budget) {
                         job.push_back(*it);
                         bytes += it->bytes;
@@ -275,7 +281,7 @@ void worker_main(rla_server *S, int w) {
         if (!job.empty()) {
             const rla_request &r0 = job.front().req;
             if (r0.kind == RLA_REQ_LS) rc = run_ls(S, ctx, r0);
-            else if (job.size() > 1 || (batched && r0.k <= 128)) rc = run_svd_group(ctx, job);
+            else if (job.size() > 1 || (batched && groupable(r0))) rc = run_svd_group(ctx, job);
             else rc = run_svd_single(S, ctx, r0);
             if (rc == RLA_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess) rc = RLA_E_CUDA;
         }
