@@ -1143,7 +1143,8 @@ def batched_arm(args):
     bytes_alg = sum(4 * 2 * m * n for (m, n, _) in shapes)   # A read twice (A*Omega, A'Q)
     flops = sum(4.0 * m * n * k for (m, n, k) in shapes)
     t_plan = time.perf_counter()
-    B = rla.RandSVDBatch(As, ks, seeds, autotune=not args.no_autotune)
+    prec = rla.RLA_PREC_SPLIT_BF16 if args.batch_precision == "split" else rla.RLA_PREC_NATIVE
+    B = rla.RandSVDBatch(As, ks, seeds, autotune=not args.no_autotune, precision=prec)
     t_plan = time.perf_counter() - t_plan
     stream = torch.cuda.current_stream(dev)
     for _ in range(args.warmup):
@@ -1170,7 +1171,8 @@ def batched_arm(args):
         out = []
         for A, k, sd in zip(As, ks, seeds):
             comp = rla.Gaussian(cardinality=rla.Right(), compression_dim=k, type=np.float32)
-            out.append(rla.rapproximate(rla.RandSVD(compressor=comp, factor_type=np.float32), A, seed=sd))
+            out.append(rla.rapproximate(rla.RandSVD(compressor=comp, factor_type=np.float32, precision=prec), A,
+                                        seed=sd))
         return out
     plain_once()
     torch.cuda.synchronize()
@@ -1242,7 +1244,9 @@ def batched_arm(args):
                "sample": f"FP64 RandSVD of the oracle (numpy/LAPACK, all BLAS threads) on {len(idx)} of the instances"}
     line = {"metric": BT_METRIC, "value": round(value, 2), "unit": "instances/s", "n_gpus": world, "steps": K,
             "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32 data, f32 products, f64 small factorizations",
+            "vs_baseline": None,
+            "dtype": ("f32 data, split-bf16 tensor-core passes over A (k <= 64), f64 small factorizations"
+                      if args.batch_precision == "split" else "f32 data, f32 products, f64 small factorizations"),
             "data": "synthetic low-rank + noise generated on device (seed 4+rank)",
             "config": {"workload": BT_WORKLOAD if n_inst == BT_COUNT else BT_WORKLOAD.replace("512", str(n_inst)),
                        "instances": n_inst, "parallelism": f"replicas x{world}",
@@ -1494,6 +1498,9 @@ def main():
                          "batched: 512 uneven RandSVD instances")
     ap.add_argument("--batch-count", type=int, default=BT_COUNT, help="instances of the batched workload")
     ap.add_argument("--no-autotune", action="store_true", help="batched workload: default tile shapes")
+    ap.add_argument("--batch-precision", choices=["split", "native"], default="split",
+                    help="batched workload: split-BF16 tensor-core passes over A (default) or FP32 CUDA-core passes; "
+                         "the plain path uses the same precision")
     ap.add_argument("--serve-requests", type=int, default=600, help="serving workload: requests per arrival rate")
     ap.add_argument("--slots", type=int, default=4, help="serving workload: concurrent workers")
     ap.add_argument("--serve-rates", default="2000,5000,10000,20000", help="serving workload: arrival rates (req/s)")

@@ -235,9 +235,12 @@ class RandSVDBatch:
     orthogonalize), A_i) with Float32 A_i; the factors U_i (m_i x k_i, Float32), S_i (k_i,
     Float64) and V_i (n_i x k_i, Float32) are allocated here.  Omega_i is the Gaussian
     sketch complete_compressor would draw with seed seeds[i].  The first run() captures the
-    grouped launch sequence as a CUDA graph; later runs replay it."""
+    grouped launch sequence as a CUDA graph; later runs replay it.  With precision =
+    RLA_PREC_SPLIT_BF16 the passes over A of the instances with k <= 64 run as grouped
+    tensor-core products (split BF16, FP64 accumulation across k-chunks)."""
 
-    def __init__(self, As, ks, seeds, power_its: int = 0, orthogonalize: bool = False, autotune: bool = True):
+    def __init__(self, As, ks, seeds, power_its: int = 0, orthogonalize: bool = False, autotune: bool = True,
+                 precision: int = 0):
         import torch
         if not (len(As) == len(ks) == len(seeds)):
             raise ArgumentError("As, ks and seeds must have the same length.")
@@ -265,7 +268,9 @@ class RandSVDBatch:
         p = L.RangeParams()
         p.power_its = int(power_its)
         p.orthogonalize = 1 if orthogonalize else 0
-        p.precision = L.RLA_PREC_NATIVE
+        if precision not in (L.RLA_PREC_NATIVE, L.RLA_PREC_SPLIT_BF16):
+            raise ArgumentError(f"Unknown precision mode {precision}.")
+        p.precision = int(precision)
         h = ctypes.c_void_p()
         L.check(L.lib().rla_randsvd_batch_create(self.ctx.handle, len(As), probs, ctypes.byref(p),
                                                  L.RLA_BATCH_AUTOTUNE if autotune else 0, ctypes.byref(h)),

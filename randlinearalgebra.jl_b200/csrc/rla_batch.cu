@@ -26,6 +26,7 @@
 
 #include "rla_internal.cuh"
 #include "rla_kernels.cuh"
+#include "rla_tc.cuh"
 
 namespace rla {
 
@@ -606,6 +607,11 @@ struct rla_batch {
     cudaGraphExec_t exec = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::vector<void *> owned;
+    // RLA_PREC_SPLIT_BF16 (classes with k <= 64): the passes over A as grouped tensor-core
+    // products, A split once per run into BF16 hi/lo, the thin factor split per product
+    bool tc = false;
+    rla::SplitGroup s_a[rla::B_NCLASS], s_om[rla::B_NCLASS], s_y[rla::B_NCLASS], s_z[rla::B_NCLASS];
+    rla::TcGroup g_ax[rla::B_NCLASS], g_atq_z[rla::B_NCLASS], g_atq_bt[rla::B_NCLASS];
 };
 
 namespace rla {
@@ -737,20 +743,40 @@ static int run_class(rla_ctx *ctx, rla_batch *b, int cls, cudaStream_t st) {
         }
         return RLA_OK;
     };
+    const bool tc = b->tc && KT <= 64;
     // Y = A * Omega
-    RLA_TRY((launch_ax_bm<AX_A_OM, KT>(ctx, b, cls, b->bm_ax[cls], st)));
+    if (tc) {
+        RLA_TRY(split_group_run(ctx, b->s_a[cls], st));
+        RLA_TRY(split_group_run(ctx, b->s_om[cls], st));
+        RLA_TRY(tc_group_run(ctx, b->g_ax[cls], st));
+    } else {
+        RLA_TRY((launch_ax_bm<AX_A_OM, KT>(ctx, b, cls, b->bm_ax[cls], st)));
+    }
     const bool ortho = b->params.orthogonalize != 0;
     if (ortho || b->params.power_its == 0) RLA_TRY(orth_m());
     for (int64_t it = 0; it < b->params.power_its; ++it) {
-        // Z = A'Q (split over row chunks), optionally orthonormalised, then Q = A Z
-        RLA_TRY((launch_xty_br<XT_A_Q_Z, KT>(ctx, b, cls, b->br_aq[cls], b->chunk_aq[cls], st)));
-        RLA_TRY((launch_reduce<RED_Z, float>(ctx, b, cls, b->chunk_aq[cls], b->chunk_n, st)));
-        RLA_TRY((launch_ax_bm<AX_A_Z, KT>(ctx, b, cls, b->bm_ax[cls], st)));
+        // Z = A'Q, optionally orthonormalised, then Q = A Z
+        if (tc) {
+            RLA_TRY(split_group_run(ctx, b->s_y[cls], st));
+            RLA_TRY(tc_group_run(ctx, b->g_atq_z[cls], st));
+            RLA_TRY(split_group_run(ctx, b->s_z[cls], st));
+            RLA_TRY(tc_group_run(ctx, b->g_ax[cls], st));
+        } else {
+            RLA_TRY((launch_xty_br<XT_A_Q_Z, KT>(ctx, b, cls, b->br_aq[cls], b->chunk_aq[cls], st)));
+            RLA_TRY((launch_reduce<RED_Z, float>(ctx, b, cls, b->chunk_aq[cls], b->chunk_n, st)));
+            RLA_TRY((launch_ax_bm<AX_A_Z, KT>(ctx, b, cls, b->bm_ax[cls], st)));
+        }
         if (ortho || it + 1 == b->params.power_its) RLA_TRY(orth_m());
     }
-    // Bt = A'Q in FP64 (partials FP32, added in FP64)
-    RLA_TRY((launch_xty_br<XT_A_Q, KT>(ctx, b, cls, b->br_aq[cls], b->chunk_aq[cls], st)));
-    RLA_TRY((launch_reduce<RED_BT, float>(ctx, b, cls, b->chunk_aq[cls], b->chunk_n, st)));
+    // Bt = A'Q in FP64 (CUDA cores: FP32 partials added in FP64; tensor cores: FP64
+    // accumulation across k-chunks, written to Bt and its copy Bt0)
+    if (tc) {
+        RLA_TRY(split_group_run(ctx, b->s_y[cls], st));
+        RLA_TRY(tc_group_run(ctx, b->g_atq_bt[cls], st));
+    } else {
+        RLA_TRY((launch_xty_br<XT_A_Q, KT>(ctx, b, cls, b->br_aq[cls], b->chunk_aq[cls], st)));
+        RLA_TRY((launch_reduce<RED_BT, float>(ctx, b, cls, b->chunk_aq[cls], b->chunk_n, st)));
+    }
     // CholeskyQR2 of Bt (n x k, FP64)
     for (int pass = 0; pass < 2; ++pass) {
         RLA_TRY((launch_xty<XT_GRAM_BT, KT, min_br<KT>()>(ctx, b, cls, b->chunk_n, st)));
@@ -899,8 +925,12 @@ int rla_randsvd_batch_create(rla_ctx *ctx, int count, const rla_svd_problem *pro
         o[7] = add(sizeof(double) * q.k * q.k);  // X
         o[8] = add(sizeof(double) * q.k * q.k);  // J
         o[9] = add(part_bytes(b, p));            // partials
+        const bool tci = params->precision == RLA_PREC_SPLIT_BF16 && q.k <= 64;
+        o[10] = add(tci ? sizeof(bf16) * 2 * (size_t)ceil_div(q.m, 8) * 8 * q.n : 16);                // A hi, lo
+        o[11] = add(tci ? sizeof(bf16) * 2 * (size_t)ceil_div(std::max(q.m, q.n), 8) * 8 * q.k : 16);  // factor hi, lo
         b->cls_h[b_kclass(q.k)].push_back(i);
     }
+    b->tc = params->precision == RLA_PREC_SPLIT_BF16;
     int rc = RLA_OK;
     auto fail = [&](int r) {
         rla_randsvd_batch_destroy(b);
@@ -919,6 +949,35 @@ int rla_randsvd_batch_create(rla_ctx *ctx, int count, const rla_svd_problem *pro
         p.Bt0 = (double *)(w + o[6]); p.X = (double *)(w + o[7]); p.J = (double *)(w + o[8]);
         p.part = w + o[9];
         p.flag = b->flagbuf + i;
+    }
+    if (b->tc) {
+        // grouped split and product tables per rank class (k <= 64), over fixed buffers
+        for (int c = 0; c < B_NCLASS - 1; ++c) {
+            if (b->cls_h[c].empty()) continue;
+            std::vector<SplitSpec> sa, so, sy, sz;
+            std::vector<TcGroupSpec> gx, gz, gb;
+            for (int i : b->cls_h[c]) {
+                const BProb &p = b->h_probs[i];
+                const int64_t lda2 = ceil_div(p.m, 8) * 8, ldn = ceil_div(p.n, 8) * 8, ldm = ceil_div(p.m, 8) * 8;
+                bf16 *ahi = (bf16 *)(w + offs[i][10]), *alo = ahi + lda2 * p.n;
+                bf16 *bhi = (bf16 *)(w + offs[i][11]), *blo = bhi + ceil_div(std::max(p.m, p.n), 8) * 8 * p.k;
+                sa.push_back(SplitSpec{p.A, p.m, p.n, p.lda, ahi, alo, lda2});
+                so.push_back(SplitSpec{p.Om, p.n, p.k, p.n, bhi, blo, ldn});
+                sy.push_back(SplitSpec{p.Y, p.m, p.k, p.m, bhi, blo, ldm});
+                sz.push_back(SplitSpec{p.Z, p.n, p.k, p.n, bhi, blo, ldn});
+                gx.push_back(TcGroupSpec{{ahi, alo}, lda2, 0, {bhi, blo}, ldn, p.m, p.k, p.n, p.Y, nullptr, p.m, 0});
+                gz.push_back(TcGroupSpec{{ahi, alo}, lda2, 1, {bhi, blo}, ldm, p.n, p.k, p.m, p.Z, nullptr, p.n, 0});
+                gb.push_back(TcGroupSpec{{ahi, alo}, lda2, 1, {bhi, blo}, ldm, p.n, p.k, p.m, p.Bt, p.Bt0, p.n, 1});
+            }
+            int r = split_group_build(ctx, sa, &b->s_a[c]);
+            if (r == RLA_OK) r = split_group_build(ctx, so, &b->s_om[c]);
+            if (r == RLA_OK) r = split_group_build(ctx, sy, &b->s_y[c]);
+            if (r == RLA_OK && params->power_its > 0) r = split_group_build(ctx, sz, &b->s_z[c]);
+            if (r == RLA_OK) r = tc_group_build(ctx, gx, &b->g_ax[c]);
+            if (r == RLA_OK && params->power_its > 0) r = tc_group_build(ctx, gz, &b->g_atq_z[c]);
+            if (r == RLA_OK) r = tc_group_build(ctx, gb, &b->g_atq_bt[c]);
+            if (r != RLA_OK) return fail(r);
+        }
     }
     if (pool_malloc_s(ctx, &b->d_probs, sizeof(BProb) * std::max(count, 1), ctx->stream) != cudaSuccess)
         return fail(set_error(ctx, RLA_E_OOM, "batch table"));
@@ -1000,6 +1059,7 @@ int rla_randsvd_batch_run(rla_ctx *ctx, rla_batch *b) {
     std::vector<int> fl(b->count);
     RLA_CUDA_TRY(ctx, cudaMemcpyAsync(fl.data(), b->flagbuf, sizeof(int) * b->count, cudaMemcpyDeviceToHost, ctx->stream));
     RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (b->tc) RLA_TRY(tc_status_check(ctx));
     for (int i = 0; i < b->count; ++i) {
         if (!fl[i]) continue;
         const rla_svd_problem &q = b->probs[i];
@@ -1032,6 +1092,15 @@ int rla_randsvd_batch_destroy(rla_batch *b) {
         if (b->join[c]) cudaEventDestroy(b->join[c]);
     }
     if (b->fork) cudaEventDestroy(b->fork);
+    for (int c = 0; c < B_NCLASS; ++c) {
+        split_group_free(&b->s_a[c]);
+        split_group_free(&b->s_om[c]);
+        split_group_free(&b->s_y[c]);
+        split_group_free(&b->s_z[c]);
+        tc_group_free(&b->g_ax[c]);
+        tc_group_free(&b->g_atq_z[c]);
+        tc_group_free(&b->g_atq_bt[c]);
+    }
     cudaStream_t st = b->ctx->stream;
     for (void *p : b->owned) cudaFreeAsync(p, st);
     for (int c = 0; c < B_NCLASS; ++c)

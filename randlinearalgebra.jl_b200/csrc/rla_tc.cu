@@ -441,9 +441,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
 // A comes from HBM about once.  Output: FP64 partial tiles, one per split.
 constexpr int TC64_THREADS = 256, TC64_BN = 64, TC_CHUNK = 4;
 
+// One CTA of the FP64-accumulating pipeline: the 128 x 64 tile (m0, n0) of op(A) * B over
+// k-blocks kb0 .. kb0+nkb-1 with MMAs mma_n columns wide, written as FP64 sums (or rounded to
+// Float32) to out[row + col*ldo].  ma / mb: the NT tensor maps of A and B (kernel parameter
+// or global memory).
 template <int NT>
-__global__ void __launch_bounds__(TC64_THREADS, 1)
-tc_gemm_f64acc_kernel(const __grid_constant__ TcMaps<NT> maps, TcParams p, double *out64) {
+__device__ __forceinline__ void f64acc_cta(const CUtensorMap *ma, const CUtensorMap *mb, const TcParams &p, int m0,
+                                           int n0, int kb0, int nkb, uint32_t mma_n, void *out, int64_t ldo,
+                                           int out_f64, void *out2 = nullptr) {
     extern __shared__ unsigned char smem_raw[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t raw = smem_u32(smem_raw);
@@ -460,11 +465,6 @@ tc_gemm_f64acc_kernel(const __grid_constant__ TcMaps<NT> maps, TcParams p, doubl
     unsigned char *gen_base = smem_raw + (base - raw);
     volatile uint32_t *tmem_slot_ptr = reinterpret_cast<volatile uint32_t *>(gen_base + (tmem_slot - base));
 
-    const int n0 = blockIdx.x * TC64_BN;
-    const int m0 = blockIdx.y * TC_BM;
-    const int split = blockIdx.z;
-    const int kb0 = split * p.kbps;
-    const int nkb = max(0, min(p.nkb - kb0, p.kbps));
     const int nchunks = (nkb + TC_CHUNK - 1) / TC_CHUNK;
 
     if (threadIdx.x == 0) {
@@ -480,8 +480,8 @@ tc_gemm_f64acc_kernel(const __grid_constant__ TcMaps<NT> maps, TcParams p, doubl
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 #pragma unroll
         for (int q = 0; q < NT; ++q) {
-            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&maps.a[q])) : "memory");
-            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&maps.b[q])) : "memory");
+            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(ma + q)) : "memory");
+            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(mb + q)) : "memory");
         }
     }
     if (warp == 2) {
@@ -512,12 +512,12 @@ tc_gemm_f64acc_kernel(const __grid_constant__ TcMaps<NT> maps, TcParams p, doubl
                     const uint32_t a_t = st + (uint32_t)t * TC_A_BYTES;
                     const uint32_t b_t = st + NT * TC_A_BYTES + (uint32_t)t * b_bytes;
                     if (p.a_kmajor) {
-                        tma_load_2d(a_t, &maps.a[t], full_bar(s), k0, m0);
+                        tma_load_2d(a_t, ma + t, full_bar(s), k0, m0);
                     } else {
 #pragma unroll
-                        for (int q = 0; q < 4; ++q) tma_load_2d(a_t + q * 2048u, &maps.a[t], full_bar(s), m0 + 32 * q, k0);
+                        for (int q = 0; q < 4; ++q) tma_load_2d(a_t + q * 2048u, ma + t, full_bar(s), m0 + 32 * q, k0);
                     }
-                    tma_load_2d(b_t, &maps.b[t], full_bar(s), k0, n0);
+                    tma_load_2d(b_t, mb + t, full_bar(s), k0, n0);
                 }
             }
             for (int kb = max(0, issued - p.stages); kb < issued; ++kb)
@@ -527,7 +527,7 @@ tc_gemm_f64acc_kernel(const __grid_constant__ TcMaps<NT> maps, TcParams p, doubl
     } else if (warp == 1) {
         if (lane == 0) {
             // ---- MMA issuer: chunk c accumulates into TMEM columns (c & 1) * 64 ----
-            const uint32_t idesc = idesc_bf16(TC_BM, TC64_BN, p.a_kmajor ? 0 : 1, 0);
+            const uint32_t idesc = idesc_bf16(TC_BM, (int)mma_n, p.a_kmajor ? 0 : 1, 0);
             for (int kb = 0; kb < nkb; ++kb) {
                 const int c = kb / TC_CHUNK, x = c & 1;
                 const bool first = kb % TC_CHUNK == 0;
@@ -590,10 +590,21 @@ tc_gemm_f64acc_kernel(const __grid_constant__ TcMaps<NT> maps, TcParams p, doubl
         }
         const int row = m0 + q * 32 + lane;
         if (row < p.M) {
-            double *o = out64 + (int64_t)split * p.split_stride + row;
+            if (out_f64) {
+                double *o = (double *)out + row;
+                double *o2 = out2 ? (double *)out2 + row : nullptr;
 #pragma unroll
-            for (int j = 0; j < TC64_BN; ++j)
-                if (n0 + j < p.N) o[(int64_t)(n0 + j) * p.ldo] = ok ? acc[j] : 0.0;
+                for (int j = 0; j < TC64_BN; ++j)
+                    if (n0 + j < p.N) {
+                        o[(int64_t)(n0 + j) * ldo] = ok ? acc[j] : 0.0;
+                        if (o2) o2[(int64_t)(n0 + j) * ldo] = ok ? acc[j] : 0.0;
+                    }
+            } else {
+                float *o = (float *)out + row;
+#pragma unroll
+                for (int j = 0; j < TC64_BN; ++j)
+                    if (n0 + j < p.N) o[(int64_t)(n0 + j) * ldo] = ok ? (float)acc[j] : 0.f;
+            }
         }
     }
     // every MMA issued (done_bar is committed on every path) has finished before the
@@ -604,6 +615,88 @@ tc_gemm_f64acc_kernel(const __grid_constant__ TcMaps<NT> maps, TcParams p, doubl
     if (warp == 2) {
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(p.tmem_cols) : "memory");
     }
+}
+
+template <int NT>
+__global__ void __launch_bounds__(TC64_THREADS, 1)
+tc_gemm_f64acc_kernel(const __grid_constant__ TcMaps<NT> maps, TcParams p, double *out64) {
+    const int n0 = blockIdx.x * TC64_BN;
+    const int m0 = blockIdx.y * TC_BM;
+    const int split = blockIdx.z;
+    const int kb0 = split * p.kbps;
+    const int nkb = max(0, min(p.nkb - kb0, p.kbps));
+    f64acc_cta<NT>(maps.a, maps.b, p, m0, n0, kb0, nkb, TC64_BN, out64 + (int64_t)split * p.split_stride, p.ldo, 1);
+}
+
+// ---- grouped products: many instances, one launch ------------------------------------
+// Item q: op(A_q) (M x K) * B_q (K x N, N <= 64) from NT BF16 terms, FP64 accumulation across
+// k-chunks, written to out (Float32 or Float64, ld ldo) and, when out2 is set, to out2 too.  CTA t takes M tile t - tstart[q]
+// of the item with tstart[q] <= t < tstart[q+1]; the tensor maps live in the item table in
+// global memory (written before the launch).
+template <int NT>
+struct alignas(64) TcGroupItem {
+    CUtensorMap a[NT], b[NT];
+    int M, N, K, a_kmajor;
+    int nkb, mma_n;
+    void *out, *out2;
+    int64_t ldo;
+    int out_f64;
+};
+
+template <int NT>
+__global__ void __launch_bounds__(TC64_THREADS, 1)
+tc_group_f64acc_kernel(const TcGroupItem<NT> *items, const int *tstart, int count, TcParams p) {
+    const int t = blockIdx.x;
+    int lo = 0, hi = count - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (tstart[mid] <= t) lo = mid;
+        else hi = mid - 1;
+    }
+    const TcGroupItem<NT> &it = items[lo];
+    p.M = it.M;
+    p.N = it.N;
+    p.K = it.K;
+    p.a_kmajor = it.a_kmajor;
+    f64acc_cta<NT>(it.a, it.b, p, (t - tstart[lo]) * TC_BM, 0, 0, it.nkb, (uint32_t)it.mma_n, it.out, it.ldo,
+                   it.out_f64, it.out2);
+}
+
+// Grouped split: item q converts X_q (rows x cols, ld ldx, FP32) into NT BF16 terms (ld ldo);
+// CTA t takes 256 groups of 8 rows of item q with bstart[q] <= t < bstart[q+1].
+struct SplitItem {
+    const float *X;
+    int64_t rows, cols, ldx;
+    bf16 *t[3];
+    int64_t ldo;
+};
+
+template <int NT>
+__global__ void split_group_kernel(const SplitItem *items, const int *bstart, int count) {
+    const int blk = blockIdx.x;
+    int lo = 0, hi = count - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (bstart[mid] <= blk) lo = mid;
+        else hi = mid - 1;
+    }
+    const SplitItem &it = items[lo];
+    const int64_t groups = (it.rows + 7) / 8;
+    const int64_t u = (int64_t)(blk - bstart[lo]) * blockDim.x + threadIdx.x;
+    if (u >= groups * it.cols) return;
+    const int64_t c = u / groups, r0 = (u - c * groups) * 8;
+    const float *xc = it.X + c * it.ldx;
+    __align__(16) bf16 t[NT][8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        bf16 ti[NT];
+        split_terms<NT>(r0 + i < it.rows ? __ldg(xc + r0 + i) : 0.f, ti);
+#pragma unroll
+        for (int q = 0; q < NT; ++q) t[q][i] = ti[q];
+    }
+#pragma unroll
+    for (int q = 0; q < NT; ++q)
+        *reinterpret_cast<uint4 *>(it.t[q] + r0 + c * it.ldo) = *reinterpret_cast<const uint4 *>(t[q]);
 }
 
 // C(i, j) = alpha * sum_s P[s](i, j) + beta * C(i, j), splits added in order.
@@ -796,6 +889,113 @@ template int tc_gemm_bf16x3<float>(rla_ctx *, int64_t, int64_t, int64_t, const b
                                    const bf16 *, const bf16 *, int64_t, float *, int64_t, double, double, int);
 template int tc_gemm_bf16x3<double>(rla_ctx *, int64_t, int64_t, int64_t, const bf16 *, const bf16 *, int64_t, int,
                                     const bf16 *, const bf16 *, int64_t, double *, int64_t, double, double, int);
+
+// ---- grouped products and splits (host side) ---------------------------------------------
+int tc_group_build(rla_ctx *ctx, const std::vector<TcGroupSpec> &specs, TcGroup *g) {
+    constexpr int NT = 2;
+    g->count = (int)specs.size();
+    g->tiles = 0;
+    if (specs.empty()) return RLA_OK;
+    std::vector<TcGroupItem<NT>> items(specs.size());
+    std::vector<int> ts(specs.size() + 1);
+    for (size_t q = 0; q < specs.size(); ++q) {
+        const TcGroupSpec &sp = specs[q];
+        TcGroupItem<NT> &it = items[q];
+        if (sp.N > TC64_BN || sp.M <= 0 || sp.N <= 0 || sp.K <= 0 || sp.M >= (1ll << 31) || sp.K >= (1ll << 31))
+            return set_error(ctx, RLA_E_UNSUPPORTED, "grouped tensor-core product: shape %lld x %lld x %lld",
+                             (long long)sp.M, (long long)sp.N, (long long)sp.K);
+        for (int t = 0; t < NT; ++t) {
+            if (sp.a_kmajor) RLA_TRY(make_map(ctx, &it.a[t], sp.a[t], sp.K, sp.M, sp.lda, TC_BK, TC_BM));
+            else RLA_TRY(make_map(ctx, &it.a[t], sp.a[t], sp.M, sp.K, sp.lda, 32, TC_BK));
+            RLA_TRY(make_map(ctx, &it.b[t], sp.b[t], sp.K, sp.N, sp.ldb, TC_BK, TC64_BN));
+        }
+        it.M = (int)sp.M;
+        it.N = (int)sp.N;
+        it.K = (int)sp.K;
+        it.a_kmajor = sp.a_kmajor;
+        it.nkb = (int)ceil_div(sp.K, TC_BK);
+        it.mma_n = (int)ceil_div(sp.N, 16) * 16;
+        it.out = sp.out;
+        it.out2 = sp.out2;
+        it.ldo = sp.ldo;
+        it.out_f64 = sp.out_f64;
+        ts[q] = g->tiles;
+        g->tiles += (int)ceil_div(sp.M, TC_BM);
+    }
+    ts[specs.size()] = g->tiles;
+    void *di = nullptr, *dt = nullptr;
+    RLA_CUDA_TRY(ctx, cudaMalloc(&di, sizeof(TcGroupItem<NT>) * items.size()));
+    RLA_CUDA_TRY(ctx, cudaMalloc(&dt, sizeof(int) * ts.size()));
+    RLA_CUDA_TRY(ctx, cudaMemcpyAsync(di, items.data(), sizeof(TcGroupItem<NT>) * items.size(), cudaMemcpyHostToDevice,
+                                      ctx->stream));
+    RLA_CUDA_TRY(ctx, cudaMemcpyAsync(dt, ts.data(), sizeof(int) * ts.size(), cudaMemcpyHostToDevice, ctx->stream));
+    g->items = di;
+    g->tstart = (int *)dt;
+    const int64_t stage = NT * TC_A_BYTES + NT * (int64_t)TC64_BN * TC_BK * 2;
+    const int64_t budget = ctx->smem_optin - 1024 - 256;
+    g->stages = (int)std::max<int64_t>(2, std::min<int64_t>(8, budget / stage));
+    g->smem = (size_t)(g->stages * stage + 1024 + 256);
+    RLA_CUDA_TRY(ctx, set_smem_max(tc_group_f64acc_kernel<NT>));
+    return tc_status_get(ctx, &g->status);
+}
+
+int tc_group_run(rla_ctx *ctx, const TcGroup &g, cudaStream_t st) {
+    if (g.tiles == 0) return RLA_OK;
+    TcParams p{};
+    p.BN = TC64_BN;
+    p.nch = 1;
+    p.stages = g.stages;
+    p.tmem_cols = 2u * TC64_BN;
+    p.status = g.status;
+    p.wait_ns = ctx->wait_ns;
+    tc_group_f64acc_kernel<2><<<g.tiles, TC64_THREADS, g.smem, st>>>((const TcGroupItem<2> *)g.items, g.tstart, g.count,
+                                                                     p);
+    return check_launch(ctx, "tc_group_f64acc");
+}
+
+int split_group_build(rla_ctx *ctx, const std::vector<SplitSpec> &specs, SplitGroup *g) {
+    g->count = (int)specs.size();
+    g->blocks = 0;
+    if (specs.empty()) return RLA_OK;
+    std::vector<SplitItem> items(specs.size());
+    std::vector<int> bs(specs.size() + 1);
+    for (size_t q = 0; q < specs.size(); ++q) {
+        const SplitSpec &sp = specs[q];
+        if (sp.ldo % 8 != 0 || sp.ldo < sp.rows || (((uintptr_t)sp.hi | (uintptr_t)sp.lo) & 15u))
+            return set_error(ctx, RLA_E_ARG, "grouped split: output leading dimension must be a multiple of 8");
+        items[q] = SplitItem{sp.X, sp.rows, sp.cols, sp.ldx, {sp.hi, sp.lo, nullptr}, sp.ldo};
+        bs[q] = g->blocks;
+        g->blocks += (int)ceil_div(ceil_div(sp.rows, 8) * sp.cols, 256);
+    }
+    bs[specs.size()] = g->blocks;
+    void *di = nullptr, *db = nullptr;
+    RLA_CUDA_TRY(ctx, cudaMalloc(&di, sizeof(SplitItem) * items.size()));
+    RLA_CUDA_TRY(ctx, cudaMalloc(&db, sizeof(int) * bs.size()));
+    RLA_CUDA_TRY(ctx, cudaMemcpyAsync(di, items.data(), sizeof(SplitItem) * items.size(), cudaMemcpyHostToDevice,
+                                      ctx->stream));
+    RLA_CUDA_TRY(ctx, cudaMemcpyAsync(db, bs.data(), sizeof(int) * bs.size(), cudaMemcpyHostToDevice, ctx->stream));
+    g->items = di;
+    g->bstart = (int *)db;
+    return RLA_OK;
+}
+
+int split_group_run(rla_ctx *ctx, const SplitGroup &g, cudaStream_t st) {
+    if (g.blocks == 0) return RLA_OK;
+    split_group_kernel<2><<<g.blocks, 256, 0, st>>>((const SplitItem *)g.items, g.bstart, g.count);
+    return check_launch(ctx, "split_group");
+}
+
+void tc_group_free(TcGroup *g) {
+    if (g->items) cudaFree(g->items);
+    if (g->tstart) cudaFree(g->tstart);
+    *g = TcGroup{};
+}
+
+void split_group_free(SplitGroup *g) {
+    if (g->items) cudaFree(g->items);
+    if (g->bstart) cudaFree(g->bstart);
+    *g = SplitGroup{};
+}
 
 // C (M x N, ld ldc) = alpha * op(A) * B + beta * C from three BF16 terms of each operand,
 // FP64 accumulation across k-chunks (tc_gemm_f64acc_kernel); split-K partials in FP64.

@@ -3,6 +3,8 @@
 
 #include <cuda_bf16.h>
 
+#include <vector>
+
 #include "rla_internal.cuh"
 
 namespace rla {
@@ -58,6 +60,49 @@ int gemm_f32_tc(rla_ctx *ctx, int64_t M, int64_t N, int64_t K, const float *A, i
 template <class TC>
 int tc_gemm_f64acc(rla_ctx *ctx, int64_t M, int64_t N, int64_t K, const bf16 *const *A, int64_t lda, int a_kmajor,
                    const bf16 *const *B, int64_t ldb, TC *C, int64_t ldc, double alpha, double beta);
+
+// Grouped products for many instances in one launch (split BF16, two terms): item q is
+// op(A_q) (M x K) * B_q (K x N, N <= 64, K-major), FP64 accumulation across k-chunks, written
+// to out (and out2 when set) as Float32 or Float64 with leading dimension ldo.  The tensor
+// maps and tile table are built once (tc_group_build) for fixed buffers and reused by every
+// launch (tc_group_run), which allocates nothing and can be captured in a graph.
+struct TcGroupSpec {
+    const bf16 *a[2];
+    int64_t lda;
+    int a_kmajor;
+    const bf16 *b[2];
+    int64_t ldb;
+    int64_t M, N, K;
+    void *out, *out2;
+    int64_t ldo;
+    int out_f64;
+};
+struct TcGroup {
+    void *items = nullptr;
+    int *tstart = nullptr;
+    int count = 0, tiles = 0, stages = 2;
+    size_t smem = 0;
+    int *status = nullptr;
+};
+int tc_group_build(rla_ctx *ctx, const std::vector<TcGroupSpec> &specs, TcGroup *g);
+int tc_group_run(rla_ctx *ctx, const TcGroup &g, cudaStream_t st);
+void tc_group_free(TcGroup *g);
+
+// Grouped FP32 -> (hi, lo) BF16 splits of many matrices in one launch.
+struct SplitSpec {
+    const float *X;
+    int64_t rows, cols, ldx;
+    bf16 *hi, *lo;
+    int64_t ldo;
+};
+struct SplitGroup {
+    void *items = nullptr;
+    int *bstart = nullptr;
+    int count = 0, blocks = 0;
+};
+int split_group_build(rla_ctx *ctx, const std::vector<SplitSpec> &specs, SplitGroup *g);
+int split_group_run(rla_ctx *ctx, const SplitGroup &g, cudaStream_t st);
+void split_group_free(SplitGroup *g);
 
 // Device status word of the tensor-core kernels (non-zero after a timed-out wait).
 int tc_status_get(rla_ctx *ctx, int **out);

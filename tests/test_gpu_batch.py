@@ -102,3 +102,37 @@ def test_batch_argument_errors(rla, dev):
         rla.RandSVDBatch([A], [30], [1])
     with pytest.raises(rla.ArgumentError):
         rla.RandSVDBatch([to_dev(np.zeros((50, 20)), dev)], [4], [1])
+
+
+@pytest.mark.parametrize("q,ortho", [(0, False), (1, True)])
+def test_batch_tensor_core_passes_vs_oracle(rla, orc, dev, q, ortho):
+    """RLA_PREC_SPLIT_BF16: the passes over A (A*Omega, A'Q, and A'Q / A*Z of the power
+    iterations) of the instances with k <= 64 run as grouped tcgen05 products of split-BF16
+    operands with FP64 accumulation across k-chunks; the rest of the algorithm is unchanged.
+    Against the FP64 oracle on the same draws: singular values, the projection error and the
+    factor product within 1e-4; the batch graph replays bit for bit."""
+    rng = np.random.default_rng(70 + q)
+    As, ks, seeds = make_batch(rng, 12, kset=(4, 16, 20, 32, 48, 64, 100))
+    As[0] = low_rank(rng, 20000, 700)  # long K for A'Q
+    ks[0] = 64
+    Ad = [to_dev(A, dev) for A in As]
+    B = rla.RandSVDBatch(Ad, ks, seeds, power_its=q, orthogonalize=ortho, autotune=False,
+                         precision=rla.RLA_PREC_SPLIT_BF16)
+    B.run()
+    first = [s.cpu().numpy().copy() for s in B.S]
+    B.run()
+    for i, (A, k, sd) in enumerate(zip(As, ks, seeds)):
+        assert np.array_equal(first[i], B.S[i].cpu().numpy()), i
+        comp = rla.Gaussian(cardinality=rla.Right(), compression_dim=k, type=np.float32)
+        rec = rla.complete_compressor(comp, Ad[i], seed=sd)
+        ref = orc.randsvd(A.astype(np.float64), oracle_recipe(orc, rec), q=q, orthogonalize=ortho)
+        S_b = B.S[i].cpu().numpy()
+        assert rel_err(S_b, ref.S) < 1e-4, (i, k, rel_err(S_b, ref.S))
+        U = B.U[i].cpu().numpy().astype(np.float64)
+        V = B.V[i].cpu().numpy().astype(np.float64)
+        A64 = A.astype(np.float64)
+        nA = np.linalg.norm(A64)
+        e_b = np.linalg.norm(A64 - U @ (U.T @ A64)) / nA
+        e_r = np.linalg.norm(A64 - ref.U @ (ref.U.T @ A64)) / nA
+        assert abs(e_b - e_r) < 1e-4, (i, k, e_b, e_r)
+        assert rel_err((U * S_b) @ V.T, (ref.U * ref.S) @ ref.V.T) < 1e-4, i
