@@ -469,6 +469,157 @@ __global__ void __launch_bounds__(BJ_THREADS) block_jacobi_round_kernel(double *
     }
 }
 
+// Gram-based variant of the pair step (Float32 data, stopping tolerance >= 1e-13): the CTA
+// forms the FP64 Gram matrix G = Xp'Xp of the pair's c <= 16 columns once, measures the
+// relative off-diagonal on it (fresh dot products of the actual columns, as above), runs the
+// inner circle-method sweep on G itself -- per round the disjoint rotations update G's
+// columns, then its rows (two phases), and accumulate V = prod R -- and finally applies V to
+// the columns of X and J in one pass (Xp <- Xp V).  A rotation then costs O(c) operations on G
+// instead of O(l) on the columns; the next visit recomputes G from the columns, so rounding
+// in the updated G does not accumulate across visits.
+__global__ void __launch_bounds__(BJ_THREADS) block_jacobi_gram_round_kernel(double *X, double *J, int64_t l, int nbp,
+                                                                             int round, double tol,
+                                                                             unsigned long long *off) {
+    extern __shared__ __align__(16) double bj_smem[];
+    __shared__ unsigned long long vis_off;
+    __shared__ int cols[2 * BJ_B];
+    __shared__ double G[2 * BJ_B][2 * BJ_B + 1], V[2 * BJ_B][2 * BJ_B + 1];
+    __shared__ double rot[BJ_B][2];  // (cs, sn) of the round's rotations, 0/0 when skipped
+    constexpr int C2 = 2 * BJ_B;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int li = (int)l, ls = (li + 1) & ~1;
+    const int nb = (li + BJ_B - 1) / BJ_B;
+    int bi, bj;
+    tourney_pair(round, blockIdx.x, nbp, &bi, &bj);
+    int c = 0;
+    for (int q = 0; q < 2; ++q) {
+        const int blk = q == 0 ? bi : bj;
+        if (blk >= nb) continue;
+        const int c0 = blk * BJ_B, c1 = min(li, c0 + BJ_B);
+        for (int cc = c0; cc < c1; ++cc) {
+            if (tid == 0) cols[c] = cc;
+            ++c;
+        }
+    }
+    __syncthreads();
+    if (c < 2) return;
+    double *Xs = bj_smem, *Js = bj_smem + C2 * ls;
+    for (int idx = tid; idx < c * ls; idx += BJ_THREADS) {
+        const int q = idx / ls, r = idx - q * ls;
+        const int64_t g = r + (int64_t)cols[q] * l;
+        Xs[idx] = r < li ? X[g] : 0.0;
+        Js[idx] = r < li ? J[g] : 0.0;
+    }
+    __syncthreads();
+    // G = Xp'Xp: entries (a, b), a <= b, round-robin over the warps
+    const int npairs = c * (c + 1) / 2;
+    for (int e = warp; e < npairs; e += BJ_THREADS / 32) {
+        int a = 0, rem = e;
+        while (rem >= c - a) {
+            rem -= c - a;
+            ++a;
+        }
+        const int b = a + rem;
+        const double2 *xa = reinterpret_cast<const double2 *>(Xs + a * ls), *xb = reinterpret_cast<const double2 *>(Xs + b * ls);
+        double d = 0.0;
+        for (int k = lane; k < ls / 2; k += 32) {
+            const double2 u = xa[k], w = xb[k];
+            d = fma(u.x, w.x, fma(u.y, w.y, d));
+        }
+        d = warp_sum(d);
+        if (lane == 0) {
+            G[a][b] = d;
+            G[b][a] = d;
+        }
+    }
+    for (int idx = tid; idx < C2 * C2; idx += BJ_THREADS) V[idx / C2][idx % C2] = (idx / C2 == idx % C2) ? 1.0 : 0.0;
+    __syncthreads();
+    // largest relative off-diagonal of the columns as they arrive (fresh dot products)
+    if (warp == 0) {
+        double mx = 0.0;
+        for (int e = lane; e < c * c; e += 32) {
+            const int a = e / c, b = e % c;
+            if (a < b) {
+                const double nrm = sqrt(G[a][a] * G[b][b]);
+                if (G[a][b] != 0.0) mx = fmax(mx, nrm > 0.0 ? fabs(G[a][b]) / nrm : 1.0);
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(FULL, mx, o));
+        if (lane == 0) vis_off = (unsigned long long)__double_as_longlong(mx);
+    }
+    __syncthreads();
+    const int cp = c + (c & 1);
+    for (int r = 0; r < cp - 1; ++r) {
+        // phase A: angles from G, then G <- G R and V <- V R (columns i, j of each rotation)
+        const int p = warp;
+        int i = 0, j = 0;
+        bool act = false;
+        if (p < cp / 2) {
+            tourney_pair(r, p, cp, &i, &j);
+            if (i < c && j < c) {
+                if (i > j) {
+                    const int t = i;
+                    i = j;
+                    j = t;
+                }
+                const double a = G[i][i], b = G[j][j], g = G[i][j];
+                const double nrm = sqrt(a * b);
+                if (g != 0.0 && fabs(g) > tol * nrm) {
+                    const double zeta = (b - a) / (2.0 * g);
+                    const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+                    const double cs = 1.0 / sqrt(1.0 + t * t), sn = cs * t;
+                    act = true;
+                    __syncwarp();
+                    if (lane < c) {
+                        const double gi = G[lane][i], gj = G[lane][j];
+                        G[lane][i] = cs * gi - sn * gj;
+                        G[lane][j] = sn * gi + cs * gj;
+                        const double vi = V[lane][i], vj = V[lane][j];
+                        V[lane][i] = cs * vi - sn * vj;
+                        V[lane][j] = sn * vi + cs * vj;
+                    }
+                    if (lane == 0) {
+                        rot[p][0] = cs;
+                        rot[p][1] = sn;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        // phase B: G <- R'G (rows i, j of each rotation)
+        if (act && lane < c) {
+            const double cs = rot[p][0], sn = rot[p][1];
+            const double gi = G[i][lane], gj = G[j][lane];
+            G[i][lane] = cs * gi - sn * gj;
+            G[j][lane] = sn * gi + cs * gj;
+        }
+        __syncthreads();
+    }
+    if (tid == 0 && vis_off) atomicMax(off, vis_off);
+    // Xp <- Xp V, Jp <- Jp V, one row per thread
+    for (int row = tid; row < li; row += BJ_THREADS) {
+        double xr[C2], jr[C2];
+#pragma unroll
+        for (int q = 0; q < C2; ++q) {
+            xr[q] = q < c ? Xs[q * ls + row] : 0.0;
+            jr[q] = q < c ? Js[q * ls + row] : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < C2; ++q) {
+            if (q >= c) break;
+            double sx = 0.0, sj = 0.0;
+#pragma unroll
+            for (int k = 0; k < C2; ++k) {
+                sx = fma(xr[k], V[k][q], sx);
+                sj = fma(jr[k], V[k][q], sj);
+            }
+            const int64_t g = row + (int64_t)cols[q] * l;
+            X[g] = sx;
+            J[g] = sj;
+        }
+    }
+}
+
 // ---- Householder QR with LAPACK's conventions (dgeqr2 + dlarfg + dorg2r) --------------
 // Used when CholeskyQR breaks down (numerically rank-deficient blocks, e.g. a compression
 // dimension above rank(A)); the explicit Q it forms has LAPACK's column signs.
@@ -769,12 +920,15 @@ int jacobi_svd(rla_ctx *ctx, double *X, double *J, double *sigma, int64_t l, dou
         const int nb = (int)ceil_div(l, BJ_B), nbp = nb + (nb & 1);
         jacobi_identity_kernel<<<ceil_div_i(l * l, 256), 256, 0, ctx->stream>>>(J, l);
         RLA_TRY(check_launch(ctx, "jacobi_identity"));
-        RLA_CUDA_TRY(ctx, set_smem_max(block_jacobi_round_kernel));
+        // Float32 data (tolerance >= 1e-13): inner rotations on the pair's Gram matrix
+        const bool gram = tol >= 1e-13;
+        auto kern = gram ? block_jacobi_gram_round_kernel : block_jacobi_round_kernel;
+        RLA_CUDA_TRY(ctx, set_smem_max(kern));
         unsigned long long *off = reinterpret_cast<unsigned long long *>(work + 2 * l * l);
         for (int sweep = 0; sweep < 40; ++sweep) {
             RLA_CUDA_TRY(ctx, cudaMemsetAsync(off, 0, sizeof(unsigned long long), ctx->stream));
             for (int r = 0; r < nbp - 1; ++r)
-                block_jacobi_round_kernel<<<nbp / 2, BJ_THREADS, smem, ctx->stream>>>(X, J, l, nbp, r, tol, off);
+                kern<<<nbp / 2, BJ_THREADS, smem, ctx->stream>>>(X, J, l, nbp, r, tol, off);
             RLA_TRY(check_launch(ctx, "block_jacobi_round"));
             unsigned long long h = 0;
             RLA_CUDA_TRY(ctx, cudaMemcpyAsync(&h, off, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
