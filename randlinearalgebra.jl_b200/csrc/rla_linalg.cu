@@ -179,14 +179,11 @@ __global__ void __launch_bounds__(CB_THREADS) chol_blocked_kernel(double *G, int
     if (tid == 0) *breakdown = bad;
 }
 
-// Rinv = R^-1 for upper-triangular R: one warp per column j solves R x = e_j by back
-// substitution, x staged in shared memory (wpc warps per CTA).
 // Column j of R^-1 (R upper triangular, l x l, ld l) by back substitution in column form:
 // x = e_j; for i = j .. 0: x_i *= 1/R_ii, then x_r -= x_i R_ri for r < i.  Each step reads
-// column i of R (contiguous), one warp per column of the inverse, x and the reciprocal
-// diagonal in shared memory.  With MT > 0 (l <= 32*MT) the columns two steps ahead are
-// loaded into registers while the current one is applied.
-template <int MT>
+// column i of R (contiguous), one warp per column of the inverse (wpc warps per CTA), x and
+// the reciprocal diagonal in shared memory.  Used for orders too large for the staged
+// variant below.
 __global__ void __launch_bounds__(256) tri_inv_upper_kernel(const double *R, int64_t l, double *Ri, int wpc) {
     extern __shared__ double xs_all[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -198,49 +195,88 @@ __global__ void __launch_bounds__(256) tri_inv_upper_kernel(const double *R, int
     double *x = xs_all + (int64_t)wib * l;
     for (int64_t i = lane; i <= j; i += 32) x[i] = i == j ? 1.0 : 0.0;
     __syncwarp();
-    if constexpr (MT > 0) {
-        // ring of three columns: r0 = column i, r1 = column i-1, r2 = column i-2
-        double r0[MT], r1[MT], r2[MT];
-        auto load = [&](int64_t col, double (&dst)[MT]) {
-#pragma unroll
-            for (int t = 0; t < MT; ++t) {
-                const int64_t r = lane + 32 * t;
-                dst[t] = (col >= 0 && r < col) ? R[r + col * l] : 0.0;
-            }
-        };
-        load(j, r0);
-        load(j - 1, r1);
-        for (int64_t i = j; i >= 0; --i) {
-            load(i - 2, r2);
-            const double xi = x[i] * dinv[i];
-            __syncwarp();
-            if (lane == 0) x[i] = xi;
-#pragma unroll
-            for (int t = 0; t < MT; ++t) {
-                const int64_t r = lane + 32 * t;
-                if (r < i) x[r] = fma(-xi, r0[t], x[r]);
-            }
-            __syncwarp();
-#pragma unroll
-            for (int t = 0; t < MT; ++t) {
-                r0[t] = r1[t];
-                r1[t] = r2[t];
-            }
-        }
-    } else {
-        for (int64_t i = j; i >= 0; --i) {
-            const double xi = x[i] * dinv[i];
-            __syncwarp();
-            if (lane == 0) x[i] = xi;
-            const double *ri = R + i * l;
-            for (int64_t r = lane; r < i; r += 32) x[r] = fma(-xi, ri[r], x[r]);
-            __syncwarp();
-        }
+    for (int64_t i = j; i >= 0; --i) {
+        const double xi = x[i] * dinv[i];
+        __syncwarp();
+        if (lane == 0) x[i] = xi;
+        const double *ri = R + i * l;
+        for (int64_t r = lane; r < i; r += 32) x[r] = fma(-xi, ri[r], x[r]);
+        __syncwarp();
     }
     double *out = Ri + j * l;
     for (int64_t i = lane; i < l; i += 32) out[i] = i <= j ? x[i] : 0.0;
 }
 
+
+// The same back substitution with the columns of R staged in shared memory: the warps of a
+// CTA take consecutive columns j of the inverse and walk i together, so column i of R is read
+// from global memory once per CTA, TI_CH columns at a time by cp.async into one half of a
+// two-chunk ring while the warps work on the other half (two barriers per chunk instead of
+// an L2 round trip per step).
+constexpr int TI_WARPS = 8, TI_CH = 16;
+
+__device__ __forceinline__ void cp_async8(double *dst, const double *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+__global__ void __launch_bounds__(TI_WARPS * 32) tri_inv_ring_kernel(const double *R, int64_t l, double *Ri) {
+    extern __shared__ __align__(16) double ti_sm[];
+    const int li = (int)l;
+    double *ring = ti_sm;                  // [2][TI_CH][l]: column q of a chunk at q*l
+    double *xs = ring + 2 * TI_CH * li;    // [TI_WARPS][l]: the warps' columns x
+    double *dinv = xs + TI_WARPS * li;     // [l]
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int j0 = blockIdx.x * TI_WARPS, j = j0 + warp;
+    const int j_hi = min(li, j0 + TI_WARPS) - 1, c_hi = j_hi / TI_CH;
+    // chunk c (columns c*TI_CH .. c*TI_CH + TI_CH - 1, rows above the diagonal) into half h
+    auto issue = [&](int c, int h) {
+        if (c >= 0) {
+            double *dst = ring + h * TI_CH * li;
+            for (int q = 0; q < TI_CH; ++q) {
+                const int i = c * TI_CH + q;
+                if (i > j_hi) break;
+                for (int r = tid; r < i; r += TI_WARPS * 32) cp_async8(dst + q * li + r, R + r + (int64_t)i * l);
+            }
+        }
+        cp_async_commit();
+    };
+    issue(c_hi, 0);
+    issue(c_hi - 1, 1);
+    for (int i = tid; i <= j_hi; i += TI_WARPS * 32) dinv[i] = 1.0 / R[i + (int64_t)i * l];
+    double *x = xs + warp * li;
+    if (j < li)
+        for (int r = lane; r <= j; r += 32) x[r] = r == j ? 1.0 : 0.0;
+    for (int k = 0, c = c_hi; c >= 0; ++k, --c) {
+        cp_async_wait<1>();  // every chunk but the newest has landed
+        __syncthreads();
+        const double *cols = ring + (k & 1) * TI_CH * li;
+        if (j < li) {
+            for (int q = TI_CH - 1; q >= 0; --q) {
+                const int i = c * TI_CH + q;
+                if (i > j) continue;
+                const double xi = x[i] * dinv[i];
+                __syncwarp();
+                if (lane == 0) x[i] = xi;
+                const double *ci = cols + q * li;
+                for (int r = lane; r < i; r += 32) x[r] = fma(-xi, ci[r], x[r]);
+                __syncwarp();
+            }
+        }
+        __syncthreads();      // every warp is done with half (k & 1)
+        issue(c - 2, k & 1);  // chunk k + 2 takes its place
+    }
+    cp_async_wait<0>();
+    if (j < li) {
+        double *out = Ri + (int64_t)j * l;
+        for (int r = lane; r < li; r += 32) out[r] = r <= j ? x[r] : 0.0;
+    }
+}
 
 // Circle-method pairing: round r (0..n2-2), pair p (0..n2/2-1) over players 0..n2-1.
 __device__ inline void tourney_pair(int r, int p, int n2, int *i, int *j) {
@@ -313,53 +349,47 @@ __global__ void __launch_bounds__(1024) jacobi_kernel(double *X, double *J, doub
 }
 
 // Column norms -> sigma, columns sorted by descending sigma (stable), X normalised, J
-// permuted alongside.  work: 2*l*l + 2*l doubles.
-__global__ void __launch_bounds__(1024) jacobi_finish_kernel(double *X, double *J, double *sigma, int64_t l,
-                                                             double *work) {
-    __shared__ int perm_done;
+// permuted alongside.  work: 2*l*l + 2*l doubles.  jacobi_rank_kernel (one CTA) forms the
+// norms and the permutation -- the rank of column c is the number of columns with a larger
+// norm plus the earlier ones with an equal norm (NaN norms sort last) -- and
+// jacobi_permute_kernel (one CTA per output column) writes the permuted columns to work.
+__global__ void __launch_bounds__(1024) jacobi_rank_kernel(const double *X, double *sigma, int64_t l, double *work) {
     const int tid = threadIdx.x, nt = blockDim.x;
     const int lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
-    // column norms
+    double *sg = work + 2 * l * l;
+    int *perm = reinterpret_cast<int *>(work + 2 * l * l + l);
     for (int c = warp; c < l; c += nwarps) {
         const double *xc = X + (int64_t)c * l;
         double a = 0;
         for (int64_t k = lane; k < l; k += 32) a += xc[k] * xc[k];
         a = warp_sum(a);
-        if (lane == 0) work[2 * l * l + c] = sqrt(a);
+        if (lane == 0) sg[c] = sqrt(a);
     }
     __syncthreads();
-    // descending order (stable), one thread
-    int *perm = reinterpret_cast<int *>(work + 2 * l * l + l);
-    if (tid == 0) {
-        const double *sg = work + 2 * l * l;
-        for (int64_t c = 0; c < l; ++c) perm[c] = (int)c;
-        for (int64_t a = 1; a < l; ++a) {
-            int v = perm[a];
-            int64_t b = a - 1;
-            while (b >= 0 && sg[perm[b]] < sg[v]) {
-                perm[b + 1] = perm[b];
-                --b;
-            }
-            perm[b + 1] = v;
+    for (int64_t c = tid; c < l; c += nt) {
+        const double v = sg[c], kv = isnan(v) ? -1.0 : v;
+        int64_t rank = 0;
+        for (int64_t d = 0; d < l; ++d) {
+            const double w = sg[d], kw = isnan(w) ? -1.0 : w;
+            rank += (kw > kv) || (kw == kv && d < c);
         }
-        perm_done = 1;
+        perm[rank] = (int)c;
+        sigma[rank] = v;
     }
-    __syncthreads();
+}
+
+__global__ void __launch_bounds__(256) jacobi_permute_kernel(const double *X, const double *J, int64_t l,
+                                                             double *work) {
     const double *sg = work + 2 * l * l;
+    const int *perm = reinterpret_cast<const int *>(work + 2 * l * l + l);
     double *Xt = work, *Jt = work + l * l;
-    for (int64_t idx = tid; idx < l * l; idx += nt) {
-        const int64_t r = idx % l, c = idx / l;
-        const int src = perm[c];
-        const double sv = sg[src];
-        Xt[idx] = sv > 0.0 ? X[r + (int64_t)src * l] / sv : 0.0;
-        Jt[idx] = J[r + (int64_t)src * l];
+    const int64_t c = blockIdx.x;
+    const int src = perm[c];
+    const double sv = sg[src];
+    for (int64_t r = threadIdx.x; r < l; r += blockDim.x) {
+        Xt[r + c * l] = sv > 0.0 ? X[r + (int64_t)src * l] / sv : 0.0;
+        Jt[r + c * l] = J[r + (int64_t)src * l];
     }
-    __syncthreads();
-    for (int64_t idx = tid; idx < l * l; idx += nt) {
-        X[idx] = Xt[idx];
-        J[idx] = Jt[idx];
-    }
-    for (int64_t c = tid; c < l; c += nt) sigma[c] = sg[perm[c]];
 }
 
 
@@ -469,156 +499,208 @@ __global__ void __launch_bounds__(BJ_THREADS) block_jacobi_round_kernel(double *
     }
 }
 
-// Gram-based variant of the pair step (Float32 data, stopping tolerance >= 1e-13): the CTA
-// forms the FP64 Gram matrix G = Xp'Xp of the pair's c <= 16 columns once, measures the
-// relative off-diagonal on it (fresh dot products of the actual columns, as above), runs the
-// inner circle-method sweep on G itself -- per round the disjoint rotations update G's
-// columns, then its rows (two phases), and accumulate V = prod R -- and finally applies V to
-// the columns of X and J in one pass (Xp <- Xp V).  A rotation then costs O(c) operations on G
-// instead of O(l) on the columns; the next visit recomputes G from the columns, so rounding
-// in the updated G does not accumulate across visits.
-__global__ void __launch_bounds__(BJ_THREADS) block_jacobi_gram_round_kernel(double *X, double *J, int64_t l, int nbp,
-                                                                             int round, double tol,
-                                                                             unsigned long long *off) {
+// Gram-based variant of the pair step (Float32 data, stopping tolerance >= 1e-13).  The CTA
+// forms the FP64 Gram matrix G = Xp'Xp of the pair's 16 columns on the FP64 tensor cores
+// (mma.m8n8k4.f64), measures the relative off-diagonal on it (fresh dot products of the
+// actual columns), runs the pair's rotations on G itself -- a rotation costs O(16) operations
+// on G instead of O(l) on the columns -- accumulates V = prod R, and applies V to the columns
+// of X and J once (Xp <- Xp V, Jp <- Jp V, again on the tensor cores).  The next visit
+// recomputes G from the columns, so rounding in the updated G does not accumulate.
+//
+// Ordering: every pair of columns is rotated once per sweep.  The 64 cross pairs of the two
+// blocks (a, 8 + (a + r) mod 8), r = 0..7, are done at the visit of the two blocks; the pairs
+// inside a block (circle method, 7 rounds) are done in outer round 0, where every block is
+// visited once.  An inner round applies 8 disjoint rotations, G <- R'GR and V <- VR, with one
+// thread per entry of G and V and one barrier.
+constexpr int BJX_THREADS = 256;  // 16 x 16: thread (x, y) owns G(x, y) and V(x, y)
+
+__device__ __forceinline__ void dmma_f64(double (&d)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d[0]), "+d"(d[1])
+                 : "d"(a), "d"(b));
+}
+
+// Partner of index x (0..15) in inner round r: inside each 8-index half by the circle method
+// (intra), or across the halves, pairs (a, 8 + (a + r) mod 8).
+__device__ __forceinline__ int bjx_partner(int x, int r, bool intra) {
+    if (intra) {
+        const int u = x & 7, r7 = r % 7;
+        const int p = u == 7 ? r7 : (u == r7 ? 7 : (2 * r7 - u + 14) % 7);
+        return (x & 8) | p;
+    }
+    return x < 8 ? 8 + ((x + r) & 7) : ((x - 8 - r) & 7);
+}
+
+// Rotation R = [cs sn; -sn cs] on columns (i, j) that makes them orthogonal, from their Gram
+// entries a = |x_i|^2, b = |x_j|^2, g = x_i'x_j: tan = sign(b - a) 2g / (|b - a| +
+// sqrt((b - a)^2 + 4g^2)), the smaller root of g t^2 + (b - a) t - g = 0 (Rutishauser's form;
+// no overflow for Gram entries of Float32 data).  Identity when g^2 <= tol^2 a b.
+__device__ __forceinline__ bool bjx_rot(double a, double b, double g, double tol, double &cs, double &sn) {
+    if (g == 0.0 || g * g <= tol * tol * a * b) {
+        cs = 1.0;
+        sn = 0.0;
+        return false;
+    }
+    const double d = b - a;
+    const double t = (d >= 0.0 ? 2.0 * g : -2.0 * g) / (fabs(d) + sqrt(fma(d, d, 4.0 * g * g)));
+    cs = rsqrt(fma(t, t, 1.0));
+    sn = cs * t;
+    return true;
+}
+
+__global__ void __launch_bounds__(BJX_THREADS) block_jacobi_gram_round_kernel(double *X, double *J, int64_t l, int nbp,
+                                                                              int round, double tol,
+                                                                              unsigned long long *off) {
     extern __shared__ __align__(16) double bj_smem[];
-    __shared__ unsigned long long vis_off;
-    __shared__ int cols[2 * BJ_B];
-    __shared__ double G[2 * BJ_B][2 * BJ_B + 1], V[2 * BJ_B][2 * BJ_B + 1];
-    __shared__ double rot[BJ_B][2];  // (cs, sn) of the round's rotations, 0/0 when skipped
-    constexpr int C2 = 2 * BJ_B;
+    __shared__ double G[2][16][17], V[2][16][17];  // ping-pong across inner rounds
+    __shared__ double part[8][3][64];              // per-warp partial Gram tiles
+    __shared__ double wmax[8];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int li = (int)l, ls = (li + 1) & ~1;
+    const int li = (int)l, kp = (li + 31) & ~31, ls = kp + 4;  // ls = 4 mod 16: conflict-free fragments
     const int nb = (li + BJ_B - 1) / BJ_B;
     int bi, bj;
     tourney_pair(round, blockIdx.x, nbp, &bi, &bj);
-    int c = 0;
-    for (int q = 0; q < 2; ++q) {
-        const int blk = q == 0 ? bi : bj;
-        if (blk >= nb) continue;
-        const int c0 = blk * BJ_B, c1 = min(li, c0 + BJ_B);
-        for (int cc = c0; cc < c1; ++cc) {
-            if (tid == 0) cols[c] = cc;
-            ++c;
+    const bool vi = bi < nb, vj = bj < nb;
+    if ((!vi && !vj) || (round > 0 && !(vi && vj))) return;  // nothing to rotate in this visit
+    auto col_of = [&](int s) -> int {
+        const int blk = s < 8 ? bi : bj, c = blk * BJ_B + (s & 7);
+        return (blk < nb && c < li) ? c : -1;
+    };
+    double *Xs = bj_smem, *Js = bj_smem + 16 * ls;
+    int cs_[16];
+#pragma unroll
+    for (int s = 0; s < 16; ++s) cs_[s] = col_of(s);
+    // all 32 loads of a row in flight before the shared stores (a store between two loads
+    // would order them: one L2 round trip per element)
+    for (int r0 = 0; r0 < kp; r0 += BJX_THREADS) {
+        const int r = r0 + tid;
+        double vx[16], vj[16];
+#pragma unroll
+        for (int s = 0; s < 16; ++s) {
+            const bool in = cs_[s] >= 0 && r < li;
+            vx[s] = in ? X[r + (int64_t)cs_[s] * l] : 0.0;
+            vj[s] = in ? J[r + (int64_t)cs_[s] * l] : 0.0;
         }
-    }
-    __syncthreads();
-    if (c < 2) return;
-    double *Xs = bj_smem, *Js = bj_smem + C2 * ls;
-    for (int idx = tid; idx < c * ls; idx += BJ_THREADS) {
-        const int q = idx / ls, r = idx - q * ls;
-        const int64_t g = r + (int64_t)cols[q] * l;
-        Xs[idx] = r < li ? X[g] : 0.0;
-        Js[idx] = r < li ? J[g] : 0.0;
-    }
-    __syncthreads();
-    // G = Xp'Xp: entries (a, b), a <= b, round-robin over the warps
-    const int npairs = c * (c + 1) / 2;
-    for (int e = warp; e < npairs; e += BJ_THREADS / 32) {
-        int a = 0, rem = e;
-        while (rem >= c - a) {
-            rem -= c - a;
-            ++a;
-        }
-        const int b = a + rem;
-        const double2 *xa = reinterpret_cast<const double2 *>(Xs + a * ls), *xb = reinterpret_cast<const double2 *>(Xs + b * ls);
-        double d = 0.0;
-        for (int k = lane; k < ls / 2; k += 32) {
-            const double2 u = xa[k], w = xb[k];
-            d = fma(u.x, w.x, fma(u.y, w.y, d));
-        }
-        d = warp_sum(d);
-        if (lane == 0) {
-            G[a][b] = d;
-            G[b][a] = d;
-        }
-    }
-    for (int idx = tid; idx < C2 * C2; idx += BJ_THREADS) V[idx / C2][idx % C2] = (idx / C2 == idx % C2) ? 1.0 : 0.0;
-    __syncthreads();
-    // largest relative off-diagonal of the columns as they arrive (fresh dot products)
-    if (warp == 0) {
-        double mx = 0.0;
-        for (int e = lane; e < c * c; e += 32) {
-            const int a = e / c, b = e % c;
-            if (a < b) {
-                const double nrm = sqrt(G[a][a] * G[b][b]);
-                if (G[a][b] != 0.0) mx = fmax(mx, nrm > 0.0 ? fabs(G[a][b]) / nrm : 1.0);
+        if (r < kp) {
+#pragma unroll
+            for (int s = 0; s < 16; ++s) {
+                Xs[s * ls + r] = vx[s];
+                Js[s * ls + r] = vj[s];
             }
         }
-        for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(FULL, mx, o));
-        if (lane == 0) vis_off = (unsigned long long)__double_as_longlong(mx);
     }
     __syncthreads();
-    const int cp = c + (c & 1);
-    for (int r = 0; r < cp - 1; ++r) {
-        // phase A: angles from G, then G <- G R and V <- V R (columns i, j of each rotation)
-        const int p = warp;
-        int i = 0, j = 0;
-        bool act = false;
-        if (p < cp / 2) {
-            tourney_pair(r, p, cp, &i, &j);
-            if (i < c && j < c) {
-                if (i > j) {
-                    const int t = i;
-                    i = j;
-                    j = t;
-                }
-                const double a = G[i][i], b = G[j][j], g = G[i][j];
-                const double nrm = sqrt(a * b);
-                if (g != 0.0 && fabs(g) > tol * nrm) {
-                    const double zeta = (b - a) / (2.0 * g);
-                    const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-                    const double cs = 1.0 / sqrt(1.0 + t * t), sn = cs * t;
-                    act = true;
-                    __syncwarp();
-                    if (lane < c) {
-                        const double gi = G[lane][i], gj = G[lane][j];
-                        G[lane][i] = cs * gi - sn * gj;
-                        G[lane][j] = sn * gi + cs * gj;
-                        const double vi = V[lane][i], vj = V[lane][j];
-                        V[lane][i] = cs * vi - sn * vj;
-                        V[lane][j] = sn * vi + cs * vj;
-                    }
-                    if (lane == 0) {
-                        rot[p][0] = cs;
-                        rot[p][1] = sn;
-                    }
-                }
+    // G = Xp'Xp: warp w sums rows [w kp/8, (w+1) kp/8); the fragment of columns 0..7 (8..15)
+    // serves as both the A operand (Xp') and the B operand (Xp).
+    {
+        double acc[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+        const int k_lo = warp * (kp / 8), k_hi = k_lo + kp / 8;
+        for (int k0 = k_lo; k0 < k_hi; k0 += 4) {
+            const int kk = k0 + (lane & 3);
+            const double f0 = Xs[(lane >> 2) * ls + kk], f1 = Xs[(8 + (lane >> 2)) * ls + kk];
+            dmma_f64(acc[0], f0, f0);
+            dmma_f64(acc[1], f0, f1);
+            dmma_f64(acc[2], f1, f1);
+        }
+#pragma unroll
+        for (int t = 0; t < 3; ++t) {
+            part[warp][t][(lane >> 2) * 8 + 2 * (lane & 3)] = acc[t][0];
+            part[warp][t][(lane >> 2) * 8 + 2 * (lane & 3) + 1] = acc[t][1];
+        }
+    }
+    __syncthreads();
+    if (tid < 192) {
+        const int t = tid >> 6, e = tid & 63, r = e >> 3, c = e & 7;
+        double s = 0.0;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) s += part[w][t][e];
+        if (t == 0) {
+            G[0][r][c] = s;
+        } else if (t == 1) {
+            G[0][r][8 + c] = s;
+            G[0][8 + c][r] = s;
+        } else {
+            G[0][8 + r][8 + c] = s;
+        }
+    }
+    const int x = tid >> 4, y = tid & 15;
+    V[0][x][y] = x == y ? 1.0 : 0.0;
+    __syncthreads();
+    // largest relative off-diagonal (squared) over the pairs this visit rotates
+    {
+        double m2 = 0.0;
+        if (x < y && (round == 0 || (x < 8 && y >= 8))) {
+            const double a = G[0][x][x], b = G[0][y][y], g = G[0][x][y];
+            if (g != 0.0 && a * b > 0.0) m2 = g * g / (a * b);
+        }
+        for (int o = 16; o > 0; o >>= 1) m2 = fmax(m2, __shfl_xor_sync(FULL, m2, o));
+        if (lane == 0) wmax[warp] = m2;
+    }
+    int cur = 0;
+    const int n_intra = round == 0 ? 7 : 0, n_in = n_intra + ((vi && vj) ? 8 : 0);
+    for (int r = 0; r < n_in; ++r) {
+        const bool intra = r < n_intra;
+        const int rr = intra ? r : r - n_intra;
+        // lanes 0..15 of every warp: the rotation of the pair holding index `lane`, as the
+        // diagonal entry e and the partner's coefficient f of that column of R
+        double e = 1.0, f = 0.0;
+        if (lane < 16) {
+            const int p = bjx_partner(lane, rr, intra), i = min(lane, p), j = max(lane, p);
+            double cs, sn;
+            if (bjx_rot(G[cur][i][i], G[cur][j][j], G[cur][i][j], tol, cs, sn)) {
+                e = cs;
+                f = lane == i ? -sn : sn;
             }
         }
+        const double ex = __shfl_sync(FULL, e, x), fx = __shfl_sync(FULL, f, x);
+        const double ey = __shfl_sync(FULL, e, y), fy = __shfl_sync(FULL, f, y);
+        const int xp = bjx_partner(x, rr, intra), yp = bjx_partner(y, rr, intra);
+        // (R'GR)(x, y), summed as (t1 + t4) + (t2 + t3) so that (y, x) rounds identically
+        const double t1 = (ex * ey) * G[cur][x][y], t4 = (fx * fy) * G[cur][xp][yp];
+        const double t2 = (ex * fy) * G[cur][x][yp], t3 = (fx * ey) * G[cur][xp][y];
+        G[cur ^ 1][x][y] = (t1 + t4) + (t2 + t3);
+        V[cur ^ 1][x][y] = ey * V[cur][x][y] + fy * V[cur][x][yp];
+        cur ^= 1;
         __syncthreads();
-        // phase B: G <- R'G (rows i, j of each rotation)
-        if (act && lane < c) {
-            const double cs = rot[p][0], sn = rot[p][1];
-            const double gi = G[i][lane], gj = G[j][lane];
-            G[i][lane] = cs * gi - sn * gj;
-            G[j][lane] = sn * gi + cs * gj;
-        }
-        __syncthreads();
     }
-    if (tid == 0 && vis_off) atomicMax(off, vis_off);
-    // Xp <- Xp V, Jp <- Jp V, one row per thread
-    for (int row = tid; row < li; row += BJ_THREADS) {
-        double xr[C2], jr[C2];
+    if (tid == 0) {
+        double m2 = 0.0;
+        for (int w = 0; w < 8; ++w) m2 = fmax(m2, wmax[w]);
+        if (m2 > 0.0) atomicMax(off, (unsigned long long)__double_as_longlong(sqrt(m2)));
+    }
+    // Xp <- Xp V, Jp <- Jp V: 8-row tiles round-robin over the warps, k = the 16 columns
+    double vb[4][2];
 #pragma unroll
-        for (int q = 0; q < C2; ++q) {
-            xr[q] = q < c ? Xs[q * ls + row] : 0.0;
-            jr[q] = q < c ? Js[q * ls + row] : 0.0;
-        }
+    for (int ks = 0; ks < 4; ++ks)
 #pragma unroll
-        for (int q = 0; q < C2; ++q) {
-            if (q >= c) break;
-            double sx = 0.0, sj = 0.0;
+        for (int nt = 0; nt < 2; ++nt) vb[ks][nt] = V[cur][4 * ks + (lane & 3)][8 * nt + (lane >> 2)];
+    const int nmt = (li + 7) >> 3;
+    for (int mt = warp; mt < nmt; mt += 8) {
+        const int row = 8 * mt + (lane >> 2);
 #pragma unroll
-            for (int k = 0; k < C2; ++k) {
-                sx = fma(xr[k], V[k][q], sx);
-                sj = fma(jr[k], V[k][q], sj);
+        for (int w = 0; w < 2; ++w) {
+            const double *S = w ? Js : Xs;
+            double *D = w ? J : X;
+            double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll
+            for (int ks = 0; ks < 4; ++ks) {
+                const double a = S[(4 * ks + (lane & 3)) * ls + 8 * mt + (lane >> 2)];
+                dmma_f64(acc[0], a, vb[ks][0]);
+                dmma_f64(acc[1], a, vb[ks][1]);
             }
-            const int64_t g = row + (int64_t)cols[q] * l;
-            X[g] = sx;
-            J[g] = sj;
+            if (row < li) {
+#pragma unroll
+                for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+                    for (int q = 0; q < 2; ++q) {
+                        const int c = col_of(8 * nt + 2 * (lane & 3) + q);
+                        if (c >= 0) D[row + (int64_t)c * l] = acc[nt][q];
+                    }
+            }
         }
     }
 }
+
 
 // ---- Householder QR with LAPACK's conventions (dgeqr2 + dlarfg + dorg2r) --------------
 // Used when CholeskyQR breaks down (numerically rank-deficient blocks, e.g. a compression
@@ -790,29 +872,59 @@ __global__ void __launch_bounds__(MP_THREADS) chol_panel_kernel(double *G, int64
         }
         if (tid == 0 && bad) *breakdown = 1;
     }
-    // panel rows X = R_pp^-T G(p, cols): thread = one column of the trailing part, solved
-    // column-oriented (y_t = y_t / r_tt, then y_q -= r_tq y_t for q > t) so that the
-    // updates of one step are independent.
-    const int64_t c0 = p + pb;
-    const int64_t col = c0 + (int64_t)blockIdx.x * MP_THREADS + tid;
-    if (col >= l) return;
-    double y[MB];
+    // panel rows X = R_pp^-T G(p, cols) for the CTA's <= 256 trailing columns: staged in
+    // shared memory (Ys[t][c], ld MP_THREADS + 1) so that G is read and written along its
+    // columns; then thread c solves column c, column-oriented (y_t = y_t / r_tt, then
+    // y_q -= r_tq y_t for q > t) so that the updates of one step are independent.
+    const int64_t cb = p + pb + (int64_t)blockIdx.x * MP_THREADS;
+    const int nc = (int)max((int64_t)0, min((int64_t)MP_THREADS, l - cb));
+    if (nc == 0) return;
+    constexpr int LDY = MP_THREADS + 1;
+    double *Ys = rowbuf + 2 * MB;
+    const int lane = tid & 31, warp = tid >> 5;
+    // 16 loads per lane in flight before the shared stores
+    for (int c0 = warp; c0 < nc; c0 += 8 * (MP_THREADS / 32)) {
+        double v[8][2];
 #pragma unroll
-    for (int t = 0; t < MB; ++t) y[t] = t < pb ? G[(p + t) + col * l] : 0.0;
+        for (int u = 0; u < 8; ++u)
 #pragma unroll
-    for (int t = 0; t < MB; ++t) {
-        if (t < pb) {
-            y[t] *= rinv[t];
+            for (int h = 0; h < 2; ++h) {
+                const int c = c0 + u * (MP_THREADS / 32), t = lane + 32 * h;
+                v[u][h] = (c < nc && t < pb) ? G[(p + t) + (cb + c) * l] : 0.0;
+            }
 #pragma unroll
-            for (int q = t + 1; q < MB; ++q) y[q] -= R[t][q] * y[t];
-        }
+        for (int u = 0; u < 8; ++u)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int c = c0 + u * (MP_THREADS / 32), t = lane + 32 * h;
+                if (c < nc && t < pb) Ys[t * LDY + c] = v[u][h];
+            }
     }
+    __syncthreads();
+    if (tid < nc) {
+        double y[MB];
 #pragma unroll
-    for (int t = 0; t < MB; ++t)
-        if (t < pb) {
-            G[(p + t) + col * l] = y[t];
-            G[col + (p + t) * l] = 0.0;
+        for (int t = 0; t < MB; ++t) y[t] = t < pb ? Ys[t * LDY + tid] : 0.0;
+#pragma unroll
+        for (int t = 0; t < MB; ++t) {
+            if (t < pb) {
+                y[t] *= rinv[t];
+#pragma unroll
+                for (int q = t + 1; q < MB; ++q) y[q] -= R[t][q] * y[t];
+            }
         }
+#pragma unroll
+        for (int t = 0; t < MB; ++t)
+            if (t < pb) Ys[t * LDY + tid] = y[t];
+    }
+    __syncthreads();
+    for (int c = warp; c < nc; c += MP_THREADS / 32)
+        for (int t = lane; t < pb; t += 32) G[(p + t) + (cb + c) * l] = Ys[t * LDY + c];
+    // the mirrored lower entries G(cols, p:p+pb), along columns of G
+    for (int e = tid; e < nc * pb; e += MP_THREADS) {
+        const int t = e / nc, c = e - t * nc;
+        G[(cb + c) + (p + t) * l] = 0.0;
+    }
 }
 
 __global__ void __launch_bounds__(256) chol_syrk_kernel(double *G, int64_t l, int64_t p, int pb) {
@@ -828,10 +940,22 @@ __global__ void __launch_bounds__(256) chol_syrk_kernel(double *G, int64_t l, in
     const int ti = idx;
     const int64_t c0 = p + pb, I0 = c0 + (int64_t)ti * MB, J0 = c0 + (int64_t)tj * MB;
     const int tid = threadIdx.x;
-    for (int e = tid; e < MB * MB; e += blockDim.x) {
-        const int t = e % MB, i = e / MB;
-        As[t][i] = (t < pb && I0 + i < l) ? G[(p + t) + (I0 + i) * l] : 0.0;
-        Bs[t][i] = (t < pb && J0 + i < l) ? G[(p + t) + (J0 + i) * l] : 0.0;
+    {
+        // all 32 loads of a thread in flight before the shared stores
+        constexpr int PER = MB * MB / 256;
+        double va[PER], vb[PER];
+#pragma unroll
+        for (int u = 0; u < PER; ++u) {
+            const int e = tid + 256 * u, t = e % MB, i = e / MB;
+            va[u] = (t < pb && I0 + i < l) ? G[(p + t) + (I0 + i) * l] : 0.0;
+            vb[u] = (t < pb && J0 + i < l) ? G[(p + t) + (J0 + i) * l] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < PER; ++u) {
+            const int e = tid + 256 * u, t = e % MB, i = e / MB;
+            As[t][i] = va[u];
+            Bs[t][i] = vb[u];
+        }
     }
     __syncthreads();
     const int tx = tid & 15, ty = tid >> 4;  // outputs (4tx + ii, 4ty + jj)
@@ -864,7 +988,7 @@ __global__ void __launch_bounds__(256) chol_syrk_kernel(double *G, int64_t l, in
 static int cholesky_upper_mc(rla_ctx *ctx, double *G, int64_t l, double shift, int *breakdown) {
     RLA_CUDA_TRY(ctx, cudaMemsetAsync(breakdown, 0, sizeof(int), ctx->stream));
     const size_t smem = sizeof(double) * 2 * MB * (MB + 1);
-    const size_t smem_panel = sizeof(double) * (MB * (MB + 2) + 3 * MB);
+    const size_t smem_panel = sizeof(double) * (MB * (MB + 2) + 3 * MB + (size_t)MB * (MP_THREADS + 1));
     RLA_CUDA_TRY(ctx, set_smem_max(chol_panel_kernel));
     RLA_CUDA_TRY(ctx, set_smem_max(chol_syrk_kernel));
     for (int64_t p = 0; p < l; p += MB) {
@@ -900,35 +1024,43 @@ int cholesky_upper(rla_ctx *ctx, double *G, int64_t l, double shift, int *breakd
 
 int tri_inv_upper(rla_ctx *ctx, const double *R, int64_t l, double *Rinv) {
     const int64_t per = sizeof(double) * std::max<int64_t>(l, 1);
+    const size_t ring_smem = (size_t)per * (2 * TI_CH + TI_WARPS + 1);
+    if (ring_smem <= (size_t)ctx->smem_optin - 1024) {
+        RLA_CUDA_TRY(ctx, set_smem_max(tri_inv_ring_kernel));
+        tri_inv_ring_kernel<<<ceil_div_i(l, TI_WARPS), TI_WARPS * 32, ring_smem, ctx->stream>>>(R, l, Rinv);
+        return check_launch(ctx, "tri_inv_ring");
+    }
     // per warp one column of x, plus the reciprocal diagonal shared by the CTA
     const int wpc = (int)std::max<int64_t>(1, std::min<int64_t>(8, (ctx->smem_optin - 1024) / per - 1));
     if (2 * per > ctx->smem_optin - 1024)
         return set_error(ctx, RLA_E_UNSUPPORTED, "triangular inverse of order %lld exceeds shared memory", (long long)l);
     const size_t smem = (size_t)per * (wpc + 1);
-    auto kern = l <= 128 ? tri_inv_upper_kernel<4> : (l <= 512 ? tri_inv_upper_kernel<16> : tri_inv_upper_kernel<0>);
-    RLA_CUDA_TRY(ctx, set_smem_max(kern));
-    kern<<<ceil_div_i(l, wpc), 32 * wpc, smem, ctx->stream>>>(R, l, Rinv, wpc);
+    RLA_CUDA_TRY(ctx, set_smem_max(tri_inv_upper_kernel));
+    tri_inv_upper_kernel<<<ceil_div_i(l, wpc), 32 * wpc, smem, ctx->stream>>>(R, l, Rinv, wpc);
     return check_launch(ctx, "tri_inv_upper");
 }
 
 int jacobi_svd(rla_ctx *ctx, double *X, double *J, double *sigma, int64_t l, double *work, double tol) {
-    const size_t smem = sizeof(double) * 4 * BJ_B * (size_t)((l + 1) & ~1);
-    if (l <= 2 * BJ_B || smem > (size_t)ctx->smem_optin - 2048) {
+    // Float32 data (tolerance >= 1e-13): the Gram-based pair step
+    const bool gram = tol >= 1e-13;
+    const size_t smem = gram ? sizeof(double) * 32 * (size_t)(((l + 31) & ~31) + 4)
+                             : sizeof(double) * 4 * BJ_B * (size_t)((l + 1) & ~1);
+    // the Gram kernel also holds 21 KB of static shared memory
+    if (l <= 2 * BJ_B || smem > (size_t)ctx->smem_optin - (gram ? 24576 : 2048)) {
         jacobi_kernel<<<1, 1024, 0, ctx->stream>>>(X, J, sigma, l, work, 60, tol);
         RLA_TRY(check_launch(ctx, "jacobi_svd"));
     } else {
         const int nb = (int)ceil_div(l, BJ_B), nbp = nb + (nb & 1);
         jacobi_identity_kernel<<<ceil_div_i(l * l, 256), 256, 0, ctx->stream>>>(J, l);
         RLA_TRY(check_launch(ctx, "jacobi_identity"));
-        // Float32 data (tolerance >= 1e-13): inner rotations on the pair's Gram matrix
-        const bool gram = tol >= 1e-13;
         auto kern = gram ? block_jacobi_gram_round_kernel : block_jacobi_round_kernel;
+        const int threads = gram ? BJX_THREADS : BJ_THREADS;
         RLA_CUDA_TRY(ctx, set_smem_max(kern));
         unsigned long long *off = reinterpret_cast<unsigned long long *>(work + 2 * l * l);
         for (int sweep = 0; sweep < 40; ++sweep) {
             RLA_CUDA_TRY(ctx, cudaMemsetAsync(off, 0, sizeof(unsigned long long), ctx->stream));
             for (int r = 0; r < nbp - 1; ++r)
-                kern<<<nbp / 2, BJ_THREADS, smem, ctx->stream>>>(X, J, l, nbp, r, tol, off);
+                kern<<<nbp / 2, threads, smem, ctx->stream>>>(X, J, l, nbp, r, tol, off);
             RLA_TRY(check_launch(ctx, "block_jacobi_round"));
             unsigned long long h = 0;
             RLA_CUDA_TRY(ctx, cudaMemcpyAsync(&h, off, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
@@ -938,8 +1070,12 @@ int jacobi_svd(rla_ctx *ctx, double *X, double *J, double *sigma, int64_t l, dou
             if (v <= tol) break;
         }
     }
-    jacobi_finish_kernel<<<1, 1024, 0, ctx->stream>>>(X, J, sigma, l, work);
-    return check_launch(ctx, "jacobi_finish");
+    jacobi_rank_kernel<<<1, 1024, 0, ctx->stream>>>(X, sigma, l, work);
+    jacobi_permute_kernel<<<(unsigned)l, 256, 0, ctx->stream>>>(X, J, l, work);
+    RLA_TRY(check_launch(ctx, "jacobi_finish"));
+    RLA_CUDA_TRY(ctx, cudaMemcpyAsync(X, work, sizeof(double) * l * l, cudaMemcpyDeviceToDevice, ctx->stream));
+    RLA_CUDA_TRY(ctx, cudaMemcpyAsync(J, work + l * l, sizeof(double) * l * l, cudaMemcpyDeviceToDevice, ctx->stream));
+    return RLA_OK;
 }
 
 }  // namespace rla

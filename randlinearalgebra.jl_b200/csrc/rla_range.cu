@@ -352,10 +352,10 @@ static int randsvd_t(rla_ctx *ctx, const rla_sketch *om, int64_t m, int64_t n, c
     own.ptrs.push_back(jw);
     // X = Rb' = Bt' Qb (l x l)
     RLA_TRY((gemm<double, double, double, double>(ctx, l, l, n, Bt, n, 1, Qb, n, 0, X, l, 1.0, 0.0)));
-    // Float32 data resolves singular triplets to about 1e-7: pairs orthogonal to 1e-12 are
+    // Float32 data resolves singular triplets to about 1e-7: pairs orthogonal to 1e-10 are
     // converged there (the last sweeps of the quadratic phase are skipped); Float64 data
     // keeps 1e-15
-    RLA_TRY(jacobi_svd(ctx, X, J, sig, l, jw, sizeof(T) == 4 ? 1e-12 : 1e-15));
+    RLA_TRY(jacobi_svd(ctx, X, J, sig, l, jw, sizeof(T) == 4 ? 1e-10 : 1e-15));
     // U = Q W, V = Qb J
     RLA_TRY((gemm<T, double, TO, double>(ctx, m, l, l, Q, m, 0, X, l, 0, U, ldu, 1.0, 0.0)));
     RLA_TRY((gemm<double, double, TO, double>(ctx, n, l, l, Qb, n, 0, J, l, 0, V, ldv, 1.0, 0.0)));
