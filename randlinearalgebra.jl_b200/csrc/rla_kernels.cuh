@@ -86,6 +86,12 @@ template <class T>
 int householder_q(rla_ctx *ctx, T *Y, int64_t m, int64_t l, int64_t ldy, double *tau);
 // Rinv = R^{-1} for upper-triangular R (l x l, ld l).
 int tri_inv_upper(rla_ctx *ctx, const double *R, int64_t l, double *Rinv);
+// Cholesky factor (into G: R upper, zero below) and Rinv = R^-1 together, blocked by 16 on the
+// FP64 tensor cores (l <= 384, see chol_inv_supported); *breakdown as cholesky_upper.  work
+// holds chol_inv_work_doubles(l) doubles.
+bool chol_inv_supported(const rla_ctx *ctx, int64_t l);
+size_t chol_inv_work_doubles(int64_t l);
+int chol_inv(rla_ctx *ctx, double *G, int64_t l, double shift, int *breakdown, double *Rinv, double *work);
 // One-sided Jacobi on X (l x l, ld l) with accumulated rotations J (initialised to I):
 // on return the columns of X are orthogonal, sigma[i] = ||X(:, i)||, columns sorted by
 // descending sigma, X(:, i) normalised, J permuted alongside.  `work` holds at least

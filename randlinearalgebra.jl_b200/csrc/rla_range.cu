@@ -114,6 +114,7 @@ template int gram_fp64<double>(rla_ctx *, const double *, int64_t, int64_t, int6
 
 struct OrthWork {
     double *G, *Rinv, *dscale, *diag, *hw;
+    double *cw = nullptr;  // chol_inv working copy (null: separate Cholesky and inverse)
     int *flag;
     void *tmp;  // rows x l of T
 };
@@ -137,7 +138,8 @@ static int orth(rla_ctx *ctx, T *Y, int64_t rows, int64_t l, int64_t ldy, OrthWo
         RLA_TRY(gram_fp64<T>(ctx, Y, rows, l, ldy, w.G));
         double shift = 0.0;
         RLA_TRY(equilibrate(ctx, w.G, l, w.dscale));
-        RLA_TRY(cholesky_upper(ctx, w.G, l, shift, w.flag));
+        if (w.cw) RLA_TRY(chol_inv(ctx, w.G, l, shift, w.flag, w.Rinv, w.cw));
+        else RLA_TRY(cholesky_upper(ctx, w.G, l, shift, w.flag));
         int bad = 0;
         RLA_CUDA_TRY(ctx, cudaMemcpyAsync(&bad, w.flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
         RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
@@ -153,14 +155,15 @@ static int orth(rla_ctx *ctx, T *Y, int64_t rows, int64_t l, int64_t ldy, OrthWo
             RLA_TRY(equilibrate(ctx, w.G, l, w.dscale));
             const double u = sizeof(T) == 4 ? 5.96e-8 : 1.11e-16;
             shift = 11.0 * ((double)rows * l + (double)l * (l + 1)) * u * (double)l;
-            RLA_TRY(cholesky_upper(ctx, w.G, l, shift, w.flag));
+            if (w.cw) RLA_TRY(chol_inv(ctx, w.G, l, shift, w.flag, w.Rinv, w.cw));
+            else RLA_TRY(cholesky_upper(ctx, w.G, l, shift, w.flag));
             RLA_CUDA_TRY(ctx, cudaMemcpyAsync(&bad, w.flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
             RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
             if (bad) return householder_q<T>(ctx, Y, rows, l, ldy, w.diag);
             shifted_done = true;
             passes = pass + 3;  // shifted pass followed by two plain passes
         }
-        RLA_TRY(tri_inv_upper(ctx, w.G, l, w.Rinv));
+        if (!w.cw) RLA_TRY(tri_inv_upper(ctx, w.G, l, w.Rinv));
         row_scale_kernel<<<ceil_div_i(l * l, 256), 256, 0, ctx->stream>>>(w.Rinv, l, w.dscale);
         RLA_TRY(check_launch(ctx, "row_scale"));
         RLA_TRY((gemm<T, double, T, double>(ctx, rows, l, l, Y, ldy, 0, w.Rinv, l, 0, tmp, rows, 1.0, 0.0, 1)));
@@ -186,6 +189,7 @@ static int alloc_orth(rla_ctx *ctx, OrthWork &w, int64_t rows, int64_t l, std::v
     RLA_TRY(get(sizeof(double) * (l * l + l), (void **)&w.hw));
     RLA_TRY(get(sizeof(int), (void **)&w.flag));
     RLA_TRY(get(sizeof(T) * rows * l, &w.tmp));
+    if (chol_inv_supported(ctx, l)) RLA_TRY(get(sizeof(double) * chol_inv_work_doubles(l), (void **)&w.cw));
     return RLA_OK;
 }
 
