@@ -4,15 +4,14 @@
 // The reference orthogonalises with Householder QR (power_its.jl:35,60,70,73); CholeskyQR
 // needs R and R^-1 (Q = Y R^-1).
 //
-//  * chol_blocked16_kernel: ONE CTA of 16 warps, right-looking over 16-column blocks J.  Warp 0
-//    factors the diagonal block with register shuffles (lane c holds column c; R_JJ goes to
-//    shared memory) and inverts it (lane i forms row i of R_JJ^-1 from the shared R_JJ) while
-//    the other warps load their operands of the next two phases; then the block row
-//    R(J, K) = R_JJ^-T G(J, K) (warps 1 .. 15, the first block's operands loaded during the
-//    diagonal factorisation) and the trailing update
-//    G(K1, K2) -= R(J, K1)' R(J, K2) (J < K1 <= K2, one warp per block pair, the next pair's
-//    tile loaded while the current one is computed) run as 8 x 8 tiles of mma.m8n8k4.f64
-//    with the block row staged in shared memory.  G is a zero-padded lp x lp working copy
+//  * chol_blocked16_kernel: ONE CTA of 16 warps, right-looking over 16-column blocks J, two
+//    barriers per block.  Warps 1 .. 15 form the block row R(J, K) = R_JJ^-T G(J, K); then all
+//    warps apply the trailing update G(K1, K2) -= R(J, K1)' R(J, K2) (J < K1 <= K2, one warp
+//    per block pair, the next pair's tile in flight while the current one is computed), both
+//    as 8 x 8 tiles of mma.m8n8k4.f64 with the block row staged in shared memory.  Warp 0
+//    updates the next diagonal block first and factors it during the rest of the update:
+//    register shuffles (lane c holds column c, R_JJ to shared memory), then its inverse (lane i
+//    forms row i of R_JJ^-1).  G is a zero-padded lp x lp working copy
 //    (lp = l rounded up to 16, identity on the padded diagonal) that stays in L2.
 //  * tri_inv_block_kernel: one CTA per 16-column block K of Z = R^-1, block back substitution
 //    Z(J, K) = -Z_JJ sum_{I=J+1..K} R(J, I) Z(I, K) for J = K-1 .. 0, with Z(:, K) in shared
@@ -75,6 +74,74 @@ __device__ __forceinline__ void load_ctile(const double *W, int lp, int r0, int 
             for (int e = 0; e < 2; ++e) c[ta][tb][e] = W[(r0 + 8 * ta + g) + (int64_t)(c0 + 8 * tb + 2 * q + e) * lp];
 }
 
+// Warp 0: 16 x 16 Cholesky of W(J, J) (lane c mod 16 owns column c), R_JJ into W and Rs,
+// R_JJ^-1 into Di and Dg (column-major 16 x 16 per block).
+__device__ __forceinline__ void chol_diag16(double *W, int lp, int J, int lane, double (*Rs)[17], double (*Di)[17],
+                                            double *rinv_s, double *Dg, int *breakdown) {
+    const int j0 = 16 * J, c = lane & 15;
+    double d[16];
+#pragma unroll
+    for (int r = 0; r < 16; ++r) d[r] = W[(j0 + r) + (int64_t)(j0 + c) * lp];
+    bool bad = false;
+#pragma unroll
+    for (int t = 0; t < 16; ++t) {
+        double piv = __shfl_sync(FULL, d[t], t);
+        if (!(piv > 0.0) || !isfinite(piv)) {
+            bad = true;
+            piv = 1.0;
+        }
+        const double ri = rsqrt(piv);
+        const double v = c == t ? piv * ri : (c > t ? d[t] * ri : 0.0);  // R(t, c)
+        if (lane < 16) Rs[t][c] = v;
+        if (lane == t) rinv_s[t] = ri;
+#pragma unroll
+        for (int r = t + 1; r < 16; ++r) d[r] = fma(-__shfl_sync(FULL, v, r), v, d[r]);
+    }
+    __syncwarp();
+    // row i = c of R_JJ^-1 (Z R = I, columns in order)
+    double z[16];
+#pragma unroll
+    for (int jj = 0; jj < 16; ++jj) {
+        double s = c == jj ? 1.0 : 0.0;
+#pragma unroll
+        for (int k = 0; k < jj; ++k) s = fma(-z[k], Rs[k][jj], s);
+        z[jj] = s * rinv_s[jj];
+    }
+    if (lane < 16) {
+#pragma unroll
+        for (int t = 0; t < 16; ++t) {
+            W[(j0 + t) + (int64_t)(j0 + c) * lp] = Rs[t][c];
+            Di[c][t] = z[t];
+            Dg[(int64_t)J * 256 + c + 16 * t] = z[t];
+        }
+    }
+    if (__any_sync(FULL, bad) && lane == 0) *breakdown = 1;
+}
+
+// One trailing-update tile pair: cur -= R(J, c1 block)' R(J, c2 block) from the panel P, then
+// the upper part written back to W.
+__device__ __forceinline__ void chol_update_pair(double *W, int lp, const double *P, int ps, int c1, int c2, bool diag,
+                                                 int g, int q, double (&cur)[2][2][2]) {
+#pragma unroll
+    for (int ks = 0; ks < 4; ++ks) {
+        const int kk = 4 * ks + q;
+        const double a0 = -P[kk * ps + c1 + g], a1 = -P[kk * ps + c1 + 8 + g];
+        const double b0 = P[kk * ps + c2 + g], b1 = P[kk * ps + c2 + 8 + g];
+        dmma8(cur[0][0], a0, b0);
+        dmma8(cur[0][1], a0, b1);
+        dmma8(cur[1][0], a1, b0);
+        dmma8(cur[1][1], a1, b1);
+    }
+#pragma unroll
+    for (int ta = 0; ta < 2; ++ta)
+#pragma unroll
+        for (int tb = 0; tb < 2; ++tb) {
+            if (diag && ta > tb) continue;  // below the diagonal of a diagonal block
+#pragma unroll
+            for (int e = 0; e < 2; ++e) W[(c1 + 8 * ta + g) + (int64_t)(c2 + 8 * tb + 2 * q + e) * lp] = cur[ta][tb][e];
+        }
+}
+
 __global__ void __launch_bounds__(CI_THREADS) chol_blocked16_kernel(double *W, int64_t lp64, int *breakdown,
                                                                     double *Dg) {
     extern __shared__ __align__(16) double ci_sm[];
@@ -82,64 +149,28 @@ __global__ void __launch_bounds__(CI_THREADS) chol_blocked16_kernel(double *W, i
     double *P = ci_sm;                                    // [16][ps]: block row R(J, :)
     __shared__ double Rs[16][17], Di[16][17], rinv_s[16];  // R_JJ, R_JJ^-1, 1 / R_JJ(t, t)
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, q = lane & 3;
+    if (warp == 0) chol_diag16(W, lp, 0, lane, Rs, Di, rinv_s, Dg, breakdown);
+    __syncthreads();
     for (int J = 0; J < nb; ++J) {
         const int j0 = 16 * J, T = nb - J - 1, np = T * (T + 1) / 2;
-        // block row blocks K = J + warp, J + warp + (CI_WARPS - 1), ... for warps 1 ..
-        auto load_bp = [&](int kb, double (&bp)[4][2]) {
+        // trailing pairs: warp 0 takes pair 0 (the next diagonal block, then factors it);
+        // warps 1 .. take pairs warp, warp + (CI_WARPS - 1), ...
+        int p = warp, t1 = 0, t2 = 0;
+        const int pstep = warp == 0 ? np : CI_WARPS - 1;
+        double cur[2][2][2];
+        if (p < np) {
+            tri_decode(p, t1, t2);
+            load_ctile(W, lp, 16 * (J + 1 + t1), 16 * (J + 1 + t2), g, q, cur);
+        }
+        // ---- block row R(J, K) = R_JJ^-T W(J, K), K = J + warp, J + warp + (CI_WARPS - 1), ... ----
+        for (int kb = J + warp; warp >= 1 && kb < nb; kb += CI_WARPS - 1) {
+            double bp[4][2];
 #pragma unroll
             for (int ks = 0; ks < 4; ++ks) {
                 const int kk = 4 * ks + q;
                 bp[ks][0] = W[(j0 + kk) + (int64_t)(16 * kb + g) * lp];
                 bp[ks][1] = W[(j0 + kk) + (int64_t)(16 * kb + 8 + g) * lp];
             }
-        };
-        double bp[4][2];
-        if (warp >= 1 && J + warp < nb) load_bp(J + warp, bp);
-        if (warp == 0) {
-            // ---- 16 x 16 Cholesky of W(J, J): lane c (mod 16) owns column c ----
-            const int c = lane & 15;
-            double d[16];
-#pragma unroll
-            for (int r = 0; r < 16; ++r) d[r] = W[(j0 + r) + (int64_t)(j0 + c) * lp];
-            bool bad = false;
-#pragma unroll
-            for (int t = 0; t < 16; ++t) {
-                double piv = __shfl_sync(FULL, d[t], t);
-                if (!(piv > 0.0) || !isfinite(piv)) {
-                    bad = true;
-                    piv = 1.0;
-                }
-                const double ri = rsqrt(piv);
-                const double v = c == t ? piv * ri : (c > t ? d[t] * ri : 0.0);  // R(t, c)
-                if (lane < 16) Rs[t][c] = v;
-                if (lane == t) rinv_s[t] = ri;
-#pragma unroll
-                for (int r = t + 1; r < 16; ++r) d[r] = fma(-__shfl_sync(FULL, v, r), v, d[r]);
-            }
-            __syncwarp();
-            // row i = c of R_JJ^-1 (Z R = I, columns in order)
-            double z[16];
-#pragma unroll
-            for (int jj = 0; jj < 16; ++jj) {
-                double s = c == jj ? 1.0 : 0.0;
-#pragma unroll
-                for (int k = 0; k < jj; ++k) s = fma(-z[k], Rs[k][jj], s);
-                z[jj] = s * rinv_s[jj];
-            }
-            if (lane < 16) {
-#pragma unroll
-                for (int t = 0; t < 16; ++t) {
-                    W[(j0 + t) + (int64_t)(j0 + c) * lp] = Rs[t][c];
-                    Di[c][t] = z[t];
-                    Dg[(int64_t)J * 256 + c + 16 * t] = z[t];  // column-major 16 x 16
-                }
-            }
-            if (__any_sync(FULL, bad) && lane == 0) *breakdown = 1;
-        }
-        __syncthreads();
-        // ---- block row R(J, K) = R_JJ^-T W(J, K) for K = J + warp ----
-        for (int kb = J + warp; warp >= 1 && kb < nb; kb += CI_WARPS - 1) {
-            if (kb != J + warp) load_bp(kb, bp);
             const int k0 = 16 * kb;
             double acc[2][2][2] = {};
 #pragma unroll
@@ -163,41 +194,16 @@ __global__ void __launch_bounds__(CI_THREADS) chol_blocked16_kernel(double *W, i
                     }
         }
         __syncthreads();
-        // ---- trailing update W(K1, K2) -= R(J, K1)' R(J, K2), J < K1 <= K2 ----
-        int p = warp, t1 = 0, t2 = 0;
-        double cur[2][2][2];
-        if (p < np) {
-            tri_decode(p, t1, t2);
-            load_ctile(W, lp, 16 * (J + 1 + t1), 16 * (J + 1 + t2), g, q, cur);
-        }
+        // ---- trailing update W(K1, K2) -= R(J, K1)' R(J, K2), J < K1 <= K2, next tile in flight ----
         while (p < np) {
-            const int pn = p + CI_WARPS;
+            const int pn = p + pstep;
             int n1 = 0, n2 = 0;
             double nxt[2][2][2];
             if (pn < np) {
                 tri_decode(pn, n1, n2);
                 load_ctile(W, lp, 16 * (J + 1 + n1), 16 * (J + 1 + n2), g, q, nxt);
             }
-            const int c1 = 16 * (J + 1 + t1), c2 = 16 * (J + 1 + t2);
-#pragma unroll
-            for (int ks = 0; ks < 4; ++ks) {
-                const int kk = 4 * ks + q;
-                const double a0 = -P[kk * ps + c1 + g], a1 = -P[kk * ps + c1 + 8 + g];
-                const double b0 = P[kk * ps + c2 + g], b1 = P[kk * ps + c2 + 8 + g];
-                dmma8(cur[0][0], a0, b0);
-                dmma8(cur[0][1], a0, b1);
-                dmma8(cur[1][0], a1, b0);
-                dmma8(cur[1][1], a1, b1);
-            }
-#pragma unroll
-            for (int ta = 0; ta < 2; ++ta)
-#pragma unroll
-                for (int tb = 0; tb < 2; ++tb) {
-                    if (t1 == t2 && ta > tb) continue;  // below the diagonal of a diagonal block
-#pragma unroll
-                    for (int e = 0; e < 2; ++e)
-                        W[(c1 + 8 * ta + g) + (int64_t)(c2 + 8 * tb + 2 * q + e) * lp] = cur[ta][tb][e];
-                }
+            chol_update_pair(W, lp, P, ps, 16 * (J + 1 + t1), 16 * (J + 1 + t2), t1 == t2, g, q, cur);
             if (pn < np) {
 #pragma unroll
                 for (int ta = 0; ta < 2; ++ta)
@@ -209,6 +215,12 @@ __global__ void __launch_bounds__(CI_THREADS) chol_blocked16_kernel(double *W, i
             p = pn;
             t1 = n1;
             t2 = n2;
+        }
+        // warp 0: the next diagonal block is final (its own pair 0): factor it now, while the
+        // other warps finish the trailing update
+        if (warp == 0 && J + 1 < nb) {
+            __syncwarp();
+            chol_diag16(W, lp, J + 1, lane, Rs, Di, rinv_s, Dg, breakdown);
         }
         __syncthreads();
     }

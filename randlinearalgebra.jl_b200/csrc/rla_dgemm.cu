@@ -8,17 +8,23 @@
 //
 //   * CTA tile 64 x 64, BK = 16, 128 threads as 2 x 2 warps of 32 x 32 (4 x 4 MMAs of 8 x 8,
 //     16 MMAs per k4 step from 4 A and 4 B fragments);
-//   * both operands staged in shared memory as [k][mn] with a row stride of 68 doubles, so
-//     the fragment loads (8 rows x 4 k per phase) hit 16 distinct bank pairs;
-//   * the next k-tile is loaded into registers while the current one is multiplied;
+//   * operands copied global -> shared in their own type by cp.async (one element per copy,
+//     zero-filled outside the matrix and below the diagonal of an upper-triangular op(B)),
+//     DG_STAGES k-tiles in flight; Float32 elements are widened when a fragment is read;
+//   * a K-major source is staged [mn][k] with a row stride of 20 elements, an MN-major one
+//     [k][mn] with a row stride of 72: the fragment loads (8 mn x 4 k) are conflict-free;
 //   * split-K over blockIdx.z with FP64 partial tiles added in split order (deterministic);
-//     symmetric products (Gram matrices) compute the upper tiles only and mirror them.
+//     symmetric products (Gram matrices) compute the upper tiles only and write the upper
+//     elements, mirrored; a warp whose 32 x 32 tile lies outside C, below the diagonal, or
+//     past the nonzero rows of an upper-triangular op(B) skips those k-steps.
 #include "rla_internal.cuh"
 #include "rla_kernels.cuh"
 
 namespace rla {
 
-constexpr int DG_BM = 64, DG_BN = 64, DG_BK = 16, DG_LD = 68, DG_THREADS = 128;
+constexpr int DG_BM = 64, DG_BN = 64, DG_BK = 16, DG_THREADS = 128, DG_STAGES = 4;
+constexpr int DG_LDK = 20, DG_LDM = 72;  // staged row strides (elements): [mn][k] and [k][mn]
+constexpr int DG_TILE = 64 * DG_LDK;      // elements per staged tile (>= DG_BK * DG_LDM)
 
 struct DgParams {
     int64_t M, N, K;
@@ -42,43 +48,44 @@ __device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
                  : "d"(a), "d"(b));
 }
 
-// Element (mn, k) of a K x MN tile source: K_MAJOR: src[k + mn*ld]; else src[mn + k*ld].
-template <class T, bool K_MAJOR>
-__device__ __forceinline__ double ld_op(const T *src, int64_t ld, int64_t mn, int64_t k, int64_t MN, int64_t K) {
-    if (mn >= MN || k >= K) return 0.0;
-    return K_MAJOR ? (double)src[k + mn * ld] : (double)src[mn + k * ld];
+// One element copy global -> shared (4 or 8 bytes); src_bytes = 0 fills zero.
+template <class T>
+__device__ __forceinline__ void cp_elem(T *dst, const T *src, bool in) {
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+    if constexpr (sizeof(T) == 4)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(d), "l"(src), "r"(in ? 4 : 0) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(in ? 8 : 0) : "memory");
 }
 
-// 8 elements per thread of a 64 (mn) x 16 (k) tile; (i, q) -> element index t + 128 q.
-// K-major sources walk k fastest (16-element runs), MN-major sources walk mn fastest.
-// `upper`: the source is upper triangular in (k, mn) (entries with k > mn read as zero).
+// Stage the 64 (mn) x 16 (k) tile at (mn0, k0) of a source with MN x K extent (k < kmax read):
+// 8 elements per thread, consecutive threads along the contiguous dimension.  `upper`:
+// entries with k > mn are zero (not read).
 template <class T, bool K_MAJOR>
-__device__ __forceinline__ void load_tile(const T *src, int64_t ld, int64_t mn0, int64_t k0, int64_t MN, int64_t K,
-                                          int64_t kmax, int t, bool upper, double (&r)[8]) {
+__device__ __forceinline__ void stage_tile(T *s, const T *src, int64_t ld, int64_t mn0, int64_t k0, int64_t MN,
+                                           int64_t kmax, int t, bool upper) {
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-        const int idx = t + DG_THREADS * q;
+    for (int r = 0; r < 8; ++r) {
+        const int idx = t + DG_THREADS * r;
         const int mn = K_MAJOR ? idx / DG_BK : idx % DG_BM;
         const int k = K_MAJOR ? idx % DG_BK : idx / DG_BM;
-        r[q] = (upper && k0 + k > mn0 + mn) ? 0.0 : ld_op<T, K_MAJOR>(src, ld, mn0 + mn, k0 + k, MN, kmax);
+        const int64_t gm = mn0 + mn, gk = k0 + k;
+        const bool in = gm < MN && gk < kmax && !(upper && gk > gm);
+        const T *g = src + (in ? (K_MAJOR ? gk + gm * ld : gm + gk * ld) : 0);
+        cp_elem<T>(s + (K_MAJOR ? mn * DG_LDK + k : k * DG_LDM + mn), g, in);
     }
 }
 
-template <bool K_MAJOR>
-__device__ __forceinline__ void store_tile(double *s, int t, const double (&r)[8]) {
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-        const int idx = t + DG_THREADS * q;
-        const int mn = K_MAJOR ? idx / DG_BK : idx % DG_BM;
-        const int k = K_MAJOR ? idx % DG_BK : idx / DG_BM;
-        s[k * DG_LD + mn] = r[q];
-    }
+template <class T, bool K_MAJOR>
+__device__ __forceinline__ double frag(const T *s, int mn, int k) {
+    return (double)(K_MAJOR ? s[mn * DG_LDK + k] : s[k * DG_LDM + mn]);
 }
 
 template <class TA, class TB, class TC, bool A_KM, bool B_KM>
 __global__ void __launch_bounds__(DG_THREADS) dgemm_kernel(DgParams p) {
-    __shared__ __align__(16) double As[2][DG_BK * DG_LD];
-    __shared__ __align__(16) double Bs[2][DG_BK * DG_LD];
+    extern __shared__ __align__(16) unsigned char dg_sm[];
+    TA *As = reinterpret_cast<TA *>(dg_sm);
+    TB *Bs = reinterpret_cast<TB *>(dg_sm + sizeof(TA) * DG_STAGES * DG_TILE);
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const int wm = warp & 1, wn = warp >> 1;
     const int64_t m0 = (int64_t)blockIdx.x * DG_BM, n0 = (int64_t)blockIdx.y * DG_BN;
@@ -93,42 +100,46 @@ __global__ void __launch_bounds__(DG_THREADS) dgemm_kernel(DgParams p) {
     for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-    double ra[8], rb[8];
-    int buf = 0;
-    if (kb < ke) {
-        load_tile<TA, A_KM>(A, p.lda, m0, kb, p.M, p.K, ke, t, false, ra);
-        load_tile<TB, B_KM>(B, p.ldb, n0, kb, p.N, p.K, ke, t, p.b_upper != 0, rb);
-        store_tile<A_KM>(As[0], t, ra);
-        store_tile<B_KM>(Bs[0], t, rb);
-    }
-    __syncthreads();
-    const int fr = lane >> 2, fk = lane & 3;
-    for (int64_t k0 = kb; k0 < ke; k0 += DG_BK) {
-        const bool next = k0 + DG_BK < ke;
-        if (next) {
-            load_tile<TA, A_KM>(A, p.lda, m0, k0 + DG_BK, p.M, p.K, ke, t, false, ra);
-            load_tile<TB, B_KM>(B, p.ldb, n0, k0 + DG_BK, p.N, p.K, ke, t, p.b_upper != 0, rb);
+    const int nkt = kb < ke ? (int)((ke - kb + DG_BK - 1) / DG_BK) : 0;
+    auto issue = [&](int kt) {
+        if (kt < nkt) {
+            const int st = kt % DG_STAGES;
+            const int64_t k0 = kb + (int64_t)kt * DG_BK;
+            stage_tile<TA, A_KM>(As + st * DG_TILE, A, p.lda, m0, k0, p.M, ke, t, false);
+            stage_tile<TB, B_KM>(Bs + st * DG_TILE, B, p.ldb, n0, k0, p.N, ke, t, p.b_upper != 0);
         }
-        const double *as = As[buf], *bs = Bs[buf];
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+#pragma unroll
+    for (int kt = 0; kt < DG_STAGES - 1; ++kt) issue(kt);
+    const int fr = lane >> 2, fk = lane & 3;
+    const int64_t wm0 = m0 + wm * 32, wn0 = n0 + wn * 32, wn_last = wn0 + 31;
+    const bool warp_live = wm0 < p.M && wn0 < p.N && !(p.sym && wm0 > wn_last);
+    for (int kt = 0; kt < nkt; ++kt) {
+        asm volatile("cp.async.wait_group %0;" ::"n"(DG_STAGES - 2) : "memory");
+        __syncthreads();
+        issue(kt + DG_STAGES - 1);  // into the stage every thread finished with at the barrier
+        const TA *as = As + (kt % DG_STAGES) * DG_TILE;
+        const TB *bs = Bs + (kt % DG_STAGES) * DG_TILE;
+        const int64_t k0 = kb + (int64_t)kt * DG_BK;
 #pragma unroll
         for (int kk = 0; kk < DG_BK; kk += 4) {
+            // a warp whose 32 x 32 tile has nothing to add skips the step (warp-uniform):
+            // outside C, below the diagonal of a symmetric product, or past the last nonzero
+            // row of an upper-triangular op(B)
+            if (!warp_live || (p.b_upper && k0 + kk > wn_last)) continue;
             double a[4], b[4];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) a[i] = as[(kk + fk) * DG_LD + wm * 32 + i * 8 + fr];
+            for (int i = 0; i < 4; ++i) a[i] = frag<TA, A_KM>(as, wm * 32 + i * 8 + fr, kk + fk);
 #pragma unroll
-            for (int j = 0; j < 4; ++j) b[j] = bs[(kk + fk) * DG_LD + wn * 32 + j * 8 + fr];
+            for (int j = 0; j < 4; ++j) b[j] = frag<TB, B_KM>(bs, wn * 32 + j * 8 + fr, kk + fk);
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
                 for (int j = 0; j < 4; ++j) dmma(acc[i][j], a[i], b[j]);
         }
-        if (next) {
-            store_tile<A_KM>(As[buf ^ 1], t, ra);
-            store_tile<B_KM>(Bs[buf ^ 1], t, rb);
-        }
-        __syncthreads();
-        buf ^= 1;
     }
+    asm volatile("cp.async.wait_all;" ::: "memory");
     // acc[i][j][e] holds C(m0 + wm*32 + i*8 + fr, n0 + wn*32 + j*8 + 2*fk + e)
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
@@ -140,6 +151,7 @@ __global__ void __launch_bounds__(DG_THREADS) dgemm_kernel(DgParams p) {
             for (int e = 0; e < 2; ++e) {
                 const int64_t n = n0 + wn * 32 + j * 8 + 2 * fk + e;
                 if (n >= p.N) continue;
+                if (p.sym && m > n) continue;  // a symmetric product keeps its upper elements
                 if (p.part) {
                     p.part[(int64_t)blockIdx.z * p.M * p.N + m + n * p.M] = acc[i][j][e];
                 } else {
@@ -147,7 +159,7 @@ __global__ void __launch_bounds__(DG_THREADS) dgemm_kernel(DgParams p) {
                     double r = p.alpha * acc[i][j][e];
                     if (!p.beta_zero) r += p.beta * (double)*cp;
                     *cp = (TC)r;
-                    if (p.sym && m != n && n0 != m0) {
+                    if (p.sym && m != n) {
                         TC *cq = (TC *)p.C + n + m * p.ldc;
                         double q = p.alpha * acc[i][j][e];
                         if (!p.beta_zero) q += p.beta * (double)*cq;
@@ -166,9 +178,9 @@ __global__ void dgemm_reduce_kernel(const double *__restrict__ part, int splits,
     const int64_t MN = M * N;
     for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < MN; idx += (int64_t)gridDim.x * blockDim.x) {
         int64_t m = idx % M, n = idx / M;
-        // a symmetric product computed only its upper tiles: read the mirrored element
+        // a symmetric product computed only its upper elements: read the mirrored element
         int64_t sm = m, sn = n;
-        if (sym && (m / DG_BM) > (n / DG_BN)) {
+        if (sym && m > n) {
             sm = n;
             sn = m;
         }
@@ -187,11 +199,18 @@ int dgemm(rla_ctx *ctx, int64_t M, int64_t N, int64_t K, const TA *A, int64_t ld
     if (M <= 0 || N <= 0) return RLA_OK;
     const int64_t mt = ceil_div(M, DG_BM), nt = ceil_div(N, DG_BN);
     if (mt > 65535 * 1024ll || nt > 65535) return set_error(ctx, RLA_E_UNSUPPORTED, "FP64 GEMM: grid too large");
-    // split K until the grid covers the GPU about twice, with at least 256 rows per split
+    const size_t smem = (sizeof(TA) + sizeof(TB)) * DG_STAGES * DG_TILE;
+    auto kern = ta ? (tb ? dgemm_kernel<TA, TB, TC, true, false> : dgemm_kernel<TA, TB, TC, true, true>)
+                   : (tb ? dgemm_kernel<TA, TB, TC, false, false> : dgemm_kernel<TA, TB, TC, false, true>);
+    RLA_CUDA_TRY(ctx, set_smem_max(kern));
+    int occ = 1;
+    RLA_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, DG_THREADS, smem));
+    // split K so that the grid fills the resident CTA slots once (no SM runs one CTA more
+    // than the others), with at least 256 rows per split
     const int64_t tiles = sym ? nt * (nt + 1) / 2 + (mt - nt > 0 ? (mt - nt) * nt : 0) : mt * nt;
+    const int64_t slots = (int64_t)ctx->sm_count * std::max(occ, 1);
     int64_t splits = 1;
-    const int64_t want = 2 * (int64_t)ctx->sm_count;
-    if (K > 0 && tiles < want) splits = std::min<int64_t>(ceil_div(want, tiles), std::max<int64_t>(1, K / 256));
+    if (K > 0 && tiles < slots) splits = std::max<int64_t>(1, std::min<int64_t>(slots / tiles, K / 256));
     splits = std::max<int64_t>(1, std::min<int64_t>(splits, 1024));
     const int64_t kps = K > 0 ? ceil_div(ceil_div(K, splits), DG_BK) * DG_BK : DG_BK;
     splits = K > 0 ? ceil_div(K, kps) : 1;
@@ -202,14 +221,7 @@ int dgemm(rla_ctx *ctx, int64_t M, int64_t N, int64_t K, const TA *A, int64_t ld
         p.part = (double *)ws;
     }
     const dim3 grid((unsigned)mt, (unsigned)nt, (unsigned)splits);
-    auto go = [&](auto kern) { kern<<<grid, DG_THREADS, 0, ctx->stream>>>(p); };
-    if (ta) {
-        if (tb) go(dgemm_kernel<TA, TB, TC, true, false>);
-        else go(dgemm_kernel<TA, TB, TC, true, true>);
-    } else {
-        if (tb) go(dgemm_kernel<TA, TB, TC, false, false>);
-        else go(dgemm_kernel<TA, TB, TC, false, true>);
-    }
+    kern<<<grid, DG_THREADS, smem, ctx->stream>>>(p);
     RLA_TRY(check_launch(ctx, "dgemm"));
     if (p.part) {
         const int64_t MN = M * N;
