@@ -1040,6 +1040,26 @@ int tri_inv_upper(rla_ctx *ctx, const double *R, int64_t l, double *Rinv) {
     return check_launch(ctx, "tri_inv_upper");
 }
 
+// Largest relative off-diagonal sqrt(g_ij^2 / (g_ii g_jj)) of a Gram matrix G (l x l), to *out.
+__global__ void __launch_bounds__(1024) jacobi_offdiag_kernel(const double *G, int64_t l, double *out) {
+    __shared__ double wm[32];
+    double m2 = 0.0;
+    for (int64_t idx = threadIdx.x; idx < l * l; idx += blockDim.x) {
+        const int64_t i = idx % l, j = idx / l;
+        if (i >= j) continue;
+        const double g = G[idx], a = G[i + i * l], b = G[j + j * l];
+        if (g != 0.0 && a * b > 0.0) m2 = fmax(m2, g * g / (a * b));
+    }
+    for (int o = 16; o > 0; o >>= 1) m2 = fmax(m2, __shfl_xor_sync(FULL, m2, o));
+    if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = m2;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        m2 = threadIdx.x < (blockDim.x >> 5) ? wm[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) m2 = fmax(m2, __shfl_xor_sync(FULL, m2, o));
+        if (threadIdx.x == 0) *out = sqrt(m2);
+    }
+}
+
 int jacobi_svd(rla_ctx *ctx, double *X, double *J, double *sigma, int64_t l, double *work, double tol) {
     // Float32 data (tolerance >= 1e-13): the Gram-based pair step
     const bool gram = tol >= 1e-13;
@@ -1068,6 +1088,21 @@ int jacobi_svd(rla_ctx *ctx, double *X, double *J, double *sigma, int64_t l, dou
             double v;
             memcpy(&v, &h, sizeof(v));
             if (v <= tol) break;
+            // Quadratic convergence: once every pair measured below sqrt(tol) this sweep, the
+            // next sweep is most likely one that rotates nothing.  Check that on the Gram matrix
+            // of X (every pair at once, fresh FP64 dot products) instead of running it: if all
+            // pairs are within tol, that sweep would leave X and J unchanged.
+            if (v <= sqrt(tol)) {
+                double *Gx = work;  // l x l, free until the final sort
+                RLA_TRY((dgemm<double, double, double>(ctx, l, l, l, X, l, 1, X, l, 0, Gx, l, 1.0, 0.0, 0, 1)));
+                double *dev_v = work + l * l;
+                jacobi_offdiag_kernel<<<1, 1024, 0, ctx->stream>>>(Gx, l, dev_v);
+                RLA_TRY(check_launch(ctx, "jacobi_offdiag"));
+                double g = 0.0;
+                RLA_CUDA_TRY(ctx, cudaMemcpyAsync(&g, dev_v, sizeof(g), cudaMemcpyDeviceToHost, ctx->stream));
+                RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+                if (g <= tol) break;
+            }
         }
     }
     jacobi_rank_kernel<<<1, 1024, 0, ctx->stream>>>(X, sigma, l, work);

@@ -126,16 +126,35 @@ struct OrthWork {
 // working precision; 1 for an intermediate basis of the power iterations, which only has
 // to span range(Y) and be well conditioned (one pass with the FP64 Gram matrix leaves
 // ||Q'Q - I|| ~ u * cond(Y) for Float32 Y, ~ u * cond(Y)^2 for Float64).
+//
+// Passes alternate between Y and w.tmp (rows x l, ld rows).  With `owned` (Y is a library
+// buffer with ld == rows) a result that ends in w.tmp is not copied back: Y and w.tmp trade
+// places.
 template <class T>
-static int orth(rla_ctx *ctx, T *Y, int64_t rows, int64_t l, int64_t ldy, OrthWork &w, bool signs = true,
-                int passes = 2) {
+static int orth(rla_ctx *ctx, T *&Y, int64_t rows, int64_t l, int64_t ldy, OrthWork &w, bool signs = true,
+                int passes = 2, bool owned = false) {
     if (l > rows)
         return set_error(ctx, RLA_E_UNSUPPORTED, "compression dimension %lld exceeds the %lld rows being orthogonalised",
                          (long long)l, (long long)rows);
     T *tmp = (T *)w.tmp;
+    // the current basis: cur (ld ldc), the product goes to the other buffer
+    T *cur = Y;
+    int64_t ldc = ldy;
     bool shifted_done = false;
+    auto finish = [&]() -> int {
+        if (cur != Y) {
+            if (owned && ldy == rows) {
+                w.tmp = Y;
+                Y = cur;
+            } else {
+                convert_kernel<T, T><<<ceil_div_i(rows * l, 256), 256, 0, ctx->stream>>>(cur, rows, l, rows, Y, ldy);
+                RLA_TRY(check_launch(ctx, "copy_back"));
+            }
+        }
+        return RLA_OK;
+    };
     for (int pass = 0; pass < passes; ++pass) {
-        RLA_TRY(gram_fp64<T>(ctx, Y, rows, l, ldy, w.G));
+        RLA_TRY(gram_fp64<T>(ctx, cur, rows, l, ldc, w.G));
         double shift = 0.0;
         RLA_TRY(equilibrate(ctx, w.G, l, w.dscale));
         if (w.cw) RLA_TRY(chol_inv(ctx, w.G, l, shift, w.flag, w.Rinv, w.cw));
@@ -146,12 +165,13 @@ static int orth(rla_ctx *ctx, T *Y, int64_t rows, int64_t l, int64_t ldy, OrthWo
         if (bad && shifted_done) {
             // numerically rank-deficient block: Householder QR gives an orthonormal basis
             // (and LAPACK's Q) whatever the rank
+            RLA_TRY(finish());
             return householder_q<T>(ctx, Y, rows, l, ldy, w.diag);
         }
         if (bad) {
             // Shifted CholeskyQR: on the equilibrated Gram matrix (unit diagonal, so
             // ||Y D||_F^2 = l) the shift is 11 (rows*l + l(l+1)) u ||Y D||_2^2 <= ... * l.
-            RLA_TRY(gram_fp64<T>(ctx, Y, rows, l, ldy, w.G));
+            RLA_TRY(gram_fp64<T>(ctx, cur, rows, l, ldc, w.G));
             RLA_TRY(equilibrate(ctx, w.G, l, w.dscale));
             const double u = sizeof(T) == 4 ? 5.96e-8 : 1.11e-16;
             shift = 11.0 * ((double)rows * l + (double)l * (l + 1)) * u * (double)l;
@@ -159,17 +179,24 @@ static int orth(rla_ctx *ctx, T *Y, int64_t rows, int64_t l, int64_t ldy, OrthWo
             else RLA_TRY(cholesky_upper(ctx, w.G, l, shift, w.flag));
             RLA_CUDA_TRY(ctx, cudaMemcpyAsync(&bad, w.flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
             RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-            if (bad) return householder_q<T>(ctx, Y, rows, l, ldy, w.diag);
+            if (bad) {
+                RLA_TRY(finish());
+                return householder_q<T>(ctx, Y, rows, l, ldy, w.diag);
+            }
             shifted_done = true;
             passes = pass + 3;  // shifted pass followed by two plain passes
         }
         if (!w.cw) RLA_TRY(tri_inv_upper(ctx, w.G, l, w.Rinv));
         row_scale_kernel<<<ceil_div_i(l * l, 256), 256, 0, ctx->stream>>>(w.Rinv, l, w.dscale);
         RLA_TRY(check_launch(ctx, "row_scale"));
-        RLA_TRY((gemm<T, double, T, double>(ctx, rows, l, l, Y, ldy, 0, w.Rinv, l, 0, tmp, rows, 1.0, 0.0, 1)));
-        convert_kernel<T, T><<<ceil_div_i(rows * l, 256), 256, 0, ctx->stream>>>(tmp, rows, l, rows, Y, ldy);
-        RLA_TRY(check_launch(ctx, "copy_back"));
+        // the product goes to the buffer the basis is not in (Y or tmp)
+        T *dst = cur == Y ? tmp : Y;
+        const int64_t ldd = cur == Y ? rows : ldy;
+        RLA_TRY((gemm<T, double, T, double>(ctx, rows, l, l, cur, ldc, 0, w.Rinv, l, 0, dst, ldd, 1.0, 0.0, 1)));
+        cur = dst;
+        ldc = ldd;
     }
+    RLA_TRY(finish());
     if (!signs) return RLA_OK;
     house_signs_kernel<T><<<1, 1024, 0, ctx->stream>>>(Y, rows, l, ldy, w.hw);
     return check_launch(ctx, "house_signs");
@@ -247,8 +274,8 @@ static int tc_apply(rla_ctx *ctx, const TcOps &ops, int at, int64_t m, int64_t n
 // only) the products with A run on the tensor cores in split BF16.
 template <class T>
 static int range_core(rla_ctx *ctx, const rla_sketch *om, int64_t m, int64_t n, const T *A, int64_t lda,
-                      const rla_range_params *pr, T *Q, int64_t ldq, Owned &own, const TcOps *tc = nullptr,
-                      bool q_signs = true) {
+                      const rla_range_params *pr, T *&Q, int64_t ldq, Owned &own, const TcOps *tc = nullptr,
+                      bool q_signs = true, bool q_owned = false) {
     const int64_t l = om->n_cols;
     // Z = A'Q, Q = A Z
     auto at_q = [&](const T *Qp, T *Zp) -> int {
@@ -280,20 +307,20 @@ static int range_core(rla_ctx *ctx, const rla_sketch *om, int64_t m, int64_t n, 
     if (!done) RLA_TRY(sketch_mul_impl(ctx, om, RLA_SIDE_RIGHT, 0, m, l, Q, ldq, 0, m, n, A, lda, 0, 1.0, 0.0));
     if (pr->orthogonalize) {
         // intermediate bases (every one but the last Q) take one CholeskyQR pass
-        RLA_TRY(orth<T>(ctx, Q, m, l, ldq, wq, q_signs && pr->power_its == 0, pr->power_its == 0 ? 2 : 1));
+        RLA_TRY(orth<T>(ctx, Q, m, l, ldq, wq, q_signs && pr->power_its == 0, pr->power_its == 0 ? 2 : 1, q_owned));
         for (int64_t it = 0; it < pr->power_its; ++it) {
             const bool last = it + 1 == pr->power_its;
             RLA_TRY(at_q(Q, Z));
-            RLA_TRY(orth<T>(ctx, Z, n, l, n, wz, false, 1));
+            RLA_TRY(orth<T>(ctx, Z, n, l, n, wz, false, 1, true));
             RLA_TRY(a_z(Z, Q));
-            RLA_TRY(orth<T>(ctx, Q, m, l, ldq, wq, q_signs && last, last ? 2 : 1));
+            RLA_TRY(orth<T>(ctx, Q, m, l, ldq, wq, q_signs && last, last ? 2 : 1, q_owned));
         }
     } else {
         for (int64_t it = 0; it < pr->power_its; ++it) {
             RLA_TRY(at_q(Q, Z));
             RLA_TRY(a_z(Z, Q));
         }
-        RLA_TRY(orth<T>(ctx, Q, m, l, ldq, wq, q_signs));
+        RLA_TRY(orth<T>(ctx, Q, m, l, ldq, wq, q_signs, 2, q_owned));
     }
     return RLA_OK;
 }
@@ -326,7 +353,7 @@ static int randsvd_t(rla_ctx *ctx, const rla_sketch *om, int64_t m, int64_t n, c
     const bool use_tc = std::is_same<T, float>::value;
     if constexpr (std::is_same<T, float>::value)
         RLA_TRY(tc_ops_make(ctx, A, m, n, lda, l, pr->precision == RLA_PREC_SPLIT_BF16 ? 2 : 3, tc, own));
-    RLA_TRY(range_core<T>(ctx, om, m, n, A, lda, pr, Q, m, own, use_tc ? &tc : nullptr, false));
+    RLA_TRY(range_core<T>(ctx, om, m, n, A, lda, pr, Q, m, own, use_tc ? &tc : nullptr, false, true));
     // Bt = A'Q (n x l) in FP64 (randsvd.jl:183-185 forms QA in Float64)
     double *Bt, *X, *J, *sig, *jw;
     RLA_CUDA_TRY(ctx, pool_malloc_s(ctx, (void **)&Bt, sizeof(double) * n * l, ctx->stream));
@@ -345,7 +372,7 @@ static int randsvd_t(rla_ctx *ctx, const rla_sketch *om, int64_t m, int64_t n, c
     RLA_CUDA_TRY(ctx, cudaMemcpyAsync(Qb, Bt, sizeof(double) * n * l, cudaMemcpyDeviceToDevice, ctx->stream));
     OrthWork wb{};
     RLA_TRY(alloc_orth<double>(ctx, wb, n, l, own.ptrs));
-    RLA_TRY(orth<double>(ctx, Qb, n, l, n, wb, false));
+    RLA_TRY(orth<double>(ctx, Qb, n, l, n, wb, false, 2, true));
     RLA_CUDA_TRY(ctx, pool_malloc_s(ctx, (void **)&X, sizeof(double) * l * l, ctx->stream));
     own.ptrs.push_back(X);
     RLA_CUDA_TRY(ctx, pool_malloc_s(ctx, (void **)&J, sizeof(double) * l * l, ctx->stream));
@@ -385,12 +412,14 @@ int rla_rangefinder(rla_ctx *ctx, const rla_sketch *om, int dtype, int64_t m, in
         TcOps tc;
         RLA_TRY(tc_ops_make(ctx, (const float *)A, m, n, lda, om->n_cols, pr->precision == RLA_PREC_SPLIT_BF16 ? 2 : 3,
                             tc, own));
-        rc = range_core<float>(ctx, om, m, n, (const float *)A, lda, pr, (float *)Q, ldq, own, &tc);
+        float *Qf = (float *)Q;  // the caller's buffer: results are copied into it
+        rc = range_core<float>(ctx, om, m, n, (const float *)A, lda, pr, Qf, ldq, own, &tc);
         RLA_TRY(rc);
         RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
         return tc_status_check(ctx);
     }
-    rc = range_core<double>(ctx, om, m, n, (const double *)A, lda, pr, (double *)Q, ldq, own);
+    double *Qd = (double *)Q;
+    rc = range_core<double>(ctx, om, m, n, (const double *)A, lda, pr, Qd, ldq, own);
     RLA_TRY(rc);
     RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     return RLA_OK;
