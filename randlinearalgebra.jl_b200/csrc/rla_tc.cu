@@ -255,6 +255,7 @@ constexpr uint32_t TC_A_BYTES = TC_BM * TC_BK * 2;  // 8 KB per operand term
 template <int NT>
 struct TcMaps {
     CUtensorMap a[NT], b[NT];
+    CUtensorMap b_rem[NT];  // NT = 2: boxes of the remainder columns (rows main .. main+rem of B)
 };
 
 // Term pairs (A term, B term) of the product, largest first.
@@ -267,7 +268,7 @@ __device__ __forceinline__ void tc_pair(int i, int &ta, int &tb) {
 
 struct TcParams {
     int M, N, K;      // op(A) is M x K, B is K x N
-    int BN;           // tile columns (multiple of 16; > 256 only as two halves of a multiple of 32)
+    int BN;           // tile columns (multiple of 16; NT = 3: > 256 only as two halves of a multiple of 32)
     int nch;          // MMA column chunks (1 or 2)
     int a_kmajor;     // 1: op(A) = A' with A column-major K x M; 0: A column-major M x K
     int nkb;          // k-blocks of TC_BK in total
@@ -278,6 +279,12 @@ struct TcParams {
     int64_t ldo, split_stride;
     int *status;
     uint64_t wait_ns;  // limit of one pipeline wait
+    // NT = 2: columns [0, main_cols) take the three term products as MMAs of N = main_cols;
+    // the remainder [main_cols, BN) takes two: A_hi x [B_hi | B_lo] (N = 2 rem, the rows of
+    // the two terms adjacent in shared memory) and A_lo x B_hi (N = rem), summed in the
+    // epilogue.  An MMA costs the same for every N <= 256, so this issues 5 MMAs per k-step
+    // at BN = 272 instead of 6, and 2 instead of 3 when BN <= 128.
+    int main_cols, rem_cols;
 };
 
 template <int NT>
@@ -312,6 +319,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
         for (int q = 0; q < NT; ++q) {
             asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&maps.a[q])) : "memory");
             asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&maps.b[q])) : "memory");
+            if (NT == 2 && p.rem_cols)
+                asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&maps.b_rem[q])) : "memory");
         }
     }
     if (warp == 2) {
@@ -349,9 +358,18 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
 #pragma unroll
                         for (int q = 0; q < 4; ++q) tma_load_2d(a_t + q * 2048u, &maps.a[t], full_bar(s), m0 + 32 * q, k0);
                     }
-                    for (int c = 0; c < p.nch; ++c) {
-                        const uint32_t off = (uint32_t)c * chunk_cols * TC_BK * 2;
-                        tma_load_2d(b_t + off, &maps.b[t], full_bar(s), k0, c * (int)chunk_cols);
+                    if constexpr (NT == 2) {
+                        // B region: [B_hi main][B_hi rem][B_lo rem][B_lo main], rows of 64 B
+                        const uint32_t b0 = st + NT * TC_A_BYTES, mc = (uint32_t)p.main_cols, rc = (uint32_t)p.rem_cols;
+                        const uint32_t main_off = t == 0 ? 0u : (mc + 2u * rc) * TC_BK * 2;
+                        const uint32_t rem_off = (mc + (uint32_t)t * rc) * TC_BK * 2;
+                        if (mc) tma_load_2d(b0 + main_off, &maps.b[t], full_bar(s), k0, 0);
+                        if (rc) tma_load_2d(b0 + rem_off, &maps.b_rem[t], full_bar(s), k0, (int)mc);
+                    } else {
+                        for (int c = 0; c < p.nch; ++c) {
+                            const uint32_t off = (uint32_t)c * chunk_cols * TC_BK * 2;
+                            tma_load_2d(b_t + off, &maps.b[t], full_bar(s), k0, c * (int)chunk_cols);
+                        }
                     }
                 }
             }
@@ -366,6 +384,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
         if (lane == 0) {
             // ---- MMA issuer ----
             const uint32_t idesc = idesc_bf16(TC_BM, (int)chunk_cols, p.a_kmajor ? 0 : 1, 0);
+            const uint32_t idesc_main = idesc_bf16(TC_BM, p.main_cols > 0 ? p.main_cols : 16, p.a_kmajor ? 0 : 1, 0);
+            const uint32_t idesc_rem2 = idesc_bf16(TC_BM, p.rem_cols > 0 ? 2 * p.rem_cols : 16, p.a_kmajor ? 0 : 1, 0);
+            const uint32_t idesc_rem = idesc_bf16(TC_BM, p.rem_cols > 0 ? p.rem_cols : 16, p.a_kmajor ? 0 : 1, 0);
             for (int kb = 0; kb < nkb; ++kb) {
                 const int s = kb % p.stages;
                 const uint32_t ph = (uint32_t)(kb / p.stages) & 1u;
@@ -382,17 +403,34 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
                         // MN-major: 32-row blocks of 2 KB; k rows 64 B apart; k-step = 16 rows.
                         da[t] = p.a_kmajor ? sdesc_sw64(a_t + kk * 32u, 16u, 512u) : sdesc_sw64(a_t + kk * 1024u, 2048u, 512u);
                     }
-                    for (int c = 0; c < p.nch; ++c) {
-                        const uint32_t off = (uint32_t)c * chunk_cols * TC_BK * 2 + kk * 32u;
-                        uint64_t db[NT];
+                    if constexpr (NT == 2) {
+                        const uint32_t b0 = st + NT * TC_A_BYTES + kk * 32u, mc = (uint32_t)p.main_cols,
+                                       rc = (uint32_t)p.rem_cols;
+                        const uint32_t first = (kb | kk) != 0 ? 1u : 0u;
+                        if (mc) {
+                            const uint64_t bh = sdesc_sw64(b0, 16u, 512u), bl = sdesc_sw64(b0 + (mc + 2u * rc) * TC_BK * 2, 16u, 512u);
+                            mma_bf16(tmem, da[0], bh, idesc_main, first);
+                            mma_bf16(tmem, da[0], bl, idesc_main, 1u);
+                            mma_bf16(tmem, da[1], bh, idesc_main, 1u);
+                        }
+                        if (rc) {
+                            const uint64_t br = sdesc_sw64(b0 + mc * TC_BK * 2, 16u, 512u);  // [B_hi rem][B_lo rem]
+                            mma_bf16(tmem + mc, da[0], br, idesc_rem2, first);
+                            mma_bf16(tmem + mc + 2u * rc, da[1], br, idesc_rem, first);
+                        }
+                    } else {
+                        for (int c = 0; c < p.nch; ++c) {
+                            const uint32_t off = (uint32_t)c * chunk_cols * TC_BK * 2 + kk * 32u;
+                            uint64_t db[NT];
 #pragma unroll
-                        for (int t = 0; t < NT; ++t) db[t] = sdesc_sw64(st + NT * TC_A_BYTES + (uint32_t)t * b_bytes + off, 16u, 512u);
-                        const uint32_t d = tmem + (uint32_t)c * chunk_cols;
+                            for (int t = 0; t < NT; ++t) db[t] = sdesc_sw64(st + NT * TC_A_BYTES + (uint32_t)t * b_bytes + off, 16u, 512u);
+                            const uint32_t d = tmem + (uint32_t)c * chunk_cols;
 #pragma unroll
-                        for (int i = 0; i < tc_pairs(NT); ++i) {
-                            int ta, tb;
-                            tc_pair(i, ta, tb);
-                            mma_bf16(d, da[ta], db[tb], idesc, (i > 0 || (kb | kk) != 0) ? 1u : 0u);
+                            for (int i = 0; i < tc_pairs(NT); ++i) {
+                                int ta, tb;
+                                tc_pair(i, ta, tb);
+                                mma_bf16(d, da[ta], db[tb], idesc, (i > 0 || (kb | kk) != 0) ? 1u : 0u);
+                            }
                         }
                     }
                 }
@@ -411,14 +449,34 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
     tc_fence_after();
     const int row = m0 + warp * 32 + lane;
     float *out = p.out + (int64_t)split * p.split_stride;
-    for (int c0 = 0; c0 < p.BN; c0 += 16) {
+    const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+    const int direct = NT == 2 ? p.main_cols : p.BN;  // columns read straight from TMEM
+    for (int c0 = 0; c0 < direct; c0 += 16) {
         uint32_t r[16];
-        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, r);
+        tmem_ld16(lane_base + (uint32_t)c0, r);
         if (row < p.M) {
 #pragma unroll
             for (int j = 0; j < 16; ++j) {
                 const int col = c0 + j;
                 if (col < p.N) out[row + (int64_t)col * p.ldo] = ok ? __uint_as_float(r[j]) : 0.f;
+            }
+        }
+    }
+    if constexpr (NT == 2) {
+        // remainder column main + c: hi.hi at main + c, hi.lo at main + rem + c, lo.hi at main + 2 rem + c
+        const int mc = p.main_cols, rc = p.rem_cols;
+        for (int c0 = 0; c0 < rc; c0 += 16) {
+            uint32_t r0[16], r1[16], r2[16];
+            tmem_ld16(lane_base + (uint32_t)(mc + c0), r0);
+            tmem_ld16(lane_base + (uint32_t)(mc + rc + c0), r1);
+            tmem_ld16(lane_base + (uint32_t)(mc + 2 * rc + c0), r2);
+            if (row < p.M) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const int col = mc + c0 + j;
+                    const float v = __uint_as_float(r0[j]) + __uint_as_float(r1[j]) + __uint_as_float(r2[j]);
+                    if (col < p.N) out[row + (int64_t)col * p.ldo] = ok ? v : 0.f;
+                }
             }
         }
     }
@@ -774,21 +832,32 @@ int tc_status_check(rla_ctx *ctx) {
 TcPlan tc_plan(const rla_ctx *ctx, int64_t M, int64_t N, int64_t K, int splits, int NT) {
     TcPlan pl;
     const int64_t nb = std::min<int64_t>(N, tc_max_bn(NT));
-    pl.BN = (int)(nb <= 256 ? ceil_div(nb, 16) * 16 : ceil_div(nb, 32) * 32);
-    pl.nch = pl.BN > 256 ? 2 : 1;
+    if (NT == 2) {
+        // one MMA of N = main for the three term products, two packed MMAs for the remainder
+        pl.BN = (int)(ceil_div(nb, 16) * 16);
+        pl.main_cols = pl.BN > 256 ? 256 : (pl.BN > 128 ? pl.BN : 0);
+        pl.rem_cols = pl.BN - pl.main_cols;
+        pl.nch = 1;
+    } else {
+        pl.BN = (int)(nb <= 256 ? ceil_div(nb, 16) * 16 : ceil_div(nb, 32) * 32);
+        pl.nch = pl.BN > 256 ? 2 : 1;
+    }
     const int64_t b_bytes = (int64_t)pl.BN * TC_BK * 2;
     const int64_t stage = NT * TC_A_BYTES + NT * b_bytes;
     const int64_t budget = ctx->smem_optin - 1024 - 256;
     pl.stages = (int)std::max<int64_t>(2, std::min<int64_t>(8, budget / stage));
     pl.smem = (size_t)(pl.stages * stage + 1024 + 256);
     pl.tmem_cols = 32;
-    while ((int)pl.tmem_cols < pl.BN) pl.tmem_cols <<= 1;
+    const int acc_cols = NT == 2 ? pl.main_cols + 3 * pl.rem_cols : pl.BN;
+    while ((int)pl.tmem_cols < acc_cols) pl.tmem_cols <<= 1;
     const int64_t mt = ceil_div(M, TC_BM), nkb = ceil_div(K, TC_BK);
     pl.mt = (int)mt;
     pl.nkb = (int)nkb;
     if (splits <= 0) {
         // model: waves x k-blocks per split x MMA time per k-block, plus partial-tile traffic
-        const double t_kb = 0.15e-6 * tc_pairs(NT) * (double)pl.BN / 288.0, bw = 6.0e12;
+        // an MMA of M = 128 costs the same for every N <= 256: time per k-block ~ MMA count
+        const int mmas = NT == 2 ? (pl.main_cols ? 3 : 0) + (pl.rem_cols ? 2 : 0) : tc_pairs(NT) * pl.nch;
+        const double t_kb = 0.25e-6 * mmas, bw = 6.0e12;
         double best = 1e30;
         splits = 1;
         for (int s = 1; s <= std::min<int64_t>(nkb, 64); ++s) {
@@ -819,11 +888,13 @@ int tc_gemm_split(rla_ctx *ctx, int64_t M, int64_t N, int64_t K, const bf16 *con
         const int64_t nb = std::min<int64_t>(max_bn, N - n0);
         TcPlan pl = tc_plan(ctx, M, nb, K, splits, NT);
         TcMaps<NT> maps;
-        const uint32_t box_n = (uint32_t)(pl.BN / pl.nch);
+        const uint32_t box_n = (uint32_t)(NT == 2 ? pl.main_cols : pl.BN / pl.nch);
         for (int t = 0; t < NT; ++t) {
             if (a_kmajor) RLA_TRY(make_map(ctx, &maps.a[t], A[t], K, M, lda, TC_BK, TC_BM));
             else RLA_TRY(make_map(ctx, &maps.a[t], A[t], M, K, lda, 32, TC_BK));
-            RLA_TRY(make_map(ctx, &maps.b[t], B[t] + n0 * ldb, K, nb, ldb, TC_BK, box_n));
+            if (box_n) RLA_TRY(make_map(ctx, &maps.b[t], B[t] + n0 * ldb, K, nb, ldb, TC_BK, box_n));
+            if (NT == 2 && pl.rem_cols)
+                RLA_TRY(make_map(ctx, &maps.b_rem[t], B[t] + n0 * ldb, K, nb, ldb, TC_BK, (uint32_t)pl.rem_cols));
         }
         TC *Cn = C + n0 * ldc;
         const bool direct = pl.splits == 1 && std::is_same<TC, float>::value && alpha == 1.0 && beta == 0.0;
@@ -841,7 +912,7 @@ int tc_gemm_split(rla_ctx *ctx, int64_t M, int64_t N, int64_t K, const bf16 *con
             out = (float *)ws;
         }
         TcParams p{(int)M, (int)nb, (int)K, pl.BN, pl.nch, a_kmajor, pl.nkb, pl.kbps, pl.stages, pl.tmem_cols,
-                   out, ldo, sstride, status, ctx->wait_ns};
+                   out, ldo, sstride, status, ctx->wait_ns, pl.main_cols, pl.rem_cols};
         RLA_CUDA_TRY(ctx, set_smem_max(tc_gemm_kernel<NT>));
         cudaEvent_t e0 = nullptr, e1 = nullptr;
         if (ctx->timing) {

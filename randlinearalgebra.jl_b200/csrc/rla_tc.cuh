@@ -34,6 +34,7 @@ constexpr int tc_max_bn(int NT) { return NT == 2 ? 288 : 160; }
 // Launch shape of one tensor-core GEMM (columns of B handled tc_max_bn(NT) at a time).
 struct TcPlan {
     int BN = 0, nch = 1, stages = 2, mt = 0, nkb = 0, kbps = 0, splits = 1;
+    int main_cols = 0, rem_cols = 0;  // NT = 2: column split of the tile (see TcParams)
     uint32_t tmem_cols = 32;
     size_t smem = 0;
 };
