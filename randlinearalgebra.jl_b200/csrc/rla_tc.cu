@@ -492,12 +492,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
 // The tensor cores accumulate in FP32, and over a long K that running sum drifts well above
 // the FP32 rounding of the result.  Here the MMAs of every TC_CHUNK k-blocks go into one of
 // two TMEM accumulators (ping-pong); four epilogue warps add each finished chunk into FP64
-// registers while the MMAs fill the other one.  Warps: 0 TMA producer (lane 0), 1 MMA
+// registers while the MMAs fill the other one (the NT term products of A_t with all the B
+// terms of lower order form one MMA each: 3 MMAs per k-step for NT = 3, 2 for NT = 2).
+// Warps: 0 TMA producer (lane 0), 1 MMA
 // issuer (lane 0), 2 TMEM allocator, 4..7 chunk drain / epilogue (warp 4+q reads TMEM
 // lanes 32q .. 32q+31, the tile rows of its quarter).  Tiles are 128 x 64; the grid is
 // (N tiles, M tiles, splits), N fastest, so the CTAs that share an A tile run together and
 // A comes from HBM about once.  Output: FP64 partial tiles, one per split.
 constexpr int TC64_THREADS = 256, TC64_BN = 64, TC_CHUNK = 4;
+// TMEM columns of the two chunk accumulators (64 NT columns each), a power of two
+constexpr uint32_t tc64_tmem_cols(int NT) { return NT >= 3 ? 512u : (NT == 2 ? 256u : 128u); }
 
 // One CTA of the FP64-accumulating pipeline: the 128 x 64 tile (m0, n0) of op(A) * B over
 // k-blocks kb0 .. kb0+nkb-1 with MMAs mma_n columns wide, written as FP64 sums (or rounded to
@@ -584,8 +588,15 @@ __device__ __forceinline__ void f64acc_cta(const CUtensorMap *ma, const CUtensor
         __syncwarp();
     } else if (warp == 1) {
         if (lane == 0) {
-            // ---- MMA issuer: chunk c accumulates into TMEM columns (c & 1) * 64 ----
-            const uint32_t idesc = idesc_bf16(TC_BM, (int)mma_n, p.a_kmajor ? 0 : 1, 0);
+            // ---- MMA issuer: chunk c accumulates into TMEM columns (c & 1) * 64 NT ----
+            // The B terms' 64-row tiles are adjacent in shared memory, so A_t x [B_0 | .. |
+            // B_(NT-1-t)] is one MMA (an MMA costs the same for every N <= 256); column group u
+            // of the accumulator collects the products with B_u, the drain adds the groups.
+            const uint32_t a_mn = p.a_kmajor ? 0 : 1;
+            const uint32_t idesc_n[3] = {idesc_bf16(TC_BM, TC64_BN * (NT >= 1 ? NT : 1), a_mn, 0),
+                                         idesc_bf16(TC_BM, TC64_BN * (NT >= 2 ? NT - 1 : 1), a_mn, 0),
+                                         idesc_bf16(TC_BM, TC64_BN * (NT >= 3 ? NT - 2 : 1), a_mn, 0)};
+            (void)mma_n;
             for (int kb = 0; kb < nkb; ++kb) {
                 const int c = kb / TC_CHUNK, x = c & 1;
                 const bool first = kb % TC_CHUNK == 0;
@@ -599,21 +610,16 @@ __device__ __forceinline__ void f64acc_cta(const CUtensorMap *ma, const CUtensor
                 if (!mbar_wait(full_bar(s), ph, p.status, p.wait_ns)) break;
                 tc_fence_after();
                 const uint32_t st = base + (uint32_t)s * stage_bytes;
-                const uint32_t d = tmem + (uint32_t)x * TC64_BN;
+                const uint32_t d = tmem + (uint32_t)x * TC64_BN * NT;
 #pragma unroll
                 for (int kk = 0; kk < TC_BK / 16; ++kk) {
-                    uint64_t da[NT], db[NT];
+                    const uint64_t db = sdesc_sw64(st + NT * TC_A_BYTES + kk * 32u, 16u, 512u);  // from B_0 on
 #pragma unroll
                     for (int t = 0; t < NT; ++t) {
                         const uint32_t a_t = st + (uint32_t)t * TC_A_BYTES;
-                        da[t] = p.a_kmajor ? sdesc_sw64(a_t + kk * 32u, 16u, 512u) : sdesc_sw64(a_t + kk * 1024u, 2048u, 512u);
-                        db[t] = sdesc_sw64(st + NT * TC_A_BYTES + (uint32_t)t * b_bytes + kk * 32u, 16u, 512u);
-                    }
-#pragma unroll
-                    for (int i = 0; i < tc_pairs(NT); ++i) {
-                        int ta, tb;
-                        tc_pair(i, ta, tb);
-                        mma_bf16(d, da[ta], db[tb], idesc, (first && kk == 0 && i == 0) ? 0u : 1u);
+                        const uint64_t da = p.a_kmajor ? sdesc_sw64(a_t + kk * 32u, 16u, 512u)
+                                                       : sdesc_sw64(a_t + kk * 1024u, 2048u, 512u);
+                        mma_bf16(d, da, db, idesc_n[t], (first && kk == 0 && t == 0) ? 0u : 1u);
                     }
                 }
                 mma_commit(empty_bar(s));
@@ -637,10 +643,13 @@ __device__ __forceinline__ void f64acc_cta(const CUtensorMap *ma, const CUtensor
             tc_fence_after();
 #pragma unroll
             for (int c0 = 0; c0 < TC64_BN; c0 += 16) {
-                uint32_t r[16];
-                tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(x * TC64_BN + c0), r);
 #pragma unroll
-                for (int j = 0; j < 16; ++j) acc[c0 + j] += (double)__uint_as_float(r[j]);
+                for (int u = 0; u < NT; ++u) {
+                    uint32_t r[16];
+                    tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(x * TC64_BN * NT + u * TC64_BN + c0), r);
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) acc[c0 + j] += (double)__uint_as_float(r[j]);
+                }
             }
             tc_fence_before();
             __syncwarp();
@@ -1016,7 +1025,7 @@ int tc_group_run(rla_ctx *ctx, const TcGroup &g, cudaStream_t st) {
     p.BN = TC64_BN;
     p.nch = 1;
     p.stages = g.stages;
-    p.tmem_cols = 2u * TC64_BN;
+    p.tmem_cols = tc64_tmem_cols(2);  // grouped products are split-BF16 (NT = 2)
     p.status = g.status;
     p.wait_ns = ctx->wait_ns;
     tc_group_f64acc_kernel<2><<<g.tiles, TC64_THREADS, g.smem, st>>>((const TcGroupItem<2> *)g.items, g.tstart, g.count,
@@ -1100,7 +1109,7 @@ int tc_gemm_f64acc(rla_ctx *ctx, int64_t M, int64_t N, int64_t K, const bf16 *co
     const int64_t ldo = M, sstride = M * N;
     void *ws = nullptr;
     RLA_TRY(scratch_get(ctx, sizeof(double) * (size_t)sstride * splits, &ws));
-    TcParams p{(int)M, (int)N, (int)K, TC64_BN, 1, a_kmajor, (int)nkb, (int)kbps, stages, 2u * TC64_BN,
+    TcParams p{(int)M, (int)N, (int)K, TC64_BN, 1, a_kmajor, (int)nkb, (int)kbps, stages, tc64_tmem_cols(NT),
                nullptr, ldo, sstride, status, ctx->wait_ns};
     RLA_CUDA_TRY(ctx, set_smem_max(tc_gemm_f64acc_kernel<NT>));
     cudaEvent_t e0 = timing_begin(ctx);
