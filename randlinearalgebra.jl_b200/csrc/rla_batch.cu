@@ -156,6 +156,46 @@ struct Tile {
     static_assert(NP * B_THREADS == BK * BM, "slice shape");
 };
 
+// FP64 tensor-core form of the slice product for the FP64-accumulating kinds: the CTA's R x KT
+// output tile as 8 x 8 mma.m8n8k4.f64 blocks, 8 warps in a WM x WN grid (each warp 16 columns,
+// R / WM rows).  Operands as staged: A(mn, k) = SA[k * LDA + mn], B(k, n) = SB[k * LDB + n]
+// (row strides 4 mod 16 doubles: conflict-free fragment loads).  Fragment (i, j, e) of a lane
+// (g = lane >> 2, q = lane & 3) is element (wm*RW + 8i + g, wn*16 + 8j + 2q + e).
+__device__ __forceinline__ void b_dmma(double (&d)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d[0]), "+d"(d[1])
+                 : "d"(a), "d"(b));
+}
+template <int R, int KT, int BK, int LDA, int LDB>
+struct BDmma {
+    static constexpr int WN = KT / 16, WM = (B_THREADS / 32) / WN, RW = R / WM, MB = RW / 8;
+    static_assert(KT % 16 == 0 && WN >= 1 && WM * WN == B_THREADS / 32 && RW % 8 == 0 && MB >= 1, "dmma tile");
+    double acc[MB][2][2];
+    __device__ __forceinline__ void zero() {
+#pragma unroll
+        for (int i = 0; i < MB; ++i)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    }
+    __device__ __forceinline__ void slice(const double *SA, const double *SB, int warp, int lane) {
+        const int wm = warp / WN, wn = warp % WN, g = lane >> 2, q = lane & 3;
+#pragma unroll
+        for (int k0 = 0; k0 < BK; k0 += 4) {
+            double a[MB], b[2];
+#pragma unroll
+            for (int i = 0; i < MB; ++i) a[i] = SA[(k0 + q) * LDA + wm * RW + 8 * i + g];
+#pragma unroll
+            for (int j = 0; j < 2; ++j) b[j] = SB[(k0 + q) * LDB + wn * 16 + 8 * j + g];
+#pragma unroll
+            for (int i = 0; i < MB; ++i)
+#pragma unroll
+                for (int j = 0; j < 2; ++j) b_dmma(acc[i][j], a[i], b[j]);
+        }
+    }
+    __device__ static int row(int warp, int lane, int i) { return (warp / WN) * RW + 8 * i + (lane >> 2); }
+    __device__ static int col(int warp, int lane, int j, int e) { return (warp % WN) * 16 + 8 * j + 2 * (lane & 3) + e; }
+};
+
 // out (rows x k) = X (rows x K) * W (K x k); CTA = BM rows of one instance, all k columns.
 // In-place use (out == X) is safe: a CTA reads all of its rows before it writes them.
 template <int KIND, int KT, int BM>
@@ -168,7 +208,10 @@ __global__ void __launch_bounds__(B_THREADS) b_ax_kernel(BProb *P, const int *id
     using Tl = Tile<TAcc, KT, BM>;
     constexpr int BK = Tl::BK, TM = Tl::TM, TN = Tl::TN, TXN = Tl::TXN, TYM = Tl::TYM, NP = Tl::NP, NW = Tl::NW;
     __shared__ __align__(16) TAcc Xs[BK][BM + 4];
-    __shared__ __align__(16) TAcc Ws[BK][KT];
+    __shared__ __align__(16) TAcc Ws[BK][KT + 4];
+    constexpr bool TC = sizeof(TAcc) == 8;  // FP64 accumulation: on the FP64 tensor cores
+    using Dm = BDmma<BM, KT, BK, BM + 4, KT + 4>;
+    Dm dm;
     const int t = blockIdx.x;
     const int q = b_find(tstart, count, t);
     const BProb &p = P[idx[q]];
@@ -211,24 +254,43 @@ __global__ void __launch_bounds__(B_THREADS) b_ax_kernel(BProb *P, const int *id
             if (e < BK * KT) Ws[e % BK][e / BK] = pw[u];
         }
     };
+    if constexpr (TC) dm.zero();
     fetch(0);
     for (int64_t c0 = 0; c0 < K; c0 += BK) {
         stash();
         __syncthreads();
         if (c0 + BK < K) fetch(c0 + BK);
+        if constexpr (TC) {
+            dm.slice(reinterpret_cast<const double *>(&Xs[0][0]), reinterpret_cast<const double *>(&Ws[0][0]), tid >> 5,
+                     tid & 31);
+        } else {
 #pragma unroll 8
-        for (int c = 0; c < BK; ++c) {
-            TAcc a[TM], b[TN];
+            for (int c = 0; c < BK; ++c) {
+                TAcc a[TM], b[TN];
 #pragma unroll
-            for (int i = 0; i < TM; ++i) a[i] = Xs[c][ty + TYM * i];
+                for (int i = 0; i < TM; ++i) a[i] = Xs[c][ty + TYM * i];
 #pragma unroll
-            for (int j = 0; j < TN; ++j) b[j] = Ws[c][tx * TN + j];
+                for (int j = 0; j < TN; ++j) b[j] = Ws[c][tx * TN + j];
 #pragma unroll
-            for (int i = 0; i < TM; ++i)
+                for (int i = 0; i < TM; ++i)
 #pragma unroll
-                for (int j = 0; j < TN; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+                    for (int j = 0; j < TN; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+            }
         }
         __syncthreads();
+    }
+    if constexpr (TC) {
+        const int w = tid >> 5, l = tid & 31;
+#pragma unroll
+        for (int i = 0; i < Dm::MB; ++i)
+#pragma unroll
+            for (int j = 0; j < 2; ++j)
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const int64_t gr = r0 + Dm::row(w, l, i), gj = Dm::col(w, l, j, e);
+                    if (gr < rows && gj < kk) Out[gr + gj * ldo] = (TO)dm.acc[i][j][e];
+                }
+        return;
     }
 #pragma unroll
     for (int j = 0; j < TN; ++j) {
@@ -291,7 +353,10 @@ __global__ void __launch_bounds__(B_THREADS) b_xty_kernel(BProb *P, const int *i
     using Tl = Tile<TAcc, KT, BR>;
     constexpr int BK = Tl::BK, TM = Tl::TM, TN = Tl::TN, TXN = Tl::TXN, TYM = Tl::TYM, NP = Tl::NP, NW = Tl::NW;
     __shared__ __align__(16) TAcc Xs[BK][BR + 4];
-    __shared__ __align__(16) TAcc Ys[BK][KT];
+    __shared__ __align__(16) TAcc Ys[BK][KT + 4];
+    constexpr bool TC = sizeof(TAcc) == 8;  // FP64 accumulation: on the FP64 tensor cores
+    using Dm = BDmma<BR, KT, BK, BR + 4, KT + 4>;
+    Dm dm;
     const int t = blockIdx.x;
     const int q = b_find(tstart, count, t);
     const BProb &p = P[idx[q]];
@@ -336,26 +401,45 @@ __global__ void __launch_bounds__(B_THREADS) b_xty_kernel(BProb *P, const int *i
             if (e < BK * KT) Ys[e % BK][e / BK] = py[u];
         }
     };
+    if constexpr (TC) dm.zero();
     if (rs < re) fetch(rs);
     for (int64_t r0 = rs; r0 < re; r0 += BK) {
         stash();
         __syncthreads();
         if (r0 + BK < re) fetch(r0 + BK);
+        if constexpr (TC) {
+            dm.slice(reinterpret_cast<const double *>(&Xs[0][0]), reinterpret_cast<const double *>(&Ys[0][0]), tid >> 5,
+                     tid & 31);
+        } else {
 #pragma unroll 8
-        for (int r = 0; r < BK; ++r) {
-            TAcc a[TM], b[TN];
+            for (int r = 0; r < BK; ++r) {
+                TAcc a[TM], b[TN];
 #pragma unroll
-            for (int i = 0; i < TM; ++i) a[i] = Xs[r][ty + TYM * i];
+                for (int i = 0; i < TM; ++i) a[i] = Xs[r][ty + TYM * i];
 #pragma unroll
-            for (int j = 0; j < TN; ++j) b[j] = Ys[r][tx * TN + j];
+                for (int j = 0; j < TN; ++j) b[j] = Ys[r][tx * TN + j];
 #pragma unroll
-            for (int i = 0; i < TM; ++i)
+                for (int i = 0; i < TM; ++i)
 #pragma unroll
-                for (int j = 0; j < TN; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+                    for (int j = 0; j < TN; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+            }
         }
         __syncthreads();
     }
     TAcc *part = reinterpret_cast<TAcc *>(p.part) + split * nx * kk;
+    if constexpr (TC) {
+        const int w = tid >> 5, l = tid & 31;
+#pragma unroll
+        for (int i = 0; i < Dm::MB; ++i)
+#pragma unroll
+            for (int j = 0; j < 2; ++j)
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const int64_t gi = i0 + Dm::row(w, l, i), gj = Dm::col(w, l, j, e);
+                    if (gi < nx && gj < kk) part[gi * kk + gj] = dm.acc[i][j][e];
+                }
+        return;
+    }
 #pragma unroll
     for (int i = 0; i < TM; ++i) {
         const int64_t gi = i0 + ty + TYM * i;
