@@ -532,19 +532,22 @@ __device__ __forceinline__ int bjx_partner(int x, int r, bool intra) {
 }
 
 // Rotation R = [cs sn; -sn cs] on columns (i, j) that makes them orthogonal, from their Gram
-// entries a = |x_i|^2, b = |x_j|^2, g = x_i'x_j: tan = sign(b - a) 2g / (|b - a| +
-// sqrt((b - a)^2 + 4g^2)), the smaller root of g t^2 + (b - a) t - g = 0 (Rutishauser's form;
-// no overflow for Gram entries of Float32 data).  Identity when g^2 <= tol^2 a b.
+// entries a = |x_i|^2, b = |x_j|^2, g = x_i'x_j: the smaller angle, tan = sign(b - a) 2g /
+// (|b - a| + h) with h = sqrt((b - a)^2 + 4g^2).  With w = h + |b - a| and r = 1/sqrt(2hw):
+// cs = w r and sn = sign(b - a) 2g r (cs^2 + sn^2 = (w^2 + 4g^2) / (2hw) = 1), two reciprocal
+// square roots and no division.  No overflow for Gram entries of Float32 data.  Identity when
+// g^2 <= tol^2 a b.
 __device__ __forceinline__ bool bjx_rot(double a, double b, double g, double tol, double &cs, double &sn) {
     if (g == 0.0 || g * g <= tol * tol * a * b) {
         cs = 1.0;
         sn = 0.0;
         return false;
     }
-    const double d = b - a;
-    const double t = (d >= 0.0 ? 2.0 * g : -2.0 * g) / (fabs(d) + sqrt(fma(d, d, 4.0 * g * g)));
-    cs = rsqrt(fma(t, t, 1.0));
-    sn = cs * t;
+    const double d = b - a, q = fma(d, d, 4.0 * g * g);
+    const double h = q * rsqrt(q), w = h + fabs(d);
+    const double r = rsqrt(2.0 * h * w);
+    cs = w * r;
+    sn = (d >= 0.0 ? 2.0 * g : -2.0 * g) * r;
     return true;
 }
 
