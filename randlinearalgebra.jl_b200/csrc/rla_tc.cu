@@ -753,11 +753,35 @@ __global__ void split_group_kernel(const SplitItem *items, const int *bstart, in
     if (u >= groups * it.cols) return;
     const int64_t c = u / groups, r0 = (u - c * groups) * 8;
     const float *xc = it.X + c * it.ldx;
+    float v[8];
+    if (r0 >= 4 && r0 + 12 <= it.rows) {
+        // three 16-byte loads of the aligned window around the 8 elements (columns of an
+        // instance need not start on a 16-byte boundary); the window stays inside the column
+        const uintptr_t addr = reinterpret_cast<uintptr_t>(xc + r0);
+        const int a = (int)((addr >> 2) & 3u);
+        const float4 *w = reinterpret_cast<const float4 *>(addr - 4u * (uintptr_t)a);
+        const float4 f0 = __ldg(w), f1 = __ldg(w + 1), f2 = __ldg(w + 2);
+        const float win[12] = {f0.x, f0.y, f0.z, f0.w, f1.x, f1.y, f1.z, f1.w, f2.x, f2.y, f2.z, f2.w};
+        switch (a) {
+#define RLA_WIN(A)                                   \
+    case A:                                          \
+        _Pragma("unroll") for (int i = 0; i < 8; ++i) v[i] = win[A + i]; \
+        break;
+            RLA_WIN(0)
+            RLA_WIN(1)
+            RLA_WIN(2)
+            RLA_WIN(3)
+#undef RLA_WIN
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) v[i] = r0 + i < it.rows ? __ldg(xc + r0 + i) : 0.f;
+    }
     __align__(16) bf16 t[NT][8];
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
         bf16 ti[NT];
-        split_terms<NT>(r0 + i < it.rows ? __ldg(xc + r0 + i) : 0.f, ti);
+        split_terms<NT>(v[i], ti);
 #pragma unroll
         for (int q = 0; q < NT; ++q) t[q][i] = ti[q];
     }
