@@ -640,6 +640,7 @@ __global__ void __launch_bounds__(BJX_THREADS) block_jacobi_gram_round_kernel(do
         if (lane == 0) wmax[warp] = m2;
     }
     int cur = 0;
+    bool rotated = false;  // block-uniform: every warp computes the same rotations
     const int n_intra = round == 0 ? 7 : 0, n_in = n_intra + ((vi && vj) ? 8 : 0);
     for (int r = 0; r < n_in; ++r) {
         const bool intra = r < n_intra;
@@ -655,6 +656,9 @@ __global__ void __launch_bounds__(BJX_THREADS) block_jacobi_gram_round_kernel(do
                 f = lane == i ? -sn : sn;
             }
         }
+        // a round that rotates no pair leaves G and V as they are
+        if (!__any_sync(FULL, f != 0.0)) continue;
+        rotated = true;
         const double ex = __shfl_sync(FULL, e, x), fx = __shfl_sync(FULL, f, x);
         const double ey = __shfl_sync(FULL, e, y), fy = __shfl_sync(FULL, f, y);
         const int xp = bjx_partner(x, rr, intra), yp = bjx_partner(y, rr, intra);
@@ -666,11 +670,13 @@ __global__ void __launch_bounds__(BJX_THREADS) block_jacobi_gram_round_kernel(do
         cur ^= 1;
         __syncthreads();
     }
+    __syncthreads();  // wmax (also when no round ran its barrier)
     if (tid == 0) {
         double m2 = 0.0;
         for (int w = 0; w < 8; ++w) m2 = fmax(m2, wmax[w]);
         if (m2 > 0.0) atomicMax(off, (unsigned long long)__double_as_longlong(sqrt(m2)));
     }
+    if (!rotated) return;  // V = I: the columns of X and J are unchanged
     // Xp <- Xp V, Jp <- Jp V: 8-row tiles round-robin over the warps, k = the 16 columns
     double vb[4][2];
 #pragma unroll
