@@ -795,14 +795,43 @@ template <class TC, class TP = float>
 __global__ void splitk_reduce_kernel(const TP *__restrict__ P, int splits, int64_t split_stride, int64_t ldp,
                                      int64_t M, int64_t N, TC *C, int64_t ldc, double alpha, double beta,
                                      int beta_zero) {
+    // four consecutive rows per thread: 16-byte partial loads (ldp and split_stride are
+    // multiples of 4 floats), and 16-byte stores when C's columns allow them
+    constexpr bool V4 = sizeof(TP) == 4;
+    const bool c_vec = V4 && sizeof(TC) == 4 && ldc % 4 == 0 && ((uintptr_t)C & 15u) == 0;
+    const int64_t M4 = V4 ? (M + 3) / 4 : M;
     for (int64_t j = blockIdx.y; j < N; j += gridDim.y) {
-        for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < M; i += (int64_t)gridDim.x * blockDim.x) {
-            double acc = 0.0;
-            for (int s = 0; s < splits; ++s) acc += (double)P[s * split_stride + i + j * ldp];
-            TC *cp = C + i + j * ldc;
-            double r = alpha * acc;
-            if (!beta_zero) r += beta * (double)*cp;
-            *cp = (TC)r;
+        for (int64_t i4 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i4 < M4; i4 += (int64_t)gridDim.x * blockDim.x) {
+            if (V4 && 4 * i4 + 4 <= M) {
+                const int64_t i = 4 * i4;
+                double acc[4] = {0.0, 0.0, 0.0, 0.0};
+                for (int s = 0; s < splits; ++s) {
+                    const float4 v = *reinterpret_cast<const float4 *>(P + s * split_stride + i + j * ldp);
+                    acc[0] += (double)v.x;
+                    acc[1] += (double)v.y;
+                    acc[2] += (double)v.z;
+                    acc[3] += (double)v.w;
+                }
+                TC *cp = C + i + j * ldc;
+                TC r[4];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) r[e] = (TC)(alpha * acc[e] + (beta_zero ? 0.0 : beta * (double)cp[e]));
+                if (c_vec) {
+                    *reinterpret_cast<float4 *>(cp) = make_float4((float)r[0], (float)r[1], (float)r[2], (float)r[3]);
+                } else {
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) cp[e] = r[e];
+                }
+            } else {
+                for (int64_t i = V4 ? 4 * i4 : i4; i < (V4 ? min(M, 4 * i4 + 4) : i4 + 1); ++i) {
+                    double acc = 0.0;
+                    for (int s = 0; s < splits; ++s) acc += (double)P[s * split_stride + i + j * ldp];
+                    TC *cp = C + i + j * ldc;
+                    double r = alpha * acc;
+                    if (!beta_zero) r += beta * (double)*cp;
+                    *cp = (TC)r;
+                }
+            }
         }
     }
 }
@@ -960,7 +989,7 @@ int tc_gemm_split(rla_ctx *ctx, int64_t M, int64_t N, int64_t K, const bf16 *con
             ctx->timed[0].emplace_back(e0, e1);
         }
         if (!direct) {
-            const unsigned gx = (unsigned)std::min<int64_t>(ceil_div(M, 256), 1024);
+            const unsigned gx = (unsigned)std::min<int64_t>(ceil_div(M, 1024), 1024);  // 4 rows per thread
             const unsigned gy = (unsigned)std::min<int64_t>(nb, 65535);
             splitk_reduce_kernel<TC><<<dim3(gx, gy), 256, 0, ctx->stream>>>(out, pl.splits, sstride, ldo, M, nb, Cn, ldc,
                                                                             alpha, beta, beta == 0.0);

@@ -288,3 +288,22 @@ def test_randsvd_split_bf16_full_size_vs_oracle(rla, orc, dev):
     assert abs(e_gpu - e_ref) < 1e-4, (e_gpu, e_ref)
     I = torch.eye(l, device=dev, dtype=torch.float64)
     assert float(torch.max(torch.abs(U.t() @ U - I))) < 1e-5
+
+
+@pytest.mark.parametrize("l", [1, 16, 17, 100, 272, 383, 384, 385, 520])
+def test_cholesky_qr_orders(rla, dev, l):
+    """The orthogonalisation at orders around the blocked Cholesky/inverse kernels' limits
+    (blocks of 16, l <= 384) and past them (the panel kernels): Q of a rangefinder without power
+    iterations equals the Householder Q of A*Omega, sign convention included, and is
+    orthonormal."""
+    rng = np.random.default_rng(100 + l)
+    m, n = 2 * l + 64, l + 40
+    A = rng.standard_normal((m, n))
+    comp = rla.Gaussian(cardinality=rla.Right(), compression_dim=l)
+    R = rla.complete_approximator(rla.RangeFinder(compressor=comp, power_its=0, orthogonalize=True),
+                                  to_dev(A, dev), seed=7)
+    rla.rapproximate_(R, to_dev(A, dev))
+    Q = R.range.cpu().numpy()
+    Qt = qr_Q(A @ R.compressor.op)
+    assert rel_err(Q, Qt) < 1e-9, l
+    assert np.abs(Q.T @ Q - np.eye(l)).max() < 1e-12, l
