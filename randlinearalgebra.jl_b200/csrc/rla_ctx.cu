@@ -26,17 +26,30 @@ int check_launch(rla_ctx *ctx, const char *what) {
     return RLA_OK;
 }
 
+// Grows a context buffer in the order of ctx->stream, the only stream its users launch on:
+// the old buffer goes back to the context's pool after the work already queued there, and the
+// new one comes from the pool.  Nothing waits on the host: a synchronous cudaFree waits for
+// every stream of every context on the device, which stalls the other workers of a server
+// for as long as they keep the device busy.  Growth is refused while ctx->stream captures a
+// graph (the captured launches would keep a buffer that the next growth releases).
+static int grow_stream_ordered(rla_ctx *ctx, rla::Scratch *buf, size_t bytes, const char *what) {
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    RLA_CUDA_TRY(ctx, cudaStreamIsCapturing(ctx->stream, &cap));
+    if (cap != cudaStreamCaptureStatusNone)
+        return set_error(ctx, RLA_E_ARG, "%s must be sized before graph capture (%zu bytes needed)", what, bytes);
+    if (buf->ptr) RLA_CUDA_TRY(ctx, cudaFreeAsync(buf->ptr, ctx->stream));
+    buf->ptr = nullptr;
+    buf->bytes = 0;
+    RLA_CUDA_TRY(ctx, pool_malloc_s(ctx, &buf->ptr, bytes, ctx->stream));
+    buf->bytes = bytes;
+    return RLA_OK;
+}
+
 int scratch_get(rla_ctx *ctx, size_t bytes, void **out) {
     bytes = (bytes + 255) & ~size_t(255);
     if (bytes == 0) bytes = 256;
     if (ctx->scratch.bytes < bytes) {
-        // Work already queued may still use the old buffer.
-        RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-        if (ctx->scratch.ptr) RLA_CUDA_TRY(ctx, cudaFree(ctx->scratch.ptr));
-        ctx->scratch.ptr = nullptr;
-        ctx->scratch.bytes = 0;
-        RLA_CUDA_TRY(ctx, cudaMalloc(&ctx->scratch.ptr, bytes));
-        ctx->scratch.bytes = bytes;
+        RLA_TRY(grow_stream_ordered(ctx, &ctx->scratch, bytes, "scratch"));
         if ((int64_t)bytes > ctx->scratch_high_water) ctx->scratch_high_water = (int64_t)bytes;
     }
     *out = ctx->scratch.ptr;
@@ -47,13 +60,8 @@ int counters_get(rla_ctx *ctx, size_t n, int **out) {
     size_t bytes = ((n * sizeof(int)) + 255) & ~size_t(255);
     if (bytes == 0) bytes = 256;
     if (ctx->counters.bytes < bytes) {
-        RLA_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-        if (ctx->counters.ptr) RLA_CUDA_TRY(ctx, cudaFree(ctx->counters.ptr));
-        ctx->counters.ptr = nullptr;
-        ctx->counters.bytes = 0;
-        RLA_CUDA_TRY(ctx, cudaMalloc(&ctx->counters.ptr, bytes));
+        RLA_TRY(grow_stream_ordered(ctx, &ctx->counters, bytes, "counters"));
         RLA_CUDA_TRY(ctx, cudaMemsetAsync(ctx->counters.ptr, 0, bytes, ctx->stream));
-        ctx->counters.bytes = bytes;
     }
     *out = (int *)ctx->counters.ptr;
     return RLA_OK;
@@ -137,9 +145,9 @@ int rla_ctx_create(int device, void *stream, rla_ctx **out) {
 int rla_ctx_destroy(rla_ctx *ctx) {
     if (!ctx) return RLA_OK;
     cudaSetDevice(ctx->device);
+    if (ctx->scratch.ptr) cudaFreeAsync(ctx->scratch.ptr, ctx->stream);
+    if (ctx->counters.ptr) cudaFreeAsync(ctx->counters.ptr, ctx->stream);
     cudaStreamSynchronize(ctx->stream);
-    if (ctx->scratch.ptr) cudaFree(ctx->scratch.ptr);
-    if (ctx->counters.ptr) cudaFree(ctx->counters.ptr);
     if (ctx->tc_status) cudaFree(ctx->tc_status);
     for (auto &v : ctx->timed)
         for (auto &e : v) {

@@ -1057,13 +1057,14 @@ int tc_group_build(rla_ctx *ctx, const std::vector<TcGroupSpec> &specs, TcGroup 
     }
     ts[specs.size()] = g->tiles;
     void *di = nullptr, *dt = nullptr;
-    RLA_CUDA_TRY(ctx, cudaMalloc(&di, sizeof(TcGroupItem<NT>) * items.size()));
-    RLA_CUDA_TRY(ctx, cudaMalloc(&dt, sizeof(int) * ts.size()));
+    g->stream = ctx->stream;
+    RLA_CUDA_TRY(ctx, pool_malloc_s(ctx, &di, sizeof(TcGroupItem<NT>) * items.size(), ctx->stream));
+    g->items = di;
+    RLA_CUDA_TRY(ctx, pool_malloc_s(ctx, &dt, sizeof(int) * ts.size(), ctx->stream));
+    g->tstart = (int *)dt;
     RLA_CUDA_TRY(ctx, cudaMemcpyAsync(di, items.data(), sizeof(TcGroupItem<NT>) * items.size(), cudaMemcpyHostToDevice,
                                       ctx->stream));
     RLA_CUDA_TRY(ctx, cudaMemcpyAsync(dt, ts.data(), sizeof(int) * ts.size(), cudaMemcpyHostToDevice, ctx->stream));
-    g->items = di;
-    g->tstart = (int *)dt;
     const int64_t stage = NT * TC_A_BYTES + NT * (int64_t)TC64_BN * TC_BK * 2;
     const int64_t budget = ctx->smem_optin - 1024 - 256;
     g->stages = (int)std::max<int64_t>(2, std::min<int64_t>(8, budget / stage));
@@ -1102,13 +1103,14 @@ int split_group_build(rla_ctx *ctx, const std::vector<SplitSpec> &specs, SplitGr
     }
     bs[specs.size()] = g->blocks;
     void *di = nullptr, *db = nullptr;
-    RLA_CUDA_TRY(ctx, cudaMalloc(&di, sizeof(SplitItem) * items.size()));
-    RLA_CUDA_TRY(ctx, cudaMalloc(&db, sizeof(int) * bs.size()));
+    g->stream = ctx->stream;
+    RLA_CUDA_TRY(ctx, pool_malloc_s(ctx, &di, sizeof(SplitItem) * items.size(), ctx->stream));
+    g->items = di;
+    RLA_CUDA_TRY(ctx, pool_malloc_s(ctx, &db, sizeof(int) * bs.size(), ctx->stream));
+    g->bstart = (int *)db;
     RLA_CUDA_TRY(ctx, cudaMemcpyAsync(di, items.data(), sizeof(SplitItem) * items.size(), cudaMemcpyHostToDevice,
                                       ctx->stream));
     RLA_CUDA_TRY(ctx, cudaMemcpyAsync(db, bs.data(), sizeof(int) * bs.size(), cudaMemcpyHostToDevice, ctx->stream));
-    g->items = di;
-    g->bstart = (int *)db;
     return RLA_OK;
 }
 
@@ -1118,15 +1120,17 @@ int split_group_run(rla_ctx *ctx, const SplitGroup &g, cudaStream_t st) {
     return check_launch(ctx, "split_group");
 }
 
+// Released after the work queued on the building stream; launches on other streams that read
+// the tables are joined into that stream (or synchronised) before the free is issued.
 void tc_group_free(TcGroup *g) {
-    if (g->items) cudaFree(g->items);
-    if (g->tstart) cudaFree(g->tstart);
+    if (g->items) cudaFreeAsync(g->items, g->stream);
+    if (g->tstart) cudaFreeAsync(g->tstart, g->stream);
     *g = TcGroup{};
 }
 
 void split_group_free(SplitGroup *g) {
-    if (g->items) cudaFree(g->items);
-    if (g->bstart) cudaFree(g->bstart);
+    if (g->items) cudaFreeAsync(g->items, g->stream);
+    if (g->bstart) cudaFreeAsync(g->bstart, g->stream);
     *g = SplitGroup{};
 }
 

@@ -78,12 +78,15 @@ struct TcGroupSpec {
     int64_t ldo;
     int out_f64;
 };
+// The item tables live in the building context's memory pool and are released in the order
+// of its stream (a synchronous free would wait for every stream on the device).
 struct TcGroup {
     void *items = nullptr;
     int *tstart = nullptr;
     int count = 0, tiles = 0, stages = 2;
     size_t smem = 0;
     int *status = nullptr;
+    cudaStream_t stream = nullptr;  // stream the tables are allocated and released on
 };
 int tc_group_build(rla_ctx *ctx, const std::vector<TcGroupSpec> &specs, TcGroup *g);
 int tc_group_run(rla_ctx *ctx, const TcGroup &g, cudaStream_t st);
@@ -100,6 +103,7 @@ struct SplitGroup {
     void *items = nullptr;
     int *bstart = nullptr;
     int count = 0, blocks = 0;
+    cudaStream_t stream = nullptr;  // stream the tables are allocated and released on
 };
 int split_group_build(rla_ctx *ctx, const std::vector<SplitSpec> &specs, SplitGroup *g);
 int split_group_run(rla_ctx *ctx, const SplitGroup &g, cudaStream_t st);
