@@ -339,12 +339,13 @@ def b200_arm(args):
                              "tflops": round(r["flops"] / (r["ms"] / 1e3) / 1e12, 2),
                              "roofline": rs_roofline(RS_M, RS_N, r), "error": r["error"], "clocks": r["clocks"]}
         ls, svd, servers = serve_setup(rla, torch, dev, 4)
-        curve = sv_curve(rla, torch, dev, ls, svd, servers, SV_SLO_RATES, 200, 1, seed0=20)
+        # median of SV_REPS runs per rate and mode, as in the serving workload's own line
+        curve = sv_curve(rla, torch, dev, ls, svd, servers, SV_SLO_RATES, 200, SV_REPS, seed0=20)
         for srv in servers.values():
             srv.stop()
         del ls, svd
         torch.cuda.empty_cache()
-        extras["serve"] = {"workload": SV_WORKLOAD + "; offered rates below saturation, 200 requests per rate",
+        extras["serve"] = {"workload": SV_WORKLOAD + f"; offered rates below saturation, 200 requests per rate, median of {SV_REPS} runs",
                            "curve": curve, "at_slo": sv_at_slo(curve, SV_SLO_RATES)}
 
     if rank != 0:
@@ -1367,16 +1368,19 @@ SV_SLO_RATES = [100, 200, 400, 700, 1000, 1500]  # offered rates of the latency-
 
 
 def sv_curve(rla, torch, dev, ls, svd, servers, rates, nreq, reps, seed0=10):
-    """Latency-throughput curve of both modes: per offered rate, the median (by throughput) of
-    `reps` runs of nreq requests.  Returns {"batched": {rate: ...}, "plain": {rate: ...}}."""
+    """Latency-throughput curve of both modes: per offered rate, `reps` runs of nreq requests
+    and, field by field, the median over the runs of the throughput, p50 and p99 latency.
+    Returns {"batched": {rate: ...}, "plain": {rate: ...}}."""
+    import numpy as np
     res = {"batched": {}, "plain": {}}
     for lam in rates:
         for mode, plain in (("batched", False), ("plain", True)):
-            runs = sorted((sv_run(rla, torch, dev, ls, svd, lam, nreq, servers[plain], seed0 + lam + 1000 * r)
-                           for r in range(reps)), key=lambda x: x[0])
-            thr, p50, p99 = runs[len(runs) // 2]
+            runs = [sv_run(rla, torch, dev, ls, svd, lam, nreq, servers[plain], seed0 + lam + 1000 * r)
+                    for r in range(reps)]
+            thr, p50, p99 = (float(np.median([x[i] for x in runs])) for i in range(3))
             res[mode][lam] = {"req_per_s": round(thr, 1), "p50_ms": round(1e3 * p50, 3), "p99_ms": round(1e3 * p99, 3),
-                              "runs_req_per_s": [round(x[0], 1) for x in runs]}
+                              "runs_req_per_s": [round(x[0], 1) for x in runs],
+                              "runs_p99_ms": [round(1e3 * x[2], 3) for x in runs]}
     return res
 
 
@@ -1431,11 +1435,11 @@ def serve_arm(args):
     props = torch.cuda.get_device_properties(dev)
     clocks = ClockSampler(f"GPU-{props.uuid}" if getattr(props, "uuid", None) else dev.index)
     clocks.start()
-    # SV_REPS runs per rate and mode; the median run (by throughput) is reported, so one run
+    # SV_REPS runs per rate and mode; per-field medians over the runs are reported, so one run
     # disturbed by other work on the shared host does not decide the line
     res = sv_curve(rla, torch, dev, ls, svd, servers, lams, args.serve_requests, SV_REPS)
     # below saturation: the latency-throughput curve and the throughput at a fixed p99 SLO
-    slo_curve = sv_curve(rla, torch, dev, ls, svd, servers, SV_SLO_RATES, args.serve_requests // 2, 1, seed0=20)
+    slo_curve = sv_curve(rla, torch, dev, ls, svd, servers, SV_SLO_RATES, args.serve_requests // 2, SV_REPS, seed0=20)
     clk = clocks.stop()
     for srv in servers.values():
         srv.stop()
